@@ -1,0 +1,659 @@
+// fortfem hot-path ORACLE (test infrastructure only; see oracle.h).
+//
+// FP64 CPU restatement of first-kind tetrahedral Nedelec assembly: candidate
+// evaluation x dual-basis coefficients, covariant Piola map, edge/face DoF
+// numbering, orientation transforms, curl-mass element and CSC, sampled loads
+// and the zero-tangential (PEC) mask.  The exact coefficient and face tables
+// are the repository's generated data (fortfem_b200/csrc/nedelec_tables.inc),
+// which the tests pin against the reference's own generated tables.
+#include "oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "../fortfem_b200/csrc/nedelec_tables.inc"
+
+namespace {
+const double kEps = 2.220446049250313e-16;
+
+double det3(const double *J) {
+  return J[0] * (J[4] * J[8] - J[7] * J[5]) - J[3] * (J[1] * J[8] - J[7] * J[2]) +
+         J[6] * (J[1] * J[5] - J[4] * J[2]);
+}
+void inv3(const double *J, double det, double *Ji) {
+  Ji[0] = (J[4] * J[8] - J[7] * J[5]) / det;
+  Ji[3] = -(J[3] * J[8] - J[6] * J[5]) / det;
+  Ji[6] = (J[3] * J[7] - J[6] * J[4]) / det;
+  Ji[1] = -(J[1] * J[8] - J[7] * J[2]) / det;
+  Ji[4] = (J[0] * J[8] - J[6] * J[2]) / det;
+  Ji[7] = -(J[0] * J[7] - J[6] * J[1]) / det;
+  Ji[2] = (J[1] * J[5] - J[4] * J[2]) / det;
+  Ji[5] = -(J[0] * J[5] - J[3] * J[2]) / det;
+  Ji[8] = (J[0] * J[4] - J[3] * J[1]) / det;
+}
+void tetra_jacobian(const double *v, double *J) {
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) J[r + 3 * c] = v[r + 3 * (c + 1)] - v[r];
+}
+// tetra_geometry, src/assembly/assembly_tetra_nedelec_3d.f90:2555-2568
+bool tetra_geometry(const double *v, double *J, double *det) {
+  tetra_jacobian(v, J);
+  *det = det3(J);
+  double m = 0.0;
+  for (int i = 0; i < 9; ++i) m = std::max(m, std::fabs(J[i]));
+  double s = std::max(1.0, m);
+  return *det > 64.0 * kEps * s * s * s;
+}
+
+double ipow(double x, int n) {
+  // Fortran x**n for small non-negative integer n
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+
+struct Term {
+  int comp;
+  double coef;
+  int pw[3];
+};
+
+// Candidate list of evaluate_runtime_candidates for order <= 5,
+// src/elements/tetra_nedelec_arbitrary_order.f90:318-396.
+std::vector<std::vector<Term>> candidate_terms(int k) {
+  std::vector<std::vector<Term>> c;
+  for (int comp = 0; comp < 3; ++comp)
+    for (int d = 0; d <= k - 1; ++d)
+      for (int a = 0; a <= d; ++a)
+        for (int b = 0; b <= d - a; ++b) c.push_back({{comp, 1.0, {a, b, d - a - b}}});
+  int d = k - 1;
+  for (int fam = 4; fam <= 5; ++fam)
+    for (int a = 0; a <= d; ++a)
+      for (int b = 0; b <= d - a; ++b) {
+        int cc = d - a - b;
+        if (fam == 4)
+          c.push_back({{0, -1.0, {a, b + 1, cc}}, {1, 1.0, {a + 1, b, cc}}});
+        else
+          c.push_back({{0, -1.0, {a, b, cc + 1}}, {2, 1.0, {a + 1, b, cc}}});
+      }
+  for (int b = 0; b <= d; ++b) {
+    int cc = d - b;
+    c.push_back({{1, -1.0, {0, b, cc + 1}}, {2, 1.0, {0, b + 1, cc}}});
+  }
+  return c;
+}
+
+// add_candidate_term, tetra_nedelec_arbitrary_order.f90:710-737
+void candidates(int k, const double *p, double *vals, double *curls) {
+  auto terms = candidate_terms(k);
+  int n = (int)terms.size();
+  std::fill(vals, vals + 3 * n, 0.0);
+  std::fill(curls, curls + 3 * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (auto &t : terms[i]) {
+      double value = t.coef * ipow(p[0], t.pw[0]) * ipow(p[1], t.pw[1]) * ipow(p[2], t.pw[2]);
+      double der[3];
+      for (int dir = 0; dir < 3; ++dir) {
+        if (t.pw[dir] == 0) { der[dir] = 0.0; continue; }
+        int red[3] = {t.pw[0], t.pw[1], t.pw[2]};
+        red[dir] -= 1;
+        der[dir] = t.coef * ((double)t.pw[dir] *
+                             (ipow(p[0], red[0]) * ipow(p[1], red[1]) * ipow(p[2], red[2])));
+      }
+      vals[3 * i + t.comp] += value;
+      double *cu = curls + 3 * i;
+      switch (t.comp) {
+        case 0: cu[1] += der[2]; cu[2] -= der[1]; break;
+        case 1: cu[0] -= der[2]; cu[2] += der[0]; break;
+        case 2: cu[0] += der[1]; cu[1] -= der[0]; break;
+      }
+    }
+}
+
+int face_perm_index(const int *perm) {
+  int code = 100 * perm[0] + 10 * perm[1] + perm[2];
+  switch (code) {
+    case 123: return 0;
+    case 132: return 1;
+    case 213: return 2;
+    case 231: return 3;
+    case 312: return 4;
+    case 321: return 5;
+  }
+  return -1;
+}
+
+struct RuleN {
+  std::vector<double> x, y, z, w;
+};
+bool make_rule(int rule, int q, RuleN &r) {
+  if (rule == 1) {
+    double P[12], W[4];
+    or_tetra_degree_two_rule(P, W);
+    for (int i = 0; i < 4; ++i) {
+      r.x.push_back(P[3 * i]); r.y.push_back(P[3 * i + 1]); r.z.push_back(P[3 * i + 2]);
+      r.w.push_back(W[i]);
+    }
+    return true;
+  }
+  if (q < 0) return false;
+  int n = or_tetra_duffy_count(q);
+  r.x.resize(n); r.y.resize(n); r.z.resize(n); r.w.resize(n);
+  or_tetra_duffy(q, r.x.data(), r.y.data(), r.z.data(), r.w.data());
+  return true;
+}
+
+// map_tetra_nedelec_covariant, src/elements/tetra_piola_maps.f90:18-57
+void covariant(const double *J, double det, const double *Ji, int n, const double *rv,
+               const double *rc, double *pv, double *pc) {
+  for (int b = 0; b < n; ++b)
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.0, t = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        s += Ji[k + 3 * i] * rv[3 * b + k];  // transpose(Ji) * v
+        t += J[i + 3 * k] * rc[3 * b + k];   // J * c
+      }
+      pv[3 * b + i] = s;
+      pc[3 * b + i] = t / det;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int or_nedelec_dof_count(int k) { return k * (k + 2) * (k + 3) / 2; }
+
+// evaluate_tetra_nedelec_first_kind, tetra_nedelec_arbitrary_order.f90:75-106
+int or_nedelec_evaluate(int k, const double *p, double *vals, double *curls) {
+  if (k < 1 || k > FFG_NEDELEC_TABLE_MAX_ORDER) return 1;
+  double tol = 64.0 * kEps;
+  if (p[0] < -tol || p[1] < -tol || p[2] < -tol) return 1;
+  if (p[0] + p[1] + p[2] > 1.0 + tol) return 1;
+  int n = or_nedelec_dof_count(k);
+  std::vector<double> cv(3 * n), cc(3 * n);
+  candidates(k, p, cv.data(), cc.data());
+  const double *C = kNedelecCoefficientTables[k];
+  for (int b = 0; b < n; ++b)
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.0, t = 0.0;
+      for (int c = 0; c < n; ++c) {
+        s += cv[3 * c + i] * C[c + (size_t)n * b];
+        t += cc[3 * c + i] * C[c + (size_t)n * b];
+      }
+      vals[3 * b + i] = s;
+      curls[3 * b + i] = t;
+    }
+  return 0;
+}
+
+// evaluate_tetra_nedelec_first_order, src/elements/tetra_nedelec_first_order.f90:11-51
+int or_whitney_evaluate(const double *p, double *vals, double *curls) {
+  double tol = 64.0 * kEps;
+  double lam[4] = {1.0 - p[0] - p[1] - p[2], p[0], p[1], p[2]};
+  for (int i = 0; i < 4; ++i)
+    if (lam[i] < -tol || lam[i] > 1.0 + tol) return 1;
+  const double g[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  const int ev[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+  for (int e = 0; e < 6; ++e) {
+    int a = ev[e][0], b = ev[e][1];
+    for (int i = 0; i < 3; ++i) vals[3 * e + i] = lam[a] * g[b][i] - lam[b] * g[a][i];
+    curls[3 * e + 0] = 2.0 * (g[a][1] * g[b][2] - g[a][2] * g[b][1]);
+    curls[3 * e + 1] = 2.0 * (g[a][2] * g[b][0] - g[a][0] * g[b][2]);
+    curls[3 * e + 2] = 2.0 * (g[a][0] * g[b][1] - g[a][1] * g[b][0]);
+  }
+  return 0;
+}
+
+static const int kLocalEdges[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+static const int kLocalFaces[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+
+static bool distinct4(const int *t) {
+  for (int a = 0; a < 4; ++a)
+    for (int b = a + 1; b < 4; ++b)
+      if (t[a] == t[b]) return false;
+  return true;
+}
+
+// build_tetra_edge_dof_map, src/elements/tetra_edge_dof_map.f90:10-77 (literal,
+// linear search :54-60).  edges: 2 x E (zero-based vertex ids).
+int or_edge_dof_map_faithful(int nt, const int *tets, int *edges, int *gd, int *orient,
+                             int *n_edges) {
+  if (nt < 1) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0) return 1;
+  std::vector<std::pair<int, int>> ed;
+  for (int t = 0; t < nt; ++t) {
+    if (!distinct4(tets + 4 * t)) return 1;
+    for (int le = 0; le < 6; ++le) {
+      int fv = tets[4 * t + kLocalEdges[le][0]], sv = tets[4 * t + kLocalEdges[le][1]];
+      int a = std::min(fv, sv), b = std::max(fv, sv);
+      int found = -1;
+      for (size_t e = 0; e < ed.size(); ++e)
+        if (ed[e].first == a && ed[e].second == b) { found = (int)e; break; }
+      if (found < 0) { ed.emplace_back(a, b); found = (int)ed.size() - 1; }
+      gd[6 * t + le] = found;
+      orient[6 * t + le] = (fv < sv) ? 1 : -1;
+    }
+  }
+  *n_edges = (int)ed.size();
+  if (edges)
+    for (size_t e = 0; e < ed.size(); ++e) { edges[2 * e] = ed[e].first; edges[2 * e + 1] = ed[e].second; }
+  return 0;
+}
+
+int or_edge_dof_map(int nt, const int *tets, int *edges, int *gd, int *orient, int *n_edges) {
+  if (nt < 1) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0) return 1;
+  std::unordered_map<uint64_t, int> map;
+  map.reserve((size_t)nt * 2);
+  std::vector<std::pair<int, int>> ed;
+  for (int t = 0; t < nt; ++t) {
+    if (!distinct4(tets + 4 * t)) return 1;
+    for (int le = 0; le < 6; ++le) {
+      int fv = tets[4 * t + kLocalEdges[le][0]], sv = tets[4 * t + kLocalEdges[le][1]];
+      int a = std::min(fv, sv), b = std::max(fv, sv);
+      uint64_t key = ((uint64_t)(uint32_t)a << 32) | (uint32_t)b;
+      auto it = map.find(key);
+      int id;
+      if (it == map.end()) { id = (int)ed.size(); ed.emplace_back(a, b); map.emplace(key, id); }
+      else id = it->second;
+      gd[6 * t + le] = id;
+      orient[6 * t + le] = (fv < sv) ? 1 : -1;
+    }
+  }
+  *n_edges = (int)ed.size();
+  if (edges)
+    for (size_t e = 0; e < ed.size(); ++e) { edges[2 * e] = ed[e].first; edges[2 * e + 1] = ed[e].second; }
+  return 0;
+}
+
+// build_tetra_nedelec_dof_map, src/elements/tetra_nedelec_global_dof_map.f90:15-105.
+// Output arrays: edges 2 x E, faces 3 x F (sorted vertex triples), global_dofs
+// n_b x T, edge_orientations 6 x T, face_permutations 3 x 4 x T (1-based
+// positions as in the reference).  Pass null output pointers to query counts.
+int or_nedelec_dof_map(int k, int nt, const int *tets, int faithful, int *edges, int *n_edges,
+                       int *faces, int *n_faces, int *gd, int *eo, int *fp, int *n_global) {
+  if (k < 1) return 1;
+  std::vector<int> egd(6 * (size_t)nt), eor(6 * (size_t)nt);
+  int ne = 0;
+  std::vector<int> edv(2 * (size_t)nt * 6);
+  int st = faithful ? or_edge_dof_map_faithful(nt, tets, edv.data(), egd.data(), eor.data(), &ne)
+                    : or_edge_dof_map(nt, tets, edv.data(), egd.data(), eor.data(), &ne);
+  if (st) return st;
+  int nb = or_nedelec_dof_count(k);
+  int fdc = k * (k - 1), cdc = k * (k - 1) * (k - 2) / 2;
+  int64_t edc = (int64_t)k * ne;
+  std::vector<std::array<int, 3>> fl;
+  std::unordered_map<uint64_t, int> fmap;
+  if (!faithful) fmap.reserve((size_t)nt * 3);
+  std::vector<int> tgd(gd ? 0 : (size_t)nb * nt);
+  int *G = gd ? gd : tgd.data();
+  for (int t = 0; t < nt; ++t)
+    for (int e = 0; e < 6; ++e)
+      for (int m = 0; m < k; ++m) G[(size_t)nb * t + e * k + m] = (int)((int64_t)egd[6 * t + e] * k + m);
+  std::vector<int> face_of(4 * (size_t)nt);
+  for (int t = 0; t < nt; ++t)
+    for (int lf = 0; lf < 4; ++lf) {
+      int lv[3], cv[3];
+      for (int i = 0; i < 3; ++i) lv[i] = cv[i] = tets[4 * t + kLocalFaces[lf][i]];
+      std::sort(cv, cv + 3);  // sort_three
+      int found = -1;
+      if (faithful) {
+        for (size_t f = 0; f < fl.size(); ++f)
+          if (fl[f][0] == cv[0] && fl[f][1] == cv[1] && fl[f][2] == cv[2]) { found = (int)f; break; }
+      } else {
+        uint64_t key = ((uint64_t)(uint32_t)cv[0] << 42) ^ ((uint64_t)(uint32_t)cv[1] << 21) ^
+                       (uint64_t)(uint32_t)cv[2];
+        auto it = fmap.find(key);
+        if (it != fmap.end()) found = it->second;
+        else { fmap.emplace(key, (int)fl.size()); }
+      }
+      if (found < 0) { fl.push_back({cv[0], cv[1], cv[2]}); found = (int)fl.size() - 1; }
+      face_of[4 * t + lf] = found;
+      if (fp)
+        for (int i = 0; i < 3; ++i) {
+          int pos = 0;
+          for (int j = 0; j < 3; ++j)
+            if (cv[j] == lv[i]) { pos = j + 1; break; }
+          fp[(size_t)12 * t + 3 * lf + i] = pos;
+        }
+      int fs = 6 * k + lf * fdc;
+      for (int m = 0; m < fdc; ++m)
+        G[(size_t)nb * t + fs + m] = (int)(edc + (int64_t)found * fdc + m);
+    }
+  int nf = (int)fl.size();
+  int cs = 6 * k + 4 * fdc;
+  for (int t = 0; t < nt; ++t)
+    for (int m = 0; m < cdc; ++m)
+      G[(size_t)nb * t + cs + m] = (int)(edc + (int64_t)nf * fdc + (int64_t)t * cdc + m);
+  if (n_edges) *n_edges = ne;
+  if (n_faces) *n_faces = nf;
+  if (n_global) *n_global = (int)(edc + (int64_t)nf * fdc + (int64_t)nt * cdc);
+  if (edges) std::memcpy(edges, edv.data(), sizeof(int) * 2 * ne);
+  if (faces)
+    for (int f = 0; f < nf; ++f)
+      for (int i = 0; i < 3; ++i) faces[3 * f + i] = fl[f][i];
+  if (eo) std::memcpy(eo, eor.data(), sizeof(int) * 6 * (size_t)nt);
+  return 0;
+}
+
+// build_tetra_face_basis_to_local_matrix, tetra_face_moment_transforms.f90:23-52
+// (generated tables for the orders the repository tabulates).
+int or_face_basis_to_local(int k, const int *perm, double *T) {
+  int m = k * (k - 1);
+  int pi = face_perm_index(perm);
+  if (pi < 0 || k < 2 || k > FFG_NEDELEC_TABLE_MAX_ORDER) return 1;
+  std::memcpy(T, kFaceTransformTable(k, pi), sizeof(double) * m * m);
+  return 0;
+}
+
+// build_tetra_nedelec_basis_transform, tetra_nedelec_global_dof_map.f90:107-155
+int or_nedelec_transform(int k, const int *eo, const int *fp, double *T) {
+  int n = or_nedelec_dof_count(k);
+  std::fill(T, T + (size_t)n * n, 0.0);
+  for (int d = 0; d < n; ++d) T[d + (size_t)n * d] = 1.0;
+  for (int e = 0; e < 6; ++e) {
+    if (eo[e] == 1) continue;
+    if (eo[e] != -1) return 1;
+    for (int m = 0; m < k; m += 2) {
+      int s = e * k + m;
+      T[s + (size_t)n * s] = -1.0;
+    }
+  }
+  int fdc = k * (k - 1);
+  if (fdc == 0) return 0;
+  std::vector<double> F((size_t)fdc * fdc);
+  for (int f = 0; f < 4; ++f) {
+    int s = 6 * k + f * fdc;
+    if (or_face_basis_to_local(k, fp + 3 * f, F.data())) return 1;
+    for (int c = 0; c < fdc; ++c)
+      for (int r = 0; r < fdc; ++r) T[(s + r) + (size_t)n * (s + c)] = F[r + (size_t)fdc * c];
+  }
+  return 0;
+}
+
+// assemble_tetra_nedelec_curl_mass_element, src/assembly/assembly_tetra_nedelec_3d.f90:584-643
+int or_nedelec_element(const double *v, int k, int q, double cw, double mw, double *M) {
+  if (k < 1 || q < 0) return 1;
+  double J[9], Ji[9], det;
+  if (!tetra_geometry(v, J, &det)) return 1;
+  inv3(J, det, Ji);
+  RuleN R;
+  make_rule(0, q, R);
+  int n = or_nedelec_dof_count(k);
+  std::vector<double> rv(3 * n), rc(3 * n), pv(3 * n), pc(3 * n);
+  std::fill(M, M + (size_t)n * n, 0.0);
+  for (size_t pt = 0; pt < R.w.size(); ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    if (or_nedelec_evaluate(k, P, rv.data(), rc.data())) return 1;
+    covariant(J, det, Ji, n, rv.data(), rc.data(), pv.data(), pc.data());
+    double pw = det * R.w[pt];
+    for (int col = 0; col < n; ++col)
+      for (int row = 0; row < n; ++row) {
+        double dc = 0.0, dv = 0.0;
+        for (int i = 0; i < 3; ++i) dc += pc[3 * row + i] * pc[3 * col + i];
+        for (int i = 0; i < 3; ++i) dv += pv[3 * row + i] * pv[3 * col + i];
+        M[row + (size_t)n * col] += pw * (cw * dc + mw * dv);
+      }
+  }
+  return 0;
+}
+
+// assemble_tetra_nedelec_element (order 1, 4-point rule), assembly_tetra_nedelec_3d.f90:2357-2404
+int or_nedelec_whitney_element(const double *v, double cw, double mw, double *M) {
+  double J[9], Ji[9], det;
+  if (!tetra_geometry(v, J, &det)) return 1;
+  inv3(J, det, Ji);
+  double P[12], W[4];
+  or_tetra_degree_two_rule(P, W);
+  double rv[18], rc[18], pv[18], pc[18];
+  std::fill(M, M + 36, 0.0);
+  for (int pt = 0; pt < 4; ++pt) {
+    if (or_whitney_evaluate(P + 3 * pt, rv, rc)) return 1;
+    covariant(J, det, Ji, 6, rv, rc, pv, pc);
+    for (int col = 0; col < 6; ++col)
+      for (int row = 0; row < 6; ++row) {
+        double dc = 0.0, dv = 0.0;
+        for (int i = 0; i < 3; ++i) dc += pc[3 * row + i] * pc[3 * col + i];
+        for (int i = 0; i < 3; ++i) dv += pv[3 * row + i] * pv[3 * col + i];
+        M[row + 6 * col] += det * (1.0 / 24.0) * (cw * dc + mw * dv);
+      }
+  }
+  return 0;
+}
+
+int64_t or_nedelec_csc_nnz(int k, int nt, const int *tets) {
+  int nb = or_nedelec_dof_count(k), ng = 0;
+  std::vector<int> gd((size_t)nb * nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), nullptr,
+                         nullptr, &ng))
+    return -1;
+  std::vector<uint64_t> keys;
+  keys.reserve((size_t)nt * nb * nb);
+  for (int t = 0; t < nt; ++t)
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i)
+        keys.push_back(((uint64_t)gd[(size_t)nb * t + j] << 32) | (uint32_t)gd[(size_t)nb * t + i]);
+  std::sort(keys.begin(), keys.end());
+  return std::unique(keys.begin(), keys.end()) - keys.begin();
+}
+
+// assemble_tetra_nedelec_curl_mass_csc (order 1: :2042-2112 with s_i s_j; order >= 2:
+// assemble_arbitrary_order_curl_mass_csc :2289-2355 with T^T K T and q = 2k).
+// Optional per-cell arrays scale the curl / mass coefficients cellwise.
+int or_nedelec_csc(int nv, const double *verts, int nt, const int *tets, int k, double cw,
+                   double mw, const double *ccurl, const double *cmass, int64_t cap, int *n_dofs,
+                   int64_t *nnz, int64_t *col_ptr, int *row_idx, double *values) {
+  if (k < 1 || nt < 1) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  int nb = or_nedelec_dof_count(k), ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  *n_dofs = ng;
+  int64_t ntrip = (int64_t)nt * nb * nb;
+  std::vector<int> rows(ntrip), cols(ntrip);
+  std::vector<double> tv(ntrip), K((size_t)nb * nb), T((size_t)nb * nb), KT((size_t)nb * nb),
+      O((size_t)nb * nb);
+  int64_t e = 0;
+  for (int t = 0; t < nt; ++t) {
+    double v[12];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+    double c = ccurl ? cw * ccurl[t] : cw, m = cmass ? mw * cmass[t] : mw;
+    if (k == 1) {
+      if (or_nedelec_whitney_element(v, c, m, K.data())) return 1;
+      for (int col = 0; col < 6; ++col)
+        for (int row = 0; row < 6; ++row, ++e) {
+          rows[e] = gd[(size_t)nb * t + row];
+          cols[e] = gd[(size_t)nb * t + col];
+          tv[e] = (double)(eo[6 * t + row] * eo[6 * t + col]) * K[row + 6 * col];
+        }
+      continue;
+    }
+    if (or_nedelec_element(v, k, 2 * k, c, m, K.data())) return 1;
+    if (or_nedelec_transform(k, eo.data() + 6 * t, fp.data() + 12 * t, T.data())) return 1;
+    // oriented = matmul(transpose(T), matmul(K, T))
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        double s = 0.0;
+        for (int l = 0; l < nb; ++l) s += K[i + (size_t)nb * l] * T[l + (size_t)nb * j];
+        KT[i + (size_t)nb * j] = s;
+      }
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        double s = 0.0;
+        for (int l = 0; l < nb; ++l) s += T[l + (size_t)nb * i] * KT[l + (size_t)nb * j];
+        O[i + (size_t)nb * j] = s;
+      }
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row, ++e) {
+        rows[e] = gd[(size_t)nb * t + row];
+        cols[e] = gd[(size_t)nb * t + col];
+        tv[e] = O[row + (size_t)nb * col];
+      }
+  }
+  return or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tv.data(), cap, nnz, col_ptr,
+                             row_idx, values);
+}
+
+static int nedelec_load_rule(int k, RuleN &R) {
+  // order 1: the 4-point rule (assemble_tetra_nedelec_load_element :2516-2553);
+  // order >= 2: Duffy with q = 2k+2 (assemble_tetra_nedelec_load_element_order :547)
+  return make_rule(k == 1 ? 1 : 0, 2 * k + 2, R) ? 0 : 1;
+}
+
+int or_nedelec_load_points(int nv, const double *verts, int nt, const int *tets, int k,
+                           double *out) {
+  RuleN R;
+  if (nedelec_load_rule(k, R)) return 1;
+  int nq = (int)R.w.size();
+  for (int t = 0; t < nt; ++t) {
+    double v[12], J[9];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+    tetra_jacobian(v, J);
+    for (int pt = 0; pt < nq; ++pt) {
+      double xi[3] = {R.x[pt], R.y[pt], R.z[pt]};
+      for (int r = 0; r < 3; ++r) {
+        double s = v[r];
+        for (int c = 0; c < 3; ++c) s = s + J[r + 3 * c] * xi[c];
+        out[3 * ((size_t)nq * t + pt) + r] = s;
+      }
+    }
+  }
+  return 0;
+}
+
+// Vector load with per-quadrature-point source samples: order 1 as
+// assemble_tetra_nedelec_vector_load (:2002-2040, signs), order >= 2 as
+// assemble_tetra_nedelec_vector_load_order (:71-127, T^T b_e).  rhs has n_dofs entries.
+int or_nedelec_load_samples(int nv, const double *verts, int nt, const int *tets, int k,
+                            const double *src, double *rhs) {
+  int nb = or_nedelec_dof_count(k), ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  RuleN R;
+  if (nedelec_load_rule(k, R)) return 1;
+  int nq = (int)R.w.size();
+  for (int i = 0; i < ng; ++i) rhs[i] = 0.0;
+  std::vector<double> rv(3 * (size_t)nb * nq), rc(3 * (size_t)nb * nq), pv(3 * nb), pc(3 * nb),
+      ev(nb), T((size_t)nb * nb);
+  for (int pt = 0; pt < nq; ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    int st = (k == 1) ? or_whitney_evaluate(P, rv.data() + 3 * (size_t)nb * pt,
+                                            rc.data() + 3 * (size_t)nb * pt)
+                      : or_nedelec_evaluate(k, P, rv.data() + 3 * (size_t)nb * pt,
+                                            rc.data() + 3 * (size_t)nb * pt);
+    if (st) return 1;
+  }
+  for (int t = 0; t < nt; ++t) {
+    double v[12], J[9], Ji[9], det;
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+    if (!tetra_geometry(v, J, &det)) return 1;
+    inv3(J, det, Ji);
+    std::fill(ev.begin(), ev.end(), 0.0);
+    for (int pt = 0; pt < nq; ++pt) {
+      covariant(J, det, Ji, nb, rv.data() + 3 * (size_t)nb * pt, rc.data() + 3 * (size_t)nb * pt,
+                pv.data(), pc.data());
+      const double *s = src + 3 * ((size_t)nq * t + pt);
+      for (int d = 0; d < nb; ++d) {
+        double dt = 0.0;
+        for (int i = 0; i < 3; ++i) dt += s[i] * pv[3 * d + i];
+        ev[d] = ev[d] + det * R.w[pt] * dt;
+      }
+    }
+    if (k == 1) {
+      for (int d = 0; d < 6; ++d) {
+        int g = gd[(size_t)nb * t + d];
+        rhs[g] = rhs[g] + (double)eo[6 * t + d] * ev[d];
+      }
+      continue;
+    }
+    if (or_nedelec_transform(k, eo.data() + 6 * t, fp.data() + 12 * t, T.data())) return 1;
+    for (int d = 0; d < nb; ++d) {
+      double s = 0.0;
+      for (int l = 0; l < nb; ++l) s += T[l + (size_t)nb * d] * ev[l];
+      int g = gd[(size_t)nb * t + d];
+      rhs[g] = rhs[g] + s;
+    }
+  }
+  return 0;
+}
+
+// build_zero_tangential_mask, src/solvers/fortfem_tetra_nedelec_solver_3d.f90:416-458.
+// faithful = 1 runs the reference's O(F*T) incidence and O(F*E) edge scans.
+int or_pec_mask(int k, int nt, const int *tets, int faithful, uint8_t *con) {
+  int ne = 0, nf = 0, ng = 0;
+  if (or_nedelec_dof_map(k, nt, tets, faithful, nullptr, &ne, nullptr, &nf, nullptr, nullptr,
+                         nullptr, &ng))
+    return 1;
+  std::vector<int> edges(2 * (size_t)ne), faces(3 * (size_t)nf);
+  or_nedelec_dof_map(k, nt, tets, faithful, edges.data(), &ne, faces.data(), &nf, nullptr, nullptr,
+                     nullptr, &ng);
+  std::memset(con, 0, ng);
+  int64_t edc = (int64_t)k * ne;
+  int fdc = k * (k - 1);
+  std::vector<int> inc(nf, 0);
+  std::unordered_map<uint64_t, int> emap;
+  if (faithful) {
+    for (int f = 0; f < nf; ++f)
+      for (int t = 0; t < nt; ++t) {
+        bool all = true;
+        for (int a = 0; a < 3; ++a) {
+          bool any = false;
+          for (int n = 0; n < 4; ++n) any = any || tets[4 * t + n] == faces[3 * f + a];
+          all = all && any;
+        }
+        if (all) inc[f]++;
+      }
+  } else {
+    std::unordered_map<uint64_t, int> fmap;
+    for (int f = 0; f < nf; ++f)
+      fmap[((uint64_t)(uint32_t)faces[3 * f] << 42) ^ ((uint64_t)(uint32_t)faces[3 * f + 1] << 21) ^
+           (uint64_t)(uint32_t)faces[3 * f + 2]] = f;
+    for (int t = 0; t < nt; ++t)
+      for (int lf = 0; lf < 4; ++lf) {
+        int cv[3];
+        for (int i = 0; i < 3; ++i) cv[i] = tets[4 * t + kLocalFaces[lf][i]];
+        std::sort(cv, cv + 3);
+        inc[fmap[((uint64_t)(uint32_t)cv[0] << 42) ^ ((uint64_t)(uint32_t)cv[1] << 21) ^
+                 (uint64_t)(uint32_t)cv[2]]]++;
+      }
+    for (int e = 0; e < ne; ++e)
+      emap[((uint64_t)(uint32_t)edges[2 * e] << 32) | (uint32_t)edges[2 * e + 1]] = e;
+  }
+  for (int f = 0; f < nf; ++f) {
+    if (inc[f] != 1) continue;
+    const int *fv = faces.data() + 3 * f;
+    if (faithful) {
+      for (int e = 0; e < ne; ++e) {
+        bool a = fv[0] == edges[2 * e] || fv[1] == edges[2 * e] || fv[2] == edges[2 * e];
+        bool b = fv[0] == edges[2 * e + 1] || fv[1] == edges[2 * e + 1] || fv[2] == edges[2 * e + 1];
+        if (a && b)
+          for (int m = 0; m < k; ++m) con[(int64_t)e * k + m] = 1;
+      }
+    } else {
+      const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+      for (auto &pr : pairs) {
+        int a = std::min(fv[pr[0]], fv[pr[1]]), b = std::max(fv[pr[0]], fv[pr[1]]);
+        int e = emap[((uint64_t)(uint32_t)a << 32) | (uint32_t)b];
+        for (int m = 0; m < k; ++m) con[(int64_t)e * k + m] = 1;
+      }
+    }
+    for (int m = 0; m < fdc; ++m) con[edc + (int64_t)f * fdc + m] = 1;
+  }
+  return 0;
+}
+
+}  // extern "C"

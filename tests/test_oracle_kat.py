@@ -1,0 +1,313 @@
+"""Pin the CPU oracle against the reference's own known-answer tests.
+
+Each test cites the reference test it restates; tolerances are the reference's.
+"""
+import json
+import math
+import os
+import sys
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+import oracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def fact(n):
+    return math.factorial(n)
+
+
+# test/test_tetra_duffy_quadrature.f90:13-36
+def test_duffy_exactness():
+    for degree in range(8):
+        x, y, z, w = oracle.tetra_duffy(degree)
+        assert abs(w.sum() - 1.0 / 6.0) < 2e-14
+        for zd in range(degree + 1):
+            for yd in range(degree - zd + 1):
+                for xd in range(degree - yd - zd + 1):
+                    num = np.sum(w * x ** xd * y ** yd * z ** zd)
+                    exact = fact(xd) * fact(yd) * fact(zd) / fact(xd + yd + zd + 3)
+                    assert abs(num - exact) < 4e-14
+
+
+def test_gauss_legendre_matches_numpy():
+    for n in range(1, 12):
+        x, w = oracle.gauss_legendre(n, 0.0, 1.0)
+        xr, wr = np.polynomial.legendre.leggauss(n)
+        assert np.allclose(x, 0.5 * xr + 0.5, atol=1e-15, rtol=0)
+        assert np.allclose(w, 0.5 * wr, atol=1e-15, rtol=0)
+
+
+def test_degree_two_rule_is_degree_two_exact():
+    p, w = oracle.degree_two_rule()
+    for xd, yd, zd in [(0, 0, 0), (1, 0, 0), (0, 2, 0), (1, 1, 0), (0, 0, 2), (0, 1, 1)]:
+        num = np.sum(w * p[:, 0] ** xd * p[:, 1] ** yd * p[:, 2] ** zd)
+        exact = fact(xd) * fact(yd) * fact(zd) / fact(xd + yd + zd + 3)
+        assert abs(num - exact) < 1e-15
+
+
+# test/test_structured_tetra_box_mesh.f90:19-51
+def test_box_mesh_invariants():
+    bounds = ((-1.0, 0.5, 2.0), (1.0, 2.0, 3.5))
+    v, t = oracle.box_mesh([2, 1, 3], bounds)
+    assert len(v) == 3 * 2 * 4 and len(t) == 36
+    assert np.allclose(v.min(0), bounds[0], atol=1e-14) and np.allclose(v.max(0), bounds[1], atol=1e-14)
+    J = np.stack([v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]], v[t[:, 3]] - v[t[:, 0]]], axis=2)
+    det = np.linalg.det(J)
+    assert (det > 0).all()
+    assert abs(det.sum() / 6 - 2.0 * 1.5 * 1.5) < 1e-12
+
+
+# test/test_tetra_lagrange_arbitrary_order.f90:22-73 (partition of unity, nodal property)
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_lagrange_partition_and_nodal(p):
+    idx, nodes = oracle.lagrange_indices(p)
+    v, g = oracle.lagrange_evaluate(p, [0.13, 0.21, 0.37])
+    assert abs(v.sum() - 1.0) < 3e-13 and np.abs(g.sum(0)).max() < 3e-13
+    for i, node in enumerate(nodes):
+        v, _ = oracle.lagrange_evaluate(p, node)
+        e = np.zeros(len(nodes)); e[i] = 1
+        assert np.abs(v - e).max() < 3e-13
+
+
+# test/test_tetra_lagrange_global_dof_map.f90:17-47
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_lagrange_dof_map_shared_face(p):
+    tets = np.array([[0, 1, 2, 3], [2, 1, 0, 4]])
+    idx, _ = oracle.lagrange_indices(p)
+    for faithful in (False, True):
+        gd, n = oracle.lagrange_dof_map(p, tets, faithful=faithful)
+        shared = [l for l in range(len(idx)) if idx[l, 3] == 0]
+        for l in shared:
+            assert gd[0, l] in gd[1]
+        assert len(shared) == (p + 1) * (p + 2) // 2
+        assert n == 2 * (p + 1) * (p + 2) * (p + 3) // 6 - len(shared)
+
+
+def test_lagrange_dof_map_rejects():
+    tets = np.array([[0, 1, 2, 3], [2, 1, 0, 4]])
+    with pytest.raises(oracle.OracleError):
+        oracle.lagrange_dof_map(0, tets)
+    with pytest.raises(oracle.OracleError):
+        oracle.lagrange_dof_map(2, np.array([[0, 1, 2, 3], [0, 0, 1, 4]]))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_lagrange_dof_map_hash_equals_faithful(p):
+    v, t = oracle.box_mesh([2, 2, 2])
+    a, na = oracle.lagrange_dof_map(p, t, faithful=False)
+    b, nb = oracle.lagrange_dof_map(p, t, faithful=True)
+    assert na == nb and (a == b).all()
+
+
+# test/test_tetra_lagrange_arbitrary_order_assembly.f90:28-66
+def test_lagrange_element_symmetry_and_linear_energy():
+    verts = np.array([[0.2, -0.3, 0.1], [2.1, -0.5, 0.4], [0.6, 1.4, -0.2], [-0.1, 0.2, 1.6]])
+    for p in range(1, 5):
+        m = oracle.lagrange_element(verts.reshape(-1), p, 0, 2 * p + 2)
+        assert np.abs(m - m.T).max() < 2e-11
+    mv = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0, 0, -1.0]])
+    tets = np.array([[0, 1, 2, 3], [0, 2, 1, 4]])
+    n, cp, ri, val = oracle.lagrange_csc(mv, tets, 1, 0, 4)
+    gd, _ = oracle.lagrange_dof_map(1, tets)
+    coef = np.zeros(n)
+    coef[gd.reshape(-1)] = mv[tets.reshape(-1), 0]
+    y = oracle.csc_matvec(n, cp, ri, val, coef)
+    assert abs(coef @ y - 1.0 / 3.0) < 2e-12
+
+
+def test_lagrange_dirichlet_hash_equals_faithful():
+    v, t = oracle.box_mesh([2, 2, 2])
+    for p in (1, 2):
+        a, pa = oracle.lagrange_dirichlet(p, v, t, faithful=False)
+        b, pb = oracle.lagrange_dirichlet(p, v, t, faithful=True)
+        assert (a == b).all()
+        assert np.allclose(pa[a], pb[b], atol=1e-15)
+    # P2 on n^3: interior nodes are (2n-1)^3
+    a, _ = oracle.lagrange_dirichlet(2, v, t)
+    assert (~a).sum() == 3 ** 3
+
+
+def test_csc_pattern_value_independent():
+    # test/test_tetra_lagrange_stiffness_csc_ad.f90:62-67: pattern unchanged by values
+    v, t = oracle.box_mesh([2, 2, 1])
+    n1, cp1, ri1, _ = oracle.lagrange_csc(v, t, 2, 1, 0)
+    n2, cp2, ri2, _ = oracle.lagrange_csc(v, t, 2, 1, 0, stiffness=0.0, mass=0.0)
+    assert n1 == n2 and (cp1 == cp2).all() and (ri1 == ri2).all()
+
+
+def test_csc_from_triplet_sums_duplicates():
+    cp, ri, v = oracle.csc_from_triplet(3, 3, [2, 0, 2, 1], [0, 0, 0, 2], [1.0, 2.0, 3.0, 4.0])
+    assert list(cp) == [0, 2, 2, 3] and list(ri) == [0, 2, 1]
+    assert list(v) == [2.0, 4.0, 4.0]
+
+
+# test/test_advanced_solvers.f90:768-797 (sparse Jacobi-PCG agrees with the dense path)
+def test_pcg_sparse_matches_dense():
+    v, t = oracle.unit_square_mesh(9)
+    a = oracle.p1_dense(v, t, mass=1.0, stiffness=1.0)
+    n, cp, ri, val = oracle.p1_csc(v, t, mass=1.0, stiffness=1.0)
+    b = oracle.p1_load(v, t, 1.0)
+    # the reference's absolute breakdown guard |p^T A p| < 1e-14 ends small
+    # systems early, so the load is scaled to keep p^T A p above it
+    b = 1e3 * b
+    xd, sd = oracle.pcg_dense(a, b, tol=1e-10)
+    xs, ss = oracle.pcg_sparse(n, cp, ri, val, b, tol=1e-10)
+    assert sd["converged"] and ss["converged"]
+    assert np.abs(xd - xs).max() < 1e-6
+    assert np.abs(a @ xs - b).max() < 1e-8 * np.abs(b).max()
+
+
+def test_p1_csc_matches_dense_and_boundary():
+    v, t = oracle.unit_square_mesh(65)
+    assert len(v) == 4225 and len(t) == 8192
+    bnd = oracle.square_boundary(len(v), t)
+    assert bnd.sum() == 256
+    n, cp, ri, val = oracle.p1_csc(v[:400] if False else v, t)
+    assert cp[-1] == 29057
+    import scipy.sparse as sp
+    v9, t9 = oracle.unit_square_mesh(9)
+    a = oracle.p1_dense(v9, t9, 0.0, 1.0)
+    n9, cp9, ri9, val9 = oracle.p1_csc(v9, t9, 0.0, 1.0)
+    assert np.abs(sp.csc_matrix((val9, ri9, cp9), shape=(n9, n9)).toarray() - a).max() < 1e-15
+
+
+def _constant_field_dofs(k, verts, tets, dm, field):
+    """set_constant_field_dofs of test/test_tetra_nedelec_sparse_assembly_slow.f90:92-170."""
+    edges, faces, gd = dm["edges"], dm["faces"], dm["global_dofs"]
+    dofs = np.zeros(dm["n_global"])
+    for e, (a, b) in enumerate(edges):
+        dofs[e * k] = field @ (verts[b] - verts[a])
+    fdc = k * (k - 1)
+    off = k * len(edges)
+    for f, fv in enumerate(faces):
+        for comp in range(2):
+            tang = verts[fv[comp + 1]] - verts[fv[0]]
+            mono = 0
+            for d in range(k - 1):
+                for xd in range(d + 1):
+                    yd = d - xd
+                    mono += 1
+                    dof = off + f * fdc + comp * fdc // 2 + mono - 1
+                    dofs[dof] = (field @ tang) * fact(xd) * fact(yd) / fact(xd + yd + 2)
+    base = 6 * k + 4 * fdc
+    for c, tet in enumerate(tets):
+        J = np.stack([verts[tet[1]] - verts[tet[0]], verts[tet[2]] - verts[tet[0]],
+                      verts[tet[3]] - verts[tet[0]]], axis=1)
+        rf = J.T @ field
+        loc = base
+        for comp in range(3):
+            for d in range(k - 2):
+                for xd in range(d + 1):
+                    for yd in range(d - xd + 1):
+                        zd = d - xd - yd
+                        dofs[gd[c, loc]] = rf[comp] * fact(xd) * fact(yd) * fact(zd) / fact(d + 3)
+                        loc += 1
+    return dofs
+
+
+# test/test_tetra_nedelec_sparse_assembly_slow.f90:31-85
+def test_nedelec_energy_kats():
+    verts = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0, 0, -1.0]])
+    tets = np.array([[0, 1, 2, 3], [0, 2, 1, 4]])
+    edges, _, _ = oracle.edge_dof_map(tets)
+    assert len(edges) == 9
+    field = np.array([1.0, 2.0, -1.0])
+    dofs = np.array([field @ (verts[b] - verts[a]) for a, b in edges])
+    n, cp, ri, val = oracle.nedelec_csc(verts, tets, 1, 4.0, 1.5)
+    y = oracle.csc_matvec(n, cp, ri, val, dofs)
+    assert abs(dofs @ y - 3.0) < 2e-12
+    curl = np.array([1.0, -2.0, 3.0])
+    dofs = np.array([(0.5 * np.cross(curl, 0.5 * (verts[a] + verts[b]))) @ (verts[b] - verts[a])
+                     for a, b in edges])
+    n, cp, ri, val = oracle.nedelec_csc(verts, tets, 1, 2.0, 0.0)
+    y = oracle.csc_matvec(n, cp, ri, val, dofs)
+    assert abs(dofs @ y - 28.0 / 3.0) < 3e-12
+    for k in range(2, 6):
+        dm = oracle.nedelec_dof_map(k, tets)
+        dofs = _constant_field_dofs(k, verts, tets, dm, field)
+        n, cp, ri, val = oracle.nedelec_csc(verts, tets, k, 4.0, 1.5)
+        y = oracle.csc_matvec(n, cp, ri, val, dofs)
+        assert abs(dofs @ y - 3.0) < 1e-8, k
+
+
+# test/test_tetra_nedelec_global_dof_map.f90:22-74 (topology numbers at order 6)
+def test_nedelec_order6_topology():
+    tets = np.array([[0, 1, 2, 3], [2, 0, 1, 4]])
+    for faithful in (False, True):
+        dm = oracle.nedelec_dof_map(6, tets, faithful=faithful)
+        assert len(dm["edges"]) == 9 and len(dm["faces"]) == 7
+        assert dm["global_dofs"].shape[1] == 216 and dm["n_global"] == 384
+        fs = 6 * 6
+        assert (dm["global_dofs"][0, fs:fs + 30] == dm["global_dofs"][1, fs:fs + 30]).all()
+        assert list(dm["face_permutations"][0, 0]) == [1, 2, 3]
+        assert list(dm["face_permutations"][1, 0]) == [3, 1, 2]
+
+
+@pytest.mark.parametrize("k", [2, 3, 4])
+def test_nedelec_transform_signs_and_roundtrip(k):
+    tets = np.array([[0, 1, 2, 3], [2, 0, 1, 4]])
+    dm = oracle.nedelec_dof_map(k, tets)
+    T = oracle.nedelec_transform(k, dm["edge_orientations"][1], dm["face_permutations"][1])
+    signs = [T[i, i] for i in range(k)]
+    assert signs == [(-1.0 if m % 2 == 0 else 1.0) for m in range(k)]  # reversed edge 1
+    # shared face: both cells give the same canonical coefficients
+    fdc = k * (k - 1); fs = 6 * k
+    T0 = oracle.nedelec_transform(k, dm["edge_orientations"][0], dm["face_permutations"][0])
+    canonical = np.array([(2 * m - 7) / (m + 2) for m in range(1, fdc + 1)])
+    b0 = T0[fs:fs + fdc, fs:fs + fdc] @ canonical
+    assert np.allclose(b0, canonical)
+
+
+def test_nedelec_dof_maps_hash_equals_faithful():
+    v, t = oracle.box_mesh([2, 2, 2])
+    for k in (1, 2, 3):
+        a = oracle.nedelec_dof_map(k, t, faithful=False)
+        b = oracle.nedelec_dof_map(k, t, faithful=True)
+        for key in ("edges", "faces", "global_dofs", "edge_orientations", "face_permutations"):
+            assert (a[key] == b[key]).all(), key
+        assert (oracle.pec_mask(k, t, False) == oracle.pec_mask(k, t, True)).all()
+
+
+def test_whitney_equals_order1_table_basis():
+    for pt in ([0.1, 0.2, 0.3], [0.25, 0.25, 0.25], [0.0, 0.5, 0.1]):
+        a = oracle.whitney_evaluate(pt)
+        b = oracle.nedelec_evaluate(1, pt)
+        assert np.abs(a[0] - b[0]).max() < 1e-15 and np.abs(a[1] - b[1]).max() < 1e-15
+
+
+# The repository's exact generator against the reference's generated tables
+def test_generated_tables_match_reference_digests():
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_golden import canonical_digest
+    from fortfem_b200.gen_nedelec_tables import PERMUTATIONS, coefficients, face_transform
+    fx = json.load(open(os.path.join(HERE, "golden", "nedelec_tables.json")))
+    for k in (1, 2, 3, 4):
+        Cm = coefficients(k)
+        n = len(Cm)
+        ent = {(r + 1, c + 1): Cm[r][c] for r in range(n) for c in range(n) if Cm[r][c] != 0}
+        assert canonical_digest(ent) == fx["coefficients"][str(k)]["digest"]
+        for r, c, s in fx["coefficients"][str(k)]["samples"]:
+            assert Cm[r - 1][c - 1] == Fraction(s)
+    for k in (2, 3, 4):
+        for pi, perm in enumerate(PERMUTATIONS):
+            T = face_transform(k, perm)
+            n = len(T)
+            ent = {(r + 1, c + 1): T[r][c] for r in range(n) for c in range(n) if T[r][c] != 0}
+            assert canonical_digest(ent) == fx["face_transforms"][f"{k}/{pi + 1}"]["digest"]
+
+
+def test_emitted_tables_are_rounded_exact_values():
+    from fortfem_b200.gen_nedelec_tables import coefficients
+    path = os.path.join(os.path.dirname(HERE), "fortfem_b200", "csrc", "nedelec_tables.inc")
+    text = open(path).read()
+    import re
+    for k in (1, 2, 3):
+        m = re.search(rf"kNedelecCoefficients{k}\[\d+\] = \{{(.*?)\}};", text)
+        vals = [float.fromhex(s.strip()) for s in m.group(1).split(",")]
+        Cm = coefficients(k)
+        n = len(Cm)
+        assert vals == [float(Cm[r][c]) for c in range(n) for r in range(n)]
