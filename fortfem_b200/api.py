@@ -1,0 +1,591 @@
+"""Host-side mirror of fortfem's assembly and solver entry points.
+
+Function names, argument meaning and status behaviour follow the reference
+Fortran interfaces (each docstring names the routine it replaces); arrays are
+zero-based numpy arrays, and every call goes through the C-ABI of
+``libfortfem_gpu.so`` (include/fortfem_gpu.h) to the sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Callable, Optional, Union
+
+import numpy as np
+
+from . import _capi as K
+
+ArrayLike = Union[np.ndarray, list, tuple]
+
+
+class FortfemError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        super().__init__(f"{where}: {K.STATUS_TEXT.get(code, 'error')} (status {code})")
+        self.code = code
+
+
+@dataclass
+class Status:
+    """fortsparse_status_t: code 0 is success."""
+    code: int = 0
+    message: str = ""
+
+    @classmethod
+    def of(cls, code: int, where: str) -> "Status":
+        return cls(code, "" if code == 0 else f"{where}: {K.STATUS_TEXT.get(code, 'error')}")
+
+
+@dataclass
+class CscMatrix:
+    """csc_t (fortsparse): zero-based column pointers and row indices."""
+    nrow: int
+    ncol: int
+    col_ptr: np.ndarray
+    row_idx: np.ndarray
+    val: np.ndarray
+
+    @property
+    def nnz(self) -> int:
+        return int(self.col_ptr[-1])
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csc_matrix((self.val, self.row_idx, self.col_ptr), shape=(self.nrow, self.ncol))
+
+
+@dataclass
+class SolverOptions:
+    """solver_options_t (src/solvers/advanced_solvers.f90:32-44) with the
+    reference defaults, plus the GPU precision controls."""
+    method: str = "auto"
+    tolerance: float = 1.0e-6
+    max_iterations: int = 1000
+    preconditioner: str = "none"
+    tolerance_type: str = "relative"
+    verbosity: int = 0
+    precision: str = "fp64"          # "fp64" (reference semantics) or "mixed"
+    inner_tolerance: float = 1.0e-5
+    max_refinements: int = 30
+    timeout_seconds: float = 60.0
+    breakdown_guard: str = "absolute"  # "absolute" (reference) or "spd"
+
+    def to_c(self) -> K.SolverOptionsC:
+        if self.method not in ("auto", "pcg", "cg"):
+            raise FortfemError(K.FFG_INVALID_INPUT, f"method {self.method!r} is not on this path")
+        o = K.SolverOptionsC()
+        o.version = K.FFG_OPTIONS_VERSION
+        o.preconditioner = 1 if (self.preconditioner == "jacobi" and self.method != "cg") else 0
+        o.precision = K.FFG_PRECISION_MIXED if self.precision == "mixed" else K.FFG_PRECISION_FP64
+        o.tolerance_type = 1 if self.tolerance_type == "absolute" else 0
+        o.tolerance = float(self.tolerance)
+        o.max_iterations = int(self.max_iterations)
+        o.max_refinements = int(self.max_refinements)
+        o.inner_tolerance = float(self.inner_tolerance)
+        o.verbosity = int(self.verbosity)
+        o.timeout_seconds = float(self.timeout_seconds)
+        o.breakdown_guard = 1 if self.breakdown_guard == "spd" else 0
+        return o
+
+
+def solver_options(**kw) -> SolverOptions:
+    """solver_options(...) constructor (advanced_solvers.f90:1430-1465)."""
+    return SolverOptions(**kw)
+
+
+@dataclass
+class SolverStats:
+    """solver_stats_t (advanced_solvers.f90:47-57) plus GPU fields."""
+    converged: bool = False
+    iterations: int = 0
+    final_residual: float = 0.0
+    solve_time: float = 0.0
+    method_used: str = "pcg"
+    refinements: int = 0
+    true_relative_residual: float = 0.0
+    assembly_time: float = 0.0
+    status: int = 0
+
+    @classmethod
+    def from_c(cls, s: K.SolverStatsC) -> "SolverStats":
+        return cls(bool(s.converged), s.iterations, s.final_residual, s.solve_seconds, "pcg",
+                   s.refinements, s.true_relative_residual, s.assembly_seconds, s.status)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _opt(a, n, dtype=np.float64):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=dtype)
+    if a.size != n:
+        raise FortfemError(K.FFG_INVALID_INPUT, "array length")
+    return a
+
+
+# ------------------------------------------------------------------ meshes
+
+def generate_structured_tetra_box_mesh(bounds, counts):
+    """generate_structured_tetra_box_mesh (src/mesh/structured_tetra_box_mesh.f90:12-70).
+    bounds: (3, 2) [[xmin, xmax], [ymin, ymax], [zmin, zmax]]; returns
+    (vertices (n, 3), tetrahedra (T, 4) zero-based, Status)."""
+    b = np.asarray(bounds, dtype=np.float64)
+    flat = _f64([b[0, 0], b[1, 0], b[2, 0], b[0, 1], b[1, 1], b[2, 1]])
+    counts = _i32(counts)
+    nv = int(np.prod(counts.astype(np.int64) + 1))
+    nt = 6 * int(np.prod(counts.astype(np.int64)))
+    v = np.zeros((max(nv, 0), 3))
+    t = np.zeros((max(nt, 0), 4), np.int32)
+    st = C.c_int(0)
+    K.load().ffg_structured_tetra_box_mesh(_ptr(flat), _ptr(counts), _ptr(v), _ptr(t), C.byref(st))
+    return v, t, Status.of(st.value, "generate_structured_tetra_box_mesh")
+
+
+def unit_square_mesh(n: int):
+    """unit_square_mesh(n) (src/fortfem_api_mesh.f90:128-139): n vertices per side."""
+    v = np.zeros((n * n, 2))
+    t = np.zeros((2 * (n - 1) ** 2, 3), np.int32)
+    st = C.c_int(0)
+    K.load().ffg_unit_square_mesh(n, _ptr(v), _ptr(t), C.byref(st))
+    if st.value:
+        raise FortfemError(st.value, "unit_square_mesh")
+    return v, t
+
+
+# -------------------------------------------------------- drop-in assembly
+
+def _csc_call(fn, args, where, capacity_hint=None):
+    lib = K.load()
+    nd = C.c_int(0)
+    nz = C.c_int64(0)
+    st = C.c_int(0)
+    getattr(lib, fn)(*args, C.c_int64(0), C.byref(nd), C.byref(nz), None, None, None, C.byref(st))
+    if st.value not in (K.FFG_OK, K.FFG_CAPACITY):
+        return None, Status.of(st.value, where)
+    n = nd.value
+    cp = np.zeros(n + 1, np.int64)
+    ri = np.zeros(nz.value, np.int32)
+    val = np.zeros(nz.value)
+    getattr(lib, fn)(*args, C.c_int64(nz.value), C.byref(nd), C.byref(nz), _ptr(cp), _ptr(ri),
+                     _ptr(val), C.byref(st))
+    if st.value:
+        return None, Status.of(st.value, where)
+    return CscMatrix(n, n, cp, ri, val), Status()
+
+
+def assemble_tetra_lagrange_stiffness_csc(mesh_vertices, tetrahedra, degree, quadrature_degree,
+                                          stiffness_coefficient=None, mass_coefficient=None,
+                                          rule=K.FFG_RULE_DUFFY, cell_stiffness=None,
+                                          cell_mass=None):
+    """assemble_tetra_lagrange_stiffness_csc
+    (src/assembly/assembly_tetra_lagrange_arbitrary_order_3d.f90:276-334).
+    Returns (CscMatrix, Status).  cell_* scale the coefficients cellwise."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    cs = _opt(cell_stiffness, len(t))
+    cm = _opt(cell_mass, len(t))
+    args = [len(v), _ptr(v), len(t), _ptr(t), int(degree), int(rule), int(quadrature_degree),
+            1.0 if stiffness_coefficient is None else float(stiffness_coefficient),
+            0.0 if mass_coefficient is None else float(mass_coefficient), _ptr(cs), _ptr(cm)]
+    return _csc_call("ffg_assemble_tetra_lagrange_stiffness_csc", args,
+                     "Tetrahedral H1 sparse assembly failed")
+
+
+def assemble_tetra_lagrange_scalar_load_samples(mesh_vertices, tetrahedra, degree,
+                                                quadrature_degree, source_values,
+                                                rule=K.FFG_RULE_DUFFY):
+    """assemble_tetra_lagrange_scalar_load_samples (same file :473-528).
+    source_values: (T, n_q) samples at the rule's points.  Returns (rhs, Status)."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    p = Problem(K.FFG_TETRA_LAGRANGE, degree, t, len(v), rule=rule,
+                quadrature_degree=quadrature_degree, boundary="none")
+    try:
+        src = _f64(source_values)
+        if src.size != p.samples_per_cell * len(t):
+            return None, Status.of(K.FFG_INVALID_INPUT, "Sampled tetrahedral H1 scalar load failed")
+        rhs = np.zeros(p.n_dofs)
+        st = C.c_int(0)
+        K.load().ffg_assemble_tetra_lagrange_scalar_load_samples(
+            len(v), _ptr(v), len(t), _ptr(t), int(degree), int(rule), int(quadrature_degree),
+            _ptr(src), p.n_dofs, _ptr(rhs), C.byref(st))
+        return (rhs if st.value == 0 else None), Status.of(st.value, "Sampled tetrahedral H1 scalar load failed")
+    finally:
+        p.close()
+
+
+def assemble_tetra_nedelec_curl_mass_csc(mesh_vertices, tetrahedra, curl_coefficient=None,
+                                         mass_coefficient=None, order=None, cell_curl=None,
+                                         cell_mass=None):
+    """assemble_tetra_nedelec_curl_mass_csc (src/assembly/assembly_tetra_nedelec_3d.f90:2042-2112,
+    arbitrary order :2289-2355).  Returns (CscMatrix, Status)."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    args = [len(v), _ptr(v), len(t), _ptr(t), 1 if order is None else int(order),
+            1.0 if curl_coefficient is None else float(curl_coefficient),
+            1.0 if mass_coefficient is None else float(mass_coefficient),
+            _ptr(_opt(cell_curl, len(t))), _ptr(_opt(cell_mass, len(t)))]
+    return _csc_call("ffg_assemble_tetra_nedelec_curl_mass_csc", args,
+                     "Tetrahedral Nedelec assembly failed")
+
+
+def assemble_tetra_nedelec_vector_load_samples(mesh_vertices, tetrahedra, order, source_values):
+    """assemble_tetra_nedelec_vector_load_samples (assembly_tetra_nedelec_3d.f90:128-185).
+    source_values: (T, n_q, 3) at the order's load points.  Returns (rhs, Status)."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    p = Problem(K.FFG_TETRA_NEDELEC, order, t, len(v), boundary="none")
+    try:
+        src = _f64(source_values)
+        if src.size != 3 * p.samples_per_cell * len(t):
+            return None, Status.of(K.FFG_INVALID_INPUT, "Sampled tetrahedral Nedelec vector load failed")
+        rhs = np.zeros(p.n_dofs)
+        st = C.c_int(0)
+        K.load().ffg_assemble_tetra_nedelec_vector_load_samples(
+            len(v), _ptr(v), len(t), _ptr(t), int(order), _ptr(src), p.n_dofs, _ptr(rhs),
+            C.byref(st))
+        return (rhs if st.value == 0 else None), Status.of(st.value, "Sampled tetrahedral Nedelec vector load failed")
+    finally:
+        p.close()
+
+
+def assemble_scalar_p1_csc(vertices, triangles, mass_coefficient=0.0, stiffness_coefficient=1.0,
+                           cell_stiffness=None):
+    """assemble_scalar_p1_matrix (src/fortfem_forms_simple.f90:1678-1728) scattered into CSC."""
+    v = _f64(vertices).reshape(-1, 2)
+    t = _i32(triangles).reshape(-1, 3)
+    lib = K.load()
+    cs = _opt(cell_stiffness, len(t))
+    nz = C.c_int64(0)
+    st = C.c_int(0)
+    args = [len(v), _ptr(v), len(t), _ptr(t), float(mass_coefficient), float(stiffness_coefficient),
+            _ptr(cs)]
+    lib.ffg_assemble_scalar_p1_csc(*args, C.c_int64(0), C.byref(nz), None, None, None, C.byref(st))
+    if st.value not in (0, K.FFG_CAPACITY):
+        return None, Status.of(st.value, "assemble_scalar_p1_matrix")
+    n = len(v)
+    cp = np.zeros(n + 1, np.int64)
+    ri = np.zeros(nz.value, np.int32)
+    val = np.zeros(nz.value)
+    lib.ffg_assemble_scalar_p1_csc(*args, C.c_int64(nz.value), C.byref(nz), _ptr(cp), _ptr(ri),
+                                   _ptr(val), C.byref(st))
+    if st.value:
+        return None, Status.of(st.value, "assemble_scalar_p1_matrix")
+    return CscMatrix(n, n, cp, ri, val), Status()
+
+
+# -------------------------------------------------------------------- solve
+
+def solve_sparse(A_sparse: CscMatrix, b, x: np.ndarray, opts: Optional[SolverOptions] = None) -> SolverStats:
+    """solve_sparse(A_sparse, b, x, opts, stats) (src/solvers/advanced_solvers.f90:135-195):
+    x (float64 numpy array) is the initial guess and is overwritten in place."""
+    opts = opts or SolverOptions()
+    n = A_sparse.nrow
+    if A_sparse.ncol != n:
+        raise FortfemError(K.FFG_INVALID_INPUT, "solve_sparse: only square matrices are supported")
+    b = _f64(b)
+    if b.size != n or x.size != n or x.dtype != np.float64 or not x.flags.c_contiguous:
+        raise FortfemError(K.FFG_INVALID_INPUT, "solve_sparse: incompatible vector size")
+    cp = np.ascontiguousarray(A_sparse.col_ptr, dtype=np.int64)
+    ri = _i32(A_sparse.row_idx)
+    val = _f64(A_sparse.val)
+    oc = opts.to_c()
+    sc = K.SolverStatsC()
+    st = C.c_int(0)
+    K.load().ffg_solve_sparse(n, int(cp[-1]), _ptr(cp), _ptr(ri), _ptr(val), _ptr(b), _ptr(x),
+                              C.byref(oc), C.byref(sc), C.byref(st))
+    if st.value not in (0, K.FFG_NOT_CONVERGED):
+        raise FortfemError(st.value, "solve_sparse")
+    return SolverStats.from_c(sc)
+
+
+def spmv(matrix: CscMatrix, vector) -> np.ndarray:
+    """spmv (src/solvers/fortfem_sparse_matrix.f90:46-58): product = A x."""
+    x = _f64(vector)
+    y = np.zeros(matrix.nrow)
+    cp = np.ascontiguousarray(matrix.col_ptr, dtype=np.int64)
+    ri = _i32(matrix.row_idx)
+    val = _f64(matrix.val)
+    st = C.c_int(0)
+    K.load().ffg_csc_matvec(matrix.nrow, int(cp[-1]), _ptr(cp), _ptr(ri), _ptr(val), _ptr(x),
+                            _ptr(y), C.byref(st))
+    if st.value:
+        raise FortfemError(st.value, "spmv")
+    return y
+
+
+def build_topology(family: int, degree: int, cells, n_vertices: int, boundary="none"):
+    """Host-only topology (ffg_build_topology): returns dict with global_dofs
+    (cells x n_b), constrained mask, and the constrained CSC pattern."""
+    cells = _i32(cells)
+    vpc = 3 if family == K.FFG_TRIANGLE_P1 else 4
+    nc = cells.size // vpc
+    if isinstance(boundary, str):
+        mode, mask = _BOUNDARY[boundary], None
+    else:
+        mode, mask = K.FFG_BOUNDARY_MASK, np.ascontiguousarray(boundary, dtype=np.uint8)
+    nd, nf, nz = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+    st = C.c_int(0)
+    lib = K.load()
+    lib.ffg_build_topology(int(family), int(degree), int(n_vertices), nc, _ptr(cells), mode,
+                           _ptr(mask), C.c_int64(0), C.c_int64(0), C.byref(nd), C.byref(nf),
+                           C.byref(nz), None, None, None, None, C.byref(st))
+    if st.value not in (0, K.FFG_CAPACITY):
+        raise FortfemError(st.value, "ffg_build_topology")
+    if family == K.FFG_TRIANGLE_P1:
+        nb = 3
+    elif family == K.FFG_TETRA_LAGRANGE:
+        nb = (degree + 1) * (degree + 2) * (degree + 3) // 6
+    else:
+        nb = degree * (degree + 2) * (degree + 3) // 2
+    gd = np.zeros((nc, nb), np.int32)
+    con = np.zeros(nd.value, np.uint8)
+    cp = np.zeros(nf.value + 1, np.int64)
+    ri = np.zeros(nz.value, np.int32)
+    lib.ffg_build_topology(int(family), int(degree), int(n_vertices), nc, _ptr(cells), mode,
+                           _ptr(mask), C.c_int64(nd.value), C.c_int64(nz.value), C.byref(nd),
+                           C.byref(nf), C.byref(nz), _ptr(gd), _ptr(con), _ptr(cp), _ptr(ri),
+                           C.byref(st))
+    if st.value:
+        raise FortfemError(st.value, "ffg_build_topology")
+    return dict(global_dofs=gd, constrained=con.astype(bool), n_dofs=nd.value, n_free=nf.value,
+                col_ptr=cp, row_idx=ri)
+
+
+_BOUNDARY = {"none": K.FFG_BOUNDARY_NONE, "all": K.FFG_BOUNDARY_ALL}
+
+
+# ------------------------------------------------- device-resident problems
+
+class Problem:
+    """A mesh + element family whose topology, CSC pattern and slot maps live
+    in HBM (ffg_problem_create).  ``solve`` assembles and solves the
+    constrained system for new geometry, coefficients and sources."""
+
+    def __init__(self, family: int, degree: int, cells, n_vertices: int,
+                 rule: int = K.FFG_RULE_DUFFY, quadrature_degree: int = 0,
+                 boundary: Union[str, np.ndarray] = "all"):
+        self.family = family
+        self.degree = degree
+        self.cells = _i32(cells)
+        self.n_vertices = int(n_vertices)
+        self.dim = 2 if family == K.FFG_TRIANGLE_P1 else 3
+        vpc = 3 if family == K.FFG_TRIANGLE_P1 else 4
+        n_cells = self.cells.size // vpc
+        self.n_cells = n_cells
+        if isinstance(boundary, str):
+            mode, mask = _BOUNDARY[boundary], None
+        else:
+            mode, mask = K.FFG_BOUNDARY_MASK, np.ascontiguousarray(boundary, dtype=np.uint8)
+        h = C.c_int(0)
+        nd, nf, nz = C.c_int64(0), C.c_int64(0), C.c_int64(0)
+        spc = C.c_int(0)
+        st = C.c_int(0)
+        K.load().ffg_problem_create(int(family), int(degree), self.n_vertices, n_cells,
+                                    _ptr(self.cells), int(rule), int(quadrature_degree), mode,
+                                    _ptr(mask), C.byref(h), C.byref(nd), C.byref(nf), C.byref(nz),
+                                    C.byref(spc), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_create")
+        self.handle = h.value
+        self.n_dofs = nd.value
+        self.n_free = nf.value
+        self.nnz = nz.value
+        self.samples_per_cell = spc.value
+        self.sample_width = 3 if family == K.FFG_TETRA_NEDELEC else 1
+
+    def close(self):
+        if getattr(self, "handle", 0):
+            st = C.c_int(0)
+            K.load().ffg_problem_free(self.handle, C.byref(st))
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def sample_points(self, vertices) -> np.ndarray:
+        v = _f64(vertices)
+        out = np.zeros((self.n_cells, self.samples_per_cell, 3))
+        st = C.c_int(0)
+        K.load().ffg_problem_sample_points(self.handle, _ptr(v), _ptr(out), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_sample_points")
+        return out
+
+    def dof_points(self, vertices) -> np.ndarray:
+        v = _f64(vertices)
+        out = np.zeros((self.n_dofs, 3))
+        st = C.c_int(0)
+        K.load().ffg_problem_dof_points(self.handle, _ptr(v), _ptr(out), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_dof_points")
+        return out
+
+    def constrained(self) -> np.ndarray:
+        out = np.zeros(self.n_dofs, np.uint8)
+        st = C.c_int(0)
+        K.load().ffg_problem_constrained(self.handle, _ptr(out), C.byref(st))
+        return out.astype(bool)
+
+    def _inputs(self, vertices, cell_a, cell_b, samples, g):
+        v = _f64(vertices)
+        if v.size != self.n_vertices * self.dim:
+            raise FortfemError(K.FFG_INVALID_INPUT, "vertices")
+        ca = _opt(cell_a, self.n_cells)
+        cb = _opt(cell_b, self.n_cells)
+        s = _opt(samples, self.n_cells * self.samples_per_cell * self.sample_width)
+        gg = _opt(g, self.n_dofs)
+        return v, ca, cb, s, gg
+
+    def solve(self, vertices, coef_a=1.0, coef_b=0.0, cell_a=None, cell_b=None, samples=None,
+              constrained_values=None, options: Optional[SolverOptions] = None):
+        """Assemble + constrain + solve with host arrays; returns (solution, SolverStats)."""
+        v, ca, cb, s, g = self._inputs(vertices, cell_a, cell_b, samples, constrained_values)
+        opts = options or SolverOptions(precision="mixed", tolerance=1e-10, preconditioner="jacobi",
+                                        max_iterations=1000000)
+        oc = opts.to_c()
+        sc = K.SolverStatsC()
+        sol = np.zeros(self.n_dofs)
+        st = C.c_int(0)
+        K.load().ffg_problem_solve(self.handle, _ptr(v), float(coef_a), float(coef_b), _ptr(ca),
+                                   _ptr(cb), _ptr(s), _ptr(g), C.byref(oc), _ptr(sol), C.byref(sc),
+                                   0, None, C.byref(st))
+        if st.value not in (0, K.FFG_NOT_CONVERGED):
+            raise FortfemError(st.value, "ffg_problem_solve")
+        return sol, SolverStats.from_c(sc)
+
+    def solve_device(self, vertices, solution, coef_a=1.0, coef_b=0.0, cell_a=None, cell_b=None,
+                     samples=None, constrained_values=None, options: Optional[SolverOptions] = None,
+                     stream=None) -> SolverStats:
+        """Same as solve with CUDA tensors (torch) resident in HBM; writes `solution`."""
+        def p(t):
+            return None if t is None else C.c_void_p(t.data_ptr())
+        opts = options or SolverOptions(precision="mixed", tolerance=1e-10, preconditioner="jacobi",
+                                        max_iterations=1000000)
+        oc = opts.to_c()
+        sc = K.SolverStatsC()
+        st = C.c_int(0)
+        s = None if stream is None else C.c_void_p(int(stream.cuda_stream))
+        K.load().ffg_problem_solve(self.handle, p(vertices), float(coef_a), float(coef_b), p(cell_a),
+                                   p(cell_b), p(samples), p(constrained_values), C.byref(oc),
+                                   p(solution), C.byref(sc), 1, s, C.byref(st))
+        if st.value not in (0, K.FFG_NOT_CONVERGED):
+            raise FortfemError(st.value, "ffg_problem_solve")
+        return SolverStats.from_c(sc)
+
+    def reduced_system(self, vertices, coef_a=1.0, coef_b=0.0, cell_a=None, cell_b=None,
+                       samples=None, constrained_values=None):
+        """The constrained (free x free) CSC, its lifted right-hand side and the free DoFs."""
+        v, ca, cb, s, g = self._inputs(vertices, cell_a, cell_b, samples, constrained_values)
+        cp = np.zeros(self.n_free + 1, np.int64)
+        ri = np.zeros(self.nnz, np.int32)
+        val = np.zeros(self.nnz)
+        rhs = np.zeros(self.n_free)
+        free = np.zeros(self.n_free, np.int32)
+        nz = C.c_int64(0)
+        st = C.c_int(0)
+        K.load().ffg_problem_reduced_system(self.handle, _ptr(v), float(coef_a), float(coef_b),
+                                            _ptr(ca), _ptr(cb), _ptr(s), _ptr(g),
+                                            C.c_int64(self.nnz), C.byref(nz), _ptr(cp), _ptr(ri),
+                                            _ptr(val), _ptr(rhs), _ptr(free), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_reduced_system")
+        return CscMatrix(self.n_free, self.n_free, cp, ri, val), rhs, free
+
+
+def _samples(source, points, width):
+    if source is None:
+        return None
+    if callable(source):
+        vals = np.asarray(source(points[..., 0], points[..., 1], points[..., 2]), dtype=np.float64)
+        if width == 3:
+            vals = np.stack(np.broadcast_arrays(*vals), axis=-1) if vals.shape[-1] != 3 else vals
+        return vals
+    return np.asarray(source, dtype=np.float64)
+
+
+def solve_tetra_lagrange_diffusion_reaction(vertices, tetrahedra, degree, source,
+                                            stiffness_coefficient=1.0, mass_coefficient=0.0,
+                                            boundary_value=None, options=None,
+                                            quadrature_degree=None, rule=K.FFG_RULE_DUFFY,
+                                            cell_stiffness=None, cell_mass=None):
+    """solve_tetra_lagrange_diffusion_reaction
+    (src/solvers/fortfem_tetra_lagrange_solver_3d.f90:64-129) with the sparse
+    direct solve replaced by the GPU Jacobi-PCG.  source / boundary_value are
+    vectorised callables f(x, y, z) or arrays of samples / DoF values.
+    Returns (solution, Status, SolverStats)."""
+    v = _f64(vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    q = 2 * degree + 4 if quadrature_degree is None else quadrature_degree
+    bmode = "all" if boundary_value is not None else "none"
+    with Problem(K.FFG_TETRA_LAGRANGE, degree, t, len(v), rule=rule, quadrature_degree=q,
+                 boundary=bmode) as p:
+        samples = _samples(source, p.sample_points(v), 1)
+        g = None
+        if boundary_value is not None:
+            if callable(boundary_value):
+                pts = p.dof_points(v)
+                g = np.where(p.constrained(), boundary_value(pts[:, 0], pts[:, 1], pts[:, 2]), 0.0)
+            else:
+                g = _f64(boundary_value)
+        sol, stats = p.solve(v, stiffness_coefficient, mass_coefficient, cell_stiffness, cell_mass,
+                             samples, g, options)
+        return sol, Status.of(0 if stats.converged else K.FFG_NOT_CONVERGED,
+                              "Tetrahedral H1 diffusion-reaction solve failed"), stats
+
+
+def solve_tetra_lagrange_poisson(vertices, tetrahedra, degree, source, boundary_value, options=None,
+                                 **kw):
+    """solve_tetra_lagrange_poisson (fortfem_tetra_lagrange_solver_3d.f90:50-62)."""
+    return solve_tetra_lagrange_diffusion_reaction(vertices, tetrahedra, degree, source, 1.0, 0.0,
+                                                   boundary_value, options, **kw)
+
+
+def solve_tetra_nedelec_curl_mass(vertices, tetrahedra, order, source, curl_coefficient,
+                                  mass_coefficient, zero_tangential_boundary=False, options=None,
+                                  cell_curl=None, cell_mass=None):
+    """solve_tetra_nedelec_curl_mass (src/solvers/fortfem_tetra_nedelec_solver_3d.f90:361-414),
+    sparse direct solve replaced by the GPU Jacobi-PCG.  Returns (solution, Status, SolverStats)."""
+    v = _f64(vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    with Problem(K.FFG_TETRA_NEDELEC, order, t, len(v),
+                 boundary="all" if zero_tangential_boundary else "none") as p:
+        samples = _samples(source, p.sample_points(v), 3)
+        sol, stats = p.solve(v, curl_coefficient, mass_coefficient, cell_curl, cell_mass, samples,
+                             None, options)
+        return sol, Status.of(0 if stats.converged else K.FFG_NOT_CONVERGED,
+                              "Tetrahedral Nedelec curl-mass solve failed"), stats
+
+
+def solve_scalar_p1(vertices, triangles, load=1.0, stiffness_coefficient=1.0, mass_coefficient=0.0,
+                    boundary_value=0.0, options=None, cell_stiffness=None):
+    """The compiled P1 problem of solve(a == L, uh, bc)
+    (src/solvers/fortfem_solvers_laplacian.f90:59-112): P1 stiffness (+ mass),
+    load `load`*area/3, Dirichlet value on all boundary vertices.  The
+    boundary rows are eliminated as the reference does; the free block is
+    solved on the GPU.  Returns (values, SolverStats)."""
+    v = _f64(vertices).reshape(-1, 2)
+    t = _i32(triangles).reshape(-1, 3)
+    with Problem(K.FFG_TRIANGLE_P1, 1, t, len(v), boundary="all") as p:
+        samples = np.full(len(t), float(load)) if np.isscalar(load) else _f64(load)
+        g = np.where(p.constrained(), float(boundary_value), 0.0)
+        return p.solve(v, stiffness_coefficient, mass_coefficient, cell_stiffness, None, samples, g,
+                       options)

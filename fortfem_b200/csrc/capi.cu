@@ -1,0 +1,809 @@
+// C-ABI entry points of libfortfem_gpu.so (declared in include/fortfem_gpu.h).
+//
+// Handles follow the reference's registry convention (positive process-local
+// integers, src/bindings/fortfem_capi_solver.f90:10-13,108-124) but the
+// registry here is mutex-protected.  No entry point aborts: every failure is
+// reported through *status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "ffg_internal.h"
+
+namespace ffg {
+namespace {
+
+template <class T>
+int dalloc(T **p, size_t count) {
+  if (count == 0) count = 1;
+  if (cudaMalloc((void **)p, count * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return FFG_OUT_OF_MEMORY;
+  }
+  return FFG_OK;
+}
+
+template <class T>
+int upload(T **p, const std::vector<T> &h) {
+  int st = dalloc(p, h.size());
+  if (st) return st;
+  if (!h.empty() && cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  return FFG_OK;
+}
+
+// One device-resident problem: topology, tables, pattern, work buffers.
+struct Problem {
+  Topology topo;
+  ElementTables tab;
+  DeviceTopology dt;
+  DeviceCsr A;
+  SolveWork work;
+  int rule = 0, qdeg = 0, dim = 3;
+  int geo_stride = 0;
+  int samples_per_cell = 0;  // scalar samples per cell (x3 for Nedelec)
+  double *geo = nullptr, *cell_rhs = nullptr, *elem = nullptr;
+  double *rhs = nullptr, *x = nullptr, *full = nullptr;
+  double *in_vertices = nullptr, *in_cell_a = nullptr, *in_cell_b = nullptr, *in_samples = nullptr,
+         *in_g = nullptr;
+  int *free_dofs = nullptr;
+  int *err = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  ~Problem() {
+    void *ptrs[] = {dt.cells, dt.gd, dt.edge_sign, dt.face_perm, dt.free_index, dt.inc_ptr,
+                    dt.inc_cell, dt.inc_local, dt.slot, dt.ref, dt.load_basis, dt.face_blocks,
+                    A.row_ptr, A.col, A.val64, A.val32, A.dinv64, A.dinv32, A.tile_row, geo,
+                    cell_rhs, elem, rhs, x, full, in_vertices, in_cell_a, in_cell_b, in_samples,
+                    in_g, free_dofs, err};
+    for (void *p : ptrs)
+      if (p) cudaFree(p);
+    solve_work_free(work);
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+std::mutex g_mutex;
+std::map<int, std::shared_ptr<Problem>> g_problems;
+int g_next_handle = 1;
+
+std::shared_ptr<Problem> find_problem(int h) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  auto it = g_problems.find(h);
+  return it == g_problems.end() ? nullptr : it->second;
+}
+
+int device_ready() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return FFG_NO_DEVICE;
+  }
+  return FFG_OK;
+}
+
+void report(int verbosity, const std::string &msg) {
+  if (verbosity > 0 && !msg.empty()) std::fprintf(stderr, "fortfem_gpu: %s\n", msg.c_str());
+}
+
+int create_problem(int family, int degree, int n_vertices, int n_cells, const int *cells, int rule,
+                   int qdeg, int boundary_mode, const uint8_t *mask, std::shared_ptr<Problem> &out,
+                   std::string &msg) {
+  int st = device_ready();
+  if (st) return st;
+  auto P = std::make_shared<Problem>();
+  Topology &t = P->topo;
+  t.family = family;
+  t.degree = degree;
+  t.vpc = (family == FFG_TRIANGLE_P1) ? 3 : 4;
+  P->dim = (family == FFG_TRIANGLE_P1) ? 2 : 3;
+  t.n_cells = n_cells;
+  t.n_vertices = n_vertices;
+  if (n_cells < 1 || n_vertices < 1 || !cells) { msg = "empty mesh"; return FFG_INVALID_INPUT; }
+  t.cells.assign(cells, cells + (size_t)t.vpc * n_cells);
+  if ((st = build_dofs(t, msg))) return st;
+  if ((st = build_constraints(t, boundary_mode, mask, msg))) return st;
+  if ((st = build_pattern(t, msg))) return st;
+  P->rule = rule;
+  P->qdeg = qdeg;
+  if ((st = build_tables(t, rule, qdeg, P->tab, msg))) return st;
+  P->geo_stride = geo_stride_for(t, P->tab);
+  P->samples_per_cell = P->tab.nq_load;
+  // device topology
+  DeviceTopology &dt = P->dt;
+  if ((st = upload(&dt.cells, t.cells))) return st;
+  if ((st = upload(&dt.gd, t.gd))) return st;
+  if (family == FFG_TETRA_NEDELEC) {
+    if ((st = upload(&dt.edge_sign, t.edge_sign))) return st;
+    if ((st = upload(&dt.face_perm, t.face_perm))) return st;
+    if (!P->tab.face_blocks.empty() && (st = upload(&dt.face_blocks, P->tab.face_blocks))) return st;
+  }
+  if ((st = upload(&dt.free_index, t.free_index))) return st;
+  if ((st = upload(&dt.inc_ptr, t.inc_ptr))) return st;
+  if ((st = upload(&dt.inc_cell, t.inc_cell))) return st;
+  if ((st = upload(&dt.inc_local, t.inc_local))) return st;
+  if ((st = upload(&dt.slot, t.slot))) return st;
+  if (!P->tab.ref.empty() && (st = upload(&dt.ref, P->tab.ref))) return st;
+  if (!P->tab.load_basis.empty() && (st = upload(&dt.load_basis, P->tab.load_basis))) return st;
+  // matrix
+  DeviceCsr &A = P->A;
+  A.n = t.n_free();
+  A.nnz = t.nnz();
+  if ((st = upload(&A.row_ptr, t.col_ptr))) return st;
+  if ((st = upload(&A.col, t.row_idx))) return st;
+  if ((st = dalloc(&A.val64, (size_t)A.nnz))) return st;
+  if ((st = dalloc(&A.val32, (size_t)A.nnz))) return st;
+  if ((st = dalloc(&A.dinv64, (size_t)A.n))) return st;
+  if ((st = dalloc(&A.dinv32, (size_t)A.n))) return st;
+  int max_row = 0;
+  std::vector<int> tiles = make_tiles(t.col_ptr, tile_capacity(), &max_row);
+  if (max_row > tile_capacity()) { msg = "matrix row longer than an SpMV tile"; return FFG_INVALID_INPUT; }
+  A.n_tiles = (int)tiles.size() - 1;
+  if ((st = upload(&A.tile_row, tiles))) return st;
+  // per-step buffers
+  const size_t nc = (size_t)n_cells;
+  if ((st = dalloc(&P->geo, nc * std::max(P->geo_stride, 1)))) return st;
+  if (family == FFG_TETRA_NEDELEC) {
+    if ((st = dalloc(&P->cell_rhs, nc * t.nb))) return st;
+    if ((st = dalloc(&P->elem, nc * t.nb * t.nb))) return st;
+  }
+  if ((st = dalloc(&P->rhs, (size_t)A.n))) return st;
+  if ((st = dalloc(&P->x, (size_t)A.n))) return st;
+  if ((st = dalloc(&P->full, (size_t)t.n_dofs))) return st;
+  if ((st = dalloc(&P->in_vertices, (size_t)n_vertices * P->dim))) return st;
+  if ((st = dalloc(&P->in_cell_a, nc))) return st;
+  if ((st = dalloc(&P->in_cell_b, nc))) return st;
+  const int spc = P->samples_per_cell * (family == FFG_TETRA_NEDELEC ? 3 : 1);
+  if ((st = dalloc(&P->in_samples, nc * spc))) return st;
+  if ((st = dalloc(&P->in_g, (size_t)t.n_dofs))) return st;
+  if ((st = upload(&P->free_dofs, t.free_dofs))) return st;
+  if ((st = dalloc(&P->err, 4))) return st;
+  int grid = 0;
+  if ((st = pcg_grid_size(&grid))) return st;
+  if ((st = solve_work_alloc(P->work, A.n, grid))) return st;
+  for (auto &e : P->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return FFG_CUDA_ERROR;
+  out = P;
+  return FFG_OK;
+}
+
+__global__ void scatter_solution_kernel(int64_t n_free, const int *free_dofs, const double *x,
+                                        double *full) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_free) full[free_dofs[i]] = x[i];
+}
+
+// Stage inputs (host or device) and assemble the constrained system into P.A / P.rhs.
+int assemble(Problem &P, const double *vertices, double ca, double cb, const double *cell_a,
+             const double *cell_b, const double *samples, const double *g, int memory,
+             cudaStream_t s, std::string &msg) {
+  const Topology &t = P.topo;
+  AssemblyInputs in;
+  in.coef_a = ca;
+  in.coef_b = cb;
+  const size_t nc = (size_t)t.n_cells;
+  const int spc = P.samples_per_cell * (t.family == FFG_TETRA_NEDELEC ? 3 : 1);
+  if (!vertices) { msg = "vertices missing"; return FFG_INVALID_INPUT; }
+  if (memory == 0) {
+    auto h2d = [&](double *dst, const double *src, size_t count) -> const double * {
+      if (!src) return nullptr;
+      cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyHostToDevice, s);
+      return dst;
+    };
+    in.vertices = h2d(P.in_vertices, vertices, (size_t)t.n_vertices * P.dim);
+    in.cell_a = h2d(P.in_cell_a, cell_a, nc);
+    in.cell_b = h2d(P.in_cell_b, cell_b, nc);
+    in.samples = h2d(P.in_samples, samples, nc * spc);
+    in.g = h2d(P.in_g, g, (size_t)t.n_dofs);
+  } else {
+    in.vertices = vertices;
+    in.cell_a = cell_a;
+    in.cell_b = cell_b;
+    in.samples = samples;
+    in.g = g;
+  }
+  if (cudaMemsetAsync(P.err, 0, sizeof(int), s) != cudaSuccess) return FFG_CUDA_ERROR;
+  int st;
+  if (t.family == FFG_TETRA_NEDELEC) {
+    st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s);
+  } else {
+    st = launch_cell_geometry(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.err, s);
+  }
+  if (st) return st;
+  st = launch_columns(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.elem, P.A, P.rhs,
+                      P.err, s);
+  if (st) return st;
+  int herr = 0;
+  if (cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return FFG_CUDA_ERROR;
+  if (herr) { msg = "degenerate cell (det <= 64 eps max(1,|J|)^3)"; return herr; }
+  return FFG_OK;
+}
+
+void fill_default(ffg_solver_options &o) {
+  o.version = FFG_OPTIONS_VERSION;
+  o.preconditioner = 1;
+  o.precision = FFG_PRECISION_MIXED;
+  o.tolerance_type = 0;
+  o.tolerance = 1.0e-10;
+  o.max_iterations = 1000000;
+  o.max_refinements = 30;
+  o.inner_tolerance = 1.0e-5;
+  o.verbosity = 0;
+  o.timeout_seconds = 60.0;
+  o.breakdown_guard = 0;
+}
+
+int check_options(const ffg_solver_options *o, ffg_solver_options &out) {
+  fill_default(out);
+  if (!o) return FFG_OK;
+  if (o->version != FFG_OPTIONS_VERSION) return FFG_INVALID_INPUT;
+  out = *o;
+  if (out.precision != FFG_PRECISION_FP64 && out.precision != FFG_PRECISION_MIXED)
+    return FFG_INVALID_INPUT;
+  if (out.tolerance < 0 || out.max_iterations < 0) return FFG_INVALID_INPUT;
+  if (out.inner_tolerance <= 0 || out.inner_tolerance >= 1) out.inner_tolerance = 1e-5;
+  if (out.max_refinements < 0) out.max_refinements = 0;
+  return FFG_OK;
+}
+
+__global__ void set_ones_kernel(int64_t n, double *d64, float *d32) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) { d64[i] = 1.0; d32[i] = 1.0f; }
+}
+
+struct HostCsr {
+  std::vector<int64_t> rp;
+  std::vector<int> col;
+  std::vector<double> val;
+};
+// CSC -> CSR (rows ascending within each row by construction of the counting sort)
+bool csc_to_csr(int n, const int64_t *cp, const int *ri, const double *v, HostCsr &out) {
+  const int64_t nnz = cp[n];
+  out.rp.assign((size_t)n + 1, 0);
+  for (int64_t k = 0; k < nnz; ++k) {
+    if (ri[k] < 0 || ri[k] >= n) return false;
+    out.rp[ri[k] + 1]++;
+  }
+  for (int i = 0; i < n; ++i) out.rp[i + 1] += out.rp[i];
+  out.col.assign((size_t)nnz, 0);
+  out.val.assign((size_t)nnz, 0.0);
+  std::vector<int64_t> pos(out.rp.begin(), out.rp.end() - 1);
+  for (int c = 0; c < n; ++c) {
+    if (cp[c + 1] < cp[c]) return false;
+    for (int64_t k = cp[c]; k < cp[c + 1]; ++k) {
+      const int64_t p = pos[ri[k]]++;
+      out.col[p] = c;
+      out.val[p] = v[k];
+    }
+  }
+  return true;
+}
+
+struct Uploaded {
+  DeviceCsr A;
+  ~Uploaded() {
+    void *ptrs[] = {A.row_ptr, A.col, A.val64, A.val32, A.dinv64, A.dinv32, A.tile_row};
+    for (void *p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+__global__ void prepare_kernel(int64_t n, const int64_t *rp, const int *col, const double *v64,
+                               float *v32, double *d64, float *d32, int jacobi) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double d = 0.0;
+  for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+    v32[k] = (float)v64[k];
+    if (col[k] == (int)i) d = v64[k];
+  }
+  // build_sparse_preconditioner("jacobi"), advanced_solvers.f90:1139-1154
+  const double di = (jacobi && fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
+  d64[i] = di;
+  d32[i] = (float)di;
+}
+
+int upload_csr(int n, const HostCsr &h, Uploaded &U, bool jacobi) {
+  DeviceCsr &A = U.A;
+  A.n = n;
+  A.nnz = (int64_t)h.col.size();
+  int st;
+  if ((st = upload(&A.row_ptr, h.rp))) return st;
+  if ((st = upload(&A.col, h.col))) return st;
+  if ((st = upload(&A.val64, h.val))) return st;
+  if ((st = dalloc(&A.val32, h.val.size()))) return st;
+  if ((st = dalloc(&A.dinv64, (size_t)n))) return st;
+  if ((st = dalloc(&A.dinv32, (size_t)n))) return st;
+  int max_row = 0;
+  std::vector<int> tiles = make_tiles(h.rp, tile_capacity(), &max_row);
+  if (max_row > tile_capacity()) return FFG_INVALID_INPUT;
+  A.n_tiles = (int)tiles.size() - 1;
+  if ((st = upload(&A.tile_row, tiles))) return st;
+  prepare_kernel<<<(unsigned)((n + 255) / 256), 256>>>(n, A.row_ptr, A.col, A.val64, A.val32,
+                                                       A.dinv64, A.dinv32, jacobi ? 1 : 0);
+  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+}  // namespace
+}  // namespace ffg
+
+using namespace ffg;
+
+extern "C" {
+
+void ffg_default_options(ffg_solver_options *opts) {
+  if (opts) fill_default(*opts);
+}
+
+void ffg_version(int *major, int *minor, int *patch) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  if (patch) *patch = 0;
+}
+
+void ffg_device_count(int *count, int *status) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) { cudaGetLastError(); n = 0; }
+  if (count) *count = n;
+  if (status) *status = (n > 0) ? FFG_OK : FFG_NO_DEVICE;
+}
+
+void ffg_structured_tetra_box_mesh(const double *bounds, const int *counts, double *vertices,
+                                   int *tets, int *status) {
+  *status = FFG_INVALID_INPUT;
+  if (!bounds || !counts || !vertices || !tets) return;
+  for (int d = 0; d < 3; ++d)
+    if (counts[d] < 1 || !(bounds[3 + d] > bounds[d])) return;
+  const int nx = counts[0], ny = counts[1], nz = counts[2];
+  auto vid = [&](int i, int j, int k) { return i + (nx + 1) * (j + (ny + 1) * k); };
+  for (int k = 0; k <= nz; ++k)
+    for (int j = 0; j <= ny; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        const int ijk[3] = {i, j, k};
+        const int v = vid(i, j, k);
+        for (int d = 0; d < 3; ++d)
+          vertices[3 * (size_t)v + d] =
+              bounds[d] + ((double)ijk[d] / (double)counts[d]) * (bounds[3 + d] - bounds[d]);
+      }
+  // Kuhn split of each brick into six tetrahedra sharing the main diagonal
+  // (add_brick_tetrahedra, structured_tetra_box_mesh.f90:78-94)
+  static const int split[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7},
+                                  {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+  size_t cell = 0;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const int brick[8] = {vid(i, j, k),         vid(i + 1, j, k),     vid(i, j + 1, k),
+                              vid(i + 1, j + 1, k), vid(i, j, k + 1),     vid(i + 1, j, k + 1),
+                              vid(i, j + 1, k + 1), vid(i + 1, j + 1, k + 1)};
+        for (int c = 0; c < 6; ++c, ++cell) {
+          int *t = tets + 4 * cell;
+          for (int n = 0; n < 4; ++n) t[n] = brick[split[c][n]];
+          // positive orientation: swap the last two vertices when det < 0 (:56-68)
+          double J[9];
+          for (int col = 0; col < 3; ++col)
+            for (int r = 0; r < 3; ++r)
+              J[r + 3 * col] = vertices[3 * (size_t)t[col + 1] + r] - vertices[3 * (size_t)t[0] + r];
+          const double det = J[0] * (J[4] * J[8] - J[7] * J[5]) - J[3] * (J[1] * J[8] - J[7] * J[2]) +
+                             J[6] * (J[1] * J[5] - J[4] * J[2]);
+          if (det < 0.0) std::swap(t[2], t[3]);
+        }
+      }
+  *status = FFG_OK;
+}
+
+void ffg_unit_square_mesh(int n, double *vertices, int *tris, int *status) {
+  *status = FFG_INVALID_INPUT;
+  if (n < 2 || !vertices || !tris) return;
+  const double dx = 1.0 / (double)(n - 1);
+  size_t k = 0;
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i, ++k) {
+      vertices[2 * k] = i * dx;
+      vertices[2 * k + 1] = j * dx;
+    }
+  k = 0;
+  for (int j = 0; j < n - 1; ++j)
+    for (int i = 0; i < n - 1; ++i) {
+      const int v1 = j * n + i, v2 = j * n + i + 1, v3 = (j + 1) * n + i + 1, v4 = (j + 1) * n + i;
+      int *t = tris + 3 * k;
+      t[0] = v1; t[1] = v2; t[2] = v3;
+      t[3] = v1; t[4] = v3; t[5] = v4;
+      k += 2;
+    }
+  *status = FFG_OK;
+}
+
+void ffg_build_topology(int family, int degree, int n_vertices, int n_cells, const int *cells,
+                        int boundary_mode, const uint8_t *mask, int64_t dof_cap, int64_t nnz_cap,
+                        int64_t *n_dofs, int64_t *n_free, int64_t *nnz, int *global_dofs,
+                        uint8_t *constrained, int64_t *col_ptr, int *row_ind, int *status) {
+  Topology t;
+  t.family = family;
+  t.degree = degree;
+  t.vpc = (family == FFG_TRIANGLE_P1) ? 3 : 4;
+  t.n_cells = n_cells;
+  t.n_vertices = n_vertices;
+  std::string msg;
+  if (n_cells < 1 || n_vertices < 1 || !cells) { *status = FFG_INVALID_INPUT; return; }
+  t.cells.assign(cells, cells + (size_t)t.vpc * n_cells);
+  int st;
+  if ((st = build_dofs(t, msg)) || (st = build_constraints(t, boundary_mode, mask, msg)) ||
+      (st = build_pattern(t, msg))) {
+    *status = st;
+    return;
+  }
+  if (n_dofs) *n_dofs = t.n_dofs;
+  if (n_free) *n_free = t.n_free();
+  if (nnz) *nnz = t.nnz();
+  if (dof_cap < t.n_dofs || nnz_cap < t.nnz() || !global_dofs || !constrained || !col_ptr ||
+      !row_ind) {
+    *status = FFG_CAPACITY;
+    return;
+  }
+  std::memcpy(global_dofs, t.gd.data(), sizeof(int) * t.gd.size());
+  std::memcpy(constrained, t.constrained.data(), t.constrained.size());
+  std::memcpy(col_ptr, t.col_ptr.data(), sizeof(int64_t) * t.col_ptr.size());
+  std::memcpy(row_ind, t.row_idx.data(), sizeof(int) * t.row_idx.size());
+  *status = FFG_OK;
+}
+
+void ffg_problem_create(int family, int degree, int n_vertices, int n_cells, const int *cells,
+                        int rule, int qdeg, int boundary_mode, const uint8_t *mask, int *handle,
+                        int64_t *n_dofs, int64_t *n_free, int64_t *nnz, int *samples_per_cell,
+                        int *status) {
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  int st = create_problem(family, degree, n_vertices, n_cells, cells, rule, qdeg, boundary_mode,
+                          mask, P, msg);
+  if (st) {
+    if (handle) *handle = 0;
+    *status = st;
+    return;
+  }
+  {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    const int h = g_next_handle++;
+    g_problems[h] = P;
+    if (handle) *handle = h;
+  }
+  if (n_dofs) *n_dofs = P->topo.n_dofs;
+  if (n_free) *n_free = P->topo.n_free();
+  if (nnz) *nnz = P->topo.nnz();
+  if (samples_per_cell) *samples_per_cell = P->samples_per_cell;
+  *status = FFG_OK;
+}
+
+void ffg_problem_free(int handle, int *status) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  auto it = g_problems.find(handle);
+  if (it == g_problems.end()) { *status = FFG_BAD_HANDLE; return; }
+  g_problems.erase(it);
+  *status = FFG_OK;
+}
+
+void ffg_problem_constrained(int handle, uint8_t *mask, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  std::memcpy(mask, P->topo.constrained.data(), P->topo.constrained.size());
+  *status = FFG_OK;
+}
+
+void ffg_problem_sample_points(int handle, const double *vertices, double *points, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const Topology &t = P->topo;
+  const ElementTables &tab = P->tab;
+  for (int c = 0; c < t.n_cells; ++c) {
+    const int *v = t.cells.data() + (size_t)t.vpc * c;
+    if (t.family == FFG_TRIANGLE_P1) {
+      // one sample per triangle, at its centroid
+      double x = 0, y = 0;
+      for (int i = 0; i < 3; ++i) { x += vertices[2 * (size_t)v[i]]; y += vertices[2 * (size_t)v[i] + 1]; }
+      points[3 * (size_t)c] = x / 3.0;
+      points[3 * (size_t)c + 1] = y / 3.0;
+      points[3 * (size_t)c + 2] = 0.0;
+      continue;
+    }
+    const double *p0 = vertices + 3 * (size_t)v[0];
+    for (int q = 0; q < tab.nq_load; ++q) {
+      const double *xi = &tab.load_xi[3 * q];
+      for (int r = 0; r < 3; ++r) {
+        double s = p0[r];
+        for (int k = 0; k < 3; ++k) s = s + (vertices[3 * (size_t)v[k + 1] + r] - p0[r]) * xi[k];
+        points[3 * ((size_t)tab.nq_load * c + q) + r] = s;
+      }
+    }
+  }
+  *status = FFG_OK;
+}
+
+void ffg_problem_dof_points(int handle, const double *vertices, double *points, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const Topology &t = P->topo;
+  if (t.family == FFG_TETRA_NEDELEC) { *status = FFG_INVALID_INPUT; return; }
+  if (t.family == FFG_TRIANGLE_P1) {
+    for (int i = 0; i < t.n_vertices; ++i) {
+      points[3 * (size_t)i] = vertices[2 * (size_t)i];
+      points[3 * (size_t)i + 1] = vertices[2 * (size_t)i + 1];
+      points[3 * (size_t)i + 2] = 0.0;
+    }
+    *status = FFG_OK;
+    return;
+  }
+  std::vector<int> idx;
+  std::vector<double> nodes;
+  lagrange_indices(t.degree, idx, nodes);
+  for (int c = 0; c < t.n_cells; ++c) {
+    const int *v = t.cells.data() + 4 * (size_t)c;
+    const double *p0 = vertices + 3 * (size_t)v[0];
+    for (int l = 0; l < t.nb; ++l) {
+      const int g = t.gd[(size_t)t.nb * c + l];
+      for (int r = 0; r < 3; ++r) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s += (vertices[3 * (size_t)v[k + 1] + r] - p0[r]) * nodes[3 * l + k];
+        points[3 * (size_t)g + r] = p0[r] + s;
+      }
+    }
+  }
+  *status = FFG_OK;
+}
+
+void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
+                       const double *cell_a, const double *cell_b, const double *samples,
+                       const double *g, const ffg_solver_options *opts, double *solution,
+                       ffg_solver_stats *stats, int memory, void *stream, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  ffg_solver_options o;
+  if (check_options(opts, o)) { *status = FFG_INVALID_INPUT; return; }
+  if (!solution || (memory != 0 && memory != 1)) { *status = FFG_INVALID_INPUT; return; }
+  cudaStream_t s = (cudaStream_t)stream;
+  std::string msg;
+  ffg_solver_stats local;
+  std::memset(&local, 0, sizeof(local));
+  cudaEventRecord(P->ev[0], s);
+  int st = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, memory, s, msg);
+  if (st) { report(o.verbosity, msg); *status = st; if (stats) { local.status = st; *stats = local; } return; }
+  cudaEventRecord(P->ev[1], s);
+  const Topology &t = P->topo;
+  if (!o.preconditioner) {
+    set_ones_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(t.n_free(), P->A.dinv64,
+                                                                        P->A.dinv32);
+  }
+  cudaMemsetAsync(P->x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
+  if (t.n_free() > 0) {
+    st = pcg_solve(P->A, P->rhs, P->x, o, P->work, &local, s, msg);
+    if (st) { report(o.verbosity, msg); *status = st; if (stats) { local.status = st; *stats = local; } return; }
+  } else {
+    local.converged = 1;
+  }
+  cudaEventRecord(P->ev[2], s);
+  // full solution: constrained values (or zero) then the free DoFs
+  const double *gdev = (memory == 0) ? (g ? P->in_g : nullptr) : g;
+  if (gdev)
+    cudaMemcpyAsync(P->full, gdev, sizeof(double) * (size_t)t.n_dofs, cudaMemcpyDeviceToDevice, s);
+  else
+    cudaMemsetAsync(P->full, 0, sizeof(double) * (size_t)t.n_dofs, s);
+  if (t.n_free() > 0)
+    scatter_solution_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(
+        t.n_free(), P->free_dofs, P->x, P->full);
+  cudaMemcpyAsync(solution, P->full, sizeof(double) * (size_t)t.n_dofs,
+                  memory == 0 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
+  cudaEventRecord(P->ev[3], s);
+  if (cudaEventSynchronize(P->ev[3]) != cudaSuccess) { *status = FFG_CUDA_ERROR; return; }
+  float ta = 0, ts = 0;
+  cudaEventElapsedTime(&ta, P->ev[0], P->ev[1]);
+  cudaEventElapsedTime(&ts, P->ev[1], P->ev[2]);
+  local.assembly_seconds = ta * 1e-3;
+  local.solve_seconds = ts * 1e-3;
+  if (o.verbosity > 0)
+    std::fprintf(stderr,
+                 "fortfem_gpu: n_free=%lld nnz=%lld it=%d ref=%d converged=%d rel=%.3e "
+                 "assembly=%.3f ms solve=%.3f ms\n",
+                 (long long)t.n_free(), (long long)t.nnz(), local.iterations, local.refinements,
+                 local.converged, local.true_relative_residual, ta, ts);
+  if (stats) *stats = local;
+  *status = local.status == FFG_NOT_CONVERGED ? FFG_NOT_CONVERGED : local.status;
+  if (local.converged) *status = FFG_OK;
+}
+
+void ffg_problem_reduced_system(int handle, const double *vertices, double ca, double cb,
+                                const double *cell_a, const double *cell_b,
+                                const double *samples, const double *g, int64_t cap,
+                                int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values,
+                                double *rhs, int *free_dofs, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const Topology &t = P->topo;
+  if (nnz) *nnz = t.nnz();
+  if (cap < t.nnz() || !col_ptr || !row_ind || !values) { *status = FFG_CAPACITY; return; }
+  std::string msg;
+  int st = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, 0, 0, msg);
+  if (st) { *status = st; return; }
+  std::memcpy(col_ptr, t.col_ptr.data(), sizeof(int64_t) * t.col_ptr.size());
+  std::memcpy(row_ind, t.row_idx.data(), sizeof(int) * t.row_idx.size());
+  if (cudaMemcpy(values, P->A.val64, sizeof(double) * (size_t)t.nnz(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  if (rhs && cudaMemcpy(rhs, P->rhs, sizeof(double) * (size_t)t.n_free(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  if (free_dofs) std::memcpy(free_dofs, t.free_dofs.data(), sizeof(int) * t.free_dofs.size());
+  *status = FFG_OK;
+}
+
+// ------------------------------------------------------------ drop-in assembly
+static void full_csc(int family, int degree, int nv, const double *verts, int nt, const int *cells,
+                     int rule, int qdeg, double ca, double cb, const double *cell_a,
+                     const double *cell_b, int64_t cap, int *n_dofs, int64_t *nnz,
+                     int64_t *col_ptr, int *row_ind, double *values, int *status) {
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  int st = create_problem(family, degree, nv, nt, cells, rule, qdeg, FFG_BOUNDARY_NONE, nullptr, P,
+                          msg);
+  if (st) { *status = st; return; }
+  if (n_dofs) *n_dofs = (int)P->topo.n_dofs;
+  if (nnz) *nnz = P->topo.nnz();
+  if (cap < P->topo.nnz() || !col_ptr || !row_ind || !values) { *status = FFG_CAPACITY; return; }
+  st = assemble(*P, verts, ca, cb, cell_a, cell_b, nullptr, nullptr, 0, 0, msg);
+  if (st) { *status = st; return; }
+  std::memcpy(col_ptr, P->topo.col_ptr.data(), sizeof(int64_t) * P->topo.col_ptr.size());
+  std::memcpy(row_ind, P->topo.row_idx.data(), sizeof(int) * P->topo.row_idx.size());
+  if (cudaMemcpy(values, P->A.val64, sizeof(double) * (size_t)P->topo.nnz(), cudaMemcpyDeviceToHost) !=
+      cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  *status = FFG_OK;
+}
+
+static void full_load(int family, int degree, int nv, const double *verts, int nt, const int *cells,
+                      int rule, int qdeg, const double *samples, int n_dofs, double *rhs,
+                      int *status) {
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  int st = create_problem(family, degree, nv, nt, cells, rule, qdeg, FFG_BOUNDARY_NONE, nullptr, P,
+                          msg);
+  if (st) { *status = st; return; }
+  if (n_dofs != P->topo.n_dofs || !rhs || !samples) { *status = FFG_INVALID_INPUT; return; }
+  st = assemble(*P, verts, 0.0, 0.0, nullptr, nullptr, samples, nullptr, 0, 0, msg);
+  if (st) { *status = st; return; }
+  if (cudaMemcpy(rhs, P->rhs, sizeof(double) * (size_t)n_dofs, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  *status = FFG_OK;
+}
+
+void ffg_assemble_tetra_lagrange_stiffness_csc(int nv, const double *verts, int nt, const int *tets,
+                                               int degree, int rule, int qdeg, double stiffness,
+                                               double mass, const double *cell_stiffness,
+                                               const double *cell_mass, int64_t cap, int *n_dofs,
+                                               int64_t *nnz, int64_t *col_ptr, int *row_ind,
+                                               double *values, int *status) {
+  full_csc(FFG_TETRA_LAGRANGE, degree, nv, verts, nt, tets, rule, qdeg, stiffness, mass,
+           cell_stiffness, cell_mass, cap, n_dofs, nnz, col_ptr, row_ind, values, status);
+}
+
+void ffg_assemble_tetra_lagrange_scalar_load_samples(int nv, const double *verts, int nt,
+                                                     const int *tets, int degree, int rule,
+                                                     int qdeg, const double *samples, int n_dofs,
+                                                     double *rhs, int *status) {
+  full_load(FFG_TETRA_LAGRANGE, degree, nv, verts, nt, tets, rule, qdeg, samples, n_dofs, rhs,
+            status);
+}
+
+void ffg_assemble_tetra_nedelec_curl_mass_csc(int nv, const double *verts, int nt, const int *tets,
+                                              int order, double curl, double mass,
+                                              const double *cell_curl, const double *cell_mass,
+                                              int64_t cap, int *n_dofs, int64_t *nnz,
+                                              int64_t *col_ptr, int *row_ind, double *values,
+                                              int *status) {
+  full_csc(FFG_TETRA_NEDELEC, order, nv, verts, nt, tets, 0, 0, curl, mass, cell_curl, cell_mass,
+           cap, n_dofs, nnz, col_ptr, row_ind, values, status);
+}
+
+void ffg_assemble_tetra_nedelec_vector_load_samples(int nv, const double *verts, int nt,
+                                                    const int *tets, int order,
+                                                    const double *samples, int n_dofs, double *rhs,
+                                                    int *status) {
+  full_load(FFG_TETRA_NEDELEC, order, nv, verts, nt, tets, 0, 0, samples, n_dofs, rhs, status);
+}
+
+void ffg_assemble_scalar_p1_csc(int nv, const double *verts, int nt, const int *tris, double mass,
+                                double stiffness, const double *cell_stiffness, int64_t cap,
+                                int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values,
+                                int *status) {
+  int nd = 0;
+  full_csc(FFG_TRIANGLE_P1, 1, nv, verts, nt, tris, 0, 0, stiffness, mass, cell_stiffness, nullptr,
+           cap, &nd, nnz, col_ptr, row_ind, values, status);
+}
+
+// ------------------------------------------------------------------- solve_sparse
+
+void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row_ind,
+                      const double *values, const double *b, double *x,
+                      const ffg_solver_options *opts, ffg_solver_stats *stats, int *status) {
+  ffg_solver_options o;
+  if (n < 1 || !col_ptr || !row_ind || !values || !b || !x || check_options(opts, o) ||
+      col_ptr[n] != nnz || col_ptr[0] != 0) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  int st = device_ready();
+  if (st) { *status = st; return; }
+  HostCsr h;
+  if (!csc_to_csr(n, col_ptr, row_ind, values, h)) { *status = FFG_INVALID_INPUT; return; }
+  Uploaded U;
+  if ((st = upload_csr(n, h, U, o.preconditioner != 0))) { *status = st; return; }
+  double *db = nullptr, *dx = nullptr;
+  if (dalloc(&db, n) || dalloc(&dx, n)) { cudaFree(db); cudaFree(dx); *status = FFG_OUT_OF_MEMORY; return; }
+  cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  SolveWork w;
+  int grid = 0;
+  std::string msg;
+  ffg_solver_stats local;
+  std::memset(&local, 0, sizeof(local));
+  if (!(st = pcg_grid_size(&grid)) && !(st = solve_work_alloc(w, n, grid))) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    st = pcg_solve(U.A, db, dx, o, w, &local, 0, msg);
+    cudaEventRecord(e1, 0);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    local.solve_seconds = ms * 1e-3;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (!st) cudaMemcpy(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  solve_work_free(w);
+  cudaFree(db);
+  cudaFree(dx);
+  report(o.verbosity, msg);
+  if (stats) *stats = local;
+  *status = st ? st : (local.converged ? FFG_OK : FFG_NOT_CONVERGED);
+}
+
+void ffg_csc_matvec(int n, int64_t nnz, const int64_t *col_ptr, const int *row_ind,
+                    const double *values, const double *x, double *y, int *status) {
+  if (n < 1 || !col_ptr || !row_ind || !values || !x || !y || col_ptr[n] != nnz) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  int st = device_ready();
+  if (st) { *status = st; return; }
+  HostCsr h;
+  if (!csc_to_csr(n, col_ptr, row_ind, values, h)) { *status = FFG_INVALID_INPUT; return; }
+  Uploaded U;
+  if ((st = upload_csr(n, h, U, false))) { *status = st; return; }
+  double *dx = nullptr, *dy = nullptr;
+  if (dalloc(&dx, n) || dalloc(&dy, n)) { cudaFree(dx); cudaFree(dy); *status = FFG_OUT_OF_MEMORY; return; }
+  cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+  st = spmv64(U.A, dx, dy, 0);
+  if (!st && cudaMemcpy(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    st = FFG_CUDA_ERROR;
+  cudaFree(dx);
+  cudaFree(dy);
+  *status = st;
+}
+
+}  // extern "C"

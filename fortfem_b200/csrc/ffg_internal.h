@@ -1,0 +1,174 @@
+// Internal declarations of libfortfem_gpu.so (not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fortfem_gpu.h"
+
+namespace ffg {
+
+// Slot offsets are stored per (incidence pair, local row) as uint16; this value
+// marks a local row whose global DoF is constrained (dropped from the system).
+constexpr uint16_t kConstrainedSlot = 0xFFFF;
+constexpr int kMaxColumnLength = 0xFFFE;
+
+struct Error {
+  int status;
+  std::string message;
+};
+
+// ----------------------------------------------------------------- topology
+// Everything that depends on the mesh connectivity only.  Built on the host
+// once per mesh and uploaded; reused by every assembly/solve on that mesh.
+struct Topology {
+  int family = 0;         // FFG_TETRA_LAGRANGE / FFG_TETRA_NEDELEC / FFG_TRIANGLE_P1
+  int degree = 0;         // Lagrange degree or Nedelec order
+  int nb = 0;             // local DoFs per cell
+  int vpc = 0;            // vertices per cell
+  int n_cells = 0;
+  int n_vertices = 0;
+  int64_t n_dofs = 0;
+  std::vector<int> cells;        // vpc * n_cells
+  std::vector<int> gd;           // nb * n_cells, global DoF of each local DoF
+  std::vector<int8_t> edge_sign; // 6 * n_cells (Nedelec)
+  std::vector<uint8_t> face_perm;// 4 * n_cells permutation index 0..5 (Nedelec)
+  int n_edges = 0, n_faces = 0;
+  std::vector<uint8_t> constrained;  // n_dofs
+  std::vector<int> free_index;       // n_dofs -> free index or -1
+  std::vector<int> free_dofs;        // n_free
+  // constrained (free x free) pattern, CSC == CSR by symmetry
+  std::vector<int64_t> col_ptr;      // n_free + 1
+  std::vector<int> row_idx;          // nnz
+  // per free column: incident (cell, local) pairs in ascending cell order
+  std::vector<int64_t> inc_ptr;      // n_free + 1
+  std::vector<int> inc_cell;
+  std::vector<uint8_t> inc_local;
+  std::vector<uint16_t> slot;        // inc_count * nb
+  int max_column = 0;
+  int64_t n_free() const { return (int64_t)free_dofs.size(); }
+  int64_t nnz() const { return (int64_t)row_idx.size(); }
+};
+
+// Build the DoF numbering of a family (first-appearance order of the
+// reference).  Returns FFG_OK or FFG_INVALID_INPUT.
+int build_dofs(Topology &t, std::string &msg);
+// Constrained set: boundary_mode FFG_BOUNDARY_NONE / _ALL / _MASK.
+int build_constraints(Topology &t, int boundary_mode, const uint8_t *mask, std::string &msg);
+// Free numbering, CSC pattern of the free x free block, incidence lists and slots.
+int build_pattern(Topology &t, std::string &msg);
+
+// ------------------------------------------------------------ basis tables
+struct Rule {
+  std::vector<double> x, y, z, w;
+  int size() const { return (int)w.size(); }
+};
+bool make_rule(int rule, int degree, Rule &r);
+void gauss_legendre01(int n, double *x, double *w);
+
+int lagrange_dof_count(int p);
+void lagrange_indices(int p, std::vector<int> &idx, std::vector<double> &nodes);
+void lagrange_eval(int p, const std::vector<int> &idx, const double *pt, double *val, double *grad);
+int nedelec_dof_count(int k);
+bool nedelec_eval(int k, const double *pt, double *val, double *curl);
+const double *face_transform_table(int k, int perm_index);
+
+// Reference tensors for the per-cell contraction.
+struct ElementTables {
+  int nb = 0;
+  int n_terms = 0;                 // number of reference matrices
+  std::vector<double> ref;         // n_terms * nb * nb, column-major per matrix
+  int nq_load = 0;
+  std::vector<double> load_basis;  // Lagrange: nq_load * nb (w_q phi_i(q));
+                                   // Nedelec: nq_load * nb * 3 (w_q v_i(q))
+  std::vector<double> load_xi;     // nq_load * 3 reference load points
+  // Nedelec orientation transforms (per face permutation) for faces, k(k-1) blocks
+  std::vector<double> face_blocks; // 6 * fdc * fdc
+};
+int build_tables(const Topology &t, int rule, int qdeg, ElementTables &tab, std::string &msg);
+
+// -------------------------------------------------------------- device side
+struct DeviceCsr {
+  int64_t n = 0, nnz = 0;
+  int64_t *row_ptr = nullptr;  // n + 1
+  int *col = nullptr;          // nnz
+  double *val64 = nullptr;
+  float *val32 = nullptr;
+  double *dinv64 = nullptr;
+  float *dinv32 = nullptr;
+  int *tile_row = nullptr;     // n_tiles + 1 row boundaries of the SpMV tiles
+  int n_tiles = 0;
+};
+
+// Build tile boundaries (<= tile_nnz entries each) on the host from row_ptr.
+std::vector<int> make_tiles(const std::vector<int64_t> &row_ptr, int tile_nnz, int *max_row);
+
+struct SolveWork {
+  // FP64
+  double *r64 = nullptr, *partial = nullptr;
+  // FP32 inner vectors
+  float *xf = nullptr, *rf = nullptr, *zf = nullptr, *pf = nullptr, *apf = nullptr;
+  double *pd = nullptr, *apd = nullptr, *zd = nullptr;  // FP64-mode vectors
+  unsigned int *barrier = nullptr;
+  int *control = nullptr;    // [0] error flag, [1] stop flag, ...
+  double *result = nullptr;  // device statistics block
+  int grid = 0;
+  int64_t n = 0;
+};
+
+int solve_work_alloc(SolveWork &w, int64_t n, int grid);
+void solve_work_free(SolveWork &w);
+
+// Launch the persistent Jacobi-PCG (FP64 or mixed) on b -> x.  x holds the
+// initial guess (FP64).  Fills stats (reads back a small block at the end).
+int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_options &opts,
+              SolveWork &w, ffg_solver_stats *stats, cudaStream_t stream, std::string &msg);
+int pcg_grid_size(int *grid);
+
+// SpMV y = A x in FP64 (for the drop-in matvec and residual checks).
+int spmv64(const DeviceCsr &A, const double *x, double *y, cudaStream_t stream);
+
+// Kernel launchers of the assembly (kernels_assemble.cu).
+struct DeviceTopology {
+  int *cells = nullptr;
+  int *gd = nullptr;
+  int8_t *edge_sign = nullptr;
+  uint8_t *face_perm = nullptr;
+  int *free_index = nullptr;
+  int64_t *inc_ptr = nullptr;
+  int *inc_cell = nullptr;
+  uint8_t *inc_local = nullptr;
+  uint16_t *slot = nullptr;
+  double *ref = nullptr;         // reference tensors
+  double *load_basis = nullptr;
+  double *face_blocks = nullptr;
+};
+
+struct AssemblyInputs {
+  const double *vertices = nullptr;  // device
+  double coef_a = 1.0, coef_b = 0.0;
+  const double *cell_a = nullptr, *cell_b = nullptr;  // device, nullable
+  const double *samples = nullptr;                    // device, nullable
+  const double *g = nullptr;                          // device constrained values, nullable
+};
+
+// Per-cell geometry/coefficient block and element right-hand sides.
+int launch_cell_geometry(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                         const AssemblyInputs &in, double *geo, int geo_stride, double *cell_rhs,
+                         int *err, cudaStream_t s);
+// Nedelec: oriented element matrices (n_cells * nb * nb) and oriented element loads.
+int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                   const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
+                   cudaStream_t s);
+int tile_capacity();
+// Column-owner gather into the constrained CSC (values, rhs, Jacobi diagonal).
+int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                   const AssemblyInputs &in, const double *geo, int geo_stride,
+                   const double *cell_rhs, const double *elem, DeviceCsr &A, double *rhs,
+                   int *err, cudaStream_t s);
+int geo_stride_for(const Topology &t, const ElementTables &tab);
+
+}  // namespace ffg

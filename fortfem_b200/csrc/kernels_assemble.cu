@@ -1,0 +1,432 @@
+// Assembly kernels (sm_100a): per-cell geometry (K1), Nedelec element
+// matrices with orientation transform (K2), and the atomic-free,
+// column-owner scatter into the constrained CSC (K3).
+//
+// K3 gives every CSC column (a free global DoF j) to one thread.  The thread
+// walks the cells incident to j in ascending cell order, computes column l(j)
+// of each element matrix and adds it into the column's slots through the
+// precomputed slot map.  Every CSC value is therefore the sum of its element
+// contributions in the reference's triplet order (cell-major, as
+// assemble_*_csc emits them before csc_from_triplet), without atomics, and is
+// bit-reproducible run to run.  The same pass accumulates the load, the
+// Dirichlet lifting -A_fc g of sparse_direct_solve_constrained_real
+// (src/solvers/fortfem_sparse_direct.f90:329-338, by symmetry of the element
+// matrices) and the Jacobi diagonal of build_sparse_preconditioner
+// (src/solvers/advanced_solvers.f90:1139-1154).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ffg_internal.h"
+
+namespace ffg {
+
+namespace {
+
+constexpr double kEps = 2.220446049250313e-16;
+
+__device__ __forceinline__ double det3(const double *J) {
+  return J[0] * (J[4] * J[8] - J[7] * J[5]) - J[3] * (J[1] * J[8] - J[7] * J[2]) +
+         J[6] * (J[1] * J[5] - J[4] * J[2]);
+}
+
+__device__ __forceinline__ void inv3(const double *J, double det, double *Ji) {
+  const double r = 1.0 / det;
+  Ji[0] = (J[4] * J[8] - J[7] * J[5]) * r;
+  Ji[3] = -(J[3] * J[8] - J[6] * J[5]) * r;
+  Ji[6] = (J[3] * J[7] - J[6] * J[4]) * r;
+  Ji[1] = -(J[1] * J[8] - J[7] * J[2]) * r;
+  Ji[4] = (J[0] * J[8] - J[6] * J[2]) * r;
+  Ji[7] = -(J[0] * J[7] - J[6] * J[1]) * r;
+  Ji[2] = (J[1] * J[5] - J[4] * J[2]) * r;
+  Ji[5] = -(J[0] * J[5] - J[3] * J[2]) * r;
+  Ji[8] = (J[0] * J[4] - J[3] * J[1]) * r;
+}
+
+// valid_jacobian (assembly_tetra_lagrange_arbitrary_order_3d.f90:65-66, 796-802)
+__device__ __forceinline__ bool valid_jacobian(const double *J, double det) {
+  double m = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) m = fmax(m, fabs(J[i]));
+  const double s = fmax(1.0, m);
+  return det > 64.0 * kEps * s * s * s;
+}
+
+__device__ __forceinline__ void tet_jacobian(const int *cells, const double *verts, int c,
+                                             double *J, double *v0) {
+  const int4 t = *reinterpret_cast<const int4 *>(cells + 4 * (size_t)c);
+  const double *p0 = verts + 3 * (size_t)t.x;
+  const double *p1 = verts + 3 * (size_t)t.y;
+  const double *p2 = verts + 3 * (size_t)t.z;
+  const double *p3 = verts + 3 * (size_t)t.w;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const double a = p0[r];
+    v0[r] = a;
+    J[r] = p1[r] - a;
+    J[r + 3] = p2[r] - a;
+    J[r + 6] = p3[r] - a;
+  }
+}
+
+// symmetric pair order shared with basis.cpp: (0,0),(1,1),(2,2),(0,1),(0,2),(1,2)
+__constant__ int kPa[6] = {0, 1, 2, 0, 0, 1};
+__constant__ int kPb[6] = {0, 1, 2, 1, 2, 2};
+
+// ------------------------------------------------------------ K1 geometry
+// Lagrange: geo = [k det G_ab (6), m det, det f_q (n_q)], G = J^-1 J^-T.
+__global__ void lagrange_geometry_kernel(int n_cells, const int *__restrict__ cells,
+                                         const double *__restrict__ verts, double ca, double cb,
+                                         const double *__restrict__ cell_a,
+                                         const double *__restrict__ cell_b,
+                                         const double *__restrict__ samples, int nq,
+                                         double *__restrict__ geo, int stride, int *err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  double J[9], Ji[9], v0[3];
+  tet_jacobian(cells, verts, c, J, v0);
+  const double det = det3(J);
+  double *g = geo + (size_t)stride * c;
+  if (!valid_jacobian(J, det)) {
+    atomicCAS(err, 0, FFG_INVALID_INPUT);
+    for (int i = 0; i < stride; ++i) g[i] = 0.0;
+    return;
+  }
+  inv3(J, det, Ji);
+  const double kappa = ca * (cell_a ? cell_a[c] : 1.0);
+  const double mass = cb * (cell_b ? cell_b[c] : 1.0);
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    const int a = kPa[s], b = kPb[s];
+    // (J^-1 J^-T)_ab = sum_k Ji(a,k) Ji(b,k), Ji column-major Ji[a + 3k]
+    const double G = Ji[a] * Ji[b] + Ji[a + 3] * Ji[b + 3] + Ji[a + 6] * Ji[b + 6];
+    g[s] = kappa * det * G;
+  }
+  g[6] = mass * det;
+  for (int q = 0; q < nq; ++q) g[7 + q] = samples ? det * samples[(size_t)nq * c + q] : 0.0;
+}
+
+// P1 triangles: closed-form local matrix of assemble_scalar_p1_matrix
+// (src/fortfem_forms_simple.f90:1702-1717) and the load area/3 of
+// assemble_scalar_p1_load (:1749-1758) with a per-cell source value.
+__global__ void p1_geometry_kernel(int n_cells, const int *__restrict__ tris,
+                                   const double *__restrict__ verts, double stiff, double mass,
+                                   const double *__restrict__ cell_a,
+                                   const double *__restrict__ cell_b,
+                                   const double *__restrict__ samples, double *__restrict__ geo,
+                                   int *err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  double x[3], y[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int v = tris[3 * (size_t)c + i];
+    x[i] = verts[2 * (size_t)v];
+    y[i] = verts[2 * (size_t)v + 1];
+  }
+  const double det = (x[1] - x[0]) * (y[2] - y[0]) - (x[2] - x[0]) * (y[1] - y[0]);
+  double *g = geo + 10 * (size_t)c;
+  if (fabs(det) <= 64.0 * kEps) {
+    atomicCAS(err, 0, FFG_INVALID_INPUT);
+    for (int i = 0; i < 10; ++i) g[i] = 0.0;
+    return;
+  }
+  const double area = 0.5 * fabs(det);
+  const double gx[3] = {(y[1] - y[2]) / det, (y[2] - y[0]) / det, (y[0] - y[1]) / det};
+  const double gy[3] = {(x[2] - x[1]) / det, (x[0] - x[2]) / det, (x[1] - x[0]) / det};
+  const double ks = stiff * (cell_a ? cell_a[c] : 1.0);
+  const double km = mass * (cell_b ? cell_b[c] : 1.0);
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      g[a + 3 * b] = ks * area * (gx[a] * gx[b] + gy[a] * gy[b]) +
+                     km * area * (a == b ? 2.0 : 1.0) / 12.0;
+  g[9] = samples ? samples[c] * area / 3.0 : 0.0;
+}
+
+// ------------------------------------------------- K2 Nedelec element matrices
+// One CTA per cell: K = (c/det) sum C^ab (J^T J)_ab + m det sum V^ab (J^-1 J^-T)_ab,
+// then the oriented matrix T^T K T of assemble_arbitrary_order_curl_mass_csc
+// (:2340-2342; order 1: s_i s_j, :2097-2107) and the oriented load T^T F.
+// Transform structure (build_tetra_nedelec_basis_transform,
+// tetra_nedelec_global_dof_map.f90:107-155): -1 on even (0-based) moments of
+// reversed edges, dense face blocks per face permutation, identity on cells.
+struct NedDims {
+  int k, nb, fdc, edge_end, face_end;
+};
+
+__device__ __forceinline__ void ned_block(const NedDims &D, const int8_t *sg, const uint8_t *fp,
+                                          const double *face_blocks, int d, int &start, int &size,
+                                          const double *&col, double &diag) {
+  // For local DoF d, the non-zeros of column d of T: T[start + r][d] = col[r]
+  // (face block), or the single diagonal entry `diag` (edges, cells).
+  if (d < D.edge_end) {
+    const int e = d / D.k, m = d % D.k;
+    start = d;
+    size = 1;
+    col = nullptr;
+    diag = (sg[e] == -1 && (m % 2) == 0) ? -1.0 : 1.0;
+  } else if (d < D.face_end) {
+    const int f = (d - D.edge_end) / D.fdc, r = (d - D.edge_end) % D.fdc;
+    start = D.edge_end + f * D.fdc;
+    size = D.fdc;
+    col = face_blocks + (size_t)fp[f] * D.fdc * D.fdc + (size_t)D.fdc * r;
+    diag = 0.0;
+  } else {
+    start = d;
+    size = 1;
+    col = nullptr;
+    diag = 1.0;
+  }
+}
+
+__global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cells,
+                                       const double *__restrict__ verts, double ca, double cb,
+                                       const double *__restrict__ cell_a,
+                                       const double *__restrict__ cell_b,
+                                       const double *__restrict__ samples, int nql, NedDims D,
+                                       const double *__restrict__ ref,
+                                       const double *__restrict__ load_basis,
+                                       const int8_t *__restrict__ edge_sign,
+                                       const uint8_t *__restrict__ face_perm,
+                                       const double *__restrict__ face_blocks,
+                                       double *__restrict__ elem, double *__restrict__ cell_rhs,
+                                       int *err) {
+  extern __shared__ double sm[];
+  const int nb = D.nb;
+  double *K = sm;                      // nb * nb
+  double *F = K + (size_t)nb * nb;     // nb
+  double *lf = F + nb;                 // 3 * nql: det J^-1 f_q
+  __shared__ double geo[12];
+  __shared__ double Ji_s[9];
+  __shared__ double det_s;
+  __shared__ int ok_s;
+  for (int c = blockIdx.x; c < n_cells; c += gridDim.x) {
+    if (threadIdx.x == 0) {
+      double J[9], Ji[9], v0[3];
+      tet_jacobian(cells, verts, c, J, v0);
+      const double det = det3(J);
+      ok_s = valid_jacobian(J, det) ? 1 : 0;
+      if (!ok_s) atomicCAS(err, 0, FFG_INVALID_INPUT);
+      inv3(J, ok_s ? det : 1.0, Ji);
+      const double cw = ca * (cell_a ? cell_a[c] : 1.0);
+      const double mw = cb * (cell_b ? cell_b[c] : 1.0);
+      for (int s = 0; s < 6; ++s) {
+        const int a = kPa[s], b = kPb[s];
+        const double JtJ = J[3 * a] * J[3 * b] + J[3 * a + 1] * J[3 * b + 1] + J[3 * a + 2] * J[3 * b + 2];
+        const double G = Ji[a] * Ji[b] + Ji[a + 3] * Ji[b + 3] + Ji[a + 6] * Ji[b + 6];
+        geo[s] = ok_s ? cw / det * JtJ : 0.0;
+        geo[6 + s] = ok_s ? mw * det * G : 0.0;
+      }
+      for (int i = 0; i < 9; ++i) Ji_s[i] = Ji[i];
+      det_s = ok_s ? det : 0.0;
+    }
+    __syncthreads();
+    const size_t nn = (size_t)nb * nb;
+    for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+      double s = 0.0;
+#pragma unroll
+      for (int g = 0; g < 12; ++g) s += geo[g] * __ldg(ref + (size_t)g * nn + idx);
+      K[idx] = s;
+    }
+    for (int q = threadIdx.x; q < nql; q += blockDim.x) {
+      double f[3] = {0.0, 0.0, 0.0};
+      if (samples) {
+        const double *sp = samples + 3 * ((size_t)nql * c + q);
+        f[0] = sp[0]; f[1] = sp[1]; f[2] = sp[2];
+      }
+      // (J^-1 f)_a = sum_k Ji(a,k) f_k ; physical value = J^-T v, so f.v = (J^-1 f).v
+      for (int a = 0; a < 3; ++a)
+        lf[3 * q + a] = det_s * (Ji_s[a] * f[0] + Ji_s[a + 3] * f[1] + Ji_s[a + 6] * f[2]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+      double s = 0.0;
+      for (int q = 0; q < nql; ++q) {
+        const double *lb = load_basis + ((size_t)q * nb + i) * 3;
+        s += lf[3 * q] * lb[0] + lf[3 * q + 1] * lb[1] + lf[3 * q + 2] * lb[2];
+      }
+      F[i] = s;
+    }
+    __syncthreads();
+    const int8_t *sg = edge_sign + 6 * (size_t)c;
+    const uint8_t *fp = face_perm + 4 * (size_t)c;
+    double *O = elem + nn * c;
+    for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+      const int i = (int)(idx % nb), j = (int)(idx / nb);
+      int si, ni, sj, nj;
+      const double *ci, *cj;
+      double di, dj;
+      ned_block(D, sg, fp, face_blocks, i, si, ni, ci, di);
+      ned_block(D, sg, fp, face_blocks, j, sj, nj, cj, dj);
+      double s = 0.0;
+      for (int m = 0; m < ni; ++m) {
+        const double tm = ci ? ci[m] : di;
+        if (tm == 0.0) continue;
+        double inner = 0.0;
+        for (int n = 0; n < nj; ++n) {
+          const double tn = cj ? cj[n] : dj;
+          inner += K[(si + m) + (size_t)nb * (sj + n)] * tn;
+        }
+        s += tm * inner;
+      }
+      O[idx] = s;
+    }
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+      int si, ni;
+      const double *ci;
+      double di;
+      ned_block(D, sg, fp, face_blocks, i, si, ni, ci, di);
+      double s = 0.0;
+      for (int m = 0; m < ni; ++m) s += (ci ? ci[m] : di) * F[si + m];
+      cell_rhs[(size_t)nb * c + i] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------- K3 column-owner scatter
+template <int FAMILY>
+__global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_ptr,
+                              const int *__restrict__ row_idx, const int64_t *__restrict__ inc_ptr,
+                              const int *__restrict__ inc_cell,
+                              const uint8_t *__restrict__ inc_local,
+                              const uint16_t *__restrict__ slot, const int *__restrict__ gd,
+                              int nb, const double *__restrict__ geo, int stride,
+                              const double *__restrict__ ref, const double *__restrict__ load_basis,
+                              int nq, const double *__restrict__ elem,
+                              const double *__restrict__ cell_rhs, const double *__restrict__ g,
+                              double *__restrict__ val64, float *__restrict__ val32,
+                              double *__restrict__ dinv64, float *__restrict__ dinv32,
+                              double *__restrict__ rhs) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_free) return;
+  const int64_t start = col_ptr[j], end = col_ptr[j + 1];
+  for (int64_t k = start; k < end; ++k) val64[k] = 0.0;
+  double b = 0.0, lift = 0.0;
+  const size_t nn = (size_t)nb * nb;
+  for (int64_t p = inc_ptr[j]; p < inc_ptr[j + 1]; ++p) {
+    const int e = inc_cell[p];
+    const int l = inc_local[p];
+    const uint16_t *sl = slot + (size_t)p * nb;
+    const int *ge = gd + (size_t)nb * e;
+    double gco[7];
+    double F = 0.0;
+    if (FAMILY == FFG_TETRA_LAGRANGE) {
+      const double *gg = geo + (size_t)stride * e;
+#pragma unroll
+      for (int s = 0; s < 7; ++s) gco[s] = gg[s];
+      for (int q = 0; q < nq; ++q) F += gg[7 + q] * __ldg(load_basis + (size_t)q * nb + l);
+    } else if (FAMILY == FFG_TRIANGLE_P1) {
+      F = geo[10 * (size_t)e + 9];
+    } else {
+      F = cell_rhs[(size_t)nb * e + l];
+    }
+    for (int i = 0; i < nb; ++i) {
+      double kil;
+      if (FAMILY == FFG_TETRA_LAGRANGE) {
+        const size_t off = i + (size_t)nb * l;
+        kil = 0.0;
+#pragma unroll
+        for (int s = 0; s < 7; ++s) kil += gco[s] * __ldg(ref + s * nn + off);
+      } else if (FAMILY == FFG_TRIANGLE_P1) {
+        kil = geo[10 * (size_t)e + i + 3 * l];
+      } else {
+        kil = elem[nn * e + i + (size_t)nb * l];
+      }
+      const uint16_t s = sl[i];
+      if (s == kConstrainedSlot) {
+        if (g) lift += kil * g[ge[i]];
+      } else {
+        val64[start + s] += kil;
+      }
+    }
+    b += F;
+  }
+  rhs[j] = b - lift;
+  double d = 0.0;
+  for (int64_t k = start; k < end; ++k) {
+    const double v = val64[k];
+    val32[k] = (float)v;
+    if (row_idx[k] == (int)j) d = v;
+  }
+  const double di = (fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
+  dinv64[j] = di;
+  dinv32[j] = (float)di;
+}
+
+inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+int launch_cell_geometry(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                         const AssemblyInputs &in, double *geo, int stride, double *cell_rhs,
+                         int *err, cudaStream_t s) {
+  (void)cell_rhs;
+  const int T = 128;
+  if (t.family == FFG_TETRA_LAGRANGE) {
+    lagrange_geometry_kernel<<<blocks_for(t.n_cells, T), T, 0, s>>>(
+        t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
+        tab.nq_load, geo, stride, err);
+  } else if (t.family == FFG_TRIANGLE_P1) {
+    p1_geometry_kernel<<<blocks_for(t.n_cells, T), T, 0, s>>>(t.n_cells, dt.cells, in.vertices,
+                                                             in.coef_a, in.coef_b, in.cell_a,
+                                                             in.cell_b, in.samples, geo, err);
+  }
+  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+size_t nedelec_smem_bytes(const ElementTables &tab) {
+  return sizeof(double) * ((size_t)tab.nb * tab.nb + tab.nb + 3 * (size_t)tab.nq_load);
+}
+
+int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                   const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
+                   cudaStream_t s) {
+  NedDims D;
+  D.k = t.degree;
+  D.nb = t.nb;
+  D.fdc = t.degree * (t.degree - 1);
+  D.edge_end = 6 * t.degree;
+  D.face_end = D.edge_end + 4 * D.fdc;
+  const size_t smem = nedelec_smem_bytes(tab);
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(nedelec_element_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return FFG_CUDA_ERROR;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * 8);
+  nedelec_element_kernel<<<grid, 256, smem, s>>>(
+      t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
+      tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem,
+      cell_rhs, err);
+  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                   const AssemblyInputs &in, const double *geo, int stride,
+                   const double *cell_rhs, const double *elem, DeviceCsr &A, double *rhs,
+                   int *err, cudaStream_t s) {
+  (void)err;
+  const int T = 128;
+  const int64_t F = t.n_free();
+  if (F == 0) return FFG_OK;
+#define FFG_COLUMN_ARGS                                                                       \
+  F, A.row_ptr, A.col, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd, t.nb, geo,      \
+      stride, dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, A.val64, A.val32,     \
+      A.dinv64, A.dinv32, rhs
+  if (t.family == FFG_TETRA_LAGRANGE)
+    column_kernel<FFG_TETRA_LAGRANGE><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);
+  else if (t.family == FFG_TRIANGLE_P1)
+    column_kernel<FFG_TRIANGLE_P1><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);
+  else
+    column_kernel<FFG_TETRA_NEDELEC><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);
+#undef FFG_COLUMN_ARGS
+  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+}  // namespace ffg

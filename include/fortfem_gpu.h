@@ -1,0 +1,243 @@
+/*
+ * fortfem_gpu.h -- C-ABI of libfortfem_gpu.so, the B200 (sm_100a) assembly +
+ * preconditioned-CG path for lazy-fortran/fortfem.
+ *
+ * Conventions follow the reference's own C header (include/fortfem.h):
+ *   - zero-based indices; vertices are [x0,y0,z0,x1,...] (the Fortran
+ *     (3,n_vertices) array) and cells are [v0,v1,v2,v3,...];
+ *   - CSC output arrays are caller-owned with a capacity: n_dofs and nnz are
+ *     always set for valid input and status is FFG_CAPACITY (-2) when
+ *     nnz_capacity is too small (fortfem.h:140-170);
+ *   - every entry point ends with `int *status`; nothing aborts across the ABI;
+ *   - device-resident objects are positive, process-local integer handles
+ *     released by the matching *_free call (fortfem.h:186-197).
+ * Host arrays are borrowed for the duration of a call.  Column pointers are
+ * int64 so that matrices above 2^31 entries stay addressable.
+ *
+ * Each entry point cites the reference interface it replaces.  Reference
+ * paths are relative to the lazy-fortran/fortfem tree.
+ */
+#ifndef FORTFEM_GPU_H
+#define FORTFEM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes: 0, -1, -2, -3 as in src/bindings/fortfem_capi_solver.f90:33-47. */
+#define FFG_OK 0
+#define FFG_INVALID_INPUT -1
+#define FFG_CAPACITY -2
+#define FFG_BAD_HANDLE -3
+#define FFG_CUDA_ERROR -4
+#define FFG_OUT_OF_MEMORY -5
+#define FFG_NOT_CONVERGED -6
+#define FFG_TIMEOUT -7
+#define FFG_NO_DEVICE -8
+
+/* Element families of a problem handle. */
+#define FFG_TETRA_LAGRANGE 1
+#define FFG_TETRA_NEDELEC 2
+#define FFG_TRIANGLE_P1 3
+
+/* Quadrature rules: FFG_RULE_DUFFY uses tetra_duffy_quadrature(degree)
+ * (src/quadrature/tetra_duffy_quadrature.f90:12-51); FFG_RULE_DEGREE_TWO is the
+ * 4-point rule tetra_degree_two_quadrature (assembly_tetra_nedelec_3d.f90:2570-2581). */
+#define FFG_RULE_DUFFY 0
+#define FFG_RULE_DEGREE_TWO 1
+
+/* Essential boundary handling of a problem handle. */
+#define FFG_BOUNDARY_NONE 0 /* no constrained DoFs */
+#define FFG_BOUNDARY_ALL 1  /* every DoF on an incidence-one face (Lagrange:
+                               build_dirichlet_data, fortfem_tetra_lagrange_solver_3d.f90:551-610;
+                               Nedelec: build_zero_tangential_mask,
+                               fortfem_tetra_nedelec_solver_3d.f90:416-458;
+                               P1: find_boundary vertices, mesh_2d.f90:560-603) */
+#define FFG_BOUNDARY_MASK 2 /* caller-supplied uint8 mask over the global DoFs */
+
+/* Solver precision. */
+#define FFG_PRECISION_FP64 0  /* FP64 Jacobi-PCG with the reference's stopping rule */
+#define FFG_PRECISION_MIXED 1 /* FP32 inner PCG under FP64 iterative refinement */
+
+#define FFG_OPTIONS_VERSION 1
+
+/* solver_options_t (src/solvers/advanced_solvers.f90:32-44) plus GPU fields. */
+typedef struct {
+  int version;           /* FFG_OPTIONS_VERSION */
+  int preconditioner;    /* 0 = "none", 1 = "jacobi" */
+  int precision;         /* FFG_PRECISION_FP64 or FFG_PRECISION_MIXED */
+  int tolerance_type;    /* 0 = "relative", 1 = "absolute" */
+  double tolerance;      /* FP64 mode: on the recursive residual as the reference;
+                            mixed mode: on the true FP64 residual ||b-Ax|| (relative to ||b||) */
+  int max_iterations;    /* cap on (inner) PCG iterations in total */
+  int max_refinements;   /* mixed mode: outer refinement steps */
+  double inner_tolerance;/* mixed mode: relative residual reduction per inner solve */
+  int verbosity;         /* > 0 prints per-solve statistics on the host */
+  double timeout_seconds;/* device-side wall limit of one solve; <= 0 selects 60 s */
+  int breakdown_guard;   /* FP64 mode: 0 = the reference's |p^T A p| < 1e-14 test
+                            (advanced_solvers.f90:897), 1 = stop only on p^T A p <= 0 */
+} ffg_solver_options;
+
+/* solver_stats_t (src/solvers/advanced_solvers.f90:47-57) plus GPU fields. */
+typedef struct {
+  int converged;
+  int iterations;              /* PCG iterations (inner iterations summed in mixed mode) */
+  int refinements;             /* outer FP64 refinement steps (mixed mode) */
+  int status;                  /* FFG_* of the solve */
+  double final_residual;       /* reference meaning: recursive residual 2-norm */
+  double true_relative_residual; /* ||b - A x||_2 / ||b||_2 in FP64 at exit */
+  double solve_seconds;        /* device time of the solve (CUDA events) */
+  double assembly_seconds;     /* device time of assembly + load + reduction */
+} ffg_solver_stats;
+
+/* Fill opts with the library defaults (tolerance 1e-10, Jacobi, mixed). */
+void ffg_default_options(ffg_solver_options *opts);
+
+/* Library version and the number of visible CUDA devices. */
+void ffg_version(int *major, int *minor, int *patch);
+void ffg_device_count(int *count, int *status);
+
+/* ------------------------------------------------------------------ meshes */
+
+/* generate_structured_tetra_box_mesh, src/mesh/structured_tetra_box_mesh.f90:12-70.
+ * bounds = [xmin,ymin,zmin,xmax,ymax,zmax]; vertices has 3*prod(counts+1)
+ * entries and tetrahedra 4*6*prod(counts). */
+void ffg_structured_tetra_box_mesh(const double *bounds, const int *counts, double *vertices,
+                                   int *tetrahedra, int *status);
+
+/* create_rectangular / unit_square_mesh(n), src/mesh/mesh_2d.f90:90-148 and
+ * src/fortfem_api_mesh.f90:128-139: n vertices per side on [0,1]^2. */
+void ffg_unit_square_mesh(int n, double *vertices, int *triangles, int *status);
+
+/* ----------------------------------------------------- drop-in assembly */
+
+/* assemble_tetra_lagrange_stiffness_csc,
+ * src/assembly/assembly_tetra_lagrange_arbitrary_order_3d.f90:276-334.
+ * cell_stiffness / cell_mass (nullable, n_tetrahedra entries) scale the scalar
+ * coefficients cellwise as src/fortfem_forms_simple.f90:979-1045 does. */
+void ffg_assemble_tetra_lagrange_stiffness_csc(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int degree,
+    int rule, int quadrature_degree, double stiffness_coefficient, double mass_coefficient,
+    const double *cell_stiffness, const double *cell_mass, int64_t nnz_capacity, int *n_dofs,
+    int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values, int *status);
+
+/* assemble_tetra_lagrange_scalar_load_samples, same file :473-528.
+ * source_values holds n_q values per cell (n_q of the rule), cell-major. */
+void ffg_assemble_tetra_lagrange_scalar_load_samples(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int degree,
+    int rule, int quadrature_degree, const double *source_values, int n_dofs, double *rhs,
+    int *status);
+
+/* assemble_tetra_nedelec_curl_mass_csc, src/assembly/assembly_tetra_nedelec_3d.f90:2042-2112
+ * (order 1) and assemble_arbitrary_order_curl_mass_csc :2289-2355 (order >= 2). */
+void ffg_assemble_tetra_nedelec_curl_mass_csc(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int order,
+    double curl_coefficient, double mass_coefficient, const double *cell_curl,
+    const double *cell_mass, int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+    int *row_ind, double *values, int *status);
+
+/* assemble_tetra_nedelec_vector_load_samples, assembly_tetra_nedelec_3d.f90:128-185
+ * (order 1 uses the 4-point rule and edge signs, :2002-2040); source_values
+ * holds 3*n_q values per cell. */
+void ffg_assemble_tetra_nedelec_vector_load_samples(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int order,
+    const double *source_values, int n_dofs, double *rhs, int *status);
+
+/* assemble_scalar_p1_matrix / assemble_scalar_p1_load scattered into CSC,
+ * src/fortfem_forms_simple.f90:1678-1761 (the reference builds it dense). */
+void ffg_assemble_scalar_p1_csc(int n_vertices, const double *vertices, int n_triangles,
+                                const int *triangles, double mass_coefficient,
+                                double stiffness_coefficient, const double *cell_stiffness,
+                                int64_t nnz_capacity, int64_t *nnz, int64_t *col_ptr,
+                                int *row_ind, double *values, int *status);
+
+/* ------------------------------------------------------------------ solve */
+
+/* solve_sparse(A, b, x, opts, stats), src/solvers/advanced_solvers.f90:135-195, with
+ * method "pcg": square zero-based CSC in host memory; x is the initial guess
+ * on entry and the solution on exit. */
+void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row_ind,
+                      const double *values, const double *b, double *x,
+                      const ffg_solver_options *opts, ffg_solver_stats *stats, int *status);
+
+/* y = A x for a host CSC matrix (spmv / csc_matvec, src/solvers/fortfem_sparse_matrix.f90:46-58). */
+void ffg_csc_matvec(int n, int64_t nnz, const int64_t *col_ptr, const int *row_ind,
+                    const double *values, const double *x, double *y, int *status);
+
+/* Host-only topology of a problem (no device needed): the global DoF of every
+ * local DoF (build_tetra_lagrange_dof_map, tetra_lagrange_global_dof_map.f90:13-79;
+ * build_tetra_nedelec_dof_map, tetra_nedelec_global_dof_map.f90:15-105), the
+ * constrained mask of boundary_mode and the CSC pattern of the constrained
+ * (free x free) system.  Arrays are caller-owned; pass nnz_capacity = 0 and
+ * null arrays to query n_dofs and nnz (status FFG_CAPACITY). */
+void ffg_build_topology(int family, int degree, int n_vertices, int n_cells, const int *cells,
+                        int boundary_mode, const uint8_t *boundary_mask, int64_t dof_capacity,
+                        int64_t nnz_capacity, int64_t *n_dofs, int64_t *n_free, int64_t *nnz,
+                        int *global_dofs, uint8_t *constrained, int64_t *col_ptr, int *row_ind,
+                        int *status);
+
+/* ------------------------------------------------ device-resident problems */
+
+/* Build the topology of an assemble + constrain + solve problem once per mesh
+ * (DoF numbering in the reference's first-appearance order, the CSC pattern,
+ * the constrained set and the element-to-CSC slot maps) and keep it in HBM.
+ * family: FFG_TETRA_LAGRANGE (degree 1..4), FFG_TETRA_NEDELEC (order 1..5) or
+ * FFG_TRIANGLE_P1 (degree 1; vertices are then 2-D).  For Lagrange the rule
+ * and quadrature degree select the element and load quadrature; Nedelec uses
+ * the reference rules (order 1: the 4-point rule; order k >= 2: Duffy 2k for
+ * the matrix and 2k+2 for the load).  boundary_mask is read only for
+ * FFG_BOUNDARY_MASK.  Returns the global DoF count, the free DoF count, the
+ * nonzeros of the constrained (free x free) system and the number of load
+ * samples per cell. */
+void ffg_problem_create(int family, int degree, int n_vertices, int n_cells, const int *cells,
+                        int rule, int quadrature_degree, int boundary_mode,
+                        const uint8_t *boundary_mask, int *handle, int64_t *n_dofs,
+                        int64_t *n_free, int64_t *nnz, int *samples_per_cell, int *status);
+
+/* Physical sample points (3 * samples_per_cell * n_cells doubles, cell-major)
+ * at which the caller evaluates its source; 2-D meshes return (x, y, 0). */
+void ffg_problem_sample_points(int handle, const double *vertices, double *points, int *status);
+
+/* Physical location of every global DoF that carries a nodal value (Lagrange,
+ * P1): 3 * n_dofs doubles.  Callers evaluate boundary_value there. */
+void ffg_problem_dof_points(int handle, const double *vertices, double *points, int *status);
+
+/* The constrained mask of the problem (n_dofs bytes, 1 = constrained). */
+void ffg_problem_constrained(int handle, uint8_t *mask, int *status);
+
+/* Assemble the constrained system on the device and solve it:
+ *   K(c) x = F(f) on the free DoFs, x = g on the constrained DoFs,
+ * with K = coef_a * cell_a[c] * (stiffness | curl-curl) + coef_b * cell_b[c] * mass
+ * (cell arrays nullable), F from source samples (samples_per_cell values per
+ * cell for scalar families, 3 * samples_per_cell for Nedelec) and the lifting
+ * -A_fc g of sparse_direct_solve_constrained_real
+ * (src/solvers/fortfem_sparse_direct.f90:264-344).  constrained_values
+ * (nullable = zero) has n_dofs entries.  memory = 0: all pointers are host
+ * memory (synchronous, host<->device copies inside); memory = 1: vertices,
+ * cell arrays, samples, constrained_values and solution are device pointers
+ * and the call is asynchronous on `stream` (a cudaStream_t) except for the
+ * statistics, which are read back at the end.  solution has n_dofs entries. */
+void ffg_problem_solve(int handle, const double *vertices, double coef_a, double coef_b,
+                       const double *cell_a, const double *cell_b, const double *source_samples,
+                       const double *constrained_values, const ffg_solver_options *opts,
+                       double *solution, ffg_solver_stats *stats, int memory, void *stream,
+                       int *status);
+
+/* Assemble only and return the constrained (free x free) CSC matrix, its
+ * lifted right-hand side and the free-DoF list (host memory, capacity rules
+ * as above).  This is the reduced system the solve works on. */
+void ffg_problem_reduced_system(int handle, const double *vertices, double coef_a, double coef_b,
+                                const double *cell_a, const double *cell_b,
+                                const double *source_samples, const double *constrained_values,
+                                int64_t nnz_capacity, int64_t *nnz, int64_t *col_ptr, int *row_ind,
+                                double *values, double *rhs, int *free_dofs, int *status);
+
+/* Release a problem handle (fortfem_factor_free, src/bindings/fortfem_capi_solver.f90:108-124). */
+void ffg_problem_free(int handle, int *status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

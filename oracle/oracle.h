@@ -86,12 +86,14 @@ int or_reduce_constrained(int n, const int64_t *col_ptr, const int *row_idx, con
                           int64_t *r_col_ptr, int *r_row_idx, double *r_values, double *r_rhs,
                           int *free_dofs);
 /* solve_sparse(method=pcg, preconditioner=jacobi|none): returns iterations in stats[0],
- * converged in stats[1], final recursive residual norm in stats[2]. */
+ * converged in stats[1], final recursive residual norm in stats[2].  guard 0 is
+ * the reference's absolute |p^T A p| < 1e-14 test, guard 1 stops only on
+ * p^T A p <= 0 (SPD breakdown). */
 int or_pcg_sparse(int n, const int64_t *col_ptr, const int *row_idx, const double *values,
                   const double *b, double *x, double tolerance, int relative, int max_iterations,
-                  int jacobi, double *stats);
+                  int jacobi, int guard, double *stats);
 int or_pcg_dense(int n, const double *matrix, const double *b, double *x, double tolerance,
-                 int relative, int max_iterations, int jacobi, double *stats);
+                 int relative, int max_iterations, int jacobi, int guard, double *stats);
 
 /* ---- tetrahedral Nedelec (first kind) ---- */
 int or_nedelec_dof_count(int order);

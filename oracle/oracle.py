@@ -299,23 +299,24 @@ def reduce_constrained(n, cp, ri, v, rhs, constrained, values=None):
 
 
 def pcg_sparse(n, cp, ri, v, b, x0=None, tol=1e-10, relative=True, max_iterations=100000,
-               jacobi=True):
+               jacobi=True, guard=0):
     x = np.zeros(n) if x0 is None else _arr(x0, np.float64).copy()
     stats = np.zeros(4)
     _check(_call("or_pcg_sparse", n, _arr(cp, np.int64), _arr(ri, np.int32), _arr(v, np.float64),
                  _arr(b, np.float64), x, float(tol), int(relative), int(max_iterations),
-                 int(jacobi), stats), "pcg_sparse")
+                 int(jacobi), int(guard), stats), "pcg_sparse")
     return x, {"iterations": int(stats[0]), "converged": bool(stats[1]),
                "final_residual": stats[2], "initial_residual": stats[3]}
 
 
-def pcg_dense(a, b, x0=None, tol=1e-10, relative=True, max_iterations=100000, jacobi=True):
+def pcg_dense(a, b, x0=None, tol=1e-10, relative=True, max_iterations=100000, jacobi=True,
+              guard=0):
     n = len(b)
     flat = np.asfortranarray(a, dtype=np.float64).reshape(-1, order="F").copy()
     x = np.zeros(n) if x0 is None else _arr(x0, np.float64).copy()
     stats = np.zeros(4)
     _check(_call("or_pcg_dense", n, flat, _arr(b, np.float64), x, float(tol), int(relative),
-                 int(max_iterations), int(jacobi), stats), "pcg_dense")
+                 int(max_iterations), int(jacobi), int(guard), stats), "pcg_dense")
     return x, {"iterations": int(stats[0]), "converged": bool(stats[1]),
                "final_residual": stats[2], "initial_residual": stats[3]}
 

@@ -883,9 +883,13 @@ int or_reduce_constrained(int n, const int64_t *cp, const int *ri, const double 
 }  // extern "C"
 
 namespace {
+// guard = 0: the reference's absolute breakdown test |p^T A p| < 1e-14
+// (advanced_solvers.f90:897); guard = 1: stop only on p^T A p <= 0 or a
+// non-finite value (SPD breakdown), which lets scale-free tolerances be reached
+// on systems whose p^T A p falls below 1e-14 before convergence.
 template <class MatVec>
 int pcg_core(int n, MatVec matvec, const std::vector<double> &diag, const double *b, double *x,
-             double tol_in, int relative, int maxit, double *stats) {
+             double tol_in, int relative, int maxit, int guard, double *stats) {
   // pcg_solve_operator / initialize_pcg_state / pcg_iteration_loop,
   // src/solvers/advanced_solvers.f90:831-925; tolerance :1063-1073.
   std::vector<double> r(n), z(n), p(n), Ap(n), Ax(n);
@@ -904,7 +908,7 @@ int pcg_core(int n, MatVec matvec, const std::vector<double> &diag, const double
     matvec(p.data(), Ap.data());
     double pAp = 0.0;
     for (int i = 0; i < n; ++i) pAp += p[i] * Ap[i];
-    if (std::fabs(pAp) < 1.0e-14) break;
+    if (guard == 0 ? std::fabs(pAp) < 1.0e-14 : !(pAp > 0.0 && std::isfinite(pAp))) break;
     double alpha = rz_old / pAp;
     for (int i = 0; i < n; ++i) x[i] = x[i] + alpha * p[i];
     for (int i = 0; i < n; ++i) r[i] = r[i] - alpha * Ap[i];
@@ -932,7 +936,8 @@ extern "C" {
 // Jacobi diagonal found by a column search as build_sparse_preconditioner does
 // (:1139-1154).
 int or_pcg_sparse(int n, const int64_t *cp, const int *ri, const double *v, const double *b,
-                  double *x, double tol, int relative, int maxit, int jacobi, double *stats) {
+                  double *x, double tol, int relative, int maxit, int jacobi, int guard,
+                  double *stats) {
   std::vector<double> diag(n, 1.0);
   if (jacobi)
     for (int i = 0; i < n; ++i) {
@@ -942,12 +947,12 @@ int or_pcg_sparse(int n, const int64_t *cp, const int *ri, const double *v, cons
       diag[i] = (std::fabs(a) > 1.0e-14) ? 1.0 / a : 1.0;
     }
   auto mv = [&](const double *in, double *out) { or_csc_matvec(n, cp, ri, v, in, out); };
-  return pcg_core(n, mv, diag, b, x, tol, relative, maxit, stats);
+  return pcg_core(n, mv, diag, b, x, tol, relative, maxit, guard, stats);
 }
 
 // pcg_solve (dense), src/solvers/advanced_solvers.f90:800-829; Jacobi :1101-1109.
 int or_pcg_dense(int n, const double *A, const double *b, double *x, double tol, int relative,
-                 int maxit, int jacobi, double *stats) {
+                 int maxit, int jacobi, int guard, double *stats) {
   std::vector<double> diag(n, 1.0);
   if (jacobi)
     for (int i = 0; i < n; ++i) {
@@ -962,7 +967,7 @@ int or_pcg_dense(int n, const double *A, const double *b, double *x, double tol,
       for (int i = 0; i < n; ++i) out[i] += col[i] * xj;
     }
   };
-  return pcg_core(n, mv, diag, b, x, tol, relative, maxit, stats);
+  return pcg_core(n, mv, diag, b, x, tol, relative, maxit, guard, stats);
 }
 
 }  // extern "C"
