@@ -64,8 +64,8 @@ class SolverOptions:
     tolerance_type: str = "relative"
     verbosity: int = 0
     precision: str = "fp64"          # "fp64" (reference semantics) or "mixed"
-    inner_tolerance: float = 1.0e-5
-    max_refinements: int = 30
+    inner_tolerance: float = 0.1      # mixed: reliable-update threshold
+    max_refinements: int = 1000       # mixed: cap on reliable updates
     timeout_seconds: float = 60.0
     breakdown_guard: str = "absolute"  # "absolute" (reference) or "spd"
 

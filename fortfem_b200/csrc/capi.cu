@@ -31,6 +31,23 @@ int dalloc(T **p, size_t count) {
   return FFG_OK;
 }
 
+// Device copy of h followed by `pad` zeroed entries.
+template <class T>
+int upload_padded(T **p, const std::vector<T> &h, size_t pad) {
+  if (dalloc(p, h.size() + pad)) return FFG_OUT_OF_MEMORY;
+  if (!h.empty() && cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  if (cudaMemset(*p + h.size(), 0, pad * sizeof(T)) != cudaSuccess) return FFG_CUDA_ERROR;
+  return FFG_OK;
+}
+
+template <class T>
+int zeros_padded(T **p, size_t n, size_t pad) {
+  if (dalloc(p, n + pad)) return FFG_OUT_OF_MEMORY;
+  if (cudaMemset(*p, 0, (n + pad) * sizeof(T)) != cudaSuccess) return FFG_CUDA_ERROR;
+  return FFG_OK;
+}
+
 template <class T>
 int upload(T **p, const std::vector<T> &h) {
   int st = dalloc(p, h.size());
@@ -139,9 +156,10 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   A.n = t.n_free();
   A.nnz = t.nnz();
   if ((st = upload(&A.row_ptr, t.col_ptr))) return st;
-  if ((st = upload(&A.col, t.row_idx))) return st;
-  if ((st = dalloc(&A.val64, (size_t)A.nnz))) return st;
-  if ((st = dalloc(&A.val32, (size_t)A.nnz))) return st;
+  const size_t pad = (size_t)matrix_padding();
+  if ((st = upload_padded(&A.col, t.row_idx, pad))) return st;
+  if ((st = zeros_padded(&A.val64, (size_t)A.nnz, pad))) return st;
+  if ((st = zeros_padded(&A.val32, (size_t)A.nnz, pad))) return st;
   if ((st = dalloc(&A.dinv64, (size_t)A.n))) return st;
   if ((st = dalloc(&A.dinv32, (size_t)A.n))) return st;
   int max_row = 0;
@@ -237,8 +255,8 @@ void fill_default(ffg_solver_options &o) {
   o.tolerance_type = 0;
   o.tolerance = 1.0e-10;
   o.max_iterations = 1000000;
-  o.max_refinements = 30;
-  o.inner_tolerance = 1.0e-5;
+  o.max_refinements = 1000;
+  o.inner_tolerance = 0.1;
   o.verbosity = 0;
   o.timeout_seconds = 60.0;
   o.breakdown_guard = 0;
@@ -252,7 +270,7 @@ int check_options(const ffg_solver_options *o, ffg_solver_options &out) {
   if (out.precision != FFG_PRECISION_FP64 && out.precision != FFG_PRECISION_MIXED)
     return FFG_INVALID_INPUT;
   if (out.tolerance < 0 || out.max_iterations < 0) return FFG_INVALID_INPUT;
-  if (out.inner_tolerance <= 0 || out.inner_tolerance >= 1) out.inner_tolerance = 1e-5;
+  if (out.inner_tolerance <= 0 || out.inner_tolerance >= 1) out.inner_tolerance = 0.1;
   if (out.max_refinements < 0) out.max_refinements = 0;
   return FFG_OK;
 }
@@ -320,9 +338,10 @@ int upload_csr(int n, const HostCsr &h, Uploaded &U, bool jacobi) {
   A.nnz = (int64_t)h.col.size();
   int st;
   if ((st = upload(&A.row_ptr, h.rp))) return st;
-  if ((st = upload(&A.col, h.col))) return st;
-  if ((st = upload(&A.val64, h.val))) return st;
-  if ((st = dalloc(&A.val32, h.val.size()))) return st;
+  const size_t pad = (size_t)matrix_padding();
+  if ((st = upload_padded(&A.col, h.col, pad))) return st;
+  if ((st = upload_padded(&A.val64, h.val, pad))) return st;
+  if ((st = zeros_padded(&A.val32, h.val.size(), pad))) return st;
   if ((st = dalloc(&A.dinv64, (size_t)n))) return st;
   if ((st = dalloc(&A.dinv32, (size_t)n))) return st;
   int max_row = 0;

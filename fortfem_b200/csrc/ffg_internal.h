@@ -107,17 +107,21 @@ struct DeviceCsr {
 std::vector<int> make_tiles(const std::vector<int64_t> &row_ptr, int tile_nnz, int *max_row);
 
 struct SolveWork {
-  // FP64
   double *r64 = nullptr, *partial = nullptr;
-  // FP32 inner vectors
-  float *xf = nullptr, *rf = nullptr, *zf = nullptr, *pf = nullptr, *apf = nullptr;
-  double *pd = nullptr, *apd = nullptr, *zd = nullptr;  // FP64-mode vectors
+  double *rd = nullptr, *qd = nullptr;      // FP64-mode residual and A p
+  double2 *zpd0 = nullptr, *zpd1 = nullptr; // FP64-mode (z, p) pairs, double-buffered
+  float *rf = nullptr, *qf = nullptr;       // mixed-mode FP32 residual and A p
+  float2 *zpf0 = nullptr, *zpf1 = nullptr;  // mixed-mode (z, p) pairs
   unsigned int *barrier = nullptr;
-  int *control = nullptr;    // [0] error flag, [1] stop flag, ...
+  int *control = nullptr;    // [0] error status
   double *result = nullptr;  // device statistics block
   int grid = 0;
   int64_t n = 0;
 };
+
+// Matrix value/column arrays are allocated with this many padding entries so
+// that the SpMV's aligned 16-byte quads never read past the allocation.
+int matrix_padding();
 
 int solve_work_alloc(SolveWork &w, int64_t n, int grid);
 void solve_work_free(SolveWork &w);

@@ -1,22 +1,33 @@
 // Persistent Jacobi-PCG (sm_100a).
 //
 // One cooperative launch runs the whole solve.  CTAs own fixed row tiles of
-// the CSR matrix (the constrained CSC of a symmetric operator read as CSR);
-// each SpMV streams the CTA's tiles with coalesced loads into shared memory
-// and sums every row in a fixed order.  Dot products are reduced per CTA,
-// written to a per-phase partial buffer and summed by every CTA in the same
-// fixed order, so all CTAs take identical decisions and results are
-// bit-reproducible for a given grid.  Grid barriers spin with a bound and
+// the CSR matrix (the constrained CSC of a symmetric operator read as CSR).
+// Each SpMV streams the CTA's tiles with 16-byte loads into shared memory and
+// sums every row in a fixed order.  Dot products are reduced per CTA, written
+// to a per-phase partial buffer and summed by every CTA in the same fixed
+// order, so all CTAs take identical decisions and results are
+// bit-reproducible for a given grid.  Grid barriers spin with a time bound and
 // report FFG_TIMEOUT instead of hanging.
+//
+// Iteration (two grid barriers):
+//   A: p = z + beta p_old on the fly while gathering, q = A p, (p, q)
+//   B: x += alpha p (FP64), r -= alpha q, z = D^-1 r, (r, r), (r, z)
+// The (z, p) pair of every row is stored interleaved and double-buffered so
+// the gather of iteration k never races with the writes of iteration k+1.
 //
 // FP64 mode restates pcg_solve_operator / pcg_iteration_loop
 // (src/solvers/advanced_solvers.f90:831-925): stop when the recursive residual
-// ||r||_2 <= tol*||r_0||_2 (relative) or tol (absolute), or when
-// |p^T A p| < 1e-14; Jacobi z = D^-1 r with D^-1 = 1 where |a_ii| <= 1e-14.
-// Mixed mode: inner FP32 PCG on the scaled residual, outer FP64 iterative
-// refinement on the true residual b - A x until ||b - A x|| <= tol*||b||.
+// ||r||_2 <= tol*||r_0||_2 (relative) or tol (absolute), or at breakdown
+// (|p^T A p| < 1e-14 as the reference, or p^T A p <= 0 when selected);
+// Jacobi z = D^-1 r with D^-1 = 1 where |a_ii| <= 1e-14.
+// Mixed mode: the same CG recurrences in FP32 on a scaled residual with the
+// solution accumulated in FP64; whenever the FP32 residual has fallen by
+// `reliable_delta` (or claims convergence) the true FP64 residual b - A x
+// replaces it (reliable updates: the search direction is kept, rescaled), and
+// the solve ends when ||b - A x||_2 <= tol*||b||_2.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 
 #include "ffg_internal.h"
@@ -25,7 +36,7 @@ namespace ffg {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kTileNnz = 4096;
 constexpr int kSlots = 4;
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
@@ -43,14 +54,16 @@ struct PcgParams {
   const double *b;
   double *x;
   double *r64;
-  float *xf, *rf, *zf, *pf, *apf;
-  double *pd, *apd, *zd;
+  float *rf, *qf;
+  float2 *zpf0, *zpf1;
+  double *rd, *qd;
+  double2 *zpd0, *zpd1;
   double *partial;  // [2][kSlots][grid]
   unsigned int *bar;
   int *control;     // [0] error status
   double *result;   // 8 doubles
-  int precision, relative, max_it, max_ref, guard;
-  double tol, inner_tol;
+  int precision, relative, max_it, max_updates, guard;
+  double tol, delta;
   unsigned long long limit_ns;
 };
 
@@ -91,7 +104,7 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
         good = 0;
         break;
       }
-      __nanosleep(32);
+      __nanosleep(20);
     }
     __threadfence();
     ok = good && ld_volatile_int(P.control) == 0;
@@ -100,8 +113,7 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
   return ok != 0;
 }
 
-// CTA-wide sum of per-thread values for kSlots slots, written to the partial
-// buffer of this phase parity.
+// CTA-wide sums of nslot per-thread values into this phase's partial buffer.
 __device__ void write_partials(const PcgParams &P, unsigned int phase, const double *v, int nslot) {
   __shared__ double red[kSlots][kThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -138,21 +150,45 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __syncthreads();
 }
 
-// Tile SpMV: for every row r of this CTA's tiles, epi(r, sum_k A_rk x_k).
-template <typename VT, typename AT, typename XT, class Epi>
+template <typename T>
+struct Quad;
+template <>
+struct Quad<float> {
+  __device__ __forceinline__ static void load(const float *p, float v[4]) {
+    const float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  }
+};
+template <>
+struct Quad<double> {
+  __device__ __forceinline__ static void load(const double *p, double v[4]) {
+    const double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+};
+
+// Tile SpMV: for every row r of this CTA's tiles, epi(r, sum_k A_rk gather(c_k)).
+// Loads are 16-byte aligned quads of (value, column); entries outside the
+// tile are masked (the arrays are padded by one quad).
+template <typename VT, typename AT, class G, class Epi>
 __device__ __forceinline__ void spmv_tiles(const PcgParams &P, const VT *__restrict__ val,
-                                           const XT *x, AT *smem, Epi epi) {
+                                           AT *smem, G gather, Epi epi) {
   for (int t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
     const int r0 = P.tile_row[t], r1 = P.tile_row[t + 1];
-    const int64_t e0 = P.rp[r0];
-    const int E = (int)(P.rp[r1] - e0);
-    const VT *vv = val + e0;
-    const int *cc = P.col + e0;
-#pragma unroll 4
-    for (int k = threadIdx.x; k < E; k += kThreads) {
-      const VT a = __ldcs(vv + k);
-      const int c = __ldcs(cc + k);
-      smem[k] = (AT)a * (AT)x[c];
+    const int64_t e0 = P.rp[r0], e1 = P.rp[r1];
+    const int64_t a0 = e0 & ~(int64_t)3;
+#pragma unroll 2
+    for (int64_t k = a0 + 4 * threadIdx.x; k < e1; k += 4 * kThreads) {
+      VT v[4];
+      Quad<VT>::load(val + k, v);
+      const int4 c = __ldcs(reinterpret_cast<const int4 *>(P.col + k));
+      const int cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int64_t idx = k + i;
+        if (idx >= e0 && idx < e1) smem[idx - e0] = (AT)v[i] * gather(cc[i]);
+      }
     }
     __syncthreads();
     for (int r = r0 + threadIdx.x; r < r1; r += kThreads) {
@@ -175,182 +211,199 @@ __device__ __forceinline__ void for_rows(const PcgParams &P, F f) {
 
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
-__global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
-  __shared__ __align__(16) double smem_d[kTileNnz];
-  float *smem_f = reinterpret_cast<float *>(smem_d);
-  unsigned int phase = 0;
-  // only block 0 judges the wall limit; its verdict travels through a partial slot
-  const unsigned long long t_start = globaltimer();
-  double part[kSlots];
-  double red[kSlots];
-  int iterations = 0, refinements = 0, converged = 0, status = FFG_OK;
-  double final_res = 0.0, true_rel = 0.0;
+template <typename V>
+struct VecOf;
+template <>
+struct VecOf<float> {
+  using V2 = float2;
+};
+template <>
+struct VecOf<double> {
+  using V2 = double2;
+};
 
-  // ||b||
-  part[0] = 0.0;
-  for_rows(P, [&](int r) { const double v = P.b[r]; part[0] += v * v; });
-  write_partials(P, phase, part, 1);
+// The CG loop in value type V (float: mixed mode, double: FP64 mode).
+template <typename V>
+__device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
+                   unsigned long long t_start, double *res_out) {
+  using V2 = typename VecOf<V>::V2;
+  constexpr bool kMixed = sizeof(V) == 4;
+  V *smem = reinterpret_cast<V *>(smem_d);
+  const V *A = kMixed ? (const V *)P.v32 : (const V *)P.v64;
+  const V *dinv = kMixed ? (const V *)P.d32 : (const V *)P.d64;
+  V *r = kMixed ? (V *)P.rf : (V *)P.rd;
+  V *q = kMixed ? (V *)P.qf : (V *)P.qd;
+  V2 *zp[2] = {kMixed ? (V2 *)P.zpf0 : (V2 *)P.zpd0, kMixed ? (V2 *)P.zpf1 : (V2 *)P.zpd1};
+  double part[kSlots], red[kSlots];
+  int iterations = 0, updates = 0, converged = 0, status = FFG_OK;
+
+  // r64 = b - A x, ||r64||, ||b||
+  part[0] = part[1] = 0.0;
+  spmv_tiles<double, double>(P, P.v64, smem_d, [&](int c) { return P.x[c]; },
+                             [&](int row, double s) {
+                               const double bb = P.b[row];
+                               const double rr = bb - s;
+                               P.r64[row] = rr;
+                               part[0] += rr * rr;
+                               part[1] += bb * bb;
+                             });
+  write_partials(P, phase, part, 2);
   if (!grid_barrier(P, phase)) return;
-  read_partials(P, phase, red, 1);
-  const double bnorm = sqrt(red[0]);
-
-  if (P.precision == FFG_PRECISION_FP64) {
-    // r = b - A x ; z = D^-1 r ; p = z
-    part[0] = part[1] = part[2] = 0.0;
-    spmv_tiles<double, double, double>(P, P.v64, P.x, smem_d, [&](int r, double s) {
-      const double rr = P.b[r] - s;
-      const double z = P.d64[r] * rr;
-      P.r64[r] = rr;
-      P.zd[r] = z;
-      P.pd[r] = z;
-      part[0] += rr * rr;
-      part[1] += rr * z;
-    });
-    write_partials(P, phase, part, 2);
-    if (!grid_barrier(P, phase)) return;
-    read_partials(P, phase, red, 2);
-    const double initial = sqrt(red[0]);
-    double res = initial, rz_old = red[1];
-    const double tol = P.relative ? P.tol * initial : P.tol;
-    for (int it = 1; it <= P.max_it; ++it) {
-      part[0] = 0.0;
-      spmv_tiles<double, double, double>(P, P.v64, P.pd, smem_d, [&](int r, double s) {
-        P.apd[r] = s;
-        part[0] += P.pd[r] * s;
-      });
-      write_partials(P, phase, part, 1);
-      if (!grid_barrier(P, phase)) return;
-      read_partials(P, phase, red, 1);
-      const double pAp = red[0];
-      if (P.guard == 0 ? fabs(pAp) < 1.0e-14 : !(pAp > 0.0 && is_finite_d(pAp))) break;
-      const double alpha = rz_old / pAp;
-      part[0] = part[1] = 0.0;
-      part[2] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
-      for_rows(P, [&](int r) {
-        P.x[r] = P.x[r] + alpha * P.pd[r];
-        const double rr = P.r64[r] - alpha * P.apd[r];
-        P.r64[r] = rr;
-        const double z = P.d64[r] * rr;
-        P.zd[r] = z;
-        part[0] += rr * rr;
-        part[1] += rr * z;
-      });
-      write_partials(P, phase, part, 3);
-      if (!grid_barrier(P, phase)) return;
-      read_partials(P, phase, red, 3);
-      res = sqrt(red[0]);
-      iterations = it;
-      if (res <= tol) { converged = 1; break; }
-      if (red[2] != 0.0) { status = FFG_TIMEOUT; break; }
-      const double beta = red[1] / rz_old;
-      rz_old = red[1];
-      for_rows(P, [&](int r) { P.pd[r] = P.zd[r] + beta * P.pd[r]; });
-      if (!grid_barrier(P, phase)) return;
-    }
-    if (!converged && res <= tol) converged = 1;
-    final_res = res;
-  } else {
-    // mixed precision: outer FP64 refinement, inner FP32 PCG
-    const double target = P.relative ? P.tol * bnorm : P.tol;
-    int total_it = 0;
-    double rnorm = 0.0;
-    for (int outer = 0;; ++outer) {
-      part[0] = 0.0;
-      spmv_tiles<double, double, double>(P, P.v64, P.x, smem_d, [&](int r, double s) {
-        const double rr = P.b[r] - s;
-        P.r64[r] = rr;
-        part[0] += rr * rr;
-      });
-      part[1] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
-      write_partials(P, phase, part, 2);
-      if (!grid_barrier(P, phase)) return;
-      read_partials(P, phase, red, 2);
-      rnorm = sqrt(red[0]);
-      final_res = rnorm;
-      if (rnorm <= target) { converged = 1; break; }
-      if (outer >= P.max_ref || total_it >= P.max_it) break;
-      if (red[1] != 0.0) { status = FFG_TIMEOUT; break; }
-      if (!is_finite_d(rnorm)) break;
-      const double scale = 1.0 / rnorm;
-      part[0] = part[1] = 0.0;
-      for_rows(P, [&](int r) {
-        const float rr = (float)(P.r64[r] * scale);
-        const float z = P.d32[r] * rr;
-        P.rf[r] = rr;
-        P.xf[r] = 0.0f;
-        P.zf[r] = z;
-        P.pf[r] = z;
-        part[0] += (double)rr * (double)z;
-        part[1] += (double)rr * (double)rr;
-      });
-      write_partials(P, phase, part, 2);
-      if (!grid_barrier(P, phase)) return;
-      read_partials(P, phase, red, 2);
-      double rz = red[0];
-      const double rr0 = red[1];
-      const double inner_target = P.inner_tol * P.inner_tol * rr0;
-      while (total_it < P.max_it) {
-        part[0] = 0.0;
-        spmv_tiles<float, float, float>(P, P.v32, P.pf, smem_f, [&](int r, float s) {
-          P.apf[r] = s;
-          part[0] += (double)P.pf[r] * (double)s;
-        });
-        write_partials(P, phase, part, 1);
-        if (!grid_barrier(P, phase)) return;
-        read_partials(P, phase, red, 1);
-        const double pAp = red[0];
-        if (!(pAp > 0.0) || !is_finite_d(pAp)) break;
-        const float alpha = (float)(rz / pAp);
-        part[0] = part[1] = 0.0;
-        part[2] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
-        for_rows(P, [&](int r) {
-          P.xf[r] = P.xf[r] + alpha * P.pf[r];
-          const float rr = P.rf[r] - alpha * P.apf[r];
-          P.rf[r] = rr;
-          const float z = P.d32[r] * rr;
-          P.zf[r] = z;
-          part[0] += (double)rr * (double)z;
-          part[1] += (double)rr * (double)rr;
-        });
-        write_partials(P, phase, part, 3);
-        if (!grid_barrier(P, phase)) return;
-        read_partials(P, phase, red, 3);
-        ++total_it;
-        if (red[1] <= inner_target || red[2] != 0.0) break;
-        const float beta = (float)(red[0] / rz);
-        rz = red[0];
-        for_rows(P, [&](int r) { P.pf[r] = P.zf[r] + beta * P.pf[r]; });
-        if (!grid_barrier(P, phase)) return;
-      }
-      for_rows(P, [&](int r) { P.x[r] = P.x[r] + rnorm * (double)P.xf[r]; });
-      if (!grid_barrier(P, phase)) return;
-      refinements = outer + 1;
-    }
-    iterations = total_it;
-    true_rel = bnorm > 0.0 ? rnorm / bnorm : rnorm;
-  }
-
-  if (P.precision == FFG_PRECISION_FP64) {
-    // true FP64 residual of the returned x
+  read_partials(P, phase, red, 2);
+  const double bnorm = sqrt(red[1]);
+  const double rnorm = sqrt(red[0]);
+  double scale = kMixed ? (rnorm > 0.0 ? rnorm : 1.0) : 1.0;
+  const double target = P.relative ? P.tol * (kMixed ? bnorm : rnorm) : P.tol;
+  double true_res = rnorm;
+  if (rnorm <= target) converged = 1;
+  double rz = 0.0;
+  if (!converged) {
+    const double inv = 1.0 / scale;
     part[0] = 0.0;
-    spmv_tiles<double, double, double>(P, P.v64, P.x, smem_d, [&](int r, double s) {
-      const double rr = P.b[r] - s;
-      part[0] += rr * rr;
+    for_rows(P, [&](int row) {
+      const V rr = (V)(P.r64[row] * inv);
+      const V z = dinv[row] * rr;
+      r[row] = rr;
+      zp[0][row] = V2{z, (V)0};
+      part[0] += (double)rr * (double)z;
     });
     write_partials(P, phase, part, 1);
     if (!grid_barrier(P, phase)) return;
     read_partials(P, phase, red, 1);
-    true_rel = bnorm > 0.0 ? sqrt(red[0]) / bnorm : sqrt(red[0]);
+    rz = red[0];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    P.result[0] = converged;
-    P.result[1] = iterations;
-    P.result[2] = refinements;
-    P.result[3] = final_res;
-    P.result[4] = true_rel;
-    P.result[5] = status;
-    P.result[6] = bnorm;
+  double beta = 0.0, rr_last = 1.0;
+  int cur = 0;
+  for (int it = 1; !converged && it <= P.max_it; ++it) {
+    const V2 *zc = zp[cur];
+    V2 *zn = zp[cur ^ 1];
+    const V bt = (V)beta;
+    // A: p = z + beta p_old, q = A p, (p, q)
+    part[0] = 0.0;
+    spmv_tiles<V, V>(P, A, smem,
+                     [&](int c) {
+                       const V2 a = zc[c];
+                       return a.x + bt * a.y;
+                     },
+                     [&](int row, V s) {
+                       const V2 a = zc[row];
+                       const V pn = a.x + bt * a.y;
+                       zn[row].y = pn;
+                       q[row] = s;
+                       part[0] += (double)pn * (double)s;
+                     });
+    write_partials(P, phase, part, 1);
+    if (!grid_barrier(P, phase)) return;
+    read_partials(P, phase, red, 1);
+    const double pAp = red[0];
+    const bool breakdown = (!kMixed && P.guard == 0) ? (fabs(pAp) < 1.0e-14)
+                                                      : !(pAp > 0.0 && is_finite_d(pAp));
+    if (breakdown) break;
+    const double alpha = rz / pAp;
+    const V al = (V)alpha;
+    const double xs = alpha * scale;
+    // B: x += alpha p (FP64), r -= alpha q, z = D^-1 r
+    part[0] = part[1] = 0.0;
+    part[2] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
+    for_rows(P, [&](int row) {
+      const V pn = zn[row].y;
+      P.x[row] = P.x[row] + xs * (double)pn;
+      const V rr = r[row] - al * q[row];
+      r[row] = rr;
+      const V z = dinv[row] * rr;
+      zn[row].x = z;
+      part[0] += (double)rr * (double)rr;
+      part[1] += (double)rr * (double)z;
+    });
+    write_partials(P, phase, part, 3);
+    if (!grid_barrier(P, phase)) return;
+    read_partials(P, phase, red, 3);
+    iterations = it;
+    double rr = red[0], rz_new = red[1];
+    const double est = sqrt(rr) * scale;
+    if (red[2] != 0.0) { status = FFG_TIMEOUT; true_res = est; break; }
+    if (!kMixed) {
+      true_res = est;
+      if (est <= target) { converged = 1; break; }
+    } else if (est <= target || rr <= P.delta * P.delta * rr_last) {
+      // reliable update: replace the recursive residual with b - A x in FP64
+      if (updates >= P.max_updates) break;
+      ++updates;
+      part[0] = 0.0;
+      spmv_tiles<double, double>(P, P.v64, smem_d, [&](int c) { return P.x[c]; },
+                                 [&](int row, double s) {
+                                   const double v = P.b[row] - s;
+                                   P.r64[row] = v;
+                                   part[0] += v * v;
+                                 });
+      write_partials(P, phase, part, 1);
+      if (!grid_barrier(P, phase)) return;
+      read_partials(P, phase, red, 1);
+      true_res = sqrt(red[0]);
+      if (true_res <= target) { converged = 1; break; }
+      if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
+      const double ratio = scale / true_res;  // old units -> new units
+      const V rt = (V)ratio;
+      const double inv = 1.0 / true_res;
+      part[0] = 0.0;
+      for_rows(P, [&](int row) {
+        const V rr2 = (V)(P.r64[row] * inv);
+        r[row] = rr2;
+        const V z = dinv[row] * rr2;
+        V2 a = zn[row];
+        a.x = z;
+        a.y = a.y * rt;
+        zn[row] = a;
+        part[0] += (double)rr2 * (double)z;
+      });
+      write_partials(P, phase, part, 1);
+      if (!grid_barrier(P, phase)) return;
+      read_partials(P, phase, red, 1);
+      rz = rz * ratio * ratio;
+      rz_new = red[0];
+      scale = true_res;
+      rr_last = 1.0;
+    }
+    beta = rz_new / rz;
+    rz = rz_new;
+    cur ^= 1;
   }
+  if (!kMixed || !converged) {
+    // true FP64 residual of the returned x
+    part[0] = 0.0;
+    spmv_tiles<double, double>(P, P.v64, smem_d, [&](int c) { return P.x[c]; },
+                               [&](int row, double s) {
+                                 const double v = P.b[row] - s;
+                                 part[0] += v * v;
+                               });
+    write_partials(P, phase, part, 1);
+    if (!grid_barrier(P, phase)) return;
+    read_partials(P, phase, red, 1);
+    res_out[3] = kMixed ? sqrt(red[0]) : true_res;  // FP64 mode: recursive residual
+    res_out[4] = bnorm > 0.0 ? sqrt(red[0]) / bnorm : sqrt(red[0]);
+  } else {
+    res_out[3] = true_res;
+    res_out[4] = bnorm > 0.0 ? true_res / bnorm : true_res;
+  }
+  res_out[0] = converged;
+  res_out[1] = iterations;
+  res_out[2] = updates;
+  res_out[5] = status;
+  res_out[6] = bnorm;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
+  __shared__ __align__(16) double smem_d[kTileNnz];
+  unsigned int phase = 0;
+  // only block 0 judges the wall limit; its verdict travels through a partial slot
+  const unsigned long long t_start = globaltimer();
+  double res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (P.precision == FFG_PRECISION_FP64)
+    cg<double>(P, smem_d, phase, t_start, res);
+  else
+    cg<float>(P, smem_d, phase, t_start, res);
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int i = 0; i < 7; ++i) P.result[i] = res[i];
 }
 
 // Standalone FP64 tile SpMV (one CTA per tile).
@@ -376,6 +429,9 @@ __global__ void __launch_bounds__(kThreads) spmv64_kernel(int64_t n, const int64
 
 }  // namespace
 
+int tile_capacity() { return kTileNnz; }
+int matrix_padding() { return 8; }
+
 int pcg_grid_size(int *grid) {
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FFG_CUDA_ERROR;
@@ -385,7 +441,7 @@ int pcg_grid_size(int *grid) {
       cudaSuccess)
     return FFG_CUDA_ERROR;
   if (per_sm < 1) return FFG_CUDA_ERROR;
-  *grid = sms * per_sm;
+  *grid = sms * std::min(per_sm, 2);
   return FFG_OK;
 }
 
@@ -394,21 +450,24 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
   w.n = n;
   w.grid = grid;
   const size_t N = (size_t)std::max<int64_t>(n, 1);
-  cudaError_t e = cudaSuccess;
-  e = (cudaError_t)(e | cudaMalloc(&w.r64, N * sizeof(double)));
-  e = (cudaError_t)(e | cudaMalloc(&w.pd, N * sizeof(double)));
-  e = (cudaError_t)(e | cudaMalloc(&w.apd, N * sizeof(double)));
-  e = (cudaError_t)(e | cudaMalloc(&w.zd, N * sizeof(double)));
-  e = (cudaError_t)(e | cudaMalloc(&w.xf, N * sizeof(float)));
-  e = (cudaError_t)(e | cudaMalloc(&w.rf, N * sizeof(float)));
-  e = (cudaError_t)(e | cudaMalloc(&w.zf, N * sizeof(float)));
-  e = (cudaError_t)(e | cudaMalloc(&w.pf, N * sizeof(float)));
-  e = (cudaError_t)(e | cudaMalloc(&w.apf, N * sizeof(float)));
-  e = (cudaError_t)(e | cudaMalloc(&w.partial, 2 * kSlots * (size_t)grid * sizeof(double)));
-  e = (cudaError_t)(e | cudaMalloc(&w.barrier, 64));
-  e = (cudaError_t)(e | cudaMalloc(&w.control, 64));
-  e = (cudaError_t)(e | cudaMalloc(&w.result, 8 * sizeof(double)));
-  if (e != cudaSuccess) {
+  bool bad = false;
+  auto A = [&](void **p, size_t bytes) {
+    if (cudaMalloc(p, bytes) != cudaSuccess) { bad = true; *p = nullptr; }
+  };
+  A((void **)&w.r64, N * sizeof(double));
+  A((void **)&w.rd, N * sizeof(double));
+  A((void **)&w.qd, N * sizeof(double));
+  A((void **)&w.zpd0, N * sizeof(double2));
+  A((void **)&w.zpd1, N * sizeof(double2));
+  A((void **)&w.rf, N * sizeof(float));
+  A((void **)&w.qf, N * sizeof(float));
+  A((void **)&w.zpf0, N * sizeof(float2));
+  A((void **)&w.zpf1, N * sizeof(float2));
+  A((void **)&w.partial, 2 * kSlots * (size_t)grid * sizeof(double));
+  A((void **)&w.barrier, 64);
+  A((void **)&w.control, 64);
+  A((void **)&w.result, 8 * sizeof(double));
+  if (bad) {
     solve_work_free(w);
     cudaGetLastError();
     return FFG_OUT_OF_MEMORY;
@@ -417,7 +476,7 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
 }
 
 void solve_work_free(SolveWork &w) {
-  void *ptrs[] = {w.r64, w.pd, w.apd, w.zd, w.xf, w.rf, w.zf, w.pf, w.apf, w.partial,
+  void *ptrs[] = {w.r64, w.rd, w.qd, w.zpd0, w.zpd1, w.rf, w.qf, w.zpf0, w.zpf1, w.partial,
                   w.barrier, w.control, w.result};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -440,8 +499,8 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
   P.b = b;
   P.x = x;
   P.r64 = w.r64;
-  P.xf = w.xf; P.rf = w.rf; P.zf = w.zf; P.pf = w.pf; P.apf = w.apf;
-  P.pd = w.pd; P.apd = w.apd; P.zd = w.zd;
+  P.rf = w.rf; P.qf = w.qf; P.zpf0 = w.zpf0; P.zpf1 = w.zpf1;
+  P.rd = w.rd; P.qd = w.qd; P.zpd0 = w.zpd0; P.zpd1 = w.zpd1;
   P.partial = w.partial;
   P.bar = w.barrier;
   P.control = w.control;
@@ -449,19 +508,20 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
   P.precision = opts.precision;
   P.relative = opts.tolerance_type == 0;
   P.max_it = opts.max_iterations;
-  P.max_ref = opts.max_refinements;
+  P.max_updates = opts.max_refinements;
   P.tol = opts.tolerance;
-  P.inner_tol = opts.inner_tolerance;
+  P.delta = opts.inner_tolerance;
   P.guard = opts.breakdown_guard;
   const double limit = opts.timeout_seconds > 0 ? opts.timeout_seconds : 60.0;
   P.limit_ns = (unsigned long long)(limit * 1e9);
   if (cudaMemsetAsync(w.barrier, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaMemsetAsync(w.control, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   void *args[] = {&P};
-  cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid), dim3(kThreads),
-                                              args, 0, stream);
+  cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid),
+                                              dim3(kThreads), args, 0, stream);
   if (e != cudaSuccess) {
     msg = std::string("cooperative launch failed: ") + cudaGetErrorString(e);
+    cudaGetLastError();
     return FFG_CUDA_ERROR;
   }
   double res[8];
@@ -494,7 +554,5 @@ int spmv64(const DeviceCsr &A, const double *x, double *y, cudaStream_t stream) 
                                                     A.n_tiles, x, y);
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
-
-int tile_capacity() { return kTileNnz; }
 
 }  // namespace ffg

@@ -59,7 +59,8 @@ extern "C" {
 
 /* Solver precision. */
 #define FFG_PRECISION_FP64 0  /* FP64 Jacobi-PCG with the reference's stopping rule */
-#define FFG_PRECISION_MIXED 1 /* FP32 inner PCG under FP64 iterative refinement */
+#define FFG_PRECISION_MIXED 1 /* FP32 PCG recurrences, FP64 solution and reliable
+                                 FP64 residual updates (defect correction) */
 
 #define FFG_OPTIONS_VERSION 1
 
@@ -72,8 +73,10 @@ typedef struct {
   double tolerance;      /* FP64 mode: on the recursive residual as the reference;
                             mixed mode: on the true FP64 residual ||b-Ax|| (relative to ||b||) */
   int max_iterations;    /* cap on (inner) PCG iterations in total */
-  int max_refinements;   /* mixed mode: outer refinement steps */
-  double inner_tolerance;/* mixed mode: relative residual reduction per inner solve */
+  int max_refinements;   /* mixed mode: cap on reliable updates (FP64 residual replacements) */
+  double inner_tolerance;/* mixed mode: a reliable update replaces the FP32 recursive
+                            residual by b - A x (FP64) whenever it has fallen by this
+                            factor since the previous update (default 0.1) */
   int verbosity;         /* > 0 prints per-solve statistics on the host */
   double timeout_seconds;/* device-side wall limit of one solve; <= 0 selects 60 s */
   int breakdown_guard;   /* FP64 mode: 0 = the reference's |p^T A p| < 1e-14 test
@@ -84,7 +87,7 @@ typedef struct {
 typedef struct {
   int converged;
   int iterations;              /* PCG iterations (inner iterations summed in mixed mode) */
-  int refinements;             /* outer FP64 refinement steps (mixed mode) */
+  int refinements;             /* reliable updates performed (mixed mode) */
   int status;                  /* FFG_* of the solve */
   double final_residual;       /* reference meaning: recursive residual 2-norm */
   double true_relative_residual; /* ||b - A x||_2 / ||b||_2 in FP64 at exit */
