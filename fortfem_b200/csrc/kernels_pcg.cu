@@ -39,6 +39,7 @@ namespace {
 constexpr int kThreads = 512;
 constexpr int kTileNnz = 4096;
 constexpr int kSlots = 4;
+constexpr int kPartialBatch = 8;   // partial loads in flight per lane
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
 
 struct PcgParams {
@@ -132,70 +133,156 @@ __device__ void write_partials(const PcgParams &P, unsigned int phase, const dou
 }
 
 // Sum the partials of the phase that just completed (identical on every CTA).
+// Warp s reduces slot s; its loads are issued before the adds so they overlap,
+// and the summation order is fixed (lane-strided, then a butterfly), so every
+// CTA obtains the same bits.
 __device__ void read_partials(const PcgParams &P, unsigned int phase, double *out, int nslot) {
   __shared__ double res[kSlots];
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    for (int s = 0; s < nslot; ++s) {
-      const double *src = P.partial + ((size_t)(phase & 1) * kSlots + s) * gridDim.x;
-      double x = 0.0;
-      for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(src + b);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp < nslot) {
+    const int G = (int)gridDim.x;
+    const double *src = P.partial + ((size_t)(phase & 1) * kSlots + warp) * G;
+    double acc = 0.0;
+    for (int b0 = 0; b0 < G; b0 += 32 * kPartialBatch) {
+      double v[kPartialBatch];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      if (lane == 0) res[s] = x;
+      for (int j = 0; j < kPartialBatch; ++j) {
+        const int b = b0 + lane + 32 * j;
+        v[j] = b < G ? __ldcg(src + b) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < kPartialBatch; ++j) acc += v[j];
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) res[warp] = acc;
   }
   __syncthreads();
   for (int s = 0; s < nslot; ++s) out[s] = res[s];
   __syncthreads();
 }
 
-template <typename T>
-struct Quad;
-template <>
-struct Quad<float> {
-  __device__ __forceinline__ static void load(const float *p, float v[4]) {
-    const float4 a = __ldcs(reinterpret_cast<const float4 *>(p));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-  }
+// ---------------------------------------------------------------- tile staging
+// The (column, value) stream of a tile is copied global -> shared by the bulk
+// async-copy engine (cp.async.bulk, completion on an mbarrier), double
+// buffered so that the next tile streams while the current one is gathered
+// and summed.  Ranges are widened to 16-byte boundaries (the matrix arrays are
+// padded) and the extra entries are ignored.
+constexpr int kTileCap = kTileNnz + 8;
+struct __align__(16) TileBuf {
+  int col[kTileCap];
+  double val[kTileCap];  // FP32 tiles use the first half as float[]
 };
-template <>
-struct Quad<double> {
-  __device__ __forceinline__ static void load(const double *p, double v[4]) {
-    const double2 a = __ldcs(reinterpret_cast<const double2 *>(p));
-    const double2 b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
-    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-  }
+struct StageSmem {
+  TileBuf buf[2];
+  unsigned long long mbar[2];
 };
 
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *m) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(m)) : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          unsigned long long *m) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(m))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(unsigned long long *m, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait on an mbarrier phase; returns false (and flags the solve) if
+// the copy did not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *m, unsigned parity, int *control) {
+  const unsigned a = smem_addr(m);
+  for (unsigned spin = 0; spin < (1u << 26); ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  atomicCAS(control, 0, FFG_TIMEOUT);
+  return false;
+}
+
+template <typename VT>
+__device__ __forceinline__ void issue_tile(const PcgParams &P, const VT *val, int t, TileBuf &b,
+                                           unsigned long long *m) {
+  const int r0 = P.tile_row[t], r1 = P.tile_row[t + 1];
+  const int64_t a0 = P.rp[r0] & ~(int64_t)3;
+  const int64_t a1 = (P.rp[r1] + 3) & ~(int64_t)3;
+  const unsigned n = (unsigned)(a1 - a0);
+  const unsigned cb = n * 4u, vb = n * (unsigned)sizeof(VT);
+  mbar_expect(m, cb + vb);
+  bulk_load(b.col, P.col + a0, cb, m);
+  bulk_load(b.val, val + a0, vb, m);
+}
+
 // Tile SpMV: for every row r of this CTA's tiles, epi(r, sum_k A_rk gather(c_k)).
-// Loads are 16-byte aligned quads of (value, column); entries outside the
-// tile are masked (the arrays are padded by one quad).
+// Rows are summed by groups of 4 lanes in a fixed order (lane-strided partial
+// sums, then a butterfly); lane 0 of the group applies the epilogue.
 template <typename VT, typename AT, class G, class Epi>
 __device__ __forceinline__ void spmv_tiles(const PcgParams &P, const VT *__restrict__ val,
-                                           AT *smem, G gather, Epi epi) {
-  for (int t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
+                                           StageSmem &S, unsigned &parity_bits, G gather,
+                                           Epi epi) {
+  const int first = blockIdx.x;
+  if (first >= P.n_tiles) return;
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    issue_tile<VT>(P, val, first, S.buf[0], &S.mbar[0]);
+  }
+  int slot = 0;
+  for (int t = first; t < P.n_tiles; t += gridDim.x, slot ^= 1) {
+    const int nt = t + gridDim.x;
+    if (threadIdx.x == 0 && nt < P.n_tiles) {
+      // the other buffer was last read before the trailing __syncthreads of the
+      // previous tile; order those generic accesses before the async copy
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue_tile<VT>(P, val, nt, S.buf[slot ^ 1], &S.mbar[slot ^ 1]);
+    }
+    TileBuf &B = S.buf[slot];
+    const bool arrived = mbar_wait(&S.mbar[slot], (parity_bits >> slot) & 1u, P.control);
+    parity_bits ^= (1u << slot);
+    // a copy that never completed leaves the buffer undefined: its column
+    // indices are not dereferenced (the solve already reports FFG_TIMEOUT)
+    if (!__syncthreads_and(arrived)) continue;
     const int r0 = P.tile_row[t], r1 = P.tile_row[t + 1];
     const int64_t e0 = P.rp[r0], e1 = P.rp[r1];
     const int64_t a0 = e0 & ~(int64_t)3;
-#pragma unroll 2
-    for (int64_t k = a0 + 4 * threadIdx.x; k < e1; k += 4 * kThreads) {
-      VT v[4];
-      Quad<VT>::load(val + k, v);
-      const int4 c = __ldcs(reinterpret_cast<const int4 *>(P.col + k));
-      const int cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int64_t idx = k + i;
-        if (idx >= e0 && idx < e1) smem[idx - e0] = (AT)v[i] * gather(cc[i]);
-      }
+    const int lo = (int)(e0 - a0), hi = (int)(e1 - a0);
+    const VT *sv = reinterpret_cast<const VT *>(B.val);
+    AT *prod = reinterpret_cast<AT *>(B.val);
+#pragma unroll 4
+    for (int k = lo + threadIdx.x; k < hi; k += kThreads) {
+      const AT a = (AT)sv[k];
+      prod[k] = a * gather(B.col[k]);
     }
     __syncthreads();
-    for (int r = r0 + threadIdx.x; r < r1; r += kThreads) {
-      const int k0 = (int)(P.rp[r] - e0), k1 = (int)(P.rp[r + 1] - e0);
+    const int g = threadIdx.x >> 2, j = threadIdx.x & 3;
+    for (int base = r0; base < r1; base += kThreads / 4) {
+      const int row = base + g;
       AT s = 0;
-      for (int k = k0; k < k1; ++k) s += smem[k];
-      epi(r, s);
+      if (row < r1) {
+        const int k0 = (int)(P.rp[row] - a0), k1 = (int)(P.rp[row + 1] - a0);
+        for (int k = k0 + j; k < k1; k += 4) s += prod[k];
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      if (row < r1 && j == 0) epi(row, s);
     }
     __syncthreads();
   }
@@ -224,11 +311,11 @@ struct VecOf<double> {
 
 // The CG loop in value type V (float: mixed mode, double: FP64 mode).
 template <typename V>
-__device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
+__device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
                    unsigned long long t_start, double *res_out) {
   using V2 = typename VecOf<V>::V2;
   constexpr bool kMixed = sizeof(V) == 4;
-  V *smem = reinterpret_cast<V *>(smem_d);
+  unsigned parity_bits = 0;
   const V *A = kMixed ? (const V *)P.v32 : (const V *)P.v64;
   const V *dinv = kMixed ? (const V *)P.d32 : (const V *)P.d64;
   V *r = kMixed ? (V *)P.rf : (V *)P.rd;
@@ -239,7 +326,7 @@ __device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
 
   // r64 = b - A x, ||r64||, ||b||
   part[0] = part[1] = 0.0;
-  spmv_tiles<double, double>(P, P.v64, smem_d, [&](int c) { return P.x[c]; },
+  spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
                              [&](int row, double s) {
                                const double bb = P.b[row];
                                const double rr = bb - s;
@@ -280,7 +367,7 @@ __device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
     const V bt = (V)beta;
     // A: p = z + beta p_old, q = A p, (p, q)
     part[0] = 0.0;
-    spmv_tiles<V, V>(P, A, smem,
+    spmv_tiles<V, V>(P, A, S, parity_bits,
                      [&](int c) {
                        const V2 a = zc[c];
                        return a.x + bt * a.y;
@@ -330,7 +417,7 @@ __device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
       if (updates >= P.max_updates) break;
       ++updates;
       part[0] = 0.0;
-      spmv_tiles<double, double>(P, P.v64, smem_d, [&](int c) { return P.x[c]; },
+      spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
                                  [&](int row, double s) {
                                    const double v = P.b[row] - s;
                                    P.r64[row] = v;
@@ -371,7 +458,7 @@ __device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
   if (!kMixed || !converged) {
     // true FP64 residual of the returned x
     part[0] = 0.0;
-    spmv_tiles<double, double>(P, P.v64, smem_d, [&](int c) { return P.x[c]; },
+    spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
                                [&](int row, double s) {
                                  const double v = P.b[row] - s;
                                  part[0] += v * v;
@@ -393,15 +480,22 @@ __device__ void cg(const PcgParams &P, double *smem_d, unsigned int &phase,
 }
 
 __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
-  __shared__ __align__(16) double smem_d[kTileNnz];
+  extern __shared__ __align__(128) unsigned char dyn[];
+  StageSmem &S = *reinterpret_cast<StageSmem *>(dyn);
+  if (threadIdx.x == 0) {
+    mbar_init(&S.mbar[0]);
+    mbar_init(&S.mbar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
   unsigned int phase = 0;
   // only block 0 judges the wall limit; its verdict travels through a partial slot
   const unsigned long long t_start = globaltimer();
   double res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (P.precision == FFG_PRECISION_FP64)
-    cg<double>(P, smem_d, phase, t_start, res);
+    cg<double>(P, S, phase, t_start, res);
   else
-    cg<float>(P, smem_d, phase, t_start, res);
+    cg<float>(P, S, phase, t_start, res);
   if (blockIdx.x == 0 && threadIdx.x == 0)
     for (int i = 0; i < 7; ++i) P.result[i] = res[i];
 }
@@ -437,8 +531,11 @@ int pcg_grid_size(int *grid) {
   if (cudaGetDevice(&dev) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return FFG_CUDA_ERROR;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, kThreads, 0) !=
-      cudaSuccess)
+  if (cudaFuncSetAttribute(pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(StageSmem)) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, kThreads,
+                                                    sizeof(StageSmem)) != cudaSuccess)
     return FFG_CUDA_ERROR;
   if (per_sm < 1) return FFG_CUDA_ERROR;
   *grid = sms * std::min(per_sm, 2);
@@ -518,7 +615,7 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
   if (cudaMemsetAsync(w.control, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   void *args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid),
-                                              dim3(kThreads), args, 0, stream);
+                                              dim3(kThreads), args, sizeof(StageSmem), stream);
   if (e != cudaSuccess) {
     msg = std::string("cooperative launch failed: ") + cudaGetErrorString(e);
     cudaGetLastError();
