@@ -271,6 +271,7 @@ def run_ours(args):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     converged = all(s.converged and s.true_relative_residual <= TOL for s in stats)
+    phases = prob.phase_times()
     value = world * prob.n_dofs * args.steps / (ms * 1e-3)
 
     # roofline of the persistent PCG kernel (algorithmic bytes / kernel time)
@@ -305,6 +306,7 @@ def run_ours(args):
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "assembly_ms": float(np.mean([s.assembly_time for s in stats])) * 1e3,
             "setup_seconds": setup_s, "roofline": roofline, "clocks": clk,
+            "pcg_phase_ms": {k: (v * 1e3 if not isinstance(v, bool) else v) for k, v in phases.items()},
             "gpu_launches": 4 * args.steps}
 
     # plain FP64 GPU path (same kernels, FP64 values and vectors, no refinement)

@@ -92,6 +92,7 @@ SIGNATURES = {
                C.POINTER(SolverStatsC), i32, vp, pi32]),
     "ffg_problem_reduced_system": (
         None, [i32, vp, f64, f64, vp, vp, vp, vp, i64, pi64, vp, vp, vp, vp, vp, pi32]),
+    "ffg_problem_phase_times": (None, [i32, vp, pi32]),
     "ffg_problem_free": (None, [i32, pi32]),
 }
 

@@ -491,6 +491,16 @@ class Problem:
             raise FortfemError(st.value, "ffg_problem_solve")
         return SolverStats.from_c(sc)
 
+    def phase_times(self) -> dict:
+        """Device-side phase profile of the last solve (seconds, CTA 0's view)."""
+        out = np.zeros(6)
+        st = C.c_int(0)
+        K.load().ffg_problem_phase_times(self.handle, _ptr(out), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_phase_times")
+        return {"fp64_continuation": bool(out[0]), "spmv": out[1], "spmv_barrier": out[2],
+                "vector": out[3], "vector_barrier": out[4], "residual_replacement": out[5]}
+
     def reduced_system(self, vertices, coef_a=1.0, coef_b=0.0, cell_a=None, cell_b=None,
                        samples=None, constrained_values=None):
         """The constrained (free x free) CSC, its lifted right-hand side and the free DoFs."""

@@ -504,6 +504,14 @@ void ffg_problem_create(int family, int degree, int n_vertices, int n_cells, con
   *status = FFG_OK;
 }
 
+void ffg_problem_phase_times(int handle, double *seconds, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (!seconds) { *status = FFG_INVALID_INPUT; return; }
+  for (int i = 0; i < 6; ++i) seconds[i] = P->work.phase_seconds[i];
+  *status = FFG_OK;
+}
+
 void ffg_problem_free(int handle, int *status) {
   std::lock_guard<std::mutex> lock(g_mutex);
   auto it = g_problems.find(handle);

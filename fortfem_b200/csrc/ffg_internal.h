@@ -117,6 +117,9 @@ struct SolveWork {
   double *result = nullptr;  // device statistics block
   int grid = 0;
   int64_t n = 0;
+  // last solve: [0] FP64 continuation taken, then device seconds seen by CTA 0
+  // in SpMV work, barrier wait after it, vector work, wait, reliable updates
+  double phase_seconds[6] = {0, 0, 0, 0, 0, 0};
 };
 
 // Matrix value/column arrays are allocated with this many padding entries so

@@ -40,6 +40,7 @@ constexpr int kThreads = 512;
 constexpr int kTileNnz = 4096;
 constexpr int kSlots = 4;
 constexpr int kPartialBatch = 8;   // partial loads in flight per lane
+constexpr int kResultDoubles = 16;
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
 
 struct PcgParams {
@@ -186,12 +187,16 @@ __device__ __forceinline__ void mbar_init(unsigned long long *m) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(m)) : "memory");
 }
 
+// The matrix is streamed once per SpMV: evict it first from L2 so that the
+// solver vectors (a few MB, reused every phase) stay resident.
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
                                           unsigned long long *m) {
+  unsigned long long policy;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
           smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(m))
+      "l"(src), "r"(bytes), "r"(smem_addr(m)), "l"(policy)
       : "memory");
 }
 
@@ -309,22 +314,41 @@ struct VecOf<double> {
   using V2 = double2;
 };
 
+struct Outcome {
+  int iterations = 0, updates = 0, converged = 0, status = FFG_OK, stagnated = 0, aborted = 0;
+  double true_res = 0.0, final_res = 0.0, bnorm = 0.0;
+};
+
+// Device time of the phases seen by CTA 0 (the others are symmetric):
+// SpMV work, wait at the following barrier, vector work, wait, and the
+// reliable-update phases.
+struct Timing {
+  unsigned long long a = 0, aw = 0, b = 0, bw = 0, u = 0;
+};
+
+__device__ __forceinline__ unsigned long long stamp() {
+  return (blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer() : 0ull;
+}
+
 // The CG loop in value type V (float: mixed mode, double: FP64 mode).
+// `continuation` runs the FP64 loop after a stagnated mixed solve: its target
+// is the true residual tol*||b|| and its guard is the SPD one.
 template <typename V>
-__device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
-                   unsigned long long t_start, double *res_out) {
+__device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase, unsigned &parity_bits,
+                   unsigned long long t_start, bool continuation, Outcome &o, Timing &tm) {
   using V2 = typename VecOf<V>::V2;
   constexpr bool kMixed = sizeof(V) == 4;
-  unsigned parity_bits = 0;
   const V *A = kMixed ? (const V *)P.v32 : (const V *)P.v64;
   const V *dinv = kMixed ? (const V *)P.d32 : (const V *)P.d64;
   V *r = kMixed ? (V *)P.rf : (V *)P.rd;
   V *q = kMixed ? (V *)P.qf : (V *)P.qd;
   V2 *zp[2] = {kMixed ? (V2 *)P.zpf0 : (V2 *)P.zpd0, kMixed ? (V2 *)P.zpf1 : (V2 *)P.zpd1};
   double part[kSlots], red[kSlots];
-  int iterations = 0, updates = 0, converged = 0, status = FFG_OK;
+  const bool true_target = kMixed || continuation;
+  unsigned long long t0, t1, t2;
 
   // r64 = b - A x, ||r64||, ||b||
+  t0 = stamp();
   part[0] = part[1] = 0.0;
   spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
                              [&](int row, double s) {
@@ -335,14 +359,16 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
                                part[1] += bb * bb;
                              });
   write_partials(P, phase, part, 2);
-  if (!grid_barrier(P, phase)) return;
+  if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 2);
   const double bnorm = sqrt(red[1]);
   const double rnorm = sqrt(red[0]);
+  o.bnorm = bnorm;
   double scale = kMixed ? (rnorm > 0.0 ? rnorm : 1.0) : 1.0;
-  const double target = P.relative ? P.tol * (kMixed ? bnorm : rnorm) : P.tol;
-  double true_res = rnorm;
-  if (rnorm <= target) converged = 1;
+  const double target = P.relative ? P.tol * (true_target ? bnorm : rnorm) : P.tol;
+  double true_res = rnorm, last_true = rnorm;
+  int stall = 0;
+  int converged = (rnorm <= target) ? 1 : 0;
   double rz = 0.0;
   if (!converged) {
     const double inv = 1.0 / scale;
@@ -355,17 +381,20 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
       part[0] += (double)rr * (double)z;
     });
     write_partials(P, phase, part, 1);
-    if (!grid_barrier(P, phase)) return;
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
     read_partials(P, phase, red, 1);
     rz = red[0];
   }
+  tm.u += stamp() - t0;
   double beta = 0.0, rr_last = 1.0;
   int cur = 0;
-  for (int it = 1; !converged && it <= P.max_it; ++it) {
+  const int budget = P.max_it - o.iterations;
+  for (int it = 1; !converged && it <= budget; ++it) {
     const V2 *zc = zp[cur];
     V2 *zn = zp[cur ^ 1];
     const V bt = (V)beta;
     // A: p = z + beta p_old, q = A p, (p, q)
+    t0 = stamp();
     part[0] = 0.0;
     spmv_tiles<V, V>(P, A, S, parity_bits,
                      [&](int c) {
@@ -380,16 +409,22 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
                        part[0] += (double)pn * (double)s;
                      });
     write_partials(P, phase, part, 1);
-    if (!grid_barrier(P, phase)) return;
+    t1 = stamp();
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
     read_partials(P, phase, red, 1);
+    t2 = stamp();
+    tm.a += t1 - t0;
+    tm.aw += t2 - t1;
     const double pAp = red[0];
-    const bool breakdown = (!kMixed && P.guard == 0) ? (fabs(pAp) < 1.0e-14)
-                                                      : !(pAp > 0.0 && is_finite_d(pAp));
+    const bool breakdown = (!kMixed && !continuation && P.guard == 0)
+                               ? (fabs(pAp) < 1.0e-14)
+                               : !(pAp > 0.0 && is_finite_d(pAp));
     if (breakdown) break;
     const double alpha = rz / pAp;
     const V al = (V)alpha;
     const double xs = alpha * scale;
     // B: x += alpha p (FP64), r -= alpha q, z = D^-1 r
+    t0 = stamp();
     part[0] = part[1] = 0.0;
     part[2] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
     for_rows(P, [&](int row) {
@@ -403,19 +438,24 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
       part[1] += (double)rr * (double)z;
     });
     write_partials(P, phase, part, 3);
-    if (!grid_barrier(P, phase)) return;
+    t1 = stamp();
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
     read_partials(P, phase, red, 3);
-    iterations = it;
+    t2 = stamp();
+    tm.b += t1 - t0;
+    tm.bw += t2 - t1;
+    ++o.iterations;
     double rr = red[0], rz_new = red[1];
     const double est = sqrt(rr) * scale;
-    if (red[2] != 0.0) { status = FFG_TIMEOUT; true_res = est; break; }
+    if (red[2] != 0.0) { o.status = FFG_TIMEOUT; true_res = est; break; }
     if (!kMixed) {
       true_res = est;
       if (est <= target) { converged = 1; break; }
     } else if (est <= target || rr <= P.delta * P.delta * rr_last) {
       // reliable update: replace the recursive residual with b - A x in FP64
-      if (updates >= P.max_updates) break;
-      ++updates;
+      if (o.updates >= P.max_updates) break;
+      ++o.updates;
+      t0 = stamp();
       part[0] = 0.0;
       spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
                                  [&](int row, double s) {
@@ -424,11 +464,16 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
                                    part[0] += v * v;
                                  });
       write_partials(P, phase, part, 1);
-      if (!grid_barrier(P, phase)) return;
+      if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
       true_res = sqrt(red[0]);
-      if (true_res <= target) { converged = 1; break; }
+      if (true_res <= target) { converged = 1; tm.u += stamp() - t0; break; }
       if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
+      // FP32 recurrences that no longer reduce the true residual (condition
+      // number beyond FP32 reach) hand the solve to the FP64 loop
+      stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
+      last_true = true_res;
+      if (stall >= 2) { o.stagnated = 1; tm.u += stamp() - t0; break; }
       const double ratio = scale / true_res;  // old units -> new units
       const V rt = (V)ratio;
       const double inv = 1.0 / true_res;
@@ -444,8 +489,9 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
         part[0] += (double)rr2 * (double)z;
       });
       write_partials(P, phase, part, 1);
-      if (!grid_barrier(P, phase)) return;
+      if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
+      tm.u += stamp() - t0;
       rz = rz * ratio * ratio;
       rz_new = red[0];
       scale = true_res;
@@ -455,28 +501,27 @@ __device__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase,
     rz = rz_new;
     cur ^= 1;
   }
-  if (!kMixed || !converged) {
-    // true FP64 residual of the returned x
-    part[0] = 0.0;
-    spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
-                               [&](int row, double s) {
-                                 const double v = P.b[row] - s;
-                                 part[0] += v * v;
-                               });
-    write_partials(P, phase, part, 1);
-    if (!grid_barrier(P, phase)) return;
-    read_partials(P, phase, red, 1);
-    res_out[3] = kMixed ? sqrt(red[0]) : true_res;  // FP64 mode: recursive residual
-    res_out[4] = bnorm > 0.0 ? sqrt(red[0]) / bnorm : sqrt(red[0]);
-  } else {
-    res_out[3] = true_res;
-    res_out[4] = bnorm > 0.0 ? true_res / bnorm : true_res;
+  o.converged = converged;
+  o.final_res = true_res;
+  if (kMixed && converged) {
+    o.true_res = true_res;
+    return;
   }
-  res_out[0] = converged;
-  res_out[1] = iterations;
-  res_out[2] = updates;
-  res_out[5] = status;
-  res_out[6] = bnorm;
+  if (kMixed && o.stagnated) return;  // the FP64 continuation measures its own residual
+  // true FP64 residual of the returned x
+  t0 = stamp();
+  part[0] = 0.0;
+  spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
+                             [&](int row, double s) {
+                               const double v = P.b[row] - s;
+                               part[0] += v * v;
+                             });
+  write_partials(P, phase, part, 1);
+  if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+  read_partials(P, phase, red, 1);
+  tm.u += stamp() - t0;
+  o.true_res = sqrt(red[0]);
+  if (kMixed) o.final_res = o.true_res;
 }
 
 __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
@@ -489,15 +534,37 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
   }
   __syncthreads();
   unsigned int phase = 0;
+  unsigned parity_bits = 0;
   // only block 0 judges the wall limit; its verdict travels through a partial slot
   const unsigned long long t_start = globaltimer();
-  double res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (P.precision == FFG_PRECISION_FP64)
-    cg<double>(P, S, phase, t_start, res);
-  else
-    cg<float>(P, S, phase, t_start, res);
-  if (blockIdx.x == 0 && threadIdx.x == 0)
-    for (int i = 0; i < 7; ++i) P.result[i] = res[i];
+  Outcome o;
+  Timing tm;
+  int continued = 0;
+  if (P.precision == FFG_PRECISION_FP64) {
+    cg<double>(P, S, phase, parity_bits, t_start, false, o, tm);
+  } else {
+    cg<float>(P, S, phase, parity_bits, t_start, false, o, tm);
+    if (!o.aborted && o.stagnated && !o.converged && o.status == FFG_OK) {
+      continued = 1;
+      cg<double>(P, S, phase, parity_bits, t_start, true, o, tm);
+    }
+  }
+  if (o.aborted) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    P.result[0] = o.converged;
+    P.result[1] = o.iterations;
+    P.result[2] = o.updates;
+    P.result[3] = o.final_res;
+    P.result[4] = o.bnorm > 0.0 ? o.true_res / o.bnorm : o.true_res;
+    P.result[5] = o.status;
+    P.result[6] = o.bnorm;
+    P.result[7] = continued;
+    P.result[8] = 1e-9 * (double)tm.a;
+    P.result[9] = 1e-9 * (double)tm.aw;
+    P.result[10] = 1e-9 * (double)tm.b;
+    P.result[11] = 1e-9 * (double)tm.bw;
+    P.result[12] = 1e-9 * (double)tm.u;
+  }
 }
 
 // Standalone FP64 tile SpMV (one CTA per tile).
@@ -563,7 +630,7 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
   A((void **)&w.partial, 2 * kSlots * (size_t)grid * sizeof(double));
   A((void **)&w.barrier, 64);
   A((void **)&w.control, 64);
-  A((void **)&w.result, 8 * sizeof(double));
+  A((void **)&w.result, kResultDoubles * sizeof(double));
   if (bad) {
     solve_work_free(w);
     cudaGetLastError();
@@ -621,7 +688,7 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
     cudaGetLastError();
     return FFG_CUDA_ERROR;
   }
-  double res[8];
+  double res[kResultDoubles];
   int ctrl[2];
   if (cudaMemcpyAsync(res, w.result, sizeof(res), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
     return FFG_CUDA_ERROR;
@@ -642,6 +709,7 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
     stats->status = (int)res[5];
     if (stats->status == FFG_OK && !stats->converged) stats->status = FFG_NOT_CONVERGED;
   }
+  for (int i = 0; i < 6; ++i) w.phase_seconds[i] = res[7 + i];
   return FFG_OK;
 }
 

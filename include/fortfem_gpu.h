@@ -237,6 +237,12 @@ void ffg_problem_reduced_system(int handle, const double *vertices, double coef_
                                 int64_t nnz_capacity, int64_t *nnz, int64_t *col_ptr, int *row_ind,
                                 double *values, double *rhs, int *free_dofs, int *status);
 
+/* Device-side profile of the handle's last solve, measured by CTA 0 of the
+ * persistent PCG kernel: seconds[0] = 1 if the mixed solve continued in FP64
+ * after FP32 stagnation, then seconds in SpMV work, barrier wait after the
+ * SpMV, vector work, barrier wait after it, and residual-replacement phases. */
+void ffg_problem_phase_times(int handle, double *seconds, int *status);
+
 /* Release a problem handle (fortfem_factor_free, src/bindings/fortfem_capi_solver.f90:108-124). */
 void ffg_problem_free(int handle, int *status);
 
