@@ -62,7 +62,11 @@ struct Problem {
   Topology topo;
   ElementTables tab;
   DeviceTopology dt;
-  DeviceCsr A;
+  HostSell hsell;            // solver layout (host copy: permutation, positions)
+  DeviceSell S;              // solver operator (SELL-32-sigma)
+  int64_t *csc_col_ptr = nullptr;  // constrained CSC pattern (device)
+  int *csc_row = nullptr;
+  double *csc_val = nullptr;       // CSC values, allocated on first use
   SolveWork work;
   int rule = 0, qdeg = 0, dim = 3;
   int geo_stride = 0;
@@ -78,11 +82,11 @@ struct Problem {
   ~Problem() {
     void *ptrs[] = {dt.cells, dt.gd, dt.edge_sign, dt.face_perm, dt.free_index, dt.inc_ptr,
                     dt.inc_cell, dt.inc_local, dt.slot, dt.ref, dt.load_basis, dt.face_blocks,
-                    A.row_ptr, A.col, A.val64, A.val32, A.dinv64, A.dinv32, A.tile_row, geo,
-                    cell_rhs, elem, rhs, x, full, in_vertices, in_cell_a, in_cell_b, in_samples,
-                    in_g, free_dofs, err};
+                    csc_col_ptr, csc_row, csc_val, geo, cell_rhs, elem, rhs, x, full, in_vertices,
+                    in_cell_a, in_cell_b, in_samples, in_g, free_dofs, err};
     for (void *p : ptrs)
       if (p) cudaFree(p);
+    free_sell(S);
     solve_work_free(work);
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);
@@ -151,22 +155,14 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   if ((st = upload(&dt.slot, t.slot))) return st;
   if (!P->tab.ref.empty() && (st = upload(&dt.ref, P->tab.ref))) return st;
   if (!P->tab.load_basis.empty() && (st = upload(&dt.load_basis, P->tab.load_basis))) return st;
-  // matrix
-  DeviceCsr &A = P->A;
-  A.n = t.n_free();
-  A.nnz = t.nnz();
-  if ((st = upload(&A.row_ptr, t.col_ptr))) return st;
-  const size_t pad = (size_t)matrix_padding();
-  if ((st = upload_padded(&A.col, t.row_idx, pad))) return st;
-  if ((st = zeros_padded(&A.val64, (size_t)A.nnz, pad))) return st;
-  if ((st = zeros_padded(&A.val32, (size_t)A.nnz, pad))) return st;
-  if ((st = dalloc(&A.dinv64, (size_t)A.n))) return st;
-  if ((st = dalloc(&A.dinv32, (size_t)A.n))) return st;
-  int max_row = 0;
-  std::vector<int> tiles = make_tiles(t.col_ptr, tile_capacity(), &max_row);
-  if (max_row > tile_capacity()) { msg = "matrix row longer than an SpMV tile"; return FFG_INVALID_INPUT; }
-  A.n_tiles = (int)tiles.size() - 1;
-  if ((st = upload(&A.tile_row, tiles))) return st;
+  // constrained CSC pattern (assembly) and the solver's SELL layout
+  if ((st = upload(&P->csc_col_ptr, t.col_ptr))) return st;
+  if ((st = upload(&P->csc_row, t.row_idx))) return st;
+  int grid = 0;
+  if ((st = pcg_grid_size(&grid))) return st;
+  build_sell(t.col_ptr, t.row_idx, kSellSigma, P->hsell);
+  if ((st = upload_sell(P->hsell, grid, P->S))) return st;
+  const int64_t nfree = t.n_free();
   // per-step buffers
   const size_t nc = (size_t)n_cells;
   if ((st = dalloc(&P->geo, nc * std::max(P->geo_stride, 1)))) return st;
@@ -174,8 +170,8 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
     if ((st = dalloc(&P->cell_rhs, nc * t.nb))) return st;
     if ((st = dalloc(&P->elem, nc * t.nb * t.nb))) return st;
   }
-  if ((st = dalloc(&P->rhs, (size_t)A.n))) return st;
-  if ((st = dalloc(&P->x, (size_t)A.n))) return st;
+  if ((st = dalloc(&P->rhs, (size_t)nfree))) return st;
+  if ((st = dalloc(&P->x, (size_t)nfree))) return st;
   if ((st = dalloc(&P->full, (size_t)t.n_dofs))) return st;
   if ((st = dalloc(&P->in_vertices, (size_t)n_vertices * P->dim))) return st;
   if ((st = dalloc(&P->in_cell_a, nc))) return st;
@@ -185,25 +181,26 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   if ((st = dalloc(&P->in_g, (size_t)t.n_dofs))) return st;
   if ((st = upload(&P->free_dofs, t.free_dofs))) return st;
   if ((st = dalloc(&P->err, 4))) return st;
-  int grid = 0;
-  if ((st = pcg_grid_size(&grid))) return st;
-  if ((st = solve_work_alloc(P->work, A.n, grid))) return st;
+  if ((st = solve_work_alloc(P->work, nfree, grid))) return st;
   for (auto &e : P->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return FFG_CUDA_ERROR;
   out = P;
   return FFG_OK;
 }
 
-__global__ void scatter_solution_kernel(int64_t n_free, const int *free_dofs, const double *x,
-                                        double *full) {
+// x is in the solver's (SELL) row order: row i is free DoF perm[i].
+__global__ void scatter_solution_kernel(int64_t n_free, const int *perm, const int *free_dofs,
+                                        const double *x, double *full) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n_free) full[free_dofs[i]] = x[i];
+  if (i < n_free) full[free_dofs[perm[i]]] = x[i];
 }
 
-// Stage inputs (host or device) and assemble the constrained system into P.A / P.rhs.
+// Stage inputs (host or device) and assemble the constrained system: into the
+// solver's SELL operator (rhs in SELL order) when `sell`, else into the CSC
+// value array (rhs in free-DoF order).
 int assemble(Problem &P, const double *vertices, double ca, double cb, const double *cell_a,
              const double *cell_b, const double *samples, const double *g, int memory,
-             cudaStream_t s, std::string &msg) {
+             bool sell, cudaStream_t s, std::string &msg) {
   const Topology &t = P.topo;
   AssemblyInputs in;
   in.coef_a = ca;
@@ -229,6 +226,8 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
     in.samples = samples;
     in.g = g;
   }
+  if (!sell && !P.csc_val && dalloc(&P.csc_val, (size_t)std::max<int64_t>(t.nnz(), 1)))
+    return FFG_OUT_OF_MEMORY;
   if (cudaMemsetAsync(P.err, 0, sizeof(int), s) != cudaSuccess) return FFG_CUDA_ERROR;
   int st;
   if (t.family == FFG_TETRA_NEDELEC) {
@@ -237,8 +236,8 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
     st = launch_cell_geometry(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.err, s);
   }
   if (st) return st;
-  st = launch_columns(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.elem, P.A, P.rhs,
-                      P.err, s);
+  st = launch_columns(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.elem, P.csc_col_ptr,
+                      P.csc_row, sell ? &P.S : nullptr, P.csc_val, P.rhs, s);
   if (st) return st;
   int herr = 0;
   if (cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
@@ -308,50 +307,46 @@ bool csc_to_csr(int n, const int64_t *cp, const int *ri, const double *v, HostCs
   return true;
 }
 
-struct Uploaded {
-  DeviceCsr A;
-  ~Uploaded() {
-    void *ptrs[] = {A.row_ptr, A.col, A.val64, A.val32, A.dinv64, A.dinv32, A.tile_row};
-    for (void *p : ptrs)
-      if (p) cudaFree(p);
+struct DeviceCsrArrays {
+  int64_t *rp = nullptr;
+  int *ci = nullptr;
+  double *v = nullptr;
+  ~DeviceCsrArrays() {
+    if (rp) cudaFree(rp);
+    if (ci) cudaFree(ci);
+    if (v) cudaFree(v);
   }
 };
 
-__global__ void prepare_kernel(int64_t n, const int64_t *rp, const int *col, const double *v64,
-                               float *v32, double *d64, float *d32, int jacobi) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double d = 0.0;
-  for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
-    v32[k] = (float)v64[k];
-    if (col[k] == (int)i) d = v64[k];
+// SELL operator of a host CSR with its values, FP32 copy and Jacobi diagonal
+// computed on the host.
+int upload_sell_with_values(const HostCsr &h, int grid, bool jacobi, HostSell &hs,
+                            DeviceSell &d) {
+  build_sell(h.rp, h.col, kSellSigma, hs);
+  int st = upload_sell(hs, grid, d);
+  if (st) return st;
+  const int64_t n = (int64_t)h.rp.size() - 1;
+  std::vector<double> v64((size_t)std::max<int64_t>(hs.padded, 1), 0.0);
+  std::vector<float> v32(v64.size(), 0.0f);
+  std::vector<double> d64((size_t)std::max<int64_t>(n, 1), 1.0);
+  std::vector<float> d32(d64.size(), 1.0f);
+  for (int64_t i = 0; i < n; ++i) {
+    double dg = 0.0;
+    for (int64_t k = h.rp[i]; k < h.rp[i + 1]; ++k) {
+      v64[hs.pos[k]] = h.val[k];
+      v32[hs.pos[k]] = (float)h.val[k];
+      if (h.col[k] == (int)i) dg = h.val[k];
+    }
+    // build_sparse_preconditioner("jacobi"), advanced_solvers.f90:1139-1154
+    const double di = (jacobi && std::fabs(dg) > 1.0e-14) ? 1.0 / dg : 1.0;
+    d64[hs.iperm[i]] = di;
+    d32[hs.iperm[i]] = (float)di;
   }
-  // build_sparse_preconditioner("jacobi"), advanced_solvers.f90:1139-1154
-  const double di = (jacobi && fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
-  d64[i] = di;
-  d32[i] = (float)di;
-}
-
-int upload_csr(int n, const HostCsr &h, Uploaded &U, bool jacobi) {
-  DeviceCsr &A = U.A;
-  A.n = n;
-  A.nnz = (int64_t)h.col.size();
-  int st;
-  if ((st = upload(&A.row_ptr, h.rp))) return st;
-  const size_t pad = (size_t)matrix_padding();
-  if ((st = upload_padded(&A.col, h.col, pad))) return st;
-  if ((st = upload_padded(&A.val64, h.val, pad))) return st;
-  if ((st = zeros_padded(&A.val32, h.val.size(), pad))) return st;
-  if ((st = dalloc(&A.dinv64, (size_t)n))) return st;
-  if ((st = dalloc(&A.dinv32, (size_t)n))) return st;
-  int max_row = 0;
-  std::vector<int> tiles = make_tiles(h.rp, tile_capacity(), &max_row);
-  if (max_row > tile_capacity()) return FFG_INVALID_INPUT;
-  A.n_tiles = (int)tiles.size() - 1;
-  if ((st = upload(&A.tile_row, tiles))) return st;
-  prepare_kernel<<<(unsigned)((n + 255) / 256), 256>>>(n, A.row_ptr, A.col, A.val64, A.val32,
-                                                       A.dinv64, A.dinv32, jacobi ? 1 : 0);
-  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+  bool ok = cudaMemcpy(d.val64, v64.data(), sizeof(double) * hs.padded, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.val32, v32.data(), sizeof(float) * hs.padded, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.dinv64, d64.data(), sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.dinv32, d32.data(), sizeof(float) * n, cudaMemcpyHostToDevice) == cudaSuccess;
+  return ok ? FFG_OK : FFG_CUDA_ERROR;
 }
 }  // namespace
 }  // namespace ffg
@@ -602,17 +597,17 @@ void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
   ffg_solver_stats local;
   std::memset(&local, 0, sizeof(local));
   cudaEventRecord(P->ev[0], s);
-  int st = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, memory, s, msg);
+  int st = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, memory, true, s, msg);
   if (st) { report(o.verbosity, msg); *status = st; if (stats) { local.status = st; *stats = local; } return; }
   cudaEventRecord(P->ev[1], s);
   const Topology &t = P->topo;
   if (!o.preconditioner) {
-    set_ones_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(t.n_free(), P->A.dinv64,
-                                                                        P->A.dinv32);
+    set_ones_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(t.n_free(), P->S.dinv64,
+                                                                        P->S.dinv32);
   }
   cudaMemsetAsync(P->x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
   if (t.n_free() > 0) {
-    st = pcg_solve(P->A, P->rhs, P->x, o, P->work, &local, s, msg);
+    st = pcg_solve(P->S, P->rhs, P->x, o, P->work, &local, s, msg);
     if (st) { report(o.verbosity, msg); *status = st; if (stats) { local.status = st; *stats = local; } return; }
   } else {
     local.converged = 1;
@@ -626,7 +621,7 @@ void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
     cudaMemsetAsync(P->full, 0, sizeof(double) * (size_t)t.n_dofs, s);
   if (t.n_free() > 0)
     scatter_solution_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(
-        t.n_free(), P->free_dofs, P->x, P->full);
+        t.n_free(), P->S.perm, P->free_dofs, P->x, P->full);
   cudaMemcpyAsync(solution, P->full, sizeof(double) * (size_t)t.n_dofs,
                   memory == 0 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
   cudaEventRecord(P->ev[3], s);
@@ -658,11 +653,11 @@ void ffg_problem_reduced_system(int handle, const double *vertices, double ca, d
   if (nnz) *nnz = t.nnz();
   if (cap < t.nnz() || !col_ptr || !row_ind || !values) { *status = FFG_CAPACITY; return; }
   std::string msg;
-  int st = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, 0, 0, msg);
+  int st = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, 0, false, 0, msg);
   if (st) { *status = st; return; }
   std::memcpy(col_ptr, t.col_ptr.data(), sizeof(int64_t) * t.col_ptr.size());
   std::memcpy(row_ind, t.row_idx.data(), sizeof(int) * t.row_idx.size());
-  if (cudaMemcpy(values, P->A.val64, sizeof(double) * (size_t)t.nnz(), cudaMemcpyDeviceToHost) != cudaSuccess) {
+  if (cudaMemcpy(values, P->csc_val, sizeof(double) * (size_t)t.nnz(), cudaMemcpyDeviceToHost) != cudaSuccess) {
     *status = FFG_CUDA_ERROR;
     return;
   }
@@ -687,11 +682,11 @@ static void full_csc(int family, int degree, int nv, const double *verts, int nt
   if (n_dofs) *n_dofs = (int)P->topo.n_dofs;
   if (nnz) *nnz = P->topo.nnz();
   if (cap < P->topo.nnz() || !col_ptr || !row_ind || !values) { *status = FFG_CAPACITY; return; }
-  st = assemble(*P, verts, ca, cb, cell_a, cell_b, nullptr, nullptr, 0, 0, msg);
+  st = assemble(*P, verts, ca, cb, cell_a, cell_b, nullptr, nullptr, 0, false, 0, msg);
   if (st) { *status = st; return; }
   std::memcpy(col_ptr, P->topo.col_ptr.data(), sizeof(int64_t) * P->topo.col_ptr.size());
   std::memcpy(row_ind, P->topo.row_idx.data(), sizeof(int) * P->topo.row_idx.size());
-  if (cudaMemcpy(values, P->A.val64, sizeof(double) * (size_t)P->topo.nnz(), cudaMemcpyDeviceToHost) !=
+  if (cudaMemcpy(values, P->csc_val, sizeof(double) * (size_t)P->topo.nnz(), cudaMemcpyDeviceToHost) !=
       cudaSuccess) {
     *status = FFG_CUDA_ERROR;
     return;
@@ -708,7 +703,7 @@ static void full_load(int family, int degree, int nv, const double *verts, int n
                           msg);
   if (st) { *status = st; return; }
   if (n_dofs != P->topo.n_dofs || !rhs || !samples) { *status = FFG_INVALID_INPUT; return; }
-  st = assemble(*P, verts, 0.0, 0.0, nullptr, nullptr, samples, nullptr, 0, 0, msg);
+  st = assemble(*P, verts, 0.0, 0.0, nullptr, nullptr, samples, nullptr, 0, false, 0, msg);
   if (st) { *status = st; return; }
   if (cudaMemcpy(rhs, P->rhs, sizeof(double) * (size_t)n_dofs, cudaMemcpyDeviceToHost) != cudaSuccess) {
     *status = FFG_CUDA_ERROR;
@@ -776,23 +771,36 @@ void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row
   if (st) { *status = st; return; }
   HostCsr h;
   if (!csc_to_csr(n, col_ptr, row_ind, values, h)) { *status = FFG_INVALID_INPUT; return; }
-  Uploaded U;
-  if ((st = upload_csr(n, h, U, o.preconditioner != 0))) { *status = st; return; }
-  double *db = nullptr, *dx = nullptr;
-  if (dalloc(&db, n) || dalloc(&dx, n)) { cudaFree(db); cudaFree(dx); *status = FFG_OUT_OF_MEMORY; return; }
-  cudaMemcpy(db, b, sizeof(double) * n, cudaMemcpyHostToDevice);
-  cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
-  SolveWork w;
   int grid = 0;
+  if ((st = pcg_grid_size(&grid))) { *status = st; return; }
+  HostSell hs;
+  DeviceSell S;
+  if ((st = upload_sell_with_values(h, grid, o.preconditioner != 0, hs, S))) {
+    free_sell(S);
+    *status = st;
+    return;
+  }
+  // b and x in the solver's row order
+  std::vector<double> bn(n), xn(n);
+  for (int i = 0; i < n; ++i) { bn[hs.iperm[i]] = b[i]; xn[hs.iperm[i]] = x[i]; }
+  double *db = nullptr, *dx = nullptr;
+  if (dalloc(&db, n) || dalloc(&dx, n)) {
+    cudaFree(db); cudaFree(dx); free_sell(S);
+    *status = FFG_OUT_OF_MEMORY;
+    return;
+  }
+  cudaMemcpy(db, bn.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(dx, xn.data(), sizeof(double) * n, cudaMemcpyHostToDevice);
+  SolveWork w;
   std::string msg;
   ffg_solver_stats local;
   std::memset(&local, 0, sizeof(local));
-  if (!(st = pcg_grid_size(&grid)) && !(st = solve_work_alloc(w, n, grid))) {
+  if (!(st = solve_work_alloc(w, n, grid))) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, 0);
-    st = pcg_solve(U.A, db, dx, o, w, &local, 0, msg);
+    st = pcg_solve(S, db, dx, o, w, &local, 0, msg);
     cudaEventRecord(e1, 0);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -801,8 +809,12 @@ void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
-  if (!st) cudaMemcpy(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  if (!st) {
+    cudaMemcpy(xn.data(), dx, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    for (int i = 0; i < n; ++i) x[i] = xn[hs.iperm[i]];
+  }
   solve_work_free(w);
+  free_sell(S);
   cudaFree(db);
   cudaFree(dx);
   report(o.verbosity, msg);
@@ -820,12 +832,19 @@ void ffg_csc_matvec(int n, int64_t nnz, const int64_t *col_ptr, const int *row_i
   if (st) { *status = st; return; }
   HostCsr h;
   if (!csc_to_csr(n, col_ptr, row_ind, values, h)) { *status = FFG_INVALID_INPUT; return; }
-  Uploaded U;
-  if ((st = upload_csr(n, h, U, false))) { *status = st; return; }
+  DeviceCsrArrays D;
   double *dx = nullptr, *dy = nullptr;
-  if (dalloc(&dx, n) || dalloc(&dy, n)) { cudaFree(dx); cudaFree(dy); *status = FFG_OUT_OF_MEMORY; return; }
+  if (dalloc(&D.rp, h.rp.size()) || dalloc(&D.ci, h.col.size()) || dalloc(&D.v, h.val.size()) ||
+      dalloc(&dx, n) || dalloc(&dy, n)) {
+    cudaFree(dx); cudaFree(dy);
+    *status = FFG_OUT_OF_MEMORY;
+    return;
+  }
+  cudaMemcpy(D.rp, h.rp.data(), sizeof(int64_t) * h.rp.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(D.ci, h.col.data(), sizeof(int) * h.col.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(D.v, h.val.data(), sizeof(double) * h.val.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
-  st = spmv64(U.A, dx, dy, 0);
+  st = csr_spmv64(n, D.rp, D.ci, D.v, dx, dy, 0);
   if (!st && cudaMemcpy(y, dy, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
     st = FFG_CUDA_ERROR;
   cudaFree(dx);

@@ -91,20 +91,46 @@ struct ElementTables {
 int build_tables(const Topology &t, int rule, int qdeg, ElementTables &tab, std::string &msg);
 
 // -------------------------------------------------------------- device side
-struct DeviceCsr {
-  int64_t n = 0, nnz = 0;
-  int64_t *row_ptr = nullptr;  // n + 1
-  int *col = nullptr;          // nnz
-  double *val64 = nullptr;
+// The solver streams the constrained operator in sliced ELLPACK form
+// (SELL-32-sigma): rows in a permuted order sorted by length inside windows of
+// sigma rows, 32-row slices stored column-major so that a warp reads 128
+// contiguous bytes per step.  Column indices are stored as 16-bit offsets
+// from the row (new numbering) when every offset fits, else as int32.
+constexpr int kSliceRows = 32;
+constexpr int kSellSigma = 4096;
+
+struct HostSell {
+  int64_t n = 0, n_slices = 0, padded = 0;
+  std::vector<int64_t> soff;   // n_slices + 1 entry offsets
+  std::vector<int> perm;       // new row -> old row
+  std::vector<int> iperm;      // old row -> new row
+  bool narrow = false;
+  std::vector<int16_t> dcol;   // narrow: column - row (new numbering)
+  std::vector<int> col;        // wide: column (new numbering)
+  std::vector<int64_t> pos;    // position of every CSR entry (old row order) in the slices
+};
+// rp/ci: CSR of the operator (old numbering; for the symmetric constrained
+// system this is its CSC).
+void build_sell(const std::vector<int64_t> &rp, const std::vector<int> &ci, int sigma,
+                HostSell &out);
+
+struct DeviceSell {
+  int64_t n = 0, n_slices = 0, padded = 0;
+  int64_t *soff = nullptr;
+  int16_t *dcol = nullptr;  // exactly one of dcol / col is set
+  int *col = nullptr;
+  double *val64 = nullptr;  // padded entries, zero in the padding
   float *val32 = nullptr;
-  double *dinv64 = nullptr;
+  double *dinv64 = nullptr;  // Jacobi inverse diagonal, new numbering
   float *dinv32 = nullptr;
-  int *tile_row = nullptr;     // n_tiles + 1 row boundaries of the SpMV tiles
-  int n_tiles = 0;
+  int *perm = nullptr, *iperm = nullptr;
+  int *cta_slice = nullptr;  // grid + 1 slice boundaries of the CTAs
+  int grid = 0;
 };
 
-// Build tile boundaries (<= tile_nnz entries each) on the host from row_ptr.
-std::vector<int> make_tiles(const std::vector<int64_t> &row_ptr, int tile_nnz, int *max_row);
+// Upload the slice structure (values left zero) and the CTA partition.
+int upload_sell(const HostSell &h, int grid, DeviceSell &d);
+void free_sell(DeviceSell &d);
 
 struct SolveWork {
   double *r64 = nullptr, *partial = nullptr;
@@ -122,21 +148,21 @@ struct SolveWork {
   double phase_seconds[6] = {0, 0, 0, 0, 0, 0};
 };
 
-// Matrix value/column arrays are allocated with this many padding entries so
-// that the SpMV's aligned 16-byte quads never read past the allocation.
-int matrix_padding();
-
 int solve_work_alloc(SolveWork &w, int64_t n, int grid);
 void solve_work_free(SolveWork &w);
 
-// Launch the persistent Jacobi-PCG (FP64 or mixed) on b -> x.  x holds the
-// initial guess (FP64).  Fills stats (reads back a small block at the end).
-int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_options &opts,
+// Launch the persistent Jacobi-PCG (FP64 or mixed) on b -> x (both in the
+// SELL row numbering).  x holds the initial guess (FP64).  Fills stats.
+int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
               SolveWork &w, ffg_solver_stats *stats, cudaStream_t stream, std::string &msg);
 int pcg_grid_size(int *grid);
 
-// SpMV y = A x in FP64 (for the drop-in matvec and residual checks).
-int spmv64(const DeviceCsr &A, const double *x, double *y, cudaStream_t stream);
+// FP64 CSR SpMV y = A x (drop-in matvec).
+int csr_spmv64(int64_t n, const int64_t *rp, const int *ci, const double *v, const double *x,
+               double *y, cudaStream_t stream);
+// Jacobi diagonal and FP32 copy of SELL values (drop-in solve path).
+int sell_prepare(DeviceSell &A, const int64_t *csr_rp, const int *csr_ci, const int64_t *pos,
+                 bool jacobi, cudaStream_t s);
 
 // Kernel launchers of the assembly (kernels_assemble.cu).
 struct DeviceTopology {
@@ -170,12 +196,15 @@ int launch_cell_geometry(const Topology &t, const ElementTables &tab, const Devi
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
                    cudaStream_t s);
-int tile_capacity();
-// Column-owner gather into the constrained CSC (values, rhs, Jacobi diagonal).
+// Column-owner gather into the constrained operator.  With `sell` set the
+// values go to the slices (FP64 + FP32 copy, Jacobi diagonal, rhs in the
+// SELL numbering); otherwise to the CSC value array `csc_val` with the rhs in
+// free-DoF order.  row_idx is the CSC row index array (device).
 int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, const double *geo, int geo_stride,
-                   const double *cell_rhs, const double *elem, DeviceCsr &A, double *rhs,
-                   int *err, cudaStream_t s);
+                   const double *cell_rhs, const double *elem, const int64_t *col_ptr,
+                   const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
+                   cudaStream_t s);
 int geo_stride_for(const Topology &t, const ElementTables &tab);
 
 }  // namespace ffg

@@ -287,7 +287,11 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
 }
 
 // ----------------------------------------------------- K3 column-owner scatter
-template <int FAMILY>
+// SELL = false: values into the CSC value array (rhs in free-DoF order).
+// SELL = true: values into the solver's slices (row iperm[j] of the SELL
+// operator, which by symmetry is column j), with the FP32 copy, the Jacobi
+// diagonal and the rhs in the SELL numbering.
+template <int FAMILY, bool SELL>
 __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_ptr,
                               const int *__restrict__ row_idx, const int64_t *__restrict__ inc_ptr,
                               const int *__restrict__ inc_cell,
@@ -297,13 +301,25 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
                               const double *__restrict__ ref, const double *__restrict__ load_basis,
                               int nq, const double *__restrict__ elem,
                               const double *__restrict__ cell_rhs, const double *__restrict__ g,
+                              const int *__restrict__ iperm, const int64_t *__restrict__ soff,
                               double *__restrict__ val64, float *__restrict__ val32,
                               double *__restrict__ dinv64, float *__restrict__ dinv32,
                               double *__restrict__ rhs) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_free) return;
   const int64_t start = col_ptr[j], end = col_ptr[j + 1];
-  for (int64_t k = start; k < end; ++k) val64[k] = 0.0;
+  int64_t base, stride_out, out_row;
+  if (SELL) {
+    out_row = iperm[j];
+    base = soff[out_row / kSliceRows] + out_row % kSliceRows;
+    stride_out = kSliceRows;
+  } else {
+    out_row = j;
+    base = start;
+    stride_out = 1;
+  }
+  const int len = (int)(end - start);
+  for (int k = 0; k < len; ++k) val64[base + stride_out * k] = 0.0;
   double b = 0.0, lift = 0.0;
   const size_t nn = (size_t)nb * nb;
   for (int64_t p = inc_ptr[j]; p < inc_ptr[j + 1]; ++p) {
@@ -339,21 +355,23 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
       if (s == kConstrainedSlot) {
         if (g) lift += kil * g[ge[i]];
       } else {
-        val64[start + s] += kil;
+        val64[base + stride_out * s] += kil;
       }
     }
     b += F;
   }
-  rhs[j] = b - lift;
-  double d = 0.0;
-  for (int64_t k = start; k < end; ++k) {
-    const double v = val64[k];
-    val32[k] = (float)v;
-    if (row_idx[k] == (int)j) d = v;
+  rhs[out_row] = b - lift;
+  if (SELL) {
+    double d = 0.0;
+    for (int k = 0; k < len; ++k) {
+      const double v = val64[base + stride_out * k];
+      val32[base + stride_out * k] = (float)v;
+      if (row_idx[start + k] == (int)j) d = v;
+    }
+    const double di = (fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
+    dinv64[out_row] = di;
+    dinv32[out_row] = (float)di;
   }
-  const double di = (fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
-  dinv64[j] = di;
-  dinv32[j] = (float)di;
 }
 
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
@@ -409,22 +427,35 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
 
 int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, const double *geo, int stride,
-                   const double *cell_rhs, const double *elem, DeviceCsr &A, double *rhs,
-                   int *err, cudaStream_t s) {
-  (void)err;
+                   const double *cell_rhs, const double *elem, const int64_t *col_ptr,
+                   const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
+                   cudaStream_t s) {
   const int T = 128;
   const int64_t F = t.n_free();
   if (F == 0) return FFG_OK;
-#define FFG_COLUMN_ARGS                                                                       \
-  F, A.row_ptr, A.col, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd, t.nb, geo,      \
-      stride, dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, A.val64, A.val32,     \
-      A.dinv64, A.dinv32, rhs
+  const int *iperm = sell ? sell->iperm : nullptr;
+  const int64_t *soff = sell ? sell->soff : nullptr;
+  double *v64 = sell ? sell->val64 : csc_val;
+  float *v32 = sell ? sell->val32 : nullptr;
+  double *d64 = sell ? sell->dinv64 : nullptr;
+  float *d32 = sell ? sell->dinv32 : nullptr;
+#define FFG_COLUMN_ARGS                                                                        \
+  F, col_ptr, row_idx, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd, t.nb, geo, stride, \
+      dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, iperm, soff, v64, v32, d64, d32, rhs
+#define FFG_LAUNCH(FAM)                                                                        \
+  do {                                                                                         \
+    if (sell)                                                                                  \
+      column_kernel<FAM, true><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);                \
+    else                                                                                       \
+      column_kernel<FAM, false><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);               \
+  } while (0)
   if (t.family == FFG_TETRA_LAGRANGE)
-    column_kernel<FFG_TETRA_LAGRANGE><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);
+    FFG_LAUNCH(FFG_TETRA_LAGRANGE);
   else if (t.family == FFG_TRIANGLE_P1)
-    column_kernel<FFG_TRIANGLE_P1><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);
+    FFG_LAUNCH(FFG_TRIANGLE_P1);
   else
-    column_kernel<FFG_TETRA_NEDELEC><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);
+    FFG_LAUNCH(FFG_TETRA_NEDELEC);
+#undef FFG_LAUNCH
 #undef FFG_COLUMN_ARGS
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }

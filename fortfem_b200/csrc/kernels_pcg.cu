@@ -1,13 +1,16 @@
-// Persistent Jacobi-PCG (sm_100a).
+// Persistent Jacobi-PCG (sm_100a) on a SELL-32-sigma operator.
 //
-// One cooperative launch runs the whole solve.  CTAs own fixed row tiles of
-// the CSR matrix (the constrained CSC of a symmetric operator read as CSR).
-// Each SpMV streams the CTA's tiles with 16-byte loads into shared memory and
-// sums every row in a fixed order.  Dot products are reduced per CTA, written
-// to a per-phase partial buffer and summed by every CTA in the same fixed
-// order, so all CTAs take identical decisions and results are
-// bit-reproducible for a given grid.  Grid barriers spin with a time bound and
-// report FFG_TIMEOUT instead of hanging.
+// One cooperative launch runs the whole solve.  Every CTA owns a contiguous
+// range of 32-row slices (balanced by stored entries) and therefore a
+// contiguous range of rows of the permuted system.  In the SpMV a warp walks
+// one slice: lane l accumulates row 32s+l in a fixed order, reading 128
+// contiguous bytes of values and 64 (16-bit column offsets) per step with
+// evict-first streaming loads.  Vector phases walk the CTA's rows with all
+// threads, coalesced.  Dot products are reduced per CTA, written to a
+// per-phase partial buffer and summed by every CTA in the same fixed order,
+// so all CTAs take identical decisions and results are bit-reproducible for
+// a given grid.  Grid barriers spin with a time bound and report FFG_TIMEOUT
+// instead of hanging.
 //
 // Iteration (two grid barriers):
 //   A: p = z + beta p_old on the fly while gathering, q = A p, (p, q)
@@ -21,10 +24,12 @@
 // (|p^T A p| < 1e-14 as the reference, or p^T A p <= 0 when selected);
 // Jacobi z = D^-1 r with D^-1 = 1 where |a_ii| <= 1e-14.
 // Mixed mode: the same CG recurrences in FP32 on a scaled residual with the
-// solution accumulated in FP64; whenever the FP32 residual has fallen by
-// `reliable_delta` (or claims convergence) the true FP64 residual b - A x
-// replaces it (reliable updates: the search direction is kept, rescaled), and
-// the solve ends when ||b - A x||_2 <= tol*||b||_2.
+// solution accumulated in FP64; whenever the FP32 residual has fallen by the
+// reliable-update factor (or claims convergence) the true FP64 residual
+// b - A x replaces it (the search direction is kept, rescaled), and the solve
+// ends when ||b - A x||_2 <= tol*||b||_2.  If replacements stop reducing the
+// true residual (condition number beyond FP32 reach) the solve continues in
+// the FP64 loop from the current x.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,8 +41,8 @@ namespace ffg {
 
 namespace {
 
-constexpr int kThreads = 512;
-constexpr int kTileNnz = 4096;
+constexpr int kThreads = 1024;
+constexpr int kWarps = kThreads / 32;
 constexpr int kSlots = 4;
 constexpr int kPartialBatch = 8;   // partial loads in flight per lane
 constexpr int kResultDoubles = 16;
@@ -45,14 +50,14 @@ constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrie
 
 struct PcgParams {
   int64_t n;
-  const int64_t *rp;
+  const int64_t *soff;
+  const int16_t *dcol;
   const int *col;
   const float *v32;
   const double *v64;
   const float *d32;
   const double *d64;
-  const int *tile_row;
-  int n_tiles;
+  const int *cta_slice;
   const double *b;
   double *x;
   double *r64;
@@ -63,7 +68,7 @@ struct PcgParams {
   double *partial;  // [2][kSlots][grid]
   unsigned int *bar;
   int *control;     // [0] error status
-  double *result;   // 8 doubles
+  double *result;   // kResultDoubles
   int precision, relative, max_it, max_updates, guard;
   double tol, delta;
   unsigned long long limit_ns;
@@ -117,7 +122,7 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
 
 // CTA-wide sums of nslot per-thread values into this phase's partial buffer.
 __device__ void write_partials(const PcgParams &P, unsigned int phase, const double *v, int nslot) {
-  __shared__ double red[kSlots][kThreads / 32];
+  __shared__ double red[kSlots][kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int s = 0; s < nslot; ++s) {
     double x = v[s];
@@ -128,7 +133,7 @@ __device__ void write_partials(const PcgParams &P, unsigned int phase, const dou
   __syncthreads();
   if (threadIdx.x < nslot) {
     double x = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) x += red[threadIdx.x][w];
+    for (int w = 0; w < kWarps; ++w) x += red[threadIdx.x][w];
     P.partial[((size_t)((phase + 1) & 1) * kSlots + threadIdx.x) * gridDim.x + blockIdx.x] = x;
   }
 }
@@ -163,142 +168,40 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __syncthreads();
 }
 
-// ---------------------------------------------------------------- tile staging
-// The (column, value) stream of a tile is copied global -> shared by the bulk
-// async-copy engine (cp.async.bulk, completion on an mbarrier), double
-// buffered so that the next tile streams while the current one is gathered
-// and summed.  Ranges are widened to 16-byte boundaries (the matrix arrays are
-// padded) and the extra entries are ignored.
-constexpr int kTileCap = kTileNnz + 8;
-struct __align__(16) TileBuf {
-  int col[kTileCap];
-  double val[kTileCap];  // FP32 tiles use the first half as float[]
-};
-struct StageSmem {
-  TileBuf buf[2];
-  unsigned long long mbar[2];
-};
-
-__device__ __forceinline__ unsigned smem_addr(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long *m) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(m)) : "memory");
-}
-
-// The matrix is streamed once per SpMV: evict it first from L2 so that the
-// solver vectors (a few MB, reused every phase) stay resident.
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
-                                          unsigned long long *m) {
-  unsigned long long policy;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
-          smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(m)), "l"(policy)
-      : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect(unsigned long long *m, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
-               "r"(bytes)
-               : "memory");
-}
-
-// Bounded wait on an mbarrier phase; returns false (and flags the solve) if
-// the copy did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *m, unsigned parity, int *control) {
-  const unsigned a = smem_addr(m);
-  for (unsigned spin = 0; spin < (1u << 26); ++spin) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  atomicCAS(control, 0, FFG_TIMEOUT);
-  return false;
-}
-
-template <typename VT>
-__device__ __forceinline__ void issue_tile(const PcgParams &P, const VT *val, int t, TileBuf &b,
-                                           unsigned long long *m) {
-  const int r0 = P.tile_row[t], r1 = P.tile_row[t + 1];
-  const int64_t a0 = P.rp[r0] & ~(int64_t)3;
-  const int64_t a1 = (P.rp[r1] + 3) & ~(int64_t)3;
-  const unsigned n = (unsigned)(a1 - a0);
-  const unsigned cb = n * 4u, vb = n * (unsigned)sizeof(VT);
-  mbar_expect(m, cb + vb);
-  bulk_load(b.col, P.col + a0, cb, m);
-  bulk_load(b.val, val + a0, vb, m);
-}
-
-// Tile SpMV: for every row r of this CTA's tiles, epi(r, sum_k A_rk gather(c_k)).
-// Rows are summed by groups of 4 lanes in a fixed order (lane-strided partial
-// sums, then a butterfly); lane 0 of the group applies the epilogue.
-template <typename VT, typename AT, class G, class Epi>
-__device__ __forceinline__ void spmv_tiles(const PcgParams &P, const VT *__restrict__ val,
-                                           StageSmem &S, unsigned &parity_bits, G gather,
-                                           Epi epi) {
-  const int first = blockIdx.x;
-  if (first >= P.n_tiles) return;
-  if (threadIdx.x == 0) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    issue_tile<VT>(P, val, first, S.buf[0], &S.mbar[0]);
-  }
-  int slot = 0;
-  for (int t = first; t < P.n_tiles; t += gridDim.x, slot ^= 1) {
-    const int nt = t + gridDim.x;
-    if (threadIdx.x == 0 && nt < P.n_tiles) {
-      // the other buffer was last read before the trailing __syncthreads of the
-      // previous tile; order those generic accesses before the async copy
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile<VT>(P, val, nt, S.buf[slot ^ 1], &S.mbar[slot ^ 1]);
-    }
-    TileBuf &B = S.buf[slot];
-    const bool arrived = mbar_wait(&S.mbar[slot], (parity_bits >> slot) & 1u, P.control);
-    parity_bits ^= (1u << slot);
-    // a copy that never completed leaves the buffer undefined: its column
-    // indices are not dereferenced (the solve already reports FFG_TIMEOUT)
-    if (!__syncthreads_and(arrived)) continue;
-    const int r0 = P.tile_row[t], r1 = P.tile_row[t + 1];
-    const int64_t e0 = P.rp[r0], e1 = P.rp[r1];
-    const int64_t a0 = e0 & ~(int64_t)3;
-    const int lo = (int)(e0 - a0), hi = (int)(e1 - a0);
-    const VT *sv = reinterpret_cast<const VT *>(B.val);
-    AT *prod = reinterpret_cast<AT *>(B.val);
-#pragma unroll 4
-    for (int k = lo + threadIdx.x; k < hi; k += kThreads) {
-      const AT a = (AT)sv[k];
-      prod[k] = a * gather(B.col[k]);
-    }
-    __syncthreads();
-    const int g = threadIdx.x >> 2, j = threadIdx.x & 3;
-    for (int base = r0; base < r1; base += kThreads / 4) {
-      const int row = base + g;
-      AT s = 0;
-      if (row < r1) {
-        const int k0 = (int)(P.rp[row] - a0), k1 = (int)(P.rp[row + 1] - a0);
-        for (int k = k0 + j; k < k1; k += 4) s += prod[k];
+// SELL SpMV over this CTA's slices: epi(row, sum_k A_rk gather(c_k)) for every
+// real row.  Warp w takes slices s0+w, s0+w+32, ...; lane l owns row 32s+l.
+template <typename VT, class G, class Epi>
+__device__ __forceinline__ void spmv_slices(const PcgParams &P, const VT *__restrict__ val, G gather,
+                                            Epi epi) {
+  const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = s0 + warp; s < s1; s += kWarps) {
+    const int64_t base = P.soff[s] + lane;
+    const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
+    const int row = s * kSliceRows + lane;
+    VT acc = 0;
+    if (P.dcol) {
+#pragma unroll 8
+      for (int j = 0; j < len; ++j) {
+        const int64_t k = base + (int64_t)j * kSliceRows;
+        acc += __ldcs(val + k) * gather(row + (int)__ldcs(P.dcol + k));
       }
-      s += __shfl_xor_sync(0xffffffffu, s, 1);
-      s += __shfl_xor_sync(0xffffffffu, s, 2);
-      if (row < r1 && j == 0) epi(row, s);
+    } else {
+#pragma unroll 8
+      for (int j = 0; j < len; ++j) {
+        const int64_t k = base + (int64_t)j * kSliceRows;
+        acc += __ldcs(val + k) * gather(__ldcs(P.col + k));
+      }
     }
-    __syncthreads();
+    if (row < P.n) epi(row, acc);
   }
 }
 
 template <class F>
 __device__ __forceinline__ void for_rows(const PcgParams &P, F f) {
-  for (int t = blockIdx.x; t < P.n_tiles; t += gridDim.x) {
-    const int r0 = P.tile_row[t], r1 = P.tile_row[t + 1];
-    for (int r = r0 + threadIdx.x; r < r1; r += kThreads) f(r);
-  }
+  const int64_t r0 = (int64_t)P.cta_slice[blockIdx.x] * kSliceRows;
+  const int64_t r1 = min((int64_t)P.cta_slice[blockIdx.x + 1] * kSliceRows, P.n);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) f((int)r);
 }
 
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
@@ -321,7 +224,7 @@ struct Outcome {
 
 // Device time of the phases seen by CTA 0 (the others are symmetric):
 // SpMV work, wait at the following barrier, vector work, wait, and the
-// reliable-update phases.
+// residual-replacement phases.
 struct Timing {
   unsigned long long a = 0, aw = 0, b = 0, bw = 0, u = 0;
 };
@@ -334,8 +237,9 @@ __device__ __forceinline__ unsigned long long stamp() {
 // `continuation` runs the FP64 loop after a stagnated mixed solve: its target
 // is the true residual tol*||b|| and its guard is the SPD one.
 template <typename V>
-__device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &phase, unsigned &parity_bits,
-                   unsigned long long t_start, bool continuation, Outcome &o, Timing &tm) {
+__device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
+                                unsigned long long t_start, bool continuation, Outcome &o,
+                                Timing &tm) {
   using V2 = typename VecOf<V>::V2;
   constexpr bool kMixed = sizeof(V) == 4;
   const V *A = kMixed ? (const V *)P.v32 : (const V *)P.v64;
@@ -350,14 +254,14 @@ __device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &
   // r64 = b - A x, ||r64||, ||b||
   t0 = stamp();
   part[0] = part[1] = 0.0;
-  spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
-                             [&](int row, double s) {
-                               const double bb = P.b[row];
-                               const double rr = bb - s;
-                               P.r64[row] = rr;
-                               part[0] += rr * rr;
-                               part[1] += bb * bb;
-                             });
+  spmv_slices<double>(P, P.v64, [&](int c) { return P.x[c]; },
+                      [&](int row, double s) {
+                        const double bb = P.b[row];
+                        const double rr = bb - s;
+                        P.r64[row] = rr;
+                        part[0] += rr * rr;
+                        part[1] += bb * bb;
+                      });
   write_partials(P, phase, part, 2);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 2);
@@ -396,18 +300,18 @@ __device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp();
     part[0] = 0.0;
-    spmv_tiles<V, V>(P, A, S, parity_bits,
-                     [&](int c) {
-                       const V2 a = zc[c];
-                       return a.x + bt * a.y;
-                     },
-                     [&](int row, V s) {
-                       const V2 a = zc[row];
-                       const V pn = a.x + bt * a.y;
-                       zn[row].y = pn;
-                       q[row] = s;
-                       part[0] += (double)pn * (double)s;
-                     });
+    spmv_slices<V>(P, A,
+                   [&](int c) {
+                     const V2 a = zc[c];
+                     return a.x + bt * a.y;
+                   },
+                   [&](int row, V s) {
+                     const V2 a = zc[row];
+                     const V pn = a.x + bt * a.y;
+                     zn[row].y = pn;
+                     q[row] = s;
+                     part[0] += (double)pn * (double)s;
+                   });
     write_partials(P, phase, part, 1);
     t1 = stamp();
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -428,12 +332,13 @@ __device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &
     part[0] = part[1] = 0.0;
     part[2] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
     for_rows(P, [&](int row) {
-      const V pn = zn[row].y;
-      P.x[row] = P.x[row] + xs * (double)pn;
+      V2 a = zn[row];
+      P.x[row] = P.x[row] + xs * (double)a.y;
       const V rr = r[row] - al * q[row];
       r[row] = rr;
       const V z = dinv[row] * rr;
-      zn[row].x = z;
+      a.x = z;
+      zn[row] = a;
       part[0] += (double)rr * (double)rr;
       part[1] += (double)rr * (double)z;
     });
@@ -457,20 +362,18 @@ __device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &
       ++o.updates;
       t0 = stamp();
       part[0] = 0.0;
-      spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
-                                 [&](int row, double s) {
-                                   const double v = P.b[row] - s;
-                                   P.r64[row] = v;
-                                   part[0] += v * v;
-                                 });
+      spmv_slices<double>(P, P.v64, [&](int c) { return P.x[c]; },
+                          [&](int row, double s) {
+                            const double v = P.b[row] - s;
+                            P.r64[row] = v;
+                            part[0] += v * v;
+                          });
       write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
       true_res = sqrt(red[0]);
       if (true_res <= target) { converged = 1; tm.u += stamp() - t0; break; }
       if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
-      // FP32 recurrences that no longer reduce the true residual (condition
-      // number beyond FP32 reach) hand the solve to the FP64 loop
       stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
       last_true = true_res;
       if (stall >= 2) { o.stagnated = 1; tm.u += stamp() - t0; break; }
@@ -511,11 +414,11 @@ __device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &
   // true FP64 residual of the returned x
   t0 = stamp();
   part[0] = 0.0;
-  spmv_tiles<double, double>(P, P.v64, S, parity_bits, [&](int c) { return P.x[c]; },
-                             [&](int row, double s) {
-                               const double v = P.b[row] - s;
-                               part[0] += v * v;
-                             });
+  spmv_slices<double>(P, P.v64, [&](int c) { return P.x[c]; },
+                      [&](int row, double s) {
+                        const double v = P.b[row] - s;
+                        part[0] += v * v;
+                      });
   write_partials(P, phase, part, 1);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 1);
@@ -524,29 +427,20 @@ __device__ __noinline__ void cg(const PcgParams &P, StageSmem &S, unsigned int &
   if (kMixed) o.final_res = o.true_res;
 }
 
-__global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
-  extern __shared__ __align__(128) unsigned char dyn[];
-  StageSmem &S = *reinterpret_cast<StageSmem *>(dyn);
-  if (threadIdx.x == 0) {
-    mbar_init(&S.mbar[0]);
-    mbar_init(&S.mbar[1]);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
+__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(PcgParams P) {
   unsigned int phase = 0;
-  unsigned parity_bits = 0;
   // only block 0 judges the wall limit; its verdict travels through a partial slot
   const unsigned long long t_start = globaltimer();
   Outcome o;
   Timing tm;
   int continued = 0;
   if (P.precision == FFG_PRECISION_FP64) {
-    cg<double>(P, S, phase, parity_bits, t_start, false, o, tm);
+    cg<double>(P, phase, t_start, false, o, tm);
   } else {
-    cg<float>(P, S, phase, parity_bits, t_start, false, o, tm);
+    cg<float>(P, phase, t_start, false, o, tm);
     if (!o.aborted && o.stagnated && !o.converged && o.status == FFG_OK) {
       continued = 1;
-      cg<double>(P, S, phase, parity_bits, t_start, true, o, tm);
+      cg<double>(P, phase, t_start, true, o, tm);
     }
   }
   if (o.aborted) return;
@@ -567,46 +461,100 @@ __global__ void __launch_bounds__(kThreads, 2) pcg_kernel(PcgParams P) {
   }
 }
 
-// Standalone FP64 tile SpMV (one CTA per tile).
-__global__ void __launch_bounds__(kThreads) spmv64_kernel(int64_t n, const int64_t *rp,
-                                                          const int *col, const double *val,
-                                                          const int *tile_row, int n_tiles,
-                                                          const double *x, double *y) {
-  __shared__ double sm[kTileNnz];
-  const int t = blockIdx.x;
-  if (t >= n_tiles) return;
-  const int r0 = tile_row[t], r1 = tile_row[t + 1];
-  const int64_t e0 = rp[r0];
-  const int E = (int)(rp[r1] - e0);
-  for (int k = threadIdx.x; k < E; k += kThreads) sm[k] = val[e0 + k] * x[col[e0 + k]];
-  __syncthreads();
-  for (int r = r0 + threadIdx.x; r < r1; r += kThreads) {
-    const int k0 = (int)(rp[r] - e0), k1 = (int)(rp[r + 1] - e0);
-    double s = 0.0;
-    for (int k = k0; k < k1; ++k) s += sm[k];
-    y[r] = s;
+// Drop-in FP64 CSR SpMV, one thread per row (spmv / csc_matvec semantics).
+__global__ void csr_spmv64_kernel(int64_t n, const int64_t *rp, const int *ci, const double *v,
+                                  const double *x, double *y) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int64_t k = rp[i]; k < rp[i + 1]; ++k) s += v[k] * x[ci[k]];
+  y[i] = s;
+}
+
+// FP32 copy of SELL values and the Jacobi inverse diagonal, from the CSR
+// (old numbering) through the entry positions `pos`.
+__global__ void sell_prepare_kernel(int64_t n, const int64_t *rp, const int *ci,
+                                    const int64_t *pos, const int *iperm, const double *v64,
+                                    float *v32, double *d64, float *d32, int jacobi) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double d = 0.0;
+  for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+    const double a = v64[pos[k]];
+    v32[pos[k]] = (float)a;
+    if (ci[k] == (int)i) d = a;
   }
+  // build_sparse_preconditioner("jacobi"), advanced_solvers.f90:1139-1154
+  const double di = (jacobi && fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
+  d64[iperm[i]] = di;
+  d32[iperm[i]] = (float)di;
 }
 
 }  // namespace
-
-int tile_capacity() { return kTileNnz; }
-int matrix_padding() { return 8; }
 
 int pcg_grid_size(int *grid) {
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return FFG_CUDA_ERROR;
-  if (cudaFuncSetAttribute(pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(StageSmem)) != cudaSuccess)
-    return FFG_CUDA_ERROR;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, kThreads,
-                                                    sizeof(StageSmem)) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, kThreads, 0) !=
+      cudaSuccess)
     return FFG_CUDA_ERROR;
   if (per_sm < 1) return FFG_CUDA_ERROR;
-  *grid = sms * std::min(per_sm, 2);
+  *grid = sms;  // one 1024-thread CTA per SM
   return FFG_OK;
+}
+
+int upload_sell(const HostSell &h, int grid, DeviceSell &d) {
+  free_sell(d);
+  d.n = h.n;
+  d.n_slices = h.n_slices;
+  d.padded = h.padded;
+  d.grid = grid;
+  bool bad = false;
+  auto A = [&](void **p, size_t bytes) {
+    if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) { bad = true; *p = nullptr; }
+  };
+  const size_t P = (size_t)std::max<int64_t>(h.padded, 1), N = (size_t)std::max<int64_t>(h.n, 1);
+  A((void **)&d.soff, sizeof(int64_t) * h.soff.size());
+  if (h.narrow) A((void **)&d.dcol, sizeof(int16_t) * P);
+  else A((void **)&d.col, sizeof(int) * P);
+  A((void **)&d.val64, sizeof(double) * P);
+  A((void **)&d.val32, sizeof(float) * P);
+  A((void **)&d.dinv64, sizeof(double) * N);
+  A((void **)&d.dinv32, sizeof(float) * N);
+  A((void **)&d.perm, sizeof(int) * N);
+  A((void **)&d.iperm, sizeof(int) * N);
+  A((void **)&d.cta_slice, sizeof(int) * (grid + 1));
+  if (bad) { cudaGetLastError(); free_sell(d); return FFG_OUT_OF_MEMORY; }
+  // CTA partition: contiguous slice ranges with about equal stored entries
+  std::vector<int> cs(grid + 1, 0);
+  for (int b = 1; b < grid; ++b) {
+    const int64_t target = (int64_t)((double)h.padded * b / grid);
+    const int s = (int)(std::lower_bound(h.soff.begin(), h.soff.end(), target) - h.soff.begin());
+    cs[b] = std::max(cs[b - 1], std::min<int>(s, (int)h.n_slices));
+  }
+  cs[grid] = (int)h.n_slices;
+  bool ok = true;
+  ok = ok && cudaMemcpy(d.soff, h.soff.data(), sizeof(int64_t) * h.soff.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (h.narrow)
+    ok = ok && cudaMemcpy(d.dcol, h.dcol.data(), sizeof(int16_t) * h.padded, cudaMemcpyHostToDevice) == cudaSuccess;
+  else
+    ok = ok && cudaMemcpy(d.col, h.col.data(), sizeof(int) * h.padded, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemset(d.val64, 0, sizeof(double) * P) == cudaSuccess;
+  ok = ok && cudaMemset(d.val32, 0, sizeof(float) * P) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.perm, h.perm.data(), sizeof(int) * h.n, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.iperm, h.iperm.data(), sizeof(int) * h.n, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.cta_slice, cs.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice) == cudaSuccess;
+  return ok ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+void free_sell(DeviceSell &d) {
+  void *ptrs[] = {d.soff, d.dcol, d.col, d.val64, d.val32, d.dinv64, d.dinv32, d.perm, d.iperm,
+                  d.cta_slice};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  d = DeviceSell();
 }
 
 int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
@@ -647,19 +595,22 @@ void solve_work_free(SolveWork &w) {
   w = SolveWork();
 }
 
-int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_options &opts,
+int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
               SolveWork &w, ffg_solver_stats *stats, cudaStream_t stream, std::string &msg) {
-  if (w.n != A.n || w.grid <= 0) { msg = "solver workspace mismatch"; return FFG_INVALID_INPUT; }
+  if (w.n != A.n || w.grid <= 0 || A.grid != w.grid) {
+    msg = "solver workspace mismatch";
+    return FFG_INVALID_INPUT;
+  }
   PcgParams P;
   P.n = A.n;
-  P.rp = A.row_ptr;
+  P.soff = A.soff;
+  P.dcol = A.dcol;
   P.col = A.col;
   P.v32 = A.val32;
   P.v64 = A.val64;
   P.d32 = A.dinv32;
   P.d64 = A.dinv64;
-  P.tile_row = A.tile_row;
-  P.n_tiles = A.n_tiles;
+  P.cta_slice = A.cta_slice;
   P.b = b;
   P.x = x;
   P.r64 = w.r64;
@@ -682,7 +633,7 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
   if (cudaMemsetAsync(w.control, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   void *args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid),
-                                              dim3(kThreads), args, sizeof(StageSmem), stream);
+                                              dim3(kThreads), args, 0, stream);
   if (e != cudaSuccess) {
     msg = std::string("cooperative launch failed: ") + cudaGetErrorString(e);
     cudaGetLastError();
@@ -713,10 +664,18 @@ int pcg_solve(const DeviceCsr &A, const double *b, double *x, const ffg_solver_o
   return FFG_OK;
 }
 
-int spmv64(const DeviceCsr &A, const double *x, double *y, cudaStream_t stream) {
-  if (A.n_tiles == 0) return FFG_OK;
-  spmv64_kernel<<<A.n_tiles, kThreads, 0, stream>>>(A.n, A.row_ptr, A.col, A.val64, A.tile_row,
-                                                    A.n_tiles, x, y);
+int csr_spmv64(int64_t n, const int64_t *rp, const int *ci, const double *v, const double *x,
+               double *y, cudaStream_t stream) {
+  if (n <= 0) return FFG_OK;
+  csr_spmv64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(n, rp, ci, v, x, y);
+  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+int sell_prepare(DeviceSell &A, const int64_t *rp, const int *ci, const int64_t *pos, bool jacobi,
+                 cudaStream_t s) {
+  if (A.n <= 0) return FFG_OK;
+  sell_prepare_kernel<<<(unsigned)((A.n + 255) / 256), 256, 0, s>>>(
+      A.n, rp, ci, pos, A.iperm, A.val64, A.val32, A.dinv64, A.dinv32, jacobi ? 1 : 0);
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 

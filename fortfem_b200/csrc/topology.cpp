@@ -368,23 +368,79 @@ int build_pattern(Topology &t, std::string &msg) {
   return FFG_OK;
 }
 
-std::vector<int> make_tiles(const std::vector<int64_t> &rp, int tile_nnz, int *max_row) {
-  std::vector<int> tiles;
-  tiles.push_back(0);
-  int64_t n = (int64_t)rp.size() - 1;
-  int64_t start = rp[0];
-  int mr = 0;
-  for (int64_t r = 0; r < n; ++r) {
-    int64_t rl = rp[r + 1] - rp[r];
-    mr = std::max<int64_t>(mr, rl);
-    if (rp[r + 1] - start > tile_nnz && r > tiles.back()) {
-      tiles.push_back((int)r);
-      start = rp[r];
+// SELL-32-sigma layout of a CSR operator.  Rows are stably sorted by length
+// (longest first) inside windows of `sigma` rows, which keeps the padding of
+// each 32-row slice small while moving no row further than sigma; entries of
+// a row keep their CSR order.  Padding entries carry a zero value and point at
+// a valid column (the row itself, or the last row for the rows that only pad
+// the final slice).
+void build_sell(const std::vector<int64_t> &rp, const std::vector<int> &ci, int sigma,
+                HostSell &out) {
+  const int64_t n = (int64_t)rp.size() - 1;
+  out = HostSell();
+  out.n = n;
+  std::vector<int> order((size_t)n);
+  for (int64_t i = 0; i < n; ++i) order[i] = (int)i;
+  auto len = [&](int r) { return rp[r + 1] - rp[r]; };
+  for (int64_t w0 = 0; w0 < n; w0 += sigma) {
+    const int64_t w1 = std::min<int64_t>(n, w0 + sigma);
+    std::stable_sort(order.begin() + w0, order.begin() + w1,
+                     [&](int p, int q) { return len(p) > len(q); });
+  }
+  out.perm = order;
+  out.iperm.assign((size_t)n, 0);
+  for (int64_t i = 0; i < n; ++i) out.iperm[order[i]] = (int)i;
+  out.n_slices = (n + kSliceRows - 1) / kSliceRows;
+  out.soff.assign((size_t)out.n_slices + 1, 0);
+  for (int64_t s = 0; s < out.n_slices; ++s) {
+    int64_t mx = 0;
+    for (int l = 0; l < kSliceRows; ++l) {
+      const int64_t r = s * kSliceRows + l;
+      if (r < n) mx = std::max(mx, len(order[r]));
+    }
+    out.soff[s + 1] = out.soff[s] + mx * kSliceRows;
+  }
+  out.padded = out.soff[out.n_slices];
+  // narrow if every |column - row| (new numbering) fits int16
+  bool narrow = true;
+  for (int64_t i = 0; i < n && narrow; ++i) {
+    const int64_t r = out.iperm[i];
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+      const int64_t d = (int64_t)out.iperm[ci[k]] - r;
+      if (d < -32768 || d > 32767) { narrow = false; break; }
     }
   }
-  if (tiles.back() != n) tiles.push_back((int)n);
-  if (max_row) *max_row = mr;
-  return tiles;
+  out.narrow = narrow;
+  if (narrow) out.dcol.assign((size_t)out.padded, 0);
+  else out.col.assign((size_t)out.padded, 0);
+  out.pos.assign(rp.back(), 0);
+  for (int64_t s = 0; s < out.n_slices; ++s)
+    for (int l = 0; l < kSliceRows; ++l) {
+      const int64_t r = s * kSliceRows + l;
+      const int64_t slen = (out.soff[s + 1] - out.soff[s]) / kSliceRows;
+      const int64_t base = out.soff[s] + l;
+      if (r >= n) {
+        // padding row: every entry points at the last row with a zero value
+        for (int64_t k = 0; k < slen; ++k) {
+          if (narrow) out.dcol[base + k * kSliceRows] = (int16_t)((n - 1) - r);
+          else out.col[base + k * kSliceRows] = (int)(n - 1);
+        }
+        continue;
+      }
+      const int old = order[r];
+      int64_t k = 0;
+      for (int64_t e = rp[old]; e < rp[old + 1]; ++e, ++k) {
+        const int64_t p = base + k * kSliceRows;
+        out.pos[e] = p;
+        const int c = out.iperm[ci[e]];
+        if (narrow) out.dcol[p] = (int16_t)(c - r);
+        else out.col[p] = c;
+      }
+      for (; k < slen; ++k) {
+        if (narrow) out.dcol[base + k * kSliceRows] = 0;
+        else out.col[base + k * kSliceRows] = (int)r;
+      }
+    }
 }
 
 }  // namespace ffg
