@@ -168,33 +168,75 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __syncthreads();
 }
 
-// SELL SpMV over this CTA's slices: epi(row, sum_k A_rk gather(c_k)) for every
-// real row.  Warp w takes slices s0+w, s0+w+32, ...; lane l owns row 32s+l.
-template <typename VT, class G, class Epi>
-__device__ __forceinline__ void spmv_slices(const PcgParams &P, const VT *__restrict__ val, G gather,
-                                            Epi epi) {
+// SELL SpMV over this CTA's slices.  Slices are handed to warps through a
+// shared-memory counter (the CTA's slice range is fixed, so every row is still
+// produced by this CTA); lane l of the warp owns row 32s+l and accumulates it
+// in a fixed order.  Only per-row results are written here; the dot products
+// are taken afterwards in a fixed row order so that results stay
+// bit-reproducible whatever warp computed which slice.
+template <typename V, typename V2, bool NARROW>
+__device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict__ val,
+                                        const V2 *__restrict__ zc, V2 *__restrict__ zn,
+                                        V *__restrict__ q, V beta) {
+  __shared__ int next_slice;
   const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int s = s0 + warp; s < s1; s += kWarps) {
+  if (threadIdx.x == 0) next_slice = s0 + kWarps;
+  __syncthreads();
+  for (int s = s0 + warp; s < s1;) {
     const int64_t base = P.soff[s] + lane;
     const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
     const int row = s * kSliceRows + lane;
-    VT acc = 0;
-    if (P.dcol) {
+    V acc = 0;
 #pragma unroll 8
-      for (int j = 0; j < len; ++j) {
-        const int64_t k = base + (int64_t)j * kSliceRows;
-        acc += __ldcs(val + k) * gather(row + (int)__ldcs(P.dcol + k));
-      }
-    } else {
-#pragma unroll 8
-      for (int j = 0; j < len; ++j) {
-        const int64_t k = base + (int64_t)j * kSliceRows;
-        acc += __ldcs(val + k) * gather(__ldcs(P.col + k));
-      }
+    for (int j = 0; j < len; ++j) {
+      const int64_t k = base + (int64_t)j * kSliceRows;
+      const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
+      const V2 a = zc[c];
+      acc += __ldcs(val + k) * (a.x + beta * a.y);
     }
-    if (row < P.n) epi(row, acc);
+    if (row < P.n) {
+      const V2 a = zc[row];
+      zn[row].y = a.x + beta * a.y;
+      q[row] = acc;
+    }
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&next_slice, 1);
+    s = __shfl_sync(0xffffffffu, t, 0);
   }
+  __syncthreads();
+}
+
+// r64 = b - A64 x over this CTA's slices (same scheduling as spmv_pairs).
+template <bool NARROW>
+__device__ __noinline__ void spmv_residual(const PcgParams &P) {
+  __shared__ int next_slice;
+  const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) next_slice = s0 + kWarps;
+  __syncthreads();
+  for (int s = s0 + warp; s < s1;) {
+    const int64_t base = P.soff[s] + lane;
+    const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
+    const int row = s * kSliceRows + lane;
+    double acc = 0.0;
+#pragma unroll 8
+    for (int j = 0; j < len; ++j) {
+      const int64_t k = base + (int64_t)j * kSliceRows;
+      const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
+      acc += __ldcs(P.v64 + k) * P.x[c];
+    }
+    if (row < P.n) P.r64[row] = P.b[row] - acc;
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&next_slice, 1);
+    s = __shfl_sync(0xffffffffu, t, 0);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void residual(const PcgParams &P) {
+  if (P.dcol) spmv_residual<true>(P);
+  else spmv_residual<false>(P);
 }
 
 template <class F>
@@ -253,15 +295,13 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
 
   // r64 = b - A x, ||r64||, ||b||
   t0 = stamp();
+  residual(P);
   part[0] = part[1] = 0.0;
-  spmv_slices<double>(P, P.v64, [&](int c) { return P.x[c]; },
-                      [&](int row, double s) {
-                        const double bb = P.b[row];
-                        const double rr = bb - s;
-                        P.r64[row] = rr;
-                        part[0] += rr * rr;
-                        part[1] += bb * bb;
-                      });
+  for_rows(P, [&](int row) {
+    const double bb = P.b[row], rr = P.r64[row];
+    part[0] += rr * rr;
+    part[1] += bb * bb;
+  });
   write_partials(P, phase, part, 2);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 2);
@@ -300,18 +340,9 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp();
     part[0] = 0.0;
-    spmv_slices<V>(P, A,
-                   [&](int c) {
-                     const V2 a = zc[c];
-                     return a.x + bt * a.y;
-                   },
-                   [&](int row, V s) {
-                     const V2 a = zc[row];
-                     const V pn = a.x + bt * a.y;
-                     zn[row].y = pn;
-                     q[row] = s;
-                     part[0] += (double)pn * (double)s;
-                   });
+    if (P.dcol) spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
+    else spmv_pairs<V, V2, false>(P, A, zc, zn, q, bt);
+    for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
     write_partials(P, phase, part, 1);
     t1 = stamp();
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -362,12 +393,8 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       ++o.updates;
       t0 = stamp();
       part[0] = 0.0;
-      spmv_slices<double>(P, P.v64, [&](int c) { return P.x[c]; },
-                          [&](int row, double s) {
-                            const double v = P.b[row] - s;
-                            P.r64[row] = v;
-                            part[0] += v * v;
-                          });
+      residual(P);
+      for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
       write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
@@ -414,11 +441,8 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
   // true FP64 residual of the returned x
   t0 = stamp();
   part[0] = 0.0;
-  spmv_slices<double>(P, P.v64, [&](int c) { return P.x[c]; },
-                      [&](int row, double s) {
-                        const double v = P.b[row] - s;
-                        part[0] += v * v;
-                      });
+  residual(P);
+  for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
   write_partials(P, phase, part, 1);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 1);
