@@ -138,9 +138,6 @@ struct SolveWork {
   double2 *zpd0 = nullptr, *zpd1 = nullptr; // FP64-mode (z, p) pairs, double-buffered
   float *rf = nullptr, *qf = nullptr;       // mixed-mode FP32 residual and A p
   float2 *zpf0 = nullptr, *zpf1 = nullptr;  // mixed-mode (z, p) pairs
-  double *slice_dot = nullptr;         // per-slice dot partials
-  unsigned long long *work = nullptr;  // dynamic SpMV work counter
-  int64_t n_slices = 0;
   unsigned int *barrier = nullptr;
   int *control = nullptr;    // [0] error status
   double *result = nullptr;  // device statistics block

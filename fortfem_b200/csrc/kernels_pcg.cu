@@ -46,7 +46,6 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSlots = 4;
 constexpr int kPartialBatch = 8;   // partial loads in flight per lane
 constexpr int kResultDoubles = 16;
-constexpr int kChunkSlices = 4;  // slices per work grab of the dynamic SpMV
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
 
 struct PcgParams {
@@ -67,9 +66,6 @@ struct PcgParams {
   double *rd, *qd;
   double2 *zpd0, *zpd1;
   double *partial;  // [2][kSlots][grid]
-  double *slice_dot;  // per-slice dot partials of the dynamic SpMVs
-  unsigned long long *work;  // global slice-chunk counter of the dynamic SpMVs
-  int n_slices, n_chunks;
   unsigned int *bar;
   int *control;     // [0] error status
   double *result;   // kResultDoubles
@@ -172,103 +168,75 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __syncthreads();
 }
 
-// SELL SpMV, dynamically scheduled over the whole grid: warps grab chunks of
-// kChunkSlices slices from a global counter, so all CTAs finish together.
-// Lane l of a warp owns row 32s+l and accumulates it in a fixed order; the
-// slice's dot-product contribution is reduced over the lanes in a fixed order
-// and stored per slice, and every CTA later sums the slice partials in one
-// fixed order, so results are bit-reproducible whichever warp did which slice.
-// `base` is the counter value at which this call's chunks start; every warp
-// overshoots exactly once, so the next call starts at
-// base + n_chunks + gridDim.x * kWarps on every CTA.
-__device__ __forceinline__ int grab_chunk(const PcgParams &P, unsigned long long base) {
-  unsigned long long t = 0;
-  if ((threadIdx.x & 31) == 0) t = atomicAdd(P.work, 1ull);
-  t = __shfl_sync(0xffffffffu, t, 0);
-  const long long c = (long long)(t - base);
-  return c < P.n_chunks ? (int)c : -1;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
+// SELL SpMV over this CTA's slices.  Slices are handed to warps through a
+// shared-memory counter (the CTA's slice range is fixed, so every row is still
+// produced by this CTA); lane l of the warp owns row 32s+l and accumulates it
+// in a fixed order.  Only per-row results are written here; the dot products
+// are taken afterwards in a fixed row order so that results stay
+// bit-reproducible whatever warp computed which slice.
 template <typename V, typename V2, bool NARROW>
-__device__ __noinline__ void spmv_pairs(const PcgParams &P, unsigned long long base,
-                                        const V *__restrict__ val, const V2 *__restrict__ zc,
-                                        V2 *__restrict__ zn, V *__restrict__ q, V beta) {
-  const int lane = threadIdx.x & 31;
-  for (int c = grab_chunk(P, base); c >= 0; c = grab_chunk(P, base)) {
-    const int s_end = min((c + 1) * kChunkSlices, P.n_slices);
-    for (int s = c * kChunkSlices; s < s_end; ++s) {
-      const int64_t b0 = P.soff[s] + lane;
-      const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
-      const int row = s * kSliceRows + lane;
-      V acc = 0;
+__device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict__ val,
+                                        const V2 *__restrict__ zc, V2 *__restrict__ zn,
+                                        V *__restrict__ q, V beta) {
+  __shared__ int next_slice;
+  const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) next_slice = s0 + kWarps;
+  __syncthreads();
+  for (int s = s0 + warp; s < s1;) {
+    const int64_t base = P.soff[s] + lane;
+    const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
+    const int row = s * kSliceRows + lane;
+    V acc = 0;
 #pragma unroll 8
-      for (int j = 0; j < len; ++j) {
-        const int64_t k = b0 + (int64_t)j * kSliceRows;
-        const int col = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
-        const V2 a = zc[col];
-        acc += __ldcs(val + k) * (a.x + beta * a.y);
-      }
-      double d = 0.0;
-      if (row < P.n) {
-        const V2 a = zc[row];
-        const V pn = a.x + beta * a.y;
-        zn[row].y = pn;
-        q[row] = acc;
-        d = (double)pn * (double)acc;
-      }
-      d = warp_sum(d);
-      if (lane == 0) P.slice_dot[s] = d;
+    for (int j = 0; j < len; ++j) {
+      const int64_t k = base + (int64_t)j * kSliceRows;
+      const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
+      const V2 a = zc[c];
+      acc += __ldcs(val + k) * (a.x + beta * a.y);
     }
+    if (row < P.n) {
+      const V2 a = zc[row];
+      zn[row].y = a.x + beta * a.y;
+      q[row] = acc;
+    }
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&next_slice, 1);
+    s = __shfl_sync(0xffffffffu, t, 0);
   }
+  __syncthreads();
 }
 
-// r64 = b - A64 x with slice partials of ||r64||^2 (same scheduling).
+// r64 = b - A64 x over this CTA's slices (same scheduling as spmv_pairs).
 template <bool NARROW>
-__device__ __noinline__ void spmv_residual(const PcgParams &P, unsigned long long base) {
-  const int lane = threadIdx.x & 31;
-  for (int c = grab_chunk(P, base); c >= 0; c = grab_chunk(P, base)) {
-    const int s_end = min((c + 1) * kChunkSlices, P.n_slices);
-    for (int s = c * kChunkSlices; s < s_end; ++s) {
-      const int64_t b0 = P.soff[s] + lane;
-      const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
-      const int row = s * kSliceRows + lane;
-      double acc = 0.0;
+__device__ __noinline__ void spmv_residual(const PcgParams &P) {
+  __shared__ int next_slice;
+  const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) next_slice = s0 + kWarps;
+  __syncthreads();
+  for (int s = s0 + warp; s < s1;) {
+    const int64_t base = P.soff[s] + lane;
+    const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
+    const int row = s * kSliceRows + lane;
+    double acc = 0.0;
 #pragma unroll 8
-      for (int j = 0; j < len; ++j) {
-        const int64_t k = b0 + (int64_t)j * kSliceRows;
-        const int col = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
-        acc += __ldcs(P.v64 + k) * P.x[col];
-      }
-      double d = 0.0;
-      if (row < P.n) {
-        const double r = P.b[row] - acc;
-        P.r64[row] = r;
-        d = r * r;
-      }
-      d = warp_sum(d);
-      if (lane == 0) P.slice_dot[s] = d;
+    for (int j = 0; j < len; ++j) {
+      const int64_t k = base + (int64_t)j * kSliceRows;
+      const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
+      acc += __ldcs(P.v64 + k) * P.x[c];
     }
+    if (row < P.n) P.r64[row] = P.b[row] - acc;
+    int t = 0;
+    if (lane == 0) t = atomicAdd(&next_slice, 1);
+    s = __shfl_sync(0xffffffffu, t, 0);
   }
+  __syncthreads();
 }
 
-// Sum of the slice partials in a fixed order (identical on every CTA).
-__device__ double sum_slices(const PcgParams &P) {
-  __shared__ double red[kWarps];
-  double v = 0.0;
-  for (int s = threadIdx.x; s < P.n_slices; s += kThreads) v += __ldcg(P.slice_dot + s);
-  v = warp_sum(v);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double t = 0.0;
-  for (int w = 0; w < kWarps; ++w) t += red[w];
-  __syncthreads();
-  return t;
+__device__ __forceinline__ void residual(const PcgParams &P) {
+  if (P.dcol) spmv_residual<true>(P);
+  else spmv_residual<false>(P);
 }
 
 template <class F>
@@ -311,7 +279,7 @@ __device__ __forceinline__ unsigned long long stamp() {
 // `continuation` runs the FP64 loop after a stagnated mixed solve: its target
 // is the true residual tol*||b|| and its guard is the SPD one.
 template <typename V>
-__device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase, unsigned long long &work,
+__device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
                                 unsigned long long t_start, bool continuation, Outcome &o,
                                 Timing &tm) {
   using V2 = typename VecOf<V>::V2;
@@ -323,27 +291,22 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase, unsigne
   V2 *zp[2] = {kMixed ? (V2 *)P.zpf0 : (V2 *)P.zpd0, kMixed ? (V2 *)P.zpf1 : (V2 *)P.zpd1};
   double part[kSlots], red[kSlots];
   const bool true_target = kMixed || continuation;
-  const unsigned long long work_step = (unsigned long long)P.n_chunks + gridDim.x * kWarps;
-  auto residual = [&]() {
-    if (P.dcol) spmv_residual<true>(P, work);
-    else spmv_residual<false>(P, work);
-    work += work_step;
-  };
   unsigned long long t0, t1, t2;
 
   // r64 = b - A x, ||r64||, ||b||
   t0 = stamp();
-  residual();
-  part[0] = 0.0;
+  residual(P);
+  part[0] = part[1] = 0.0;
   for_rows(P, [&](int row) {
-    const double bb = P.b[row];
-    part[0] += bb * bb;
+    const double bb = P.b[row], rr = P.r64[row];
+    part[0] += rr * rr;
+    part[1] += bb * bb;
   });
-  write_partials(P, phase, part, 1);
+  write_partials(P, phase, part, 2);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
-  read_partials(P, phase, red, 1);
-  const double bnorm = sqrt(red[0]);
-  const double rnorm = sqrt(sum_slices(P));
+  read_partials(P, phase, red, 2);
+  const double bnorm = sqrt(red[1]);
+  const double rnorm = sqrt(red[0]);
   o.bnorm = bnorm;
   double scale = kMixed ? (rnorm > 0.0 ? rnorm : 1.0) : 1.0;
   const double target = P.relative ? P.tol * (true_target ? bnorm : rnorm) : P.tol;
@@ -377,15 +340,17 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase, unsigne
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp();
     part[0] = 0.0;
-    if (P.dcol) spmv_pairs<V, V2, true>(P, work, A, zc, zn, q, bt);
-    else spmv_pairs<V, V2, false>(P, work, A, zc, zn, q, bt);
-    work += work_step;
+    if (P.dcol) spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
+    else spmv_pairs<V, V2, false>(P, A, zc, zn, q, bt);
+    for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
+    write_partials(P, phase, part, 1);
     t1 = stamp();
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
-    const double pAp = sum_slices(P);
+    read_partials(P, phase, red, 1);
     t2 = stamp();
     tm.a += t1 - t0;
     tm.aw += t2 - t1;
+    const double pAp = red[0];
     const bool breakdown = (!kMixed && !continuation && P.guard == 0)
                                ? (fabs(pAp) < 1.0e-14)
                                : !(pAp > 0.0 && is_finite_d(pAp));
@@ -428,9 +393,12 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase, unsigne
       ++o.updates;
       t0 = stamp();
       part[0] = 0.0;
-      residual();
+      residual(P);
+      for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+      write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
-      true_res = sqrt(sum_slices(P));
+      read_partials(P, phase, red, 1);
+      true_res = sqrt(red[0]);
       if (true_res <= target) { converged = 1; tm.u += stamp() - t0; break; }
       if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
       stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
@@ -473,28 +441,30 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase, unsigne
   // true FP64 residual of the returned x
   t0 = stamp();
   part[0] = 0.0;
-  residual();
+  residual(P);
+  for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+  write_partials(P, phase, part, 1);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
-  o.true_res = sqrt(sum_slices(P));
+  read_partials(P, phase, red, 1);
   tm.u += stamp() - t0;
+  o.true_res = sqrt(red[0]);
   if (kMixed) o.final_res = o.true_res;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(PcgParams P) {
   unsigned int phase = 0;
-  unsigned long long work = 0;
   // only block 0 judges the wall limit; its verdict travels through a partial slot
   const unsigned long long t_start = globaltimer();
   Outcome o;
   Timing tm;
   int continued = 0;
   if (P.precision == FFG_PRECISION_FP64) {
-    cg<double>(P, phase, work, t_start, false, o, tm);
+    cg<double>(P, phase, t_start, false, o, tm);
   } else {
-    cg<float>(P, phase, work, t_start, false, o, tm);
+    cg<float>(P, phase, t_start, false, o, tm);
     if (!o.aborted && o.stagnated && !o.converged && o.status == FFG_OK) {
       continued = 1;
-      cg<double>(P, phase, work, t_start, true, o, tm);
+      cg<double>(P, phase, t_start, true, o, tm);
     }
   }
   if (o.aborted) return;
@@ -630,9 +600,6 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
   A((void **)&w.zpf0, N * sizeof(float2));
   A((void **)&w.zpf1, N * sizeof(float2));
   A((void **)&w.partial, 2 * kSlots * (size_t)grid * sizeof(double));
-  w.n_slices = (n + kSliceRows - 1) / kSliceRows;
-  A((void **)&w.slice_dot, (size_t)std::max<int64_t>(w.n_slices, 1) * sizeof(double));
-  A((void **)&w.work, 64);
   A((void **)&w.barrier, 64);
   A((void **)&w.control, 64);
   A((void **)&w.result, kResultDoubles * sizeof(double));
@@ -646,7 +613,7 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
 
 void solve_work_free(SolveWork &w) {
   void *ptrs[] = {w.r64, w.rd, w.qd, w.zpd0, w.zpd1, w.rf, w.qf, w.zpf0, w.zpf1, w.partial,
-                  w.slice_dot, w.work, w.barrier, w.control, w.result};
+                  w.barrier, w.control, w.result};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   w = SolveWork();
@@ -674,10 +641,6 @@ int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_
   P.rf = w.rf; P.qf = w.qf; P.zpf0 = w.zpf0; P.zpf1 = w.zpf1;
   P.rd = w.rd; P.qd = w.qd; P.zpd0 = w.zpd0; P.zpd1 = w.zpd1;
   P.partial = w.partial;
-  P.slice_dot = w.slice_dot;
-  P.work = w.work;
-  P.n_slices = (int)A.n_slices;
-  P.n_chunks = (int)((A.n_slices + kChunkSlices - 1) / kChunkSlices);
   P.bar = w.barrier;
   P.control = w.control;
   P.result = w.result;
@@ -692,9 +655,6 @@ int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_
   P.limit_ns = (unsigned long long)(limit * 1e9);
   if (cudaMemsetAsync(w.barrier, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaMemsetAsync(w.control, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
-  if (cudaMemsetAsync(w.work, 0, sizeof(unsigned long long), stream) != cudaSuccess)
-    return FFG_CUDA_ERROR;
-  if (w.n_slices < A.n_slices) { msg = "solver workspace too small"; return FFG_INVALID_INPUT; }
   void *args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid),
                                               dim3(kThreads), args, 0, stream);
