@@ -35,6 +35,7 @@ FFG_BOUNDARY_MASK = 2
 FFG_PRECISION_FP64 = 0
 FFG_PRECISION_MIXED = 1
 FFG_OPTIONS_VERSION = 1
+FFG_NOALLOC_MAX_ROWS = 65536
 
 STATUS_TEXT = {
     FFG_OK: "ok", FFG_INVALID_INPUT: "invalid input", FFG_CAPACITY: "capacity too small",
@@ -80,6 +81,9 @@ SIGNATURES = {
     "ffg_solve_sparse": (
         None, [i32, i64, vp, vp, vp, vp, vp, C.POINTER(SolverOptionsC), C.POINTER(SolverStatsC), pi32]),
     "ffg_csc_matvec": (None, [i32, i64, vp, vp, vp, vp, vp, pi32]),
+    "ffg_solve_csr_device_noalloc": (
+        None, [i32, i64, vp, vp, vp, vp, vp, C.POINTER(SolverOptionsC), C.POINTER(SolverStatsC),
+               vp, pi32]),
     "ffg_build_topology": (
         None, [i32, i32, i32, i32, vp, i32, vp, i64, i64, pi64, pi64, pi64, vp, vp, vp, vp, pi32]),
     "ffg_problem_create": (

@@ -23,7 +23,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
           "-I" + os.path.join(HERE, "..", "include")]
-SOURCES = ["topology.cpp", "basis.cpp", "kernels_assemble.cu", "kernels_pcg.cu", "capi.cu"]
+SOURCES = ["topology.cpp", "basis.cpp", "kernels_assemble.cu", "kernels_pcg.cu", "capi.cu",
+           "noalloc.cu"]
 
 
 def _headers():

@@ -169,6 +169,27 @@ void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row
 void ffg_csc_matvec(int n, int64_t nnz, const int64_t *col_ptr, const int *row_ind,
                     const double *values, const double *x, double *y, int *status);
 
+/* No counterpart in the reference.  FP64 Jacobi-PCG (the FP64 mode of
+ * ffg_solve_sparse) on a matrix already in device memory, for callers that
+ * may not allocate device memory: codes that own all of the GPU's memory in
+ * their own arena, and solve loops that cannot let cudaFree synchronise the
+ * device.  It calls no cudaMalloc or cudaFree; its work vectors live in one
+ * fixed device array that holds systems of up to FFG_NOALLOC_MAX_ROWS rows
+ * (larger n returns FFG_CAPACITY).  row_ptr (n+1), col_ind and values
+ * (nnz) are a zero-based CSR matrix in device memory; a symmetric matrix's
+ * CSC arrays serve unchanged.  b and x are device vectors, x holding the
+ * initial guess on entry and the solution on exit.  opts as ffg_solve_sparse,
+ * except that precision is always FP64.  The work runs on `stream` (a
+ * cudaStream_t, 0 = default); the call returns once it has finished.
+ * The first call with a device current looks up the array's address on that
+ * device, so it should come before any stream capture.  All calls share the
+ * array: calls whose work overlaps on one GPU race, so serialise them. */
+#define FFG_NOALLOC_MAX_ROWS 65536
+void ffg_solve_csr_device_noalloc(int n, int64_t nnz, const int64_t *row_ptr,
+                                  const int *col_ind, const double *values, const double *b,
+                                  double *x, const ffg_solver_options *opts,
+                                  ffg_solver_stats *stats, void *stream, int *status);
+
 /* Host-only topology of a problem (no device needed): the global DoF of every
  * local DoF (build_tetra_lagrange_dof_map, tetra_lagrange_global_dof_map.f90:13-79;
  * build_tetra_nedelec_dof_map, tetra_nedelec_global_dof_map.f90:15-105), the
