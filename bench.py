@@ -33,6 +33,13 @@ METRIC = ("assembled+solved DoF/s at rel. residual 1e-10 (mixed vs FP64); "
           "p50/p99 solve latency")
 WORKLOAD = "p2_tetra_poisson_48cube_x6_jittered_lognormal"
 TOL = 1e-10
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pcg_kernel
+# launch on the 48^3 workload, from an ncu capture of
+# `bench.py --steps 1 --warmup 3 --no-cpu --no-e2e --no-fp64`, and the
+# algorithmic bytes of that launch; the live launch's traffic is scaled by
+# its own algorithmic bytes.
+PCG_TRAFFIC_BYTES = 101.105605e9 + 1.643863e9
+PCG_TRAFFIC_ALG_BYTES = 158143482268.0
 
 
 def parse():
@@ -286,7 +293,9 @@ def run_ours(args):
     achieved = alg / kt / 1e9
     roofline = {"kernel": "pcg_kernel (persistent mixed Jacobi-PCG)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": None,
+                "peak_source": peak_kind,
+                "traffic": (PCG_TRAFFIC_BYTES * alg / PCG_TRAFFIC_ALG_BYTES
+                            if args.size == 48 else None),
                 "algorithmic_bytes_per_launch": alg, "kernel_ms": kt * 1e3}
 
     line = {"metric": METRIC, "value": value, "unit": "DoF/s", "n_gpus": world,
