@@ -38,7 +38,7 @@ TOL = 1e-10
 # `bench.py --steps 1 --warmup 3 --no-cpu --no-e2e --no-fp64`, and the
 # algorithmic bytes of that launch; the live launch's traffic is scaled by
 # its own algorithmic bytes.
-PCG_TRAFFIC_BYTES = 101.105605e9 + 1.643863e9
+PCG_TRAFFIC_BYTES = 105.395462e9 + 15.132652e9
 PCG_TRAFFIC_ALG_BYTES = 158143482268.0
 
 

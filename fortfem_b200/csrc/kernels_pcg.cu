@@ -168,12 +168,38 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __syncthreads();
 }
 
+// Asynchronous L2 prefetch of a byte range (16-byte aligned, size a nonzero
+// multiple of 16): the warp's next slice streams into L2 while the current
+// one is processed, so its loads meet L2 rather than HBM latency.
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Values and column indices of slice s.  Slice offsets are multiples of 32
+// entries, so both ranges start 64-byte aligned and are multiples of 64 bytes.
+template <typename V, bool NARROW>
+__device__ __forceinline__ void prefetch_slice(const PcgParams &P, const V *val, int s) {
+  const int64_t e0 = P.soff[s], e1 = P.soff[s + 1];
+  if (e1 <= e0) return;
+  prefetch_l2(val + e0, (unsigned)((e1 - e0) * sizeof(V)));
+  if (NARROW) prefetch_l2(P.dcol + e0, (unsigned)((e1 - e0) * sizeof(int16_t)));
+  else prefetch_l2(P.col + e0, (unsigned)((e1 - e0) * sizeof(int)));
+}
+
+// Next slice of this CTA's range for the calling warp (shared counter).
+__device__ __forceinline__ int grab_slice(int *counter, int lane) {
+  int t = 0;
+  if (lane == 0) t = atomicAdd(counter, 1);
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+
 // SELL SpMV over this CTA's slices.  Slices are handed to warps through a
 // shared-memory counter (the CTA's slice range is fixed, so every row is still
-// produced by this CTA); lane l of the warp owns row 32s+l and accumulates it
-// in a fixed order.  Only per-row results are written here; the dot products
-// are taken afterwards in a fixed row order so that results stay
-// bit-reproducible whatever warp computed which slice.
+// produced by this CTA), one slice ahead so that the next slice can be
+// prefetched; lane l of the warp owns row 32s+l and accumulates it in a fixed
+// order.  Only per-row results are written here; the dot products are taken
+// afterwards in a fixed row order so that results stay bit-reproducible
+// whatever warp computed which slice.
 template <typename V, typename V2, bool NARROW>
 __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict__ val,
                                         const V2 *__restrict__ zc, V2 *__restrict__ zn,
@@ -183,7 +209,13 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) next_slice = s0 + kWarps;
   __syncthreads();
-  for (int s = s0 + warp; s < s1;) {
+  int s = s0 + warp;
+  int nxt = s < s1 ? grab_slice(&next_slice, lane) : s1;
+  if (lane == 0) {
+    if (s < s1) prefetch_slice<V, NARROW>(P, val, s);
+    if (nxt < s1) prefetch_slice<V, NARROW>(P, val, nxt);
+  }
+  while (s < s1) {
     const int64_t base = P.soff[s] + lane;
     const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
     const int row = s * kSliceRows + lane;
@@ -200,9 +232,11 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
       zn[row].y = a.x + beta * a.y;
       q[row] = acc;
     }
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&next_slice, 1);
-    s = __shfl_sync(0xffffffffu, t, 0);
+    s = nxt;
+    if (s < s1) {
+      nxt = grab_slice(&next_slice, lane);
+      if (lane == 0 && nxt < s1) prefetch_slice<V, NARROW>(P, val, nxt);
+    }
   }
   __syncthreads();
 }
@@ -215,7 +249,13 @@ __device__ __noinline__ void spmv_residual(const PcgParams &P) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) next_slice = s0 + kWarps;
   __syncthreads();
-  for (int s = s0 + warp; s < s1;) {
+  int s = s0 + warp;
+  int nxt = s < s1 ? grab_slice(&next_slice, lane) : s1;
+  if (lane == 0) {
+    if (s < s1) prefetch_slice<double, NARROW>(P, P.v64, s);
+    if (nxt < s1) prefetch_slice<double, NARROW>(P, P.v64, nxt);
+  }
+  while (s < s1) {
     const int64_t base = P.soff[s] + lane;
     const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
     const int row = s * kSliceRows + lane;
@@ -227,9 +267,11 @@ __device__ __noinline__ void spmv_residual(const PcgParams &P) {
       acc += __ldcs(P.v64 + k) * P.x[c];
     }
     if (row < P.n) P.r64[row] = P.b[row] - acc;
-    int t = 0;
-    if (lane == 0) t = atomicAdd(&next_slice, 1);
-    s = __shfl_sync(0xffffffffu, t, 0);
+    s = nxt;
+    if (s < s1) {
+      nxt = grab_slice(&next_slice, lane);
+      if (lane == 0 && nxt < s1) prefetch_slice<double, NARROW>(P, P.v64, nxt);
+    }
   }
   __syncthreads();
 }
