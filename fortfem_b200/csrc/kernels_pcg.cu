@@ -27,9 +27,13 @@
 // solution accumulated in FP64; whenever the FP32 residual has fallen by the
 // reliable-update factor (or claims convergence) the true FP64 residual
 // b - A x replaces it (the search direction is kept, rescaled), and the solve
-// ends when ||b - A x||_2 <= tol*||b||_2.  If replacements stop reducing the
-// true residual (condition number beyond FP32 reach) the solve continues in
-// the FP64 loop from the current x.
+// ends when ||b - A x||_2 <= tol*||b||_2.  A replacement is also forced when
+// the FP32 residual grows tenfold past the last true residual (the search
+// direction then restarts) or plateaus for four times the previous
+// replacement interval.  If replacements stop reducing the true residual, or
+// the FP32 p^T A p is not positive (condition number beyond FP32 reach, as
+// for curl-curl operators with a small mass term), the solve continues in the
+// FP64 loop from the current x.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +50,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSlots = 4;
 constexpr int kPartialBatch = 8;   // partial loads in flight per lane
 constexpr int kResultDoubles = 16;
+constexpr int kMinWindow = 256;  // iterations before a plateau forces a reliable update
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
 
 struct PcgParams {
@@ -353,7 +358,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
   double scale = kMixed ? (rnorm > 0.0 ? rnorm : 1.0) : 1.0;
   const double target = P.relative ? P.tol * (true_target ? bnorm : rnorm) : P.tol;
   double true_res = rnorm, last_true = rnorm;
-  int stall = 0;
+  int stall = 0, since = 0, window = kMinWindow;
   int converged = (rnorm <= target) ? 1 : 0;
   double rz = 0.0;
   if (!converged) {
@@ -396,7 +401,13 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     const bool breakdown = (!kMixed && !continuation && P.guard == 0)
                                ? (fabs(pAp) < 1.0e-14)
                                : !(pAp > 0.0 && is_finite_d(pAp));
-    if (breakdown) break;
+    if (breakdown) {
+      // an FP32 p^T A p that is not positive (cancellation on a near-null
+      // direction of the operator) ends the FP32 phase before x is touched;
+      // the FP64 loop continues from the current x
+      if (kMixed) o.stagnated = 1;
+      break;
+    }
     const double alpha = rz / pAp;
     const V al = (V)alpha;
     const double xs = alpha * scale;
@@ -428,9 +439,53 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     if (red[2] != 0.0) { o.status = FFG_TIMEOUT; true_res = est; break; }
     if (!kMixed) {
       true_res = est;
-      if (est <= target) { converged = 1; break; }
-    } else if (est <= target || rr <= P.delta * P.delta * rr_last) {
+      if (est <= target && !continuation) { converged = 1; break; }
+      if (est <= target) {
+        // the continuation's target is the true residual: check b - A x and,
+        // while it still falls, replace the recursive residual with it
+        t0 = stamp();
+        part[0] = 0.0;
+        residual(P);
+        for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+        write_partials(P, phase, part, 1);
+        if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+        read_partials(P, phase, red, 1);
+        true_res = sqrt(red[0]);
+        if (true_res <= target) { converged = 1; tm.u += stamp() - t0; break; }
+        stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
+        last_true = true_res;
+        if (stall >= 2 || !is_finite_d(true_res)) { tm.u += stamp() - t0; break; }
+        ++o.updates;
+        part[0] = 0.0;
+        for_rows(P, [&](int row) {
+          const V rr2 = (V)P.r64[row];
+          r[row] = rr2;
+          const V z = dinv[row] * rr2;
+          V2 a = zn[row];
+          a.x = z;
+          zn[row] = a;
+          part[0] += (double)rr2 * (double)z;
+        });
+        write_partials(P, phase, part, 1);
+        if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+        read_partials(P, phase, red, 1);
+        tm.u += stamp() - t0;
+        rz_new = red[0];
+      }
+    } else {
       // reliable update: replace the recursive residual with b - A x in FP64
+      // when it has fallen by delta, claims convergence, has grown tenfold
+      // past the last true residual (the FP32 recurrence is diverging; the
+      // search then restarts), or has not triggered within `window`
+      // iterations (an FP32 plateau, judged by the stall test below)
+      const bool grew = !(est < 10.0 * scale);
+      const bool slow = o.iterations - since > window;
+      if (!(est <= target || rr <= P.delta * P.delta * rr_last || grew || slow)) {
+        beta = rz_new / rz;
+        rz = rz_new;
+        cur ^= 1;
+        continue;
+      }
       if (o.updates >= P.max_updates) break;
       ++o.updates;
       t0 = stamp();
@@ -468,8 +523,11 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       rz_new = red[0];
       scale = true_res;
       rr_last = 1.0;
+      window = max(kMinWindow, 4 * (o.iterations - since));
+      since = o.iterations;
+      if (grew) rz = 0.0;  // restart: beta = 0 below
     }
-    beta = rz_new / rz;
+    beta = rz != 0.0 ? rz_new / rz : 0.0;
     rz = rz_new;
     cur ^= 1;
   }
