@@ -20,6 +20,7 @@ FFG_OUT_OF_MEMORY = -5
 FFG_NOT_CONVERGED = -6
 FFG_TIMEOUT = -7
 FFG_NO_DEVICE = -8
+FFG_NOT_READY = -9
 
 FFG_TETRA_LAGRANGE = 1
 FFG_TETRA_NEDELEC = 2
@@ -36,11 +37,14 @@ FFG_PRECISION_FP64 = 0
 FFG_PRECISION_MIXED = 1
 FFG_OPTIONS_VERSION = 1
 FFG_NOALLOC_MAX_ROWS = 65536
+FFG_BATCH_CTA_PER_SYSTEM = 0
+FFG_BATCH_WHOLE_DEVICE = 1
 
 STATUS_TEXT = {
     FFG_OK: "ok", FFG_INVALID_INPUT: "invalid input", FFG_CAPACITY: "capacity too small",
     FFG_BAD_HANDLE: "bad handle", FFG_CUDA_ERROR: "CUDA error", FFG_OUT_OF_MEMORY: "out of memory",
     FFG_NOT_CONVERGED: "not converged", FFG_TIMEOUT: "timeout", FFG_NO_DEVICE: "no CUDA device",
+    FFG_NOT_READY: "not ready",
 }
 
 
@@ -97,6 +101,9 @@ SIGNATURES = {
     "ffg_problem_reduced_system": (
         None, [i32, vp, f64, f64, vp, vp, vp, vp, i64, pi64, vp, vp, vp, vp, vp, pi32]),
     "ffg_problem_phase_times": (None, [i32, vp, pi32]),
+    "ffg_problem_solve_batch": (
+        None, [i32, vp, vp, vp, vp, vp, vp, vp, vp, C.POINTER(SolverOptionsC), vp, i32, vp, pi32]),
+    "ffg_problem_batch_stats": (None, [i32, C.POINTER(SolverStatsC), pi32]),
     "ffg_problem_free": (None, [i32, pi32]),
 }
 

@@ -491,6 +491,18 @@ class Problem:
             raise FortfemError(st.value, "ffg_problem_solve")
         return SolverStats.from_c(sc)
 
+    def batch_stats(self) -> Optional[SolverStats]:
+        """Statistics of this problem's last batched solve (ffg_problem_batch_stats),
+        or None while its batch is still running."""
+        sc = K.SolverStatsC()
+        st = C.c_int(0)
+        K.load().ffg_problem_batch_stats(self.handle, C.byref(sc), C.byref(st))
+        if st.value == K.FFG_NOT_READY:
+            return None
+        if st.value not in (0, K.FFG_NOT_CONVERGED):
+            raise FortfemError(st.value, "ffg_problem_batch_stats")
+        return SolverStats.from_c(sc)
+
     def phase_times(self) -> dict:
         """Device-side phase profile of the last solve (seconds, CTA 0's view)."""
         out = np.zeros(6)
@@ -583,6 +595,47 @@ def solve_tetra_nedelec_curl_mass(vertices, tetrahedra, order, source, curl_coef
                              None, options)
         return sol, Status.of(0 if stats.converged else K.FFG_NOT_CONVERGED,
                               "Tetrahedral Nedelec curl-mass solve failed"), stats
+
+
+_BATCH_MODES = {"cta_per_system": K.FFG_BATCH_CTA_PER_SYSTEM,
+                "whole_device": K.FFG_BATCH_WHOLE_DEVICE}
+
+
+def solve_batch(problems, vertices, solutions, coef_a, coef_b, cell_a=None, cell_b=None,
+                samples=None, constrained_values=None, options: Optional[SolverOptions] = None,
+                mode: str = "cta_per_system", stream=None) -> None:
+    """Enqueue assemble + solve of several device-resident problems on `stream`
+    (ffg_problem_solve_batch) and return at once.  All arrays are CUDA
+    tensors, one per problem (lists; None entries where a problem has none);
+    coef_a / coef_b are sequences of floats.  Collect each result with
+    Problem.batch_stats once the stream has passed this call."""
+    n = len(problems)
+    if n == 0:
+        return
+    for seq in (vertices, solutions, coef_a, coef_b):
+        if len(seq) != n:
+            raise FortfemError(K.FFG_INVALID_INPUT, "solve_batch: one entry per problem")
+
+    def ptrs(seq):
+        if seq is None or all(t is None for t in seq):
+            return None
+        if len(seq) != n:
+            raise FortfemError(K.FFG_INVALID_INPUT, "solve_batch: one entry per problem")
+        return (C.c_void_p * n)(*[None if t is None else t.data_ptr() for t in seq])
+
+    handles = (C.c_int * n)(*[p.handle for p in problems])
+    ca = (C.c_double * n)(*[float(a) for a in coef_a])
+    cb = (C.c_double * n)(*[float(b) for b in coef_b])
+    opts = options or SolverOptions(precision="mixed", tolerance=1e-10, preconditioner="jacobi",
+                                    max_iterations=1000000)
+    oc = opts.to_c()
+    st = C.c_int(0)
+    s = None if stream is None else C.c_void_p(int(stream.cuda_stream))
+    K.load().ffg_problem_solve_batch(n, handles, ptrs(vertices), ca, cb, ptrs(cell_a), ptrs(cell_b),
+                                     ptrs(samples), ptrs(constrained_values), C.byref(oc),
+                                     ptrs(solutions), _BATCH_MODES[mode], s, C.byref(st))
+    if st.value:
+        raise FortfemError(st.value, "ffg_problem_solve_batch")
 
 
 def solve_scalar_p1(vertices, triangles, load=1.0, stiffness_coefficient=1.0, mass_coefficient=0.0,

@@ -77,6 +77,8 @@ struct Problem {
          *in_g = nullptr;
   int *free_dofs = nullptr;
   int *err = nullptr;
+  int *err_host = nullptr;   // pinned: degenerate-cell flag of a deferred check
+  bool batch_pending = false;  // enqueued by ffg_problem_solve_batch, not yet collected
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   ~Problem() {
@@ -88,6 +90,7 @@ struct Problem {
       if (p) cudaFree(p);
     free_sell(S);
     solve_work_free(work);
+    if (err_host) cudaFreeHost(err_host);
     for (auto &e : ev)
       if (e) cudaEventDestroy(e);
   }
@@ -181,6 +184,8 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   if ((st = dalloc(&P->in_g, (size_t)t.n_dofs))) return st;
   if ((st = upload(&P->free_dofs, t.free_dofs))) return st;
   if ((st = dalloc(&P->err, 4))) return st;
+  if (cudaMallocHost((void **)&P->err_host, sizeof(int)) != cudaSuccess) return FFG_OUT_OF_MEMORY;
+  *P->err_host = 0;
   if ((st = solve_work_alloc(P->work, nfree, grid))) return st;
   for (auto &e : P->ev)
     if (cudaEventCreate(&e) != cudaSuccess) return FFG_CUDA_ERROR;
@@ -200,7 +205,7 @@ __global__ void scatter_solution_kernel(int64_t n_free, const int *perm, const i
 // value array (rhs in free-DoF order).
 int assemble(Problem &P, const double *vertices, double ca, double cb, const double *cell_a,
              const double *cell_b, const double *samples, const double *g, int memory,
-             bool sell, cudaStream_t s, std::string &msg) {
+             bool sell, cudaStream_t s, std::string &msg, bool defer_check = false) {
   const Topology &t = P.topo;
   AssemblyInputs in;
   in.coef_a = ca;
@@ -239,6 +244,13 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
   st = launch_columns(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.elem, P.csc_col_ptr,
                       P.csc_row, sell ? &P.S : nullptr, P.csc_val, P.rhs, s);
   if (st) return st;
+  if (defer_check) {
+    // the flag is read with the statistics, after the stream has passed
+    return cudaMemcpyAsync(P.err_host, P.err, sizeof(int), cudaMemcpyDeviceToHost, s) ==
+                   cudaSuccess
+               ? FFG_OK
+               : FFG_CUDA_ERROR;
+  }
   int herr = 0;
   if (cudaMemcpyAsync(&herr, P.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return FFG_CUDA_ERROR;
@@ -591,7 +603,10 @@ void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
   if (!P) { *status = FFG_BAD_HANDLE; return; }
   ffg_solver_options o;
   if (check_options(opts, o)) { *status = FFG_INVALID_INPUT; return; }
-  if (!solution || (memory != 0 && memory != 1)) { *status = FFG_INVALID_INPUT; return; }
+  if (!solution || (memory != 0 && memory != 1) || P->batch_pending) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   std::string msg;
   ffg_solver_stats local;
@@ -640,6 +655,120 @@ void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
   if (stats) *stats = local;
   *status = local.status == FFG_NOT_CONVERGED ? FFG_NOT_CONVERGED : local.status;
   if (local.converged) *status = FFG_OK;
+}
+
+void ffg_problem_solve_batch(int count, const int *handles, const double *const *vertices,
+                             const double *coef_a, const double *coef_b,
+                             const double *const *cell_a, const double *const *cell_b,
+                             const double *const *samples, const double *const *g,
+                             const ffg_solver_options *opts, double *const *solutions, int mode,
+                             void *stream, int *status) {
+  if (count < 1 || !handles || !vertices || !coef_a || !coef_b || !solutions ||
+      (mode != FFG_BATCH_CTA_PER_SYSTEM && mode != FFG_BATCH_WHOLE_DEVICE)) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  ffg_solver_options o;
+  if (check_options(opts, o)) { *status = FFG_INVALID_INPUT; return; }
+  std::vector<std::shared_ptr<Problem>> probs((size_t)count);
+  for (int i = 0; i < count; ++i) {
+    probs[i] = find_problem(handles[i]);
+    if (!probs[i]) { *status = FFG_BAD_HANDLE; return; }
+    if (probs[i]->batch_pending || !vertices[i] || !solutions[i]) {
+      *status = FFG_INVALID_INPUT;
+      return;
+    }
+    for (int j = 0; j < i; ++j)
+      if (probs[j] == probs[i]) { *status = FFG_INVALID_INPUT; return; }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  std::string msg;
+  int st = FFG_OK;
+  for (int i = 0; i < count && !st; ++i) {
+    Problem &P = *probs[i];
+    cudaEventRecord(P.ev[0], s);
+    st = assemble(P, vertices[i], coef_a[i], coef_b[i], cell_a ? cell_a[i] : nullptr,
+                  cell_b ? cell_b[i] : nullptr, samples ? samples[i] : nullptr,
+                  g ? g[i] : nullptr, 1, true, s, msg, true);
+    if (st) break;
+    const Topology &t = P.topo;
+    if (!o.preconditioner)
+      set_ones_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(t.n_free(), P.S.dinv64,
+                                                                          P.S.dinv32);
+    cudaMemsetAsync(P.x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
+    cudaEventRecord(P.ev[1], s);
+  }
+  if (!st) {
+    std::vector<const DeviceSell *> A;
+    std::vector<const double *> b;
+    std::vector<double *> x;
+    std::vector<SolveWork *> w;
+    for (auto &P : probs)
+      if (P->topo.n_free() > 0) {
+        A.push_back(&P->S);
+        b.push_back(P->rhs);
+        x.push_back(P->x);
+        w.push_back(&P->work);
+      }
+    if (mode == FFG_BATCH_CTA_PER_SYSTEM) {
+      if (!A.empty())
+        st = pcg_launch_batch((int)A.size(), A.data(), b.data(), x.data(), o, w.data(), s, msg);
+    } else {
+      for (size_t i = 0; i < A.size() && !st; ++i)
+        st = pcg_launch(*A[i], b[i], x[i], o, *w[i], s, msg);
+    }
+  }
+  for (int i = 0; i < count && !st; ++i) {
+    Problem &P = *probs[i];
+    const Topology &t = P.topo;
+    cudaEventRecord(P.ev[2], s);
+    if (g && g[i])
+      cudaMemcpyAsync(P.full, g[i], sizeof(double) * (size_t)t.n_dofs, cudaMemcpyDeviceToDevice, s);
+    else
+      cudaMemsetAsync(P.full, 0, sizeof(double) * (size_t)t.n_dofs, s);
+    if (t.n_free() > 0)
+      scatter_solution_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(
+          t.n_free(), P.S.perm, P.free_dofs, P.x, P.full);
+    cudaMemcpyAsync(solutions[i], P.full, sizeof(double) * (size_t)t.n_dofs,
+                    cudaMemcpyDeviceToDevice, s);
+    if (cudaEventRecord(P.ev[3], s) != cudaSuccess) st = FFG_CUDA_ERROR;
+  }
+  if (st) {
+    report(o.verbosity, msg);
+    *status = st;
+    return;
+  }
+  for (auto &P : probs) P->batch_pending = true;
+  *status = FFG_OK;
+}
+
+void ffg_problem_batch_stats(int handle, ffg_solver_stats *stats, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (!P->batch_pending) { *status = FFG_INVALID_INPUT; return; }
+  const cudaError_t q = cudaEventQuery(P->ev[3]);
+  if (q == cudaErrorNotReady) { *status = FFG_NOT_READY; return; }
+  if (q != cudaSuccess) { cudaGetLastError(); *status = FFG_CUDA_ERROR; return; }
+  P->batch_pending = false;
+  ffg_solver_stats local;
+  std::memset(&local, 0, sizeof(local));
+  std::string msg;
+  int st = FFG_OK;
+  if (*P->err_host) {
+    st = *P->err_host;
+  } else if (P->topo.n_free() > 0) {
+    st = pcg_collect(P->work, &local, msg);
+  } else {
+    local.converged = 1;
+  }
+  float ta = 0, ts = 0;
+  cudaEventElapsedTime(&ta, P->ev[0], P->ev[1]);
+  cudaEventElapsedTime(&ts, P->ev[1], P->ev[2]);
+  local.assembly_seconds = ta * 1e-3;
+  local.solve_seconds = ts * 1e-3;
+  if (st) local.status = st;
+  if (stats) *stats = local;
+  *status = st ? st : (local.converged ? FFG_OK : FFG_NOT_CONVERGED);
 }
 
 void ffg_problem_reduced_system(int handle, const double *vertices, double ca, double cb,

@@ -141,6 +141,8 @@ struct SolveWork {
   unsigned int *barrier = nullptr;
   int *control = nullptr;    // [0] error status
   double *result = nullptr;  // device statistics block
+  double *result_host = nullptr;  // pinned copy of the statistics block
+  int *control_host = nullptr;    // pinned copy of the control word
   int grid = 0;
   int64_t n = 0;
   // last solve: [0] FP64 continuation taken, then device seconds seen by CTA 0
@@ -155,6 +157,16 @@ void solve_work_free(SolveWork &w);
 // SELL row numbering).  x holds the initial guess (FP64).  Fills stats.
 int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
               SolveWork &w, ffg_solver_stats *stats, cudaStream_t stream, std::string &msg);
+// Asynchronous halves of pcg_solve: enqueue the cooperative solve (or one
+// CTA per system for a batch of independent systems) with the statistics
+// copied to each workspace's pinned block, then decode that block once the
+// stream has reached it.
+int pcg_launch(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
+               SolveWork &w, cudaStream_t stream, std::string &msg);
+int pcg_launch_batch(int count, const DeviceSell *const *A, const double *const *b,
+                     double *const *x, const ffg_solver_options &opts, SolveWork *const *w,
+                     cudaStream_t stream, std::string &msg);
+int pcg_collect(SolveWork &w, ffg_solver_stats *stats, std::string &msg);
 int pcg_grid_size(int *grid);
 
 // FP64 CSR SpMV y = A x (drop-in matvec).

@@ -38,6 +38,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 
 #include "ffg_internal.h"
 
@@ -77,7 +78,12 @@ struct PcgParams {
   int precision, relative, max_it, max_updates, guard;
   double tol, delta;
   unsigned long long limit_ns;
+  // CTAs that solve this system: blockIdx.x - cta0 in [0, ncta).  With one
+  // CTA the system's slices are [0, n_slices) and barriers are CTA barriers.
+  int cta0, ncta, n_slices;
 };
+
+__device__ __forceinline__ int cta_of(const PcgParams &P) { return (int)blockIdx.x - P.cta0; }
 
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
@@ -101,10 +107,11 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
   __shared__ int ok;
   __syncthreads();
   ++phase;
+  if (P.ncta == 1) return true;
   if (threadIdx.x == 0) {
     __threadfence();
     atomicAdd(P.bar, 1u);
-    const unsigned int target = phase * gridDim.x;
+    const unsigned int target = phase * (unsigned int)P.ncta;
     const unsigned long long t0 = globaltimer();
     int good = 1;
     unsigned int spins = 0;
@@ -139,7 +146,7 @@ __device__ void write_partials(const PcgParams &P, unsigned int phase, const dou
   if (threadIdx.x < nslot) {
     double x = 0.0;
     for (int w = 0; w < kWarps; ++w) x += red[threadIdx.x][w];
-    P.partial[((size_t)((phase + 1) & 1) * kSlots + threadIdx.x) * gridDim.x + blockIdx.x] = x;
+    P.partial[((size_t)((phase + 1) & 1) * kSlots + threadIdx.x) * P.ncta + cta_of(P)] = x;
   }
 }
 
@@ -151,7 +158,7 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __shared__ double res[kSlots];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp < nslot) {
-    const int G = (int)gridDim.x;
+    const int G = P.ncta;
     const double *src = P.partial + ((size_t)(phase & 1) * kSlots + warp) * G;
     double acc = 0.0;
     for (int b0 = 0; b0 < G; b0 += 32 * kPartialBatch) {
@@ -171,6 +178,17 @@ __device__ void read_partials(const PcgParams &P, unsigned int phase, double *ou
   __syncthreads();
   for (int s = 0; s < nslot; ++s) out[s] = res[s];
   __syncthreads();
+}
+
+// Slices [s0, s1) of the calling CTA.
+__device__ __forceinline__ void slice_range(const PcgParams &P, int &s0, int &s1) {
+  if (P.ncta == 1) {
+    s0 = 0;
+    s1 = P.n_slices;
+  } else {
+    s0 = P.cta_slice[cta_of(P)];
+    s1 = P.cta_slice[cta_of(P) + 1];
+  }
 }
 
 // Asynchronous L2 prefetch of a byte range (16-byte aligned, size a nonzero
@@ -210,7 +228,8 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
                                         const V2 *__restrict__ zc, V2 *__restrict__ zn,
                                         V *__restrict__ q, V beta) {
   __shared__ int next_slice;
-  const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
+  int s0, s1;
+  slice_range(P, s0, s1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) next_slice = s0 + kWarps;
   __syncthreads();
@@ -250,7 +269,8 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
 template <bool NARROW>
 __device__ __noinline__ void spmv_residual(const PcgParams &P) {
   __shared__ int next_slice;
-  const int s0 = P.cta_slice[blockIdx.x], s1 = P.cta_slice[blockIdx.x + 1];
+  int s0, s1;
+  slice_range(P, s0, s1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) next_slice = s0 + kWarps;
   __syncthreads();
@@ -288,8 +308,10 @@ __device__ __forceinline__ void residual(const PcgParams &P) {
 
 template <class F>
 __device__ __forceinline__ void for_rows(const PcgParams &P, F f) {
-  const int64_t r0 = (int64_t)P.cta_slice[blockIdx.x] * kSliceRows;
-  const int64_t r1 = min((int64_t)P.cta_slice[blockIdx.x + 1] * kSliceRows, P.n);
+  int s0, s1;
+  slice_range(P, s0, s1);
+  const int64_t r0 = (int64_t)s0 * kSliceRows;
+  const int64_t r1 = min((int64_t)s1 * kSliceRows, P.n);
   for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) f((int)r);
 }
 
@@ -318,8 +340,8 @@ struct Timing {
   unsigned long long a = 0, aw = 0, b = 0, bw = 0, u = 0;
 };
 
-__device__ __forceinline__ unsigned long long stamp() {
-  return (blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer() : 0ull;
+__device__ __forceinline__ unsigned long long stamp(const PcgParams &P) {
+  return (cta_of(P) == 0 && threadIdx.x == 0) ? globaltimer() : 0ull;
 }
 
 // The CG loop in value type V (float: mixed mode, double: FP64 mode).
@@ -341,7 +363,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
   unsigned long long t0, t1, t2;
 
   // r64 = b - A x, ||r64||, ||b||
-  t0 = stamp();
+  t0 = stamp(P);
   residual(P);
   part[0] = part[1] = 0.0;
   for_rows(P, [&](int row) {
@@ -376,7 +398,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     read_partials(P, phase, red, 1);
     rz = red[0];
   }
-  tm.u += stamp() - t0;
+  tm.u += stamp(P) - t0;
   double beta = 0.0, rr_last = 1.0;
   int cur = 0;
   const int budget = P.max_it - o.iterations;
@@ -385,16 +407,16 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     V2 *zn = zp[cur ^ 1];
     const V bt = (V)beta;
     // A: p = z + beta p_old, q = A p, (p, q)
-    t0 = stamp();
+    t0 = stamp(P);
     part[0] = 0.0;
     if (P.dcol) spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
     else spmv_pairs<V, V2, false>(P, A, zc, zn, q, bt);
     for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
     write_partials(P, phase, part, 1);
-    t1 = stamp();
+    t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
     read_partials(P, phase, red, 1);
-    t2 = stamp();
+    t2 = stamp(P);
     tm.a += t1 - t0;
     tm.aw += t2 - t1;
     const double pAp = red[0];
@@ -412,9 +434,9 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     const V al = (V)alpha;
     const double xs = alpha * scale;
     // B: x += alpha p (FP64), r -= alpha q, z = D^-1 r
-    t0 = stamp();
+    t0 = stamp(P);
     part[0] = part[1] = 0.0;
-    part[2] = (blockIdx.x == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
+    part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
     for_rows(P, [&](int row) {
       V2 a = zn[row];
       P.x[row] = P.x[row] + xs * (double)a.y;
@@ -427,10 +449,10 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       part[1] += (double)rr * (double)z;
     });
     write_partials(P, phase, part, 3);
-    t1 = stamp();
+    t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
     read_partials(P, phase, red, 3);
-    t2 = stamp();
+    t2 = stamp(P);
     tm.b += t1 - t0;
     tm.bw += t2 - t1;
     ++o.iterations;
@@ -443,7 +465,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       if (est <= target) {
         // the continuation's target is the true residual: check b - A x and,
         // while it still falls, replace the recursive residual with it
-        t0 = stamp();
+        t0 = stamp(P);
         part[0] = 0.0;
         residual(P);
         for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
@@ -451,10 +473,10 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
         if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
         read_partials(P, phase, red, 1);
         true_res = sqrt(red[0]);
-        if (true_res <= target) { converged = 1; tm.u += stamp() - t0; break; }
+        if (true_res <= target) { converged = 1; tm.u += stamp(P) - t0; break; }
         stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
         last_true = true_res;
-        if (stall >= 2 || !is_finite_d(true_res)) { tm.u += stamp() - t0; break; }
+        if (stall >= 2 || !is_finite_d(true_res)) { tm.u += stamp(P) - t0; break; }
         ++o.updates;
         part[0] = 0.0;
         for_rows(P, [&](int row) {
@@ -469,7 +491,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
         write_partials(P, phase, part, 1);
         if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
         read_partials(P, phase, red, 1);
-        tm.u += stamp() - t0;
+        tm.u += stamp(P) - t0;
         rz_new = red[0];
       }
     } else {
@@ -488,7 +510,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       }
       if (o.updates >= P.max_updates) break;
       ++o.updates;
-      t0 = stamp();
+      t0 = stamp(P);
       part[0] = 0.0;
       residual(P);
       for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
@@ -496,11 +518,11 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
       true_res = sqrt(red[0]);
-      if (true_res <= target) { converged = 1; tm.u += stamp() - t0; break; }
+      if (true_res <= target) { converged = 1; tm.u += stamp(P) - t0; break; }
       if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
       stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
       last_true = true_res;
-      if (stall >= 2) { o.stagnated = 1; tm.u += stamp() - t0; break; }
+      if (stall >= 2) { o.stagnated = 1; tm.u += stamp(P) - t0; break; }
       const double ratio = scale / true_res;  // old units -> new units
       const V rt = (V)ratio;
       const double inv = 1.0 / true_res;
@@ -518,7 +540,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
-      tm.u += stamp() - t0;
+      tm.u += stamp(P) - t0;
       rz = rz * ratio * ratio;
       rz_new = red[0];
       scale = true_res;
@@ -539,19 +561,19 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
   }
   if (kMixed && o.stagnated) return;  // the FP64 continuation measures its own residual
   // true FP64 residual of the returned x
-  t0 = stamp();
+  t0 = stamp(P);
   part[0] = 0.0;
   residual(P);
   for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
   write_partials(P, phase, part, 1);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 1);
-  tm.u += stamp() - t0;
+  tm.u += stamp(P) - t0;
   o.true_res = sqrt(red[0]);
   if (kMixed) o.final_res = o.true_res;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(PcgParams P) {
+__device__ __forceinline__ void pcg_body(const PcgParams &P) {
   unsigned int phase = 0;
   // only block 0 judges the wall limit; its verdict travels through a partial slot
   const unsigned long long t_start = globaltimer();
@@ -568,7 +590,7 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(PcgParams P) {
     }
   }
   if (o.aborted) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (cta_of(P) == 0 && threadIdx.x == 0) {
     P.result[0] = o.converged;
     P.result[1] = o.iterations;
     P.result[2] = o.updates;
@@ -583,6 +605,27 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_kernel(PcgParams P) {
     P.result[11] = 1e-9 * (double)tm.bw;
     P.result[12] = 1e-9 * (double)tm.u;
   }
+}
+
+// One system solved by the whole cooperative grid.
+__global__ void __launch_bounds__(kThreads, 1) pcg_kernel(PcgParams P) { pcg_body(P); }
+
+// Up to kMaxBatch independent systems, one CTA each (no inter-CTA waits, so
+// an ordinary launch; systems never share a CTA or a reduction, so every
+// system's result is independent of what else is in the batch).
+constexpr int kMaxBatch = 48;
+struct PcgBatch {
+  PcgParams sys[kMaxBatch];
+};
+__global__ void __launch_bounds__(kThreads, 1) pcg_batch_kernel(const __grid_constant__ PcgBatch B) {
+  __shared__ PcgParams Ps;
+  if (threadIdx.x == 0) {
+    Ps = B.sys[blockIdx.x];
+    Ps.cta0 = (int)blockIdx.x;
+    Ps.ncta = 1;
+  }
+  __syncthreads();
+  pcg_body(Ps);
 }
 
 // Drop-in FP64 CSR SpMV, one thread per row (spmv / csc_matvec semantics).
@@ -703,6 +746,15 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
   A((void **)&w.barrier, 64);
   A((void **)&w.control, 64);
   A((void **)&w.result, kResultDoubles * sizeof(double));
+  if (!bad && (cudaMallocHost((void **)&w.result_host, kResultDoubles * sizeof(double)) != cudaSuccess ||
+               cudaMallocHost((void **)&w.control_host, 2 * sizeof(int)) != cudaSuccess))
+    bad = true;
+  if (!bad) {
+    std::memset(w.result_host, 0, kResultDoubles * sizeof(double));
+    w.control_host[0] = w.control_host[1] = 0;
+    if (cudaMemset(w.control, 0, 64) != cudaSuccess || cudaMemset(w.barrier, 0, 64) != cudaSuccess)
+      bad = true;
+  }
   if (bad) {
     solve_work_free(w);
     cudaGetLastError();
@@ -716,15 +768,14 @@ void solve_work_free(SolveWork &w) {
                   w.barrier, w.control, w.result};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (w.result_host) cudaFreeHost(w.result_host);
+  if (w.control_host) cudaFreeHost(w.control_host);
   w = SolveWork();
 }
 
-int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
-              SolveWork &w, ffg_solver_stats *stats, cudaStream_t stream, std::string &msg) {
-  if (w.n != A.n || w.grid <= 0 || A.grid != w.grid) {
-    msg = "solver workspace mismatch";
-    return FFG_INVALID_INPUT;
-  }
+namespace {
+PcgParams make_params(const DeviceSell &A, const double *b, double *x,
+                      const ffg_solver_options &opts, const SolveWork &w) {
   PcgParams P;
   P.n = A.n;
   P.soff = A.soff;
@@ -753,8 +804,24 @@ int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_
   P.guard = opts.breakdown_guard;
   const double limit = opts.timeout_seconds > 0 ? opts.timeout_seconds : 60.0;
   P.limit_ns = (unsigned long long)(limit * 1e9);
+  P.cta0 = 0;
+  P.ncta = A.grid;
+  P.n_slices = (int)A.n_slices;
+  return P;
+}
+}  // namespace
+
+int pcg_launch(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
+               SolveWork &w, cudaStream_t stream, std::string &msg) {
+  if (w.n != A.n || w.grid <= 0 || A.grid != w.grid) {
+    msg = "solver workspace mismatch";
+    return FFG_INVALID_INPUT;
+  }
+  PcgParams P = make_params(A, b, x, opts, w);
   if (cudaMemsetAsync(w.barrier, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaMemsetAsync(w.control, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
+  if (cudaMemsetAsync(w.result, 0, kResultDoubles * sizeof(double), stream) != cudaSuccess)
+    return FFG_CUDA_ERROR;
   void *args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid),
                                               dim3(kThreads), args, 0, stream);
@@ -763,17 +830,51 @@ int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_
     cudaGetLastError();
     return FFG_CUDA_ERROR;
   }
-  double res[kResultDoubles];
-  int ctrl[2];
-  if (cudaMemcpyAsync(res, w.result, sizeof(res), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+  if (cudaMemcpyAsync(w.result_host, w.result, kResultDoubles * sizeof(double),
+                      cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaMemcpyAsync(w.control_host, w.control, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess)
     return FFG_CUDA_ERROR;
-  if (cudaMemcpyAsync(ctrl, w.control, sizeof(ctrl), cudaMemcpyDeviceToHost, stream) != cudaSuccess)
-    return FFG_CUDA_ERROR;
-  if (cudaStreamSynchronize(stream) != cudaSuccess) return FFG_CUDA_ERROR;
-  if (ctrl[0] != 0) {
+  return FFG_OK;
+}
+
+int pcg_launch_batch(int count, const DeviceSell *const *A, const double *const *b,
+                     double *const *x, const ffg_solver_options &opts, SolveWork *const *w,
+                     cudaStream_t stream, std::string &msg) {
+  for (int i = 0; i < count; ++i)
+    if (w[i]->n != A[i]->n || A[i]->n < 1) {
+      msg = "solver workspace mismatch";
+      return FFG_INVALID_INPUT;
+    }
+  static_assert(sizeof(PcgBatch) <= 32000, "kernel parameter block too large");
+  PcgBatch B;
+  for (int c0 = 0; c0 < count; c0 += kMaxBatch) {
+    const int m = std::min(kMaxBatch, count - c0);
+    for (int i = 0; i < m; ++i) {
+      B.sys[i] = make_params(*A[c0 + i], b[c0 + i], x[c0 + i], opts, *w[c0 + i]);
+      w[c0 + i]->control_host[0] = 0;
+    }
+    pcg_batch_kernel<<<m, kThreads, 0, stream>>>(B);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      msg = std::string("batch launch failed: ") + cudaGetErrorString(e);
+      return FFG_CUDA_ERROR;
+    }
+    for (int i = 0; i < m; ++i)
+      if (cudaMemcpyAsync(w[c0 + i]->result_host, w[c0 + i]->result,
+                          kResultDoubles * sizeof(double), cudaMemcpyDeviceToHost,
+                          stream) != cudaSuccess)
+        return FFG_CUDA_ERROR;
+  }
+  return FFG_OK;
+}
+
+int pcg_collect(SolveWork &w, ffg_solver_stats *stats, std::string &msg) {
+  const double *res = w.result_host;
+  if (w.control_host[0] != 0) {
     msg = "grid barrier timed out";
-    if (stats) stats->status = ctrl[0];
-    return ctrl[0];
+    if (stats) stats->status = w.control_host[0];
+    return w.control_host[0];
   }
   if (stats) {
     stats->converged = (int)res[0];
@@ -786,6 +887,14 @@ int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_
   }
   for (int i = 0; i < 6; ++i) w.phase_seconds[i] = res[7 + i];
   return FFG_OK;
+}
+
+int pcg_solve(const DeviceSell &A, const double *b, double *x, const ffg_solver_options &opts,
+              SolveWork &w, ffg_solver_stats *stats, cudaStream_t stream, std::string &msg) {
+  int st = pcg_launch(A, b, x, opts, w, stream, msg);
+  if (st) return st;
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return FFG_CUDA_ERROR;
+  return pcg_collect(w, stats, msg);
 }
 
 int csr_spmv64(int64_t n, const int64_t *rp, const int *ci, const double *v, const double *x,

@@ -36,6 +36,7 @@ extern "C" {
 #define FFG_NOT_CONVERGED -6
 #define FFG_TIMEOUT -7
 #define FFG_NO_DEVICE -8
+#define FFG_NOT_READY -9  /* batched work still running on its stream */
 
 /* Element families of a problem handle. */
 #define FFG_TETRA_LAGRANGE 1
@@ -263,6 +264,36 @@ void ffg_problem_reduced_system(int handle, const double *vertices, double coef_
  * after FP32 stagnation, then seconds in SpMV work, barrier wait after the
  * SpMV, vector work, barrier wait after it, and residual-replacement phases. */
 void ffg_problem_phase_times(int handle, double *seconds, int *status);
+
+/* ------------------------------------------------------------ serving */
+
+/* No counterpart in the reference (its solves run one at a time on the CPU).
+ * Enqueue assembly and solve of `count` distinct device-resident problems on
+ * `stream` and return without waiting, so that a serving loop can keep
+ * several batches in flight.  Arguments are those of ffg_problem_solve with
+ * memory = 1 (device pointers), one entry per problem: coef_a and coef_b hold
+ * `count` values, the other per-problem arrays hold `count` pointers (the
+ * arrays cell_a, cell_b, source_samples, constrained_values may be null, as
+ * may their entries).  mode FFG_BATCH_CTA_PER_SYSTEM solves every system on
+ * one thread block of its own in a single launch (for many small systems;
+ * a system's result does not depend on the rest of the batch);
+ * FFG_BATCH_WHOLE_DEVICE solves them one after another on the whole GPU (for
+ * large systems).  A problem may belong to one unfinished batch at a time. */
+#define FFG_BATCH_CTA_PER_SYSTEM 0
+#define FFG_BATCH_WHOLE_DEVICE 1
+void ffg_problem_solve_batch(int count, const int *handles, const double *const *vertices,
+                             const double *coef_a, const double *coef_b,
+                             const double *const *cell_a, const double *const *cell_b,
+                             const double *const *source_samples,
+                             const double *const *constrained_values,
+                             const ffg_solver_options *opts, double *const *solutions, int mode,
+                             void *stream, int *status);
+
+/* Statistics of a problem's last batched solve: FFG_NOT_READY while the
+ * stream has not reached the end of its batch; otherwise the solve's status
+ * (assembly_seconds: its own assembly; solve_seconds: from the end of its
+ * assembly to the end of the batch's solve). */
+void ffg_problem_batch_stats(int handle, ffg_solver_stats *stats, int *status);
 
 /* Release a problem handle (fortfem_factor_free, src/bindings/fortfem_capi_solver.f90:108-124). */
 void ffg_problem_free(int handle, int *status);

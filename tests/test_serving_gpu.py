@@ -1,0 +1,68 @@
+"""Batched solves and the serving loop on the GPU.
+
+A system solved in a batch must give the same bits as the same system solved
+alone in its mode (one thread block per system, or the whole device): no
+reduction crosses systems.  Against the synchronous cooperative path
+(Problem.solve_device) solutions agree within 1e-6 of their largest entry;
+both stop at true relative residual 1e-10 on systems whose condition number
+stays below 1e4.
+"""
+import numpy as np
+import pytest
+import torch
+
+from fortfem_b200 import serving as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(eng, mode, reqs):
+    tok = eng.launch(S.Batch(mode, reqs, 0))
+    torch.cuda.synchronize()
+    assert eng.done(tok)
+    return eng.collect(tok)
+
+
+def test_batch_matches_alone_and_the_cooperative_path():
+    eng = S.DeviceEngine(keep_solutions=True)
+    reqs = [S.Request(0, "p1", 12, 101), S.Request(1, "p2", 4, 102), S.Request(2, "p1", 40, 103),
+            S.Request(3, "p2", 7, 104), S.Request(4, "p1", 25, 105)]
+    for r in reqs:
+        assert eng.can_host(r.key)
+    mixed = _run(eng, "cta_per_system", reqs)
+    for r, m in zip(reqs, mixed):
+        assert m.converged and m.true_relative_residual <= 1e-10
+        alone = _run(eng, "cta_per_system", [r])[0]
+        assert np.array_equal(alone.solution, m.solution)
+        whole = _run(eng, "whole_device", [r])[0]
+        assert whole.converged and whole.true_relative_residual <= 1e-10
+        mesh = eng.meshes[r.key]
+        v, kappa, src = eng._inputs(mesh, r)
+        ref = torch.empty(mesh.problem.n_dofs, dtype=torch.float64, device=eng.device)
+        st = mesh.problem.solve_device(v, ref, 1.0, 0.0, kappa, None, src, None, eng.options)
+        assert st.converged
+        ref = ref.cpu().numpy()
+        scale = np.abs(ref).max()
+        assert scale > 0
+        assert np.abs(m.solution - ref).max() <= 1e-6 * scale
+        assert np.abs(whole.solution - ref).max() <= 1e-6 * scale
+    eng.close()
+
+
+def test_serving_stream_results_same_alone_and_in_the_mix():
+    reqs = S.poisson_stream(40, 2000.0, seed=11, p1_range=(8, 96), p2_range=(4, 14))
+    eng = S.DeviceEngine(keep_solutions=True)
+    eng.prepare(reqs)
+    sch = S.Scheduler(small_rows=2000, max_batch=16, streams=2)
+    res = S.serve(reqs, eng, sch)
+    assert [r.rid for r in res] == list(range(40))
+    assert all(r.converged and r.true_relative_residual <= 1e-10 for r in res)
+    assert any(r.batch_size > 1 for r in res)            # requests did share batches
+    assert any(r.mode == "whole_device" for r in res)
+    lat = S.percentiles([r.latency for r in res])
+    assert 0 < lat["p50"] <= lat["p99"] <= lat["p99.9"]
+    for r, got in zip(reqs, res):
+        mode = "cta_per_system" if sch.is_small(r) else "whole_device"
+        alone = _run(eng, mode, [r])[0]
+        assert np.array_equal(alone.solution, got.solution)
+    eng.close()
