@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=128,
+                    help="requests of the serving leg (0 skips it)")
+    ap.add_argument("--serving-rate", type=float, default=20.0)
     return ap.parse_args()
 
 
@@ -363,6 +366,22 @@ def run_ours(args):
         line["e2e"] = {"value": world * prob.n_dofs * args.steps / (ems * 1e-3), "unit": "DoF/s",
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                        "ms_per_step": ems / args.steps}
+
+    # serving: a Poisson stream of P1/P2 requests through the continuous-batching
+    # server (one stream per rank); latency from arrival to solution on the host
+    if args.serving_requests > 0:
+        from fortfem_b200 import serving
+        sv = serving.run_stream(args.serving_requests, args.serving_rate, seed=4 + rank,
+                                device=local)
+        sv.pop("results")
+        line["serving"] = {k: sv[k] for k in (
+            "requests", "rate_per_s", "wall_s", "setup_s", "latency_ms", "latency_ms_by_mode",
+            "converged", "not_converged", "max_true_relative_residual", "free_dofs_per_s",
+            "whole_device", "mean_batch")}
+        line["serving"]["workload"] = ("70% P1 unit square n ~ logU[32,1024] squares/side, "
+                                       "30% P2 Kuhn box n ~ logU[8,40]; lognormal cell "
+                                       "coefficient, GRF source (RFF, corr. length 0.1), "
+                                       "Poisson arrivals; tolerance 1e-10 true residual")
 
     if rank == 0 and world == 1 and not args.no_cpu:
         n_iter = line.get("fp64_gpu", {}).get("iterations")
