@@ -39,6 +39,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "ffg_internal.h"
 
@@ -53,6 +54,16 @@ constexpr int kPartialBatch = 8;   // partial loads in flight per lane
 constexpr int kResultDoubles = 16;
 constexpr int kMinWindow = 256;  // iterations before a plateau forces a reliable update
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
+// Staged FP32 SpMV: every warp streams its slices through kStages shared-memory
+// buffers of kChunkCols columns (32 rows each): FP32 values then int16 offsets.
+// Measured on the 48^3 P2 system: 2 x 10 columns (120 KB per CTA) beats
+// 2 x 6/8/12/14/16 and 3 x 8 (wider stages take L1 the gathers need).
+constexpr int kChunkCols = 10;
+constexpr int kStageVal = kChunkCols * 32 * 4;                // 1280 B
+constexpr int kStageBytes = kStageVal + kChunkCols * 32 * 2;  // + 640 B
+constexpr int kStages = 2;                                   // chunks in flight per warp
+constexpr int kStageSmem = kWarps * kStages * kStageBytes;   // 120 KB per CTA
+constexpr unsigned long long kCopyLimitNs = 1000000000ull;   // 1 s per copy wait
 
 struct PcgParams {
   int64_t n;
@@ -81,7 +92,17 @@ struct PcgParams {
   // CTAs that solve this system: blockIdx.x - cta0 in [0, ncta).  With one
   // CTA the system's slices are [0, n_slices) and barriers are CTA barriers.
   int cta0, ncta, n_slices;
+  int staged;  // launched with kStageSmem bytes of dynamic shared memory
 };
+
+// Set when a warp's staged copy did not complete in time; every barrier
+// checks it, so the solve ends on the next one.
+__shared__ int g_abort;
+// Per-warp mbarriers of the two staging buffers, initialised once per kernel
+// (an mbarrier is not re-initialised while in use), and the parity each warp
+// waits for next on each of them.
+__shared__ unsigned long long g_mbar[kWarps][kStages];
+__shared__ unsigned g_mparity[kWarps];
 
 __device__ __forceinline__ int cta_of(const PcgParams &P) { return (int)blockIdx.x - P.cta0; }
 
@@ -107,6 +128,7 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
   __shared__ int ok;
   __syncthreads();
   ++phase;
+  if (g_abort) return false;
   if (P.ncta == 1) return true;
   if (threadIdx.x == 0) {
     __threadfence();
@@ -265,6 +287,162 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
   __syncthreads();
 }
 
+// ------------------------------------------------------ staged FP32 SpMV
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long *m) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(m)) : "memory");
+}
+
+// The operator is read once per iteration: its lines enter L2 as evict-first
+// so that they do not push the iteration vectors out.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          unsigned long long *m) {
+  uint64_t policy;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(m)), "l"(policy)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(unsigned long long *m, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(m)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait on an mbarrier phase (1 s); on failure flags the solve and
+// returns false.
+__device__ bool mbar_wait(const PcgParams &P, unsigned long long *m, unsigned parity) {
+  const unsigned a = smem_addr(m);
+  unsigned long long t0 = 0;
+  for (unsigned spin = 0;; ++spin) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((spin & 1023u) == 0) {
+      const unsigned long long t = globaltimer();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > kCopyLimitNs) break;
+    }
+  }
+  atomicCAS(P.control, 0, FFG_TIMEOUT);
+  g_abort = 1;
+  return false;
+}
+
+// Chunk c of slice s into stage buffer `buf` (values, then offsets).  Slice
+// offsets are multiples of 32 entries and chunks multiples of kChunkCols
+// columns, so both sources are 64-byte aligned and both sizes multiples of 64.
+__device__ __forceinline__ void issue_chunk(const PcgParams &P, const float *val, int s, int c,
+                                            unsigned char *buf, unsigned long long *m) {
+  const int64_t e0 = P.soff[s] + (int64_t)c * kChunkCols * 32;
+  const int len = (int)((P.soff[s + 1] - P.soff[s]) / 32);
+  const int cols = min(kChunkCols, len - c * kChunkCols);
+  const unsigned nv = (unsigned)cols * 32u * 4u, nc = (unsigned)cols * 32u * 2u;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  mbar_expect(m, nv + nc);
+  bulk_load(buf, val + e0, nv, m);
+  bulk_load(buf + kStageVal, P.dcol + e0, nc, m);
+}
+
+__device__ __forceinline__ int slice_chunks(const PcgParams &P, int s) {
+  const int len = (int)((P.soff[s + 1] - P.soff[s]) / 32);
+  return (len + kChunkCols - 1) / kChunkCols;
+}
+
+// Mixed-mode SpMV with int16 offsets, q = A (z + beta p) and p = z + beta p,
+// like spmv_pairs, with the operator streamed by the bulk-copy engine: warp w
+// takes slices s0 + w, s0 + w + 32, ... and keeps one chunk of kChunkCols
+// columns in flight while it gathers and sums the other, so the bytes in
+// flight per SM are set by shared memory rather than by registers.  The copies
+// mark their L2 lines evict-first, which keeps the iteration vectors in L2.
+// Each row is still summed by one lane in column order.
+__device__ __noinline__ void spmv_staged(const PcgParams &P, const float *__restrict__ val,
+                                         const float2 *__restrict__ zc, float2 *__restrict__ zn,
+                                         float *__restrict__ q, float beta) {
+  extern __shared__ __align__(1024) unsigned char stage_smem[];
+  unsigned long long(&mbar)[kWarps][kStages] = g_mbar;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int s0, s1;
+  slice_range(P, s0, s1);
+  unsigned char *wbuf = stage_smem + (size_t)warp * kStages * kStageBytes;
+  // producer cursor: next chunk to copy (slices with no columns are skipped)
+  int ps = s0 + warp, pc = 0;
+  while (ps < s1 && slice_chunks(P, ps) == 0) ps += kWarps;
+  auto advance = [&]() {
+    if (++pc >= slice_chunks(P, ps)) {
+      pc = 0;
+      do ps += kWarps; while (ps < s1 && slice_chunks(P, ps) == 0);
+    }
+  };
+  unsigned pending = 0;  // stages with a copy issued and not yet waited for
+  for (int k = 0; k < kStages && ps < s1; ++k) {
+    if (lane == 0) issue_chunk(P, val, ps, pc, wbuf + k * kStageBytes, &mbar[warp][k]);
+    pending |= 1u << k;
+    advance();
+  }
+  unsigned parity = g_mparity[warp], seq = 0;
+  bool ok = true;
+  for (int cs = s0 + warp; cs < s1; cs += kWarps) {
+    const int len = (int)((P.soff[cs + 1] - P.soff[cs]) / 32);
+    const int row = cs * kSliceRows + lane;
+    float acc = 0.0f;
+    for (int c = 0; c * kChunkCols < len; ++c, ++seq) {
+      const int st = (int)(seq % kStages);
+      if (ok) {
+        const bool got = mbar_wait(P, &mbar[warp][st], (parity >> st) & 1u);
+        ok = __all_sync(0xffffffffu, got);
+        if (ok) {
+          pending &= ~(1u << st);
+          parity ^= 1u << st;
+        }
+      }
+      const int cols = min(kChunkCols, len - c * kChunkCols);
+      const float *vb = reinterpret_cast<const float *>(wbuf + st * kStageBytes);
+      const int16_t *cb = reinterpret_cast<const int16_t *>(wbuf + st * kStageBytes + kStageVal);
+      if (ok) {
+#pragma unroll
+        for (int j = 0; j < kChunkCols; ++j) {
+          if (j < cols) {
+            const float2 a = zc[row + (int)cb[j * 32 + lane]];
+            acc += vb[j * 32 + lane] * (a.x + beta * a.y);
+          }
+        }
+      }
+      __syncwarp();
+      if (ps < s1) {
+        if (ok) {
+          if (lane == 0) issue_chunk(P, val, ps, pc, wbuf + st * kStageBytes, &mbar[warp][st]);
+          pending |= 1u << st;
+        }
+        advance();
+      }
+    }
+    if (row < P.n && ok) {
+      const float2 a = zc[row];
+      zn[row].y = a.x + beta * a.y;
+      q[row] = acc;
+    }
+  }
+  // after a failed wait, give the copies still in flight (bounded) time to
+  // land before the stage buffers are given up
+  for (int st = 0; st < kStages; ++st)
+    if (!ok && (pending >> st) & 1u) mbar_wait(P, &mbar[warp][st], (parity >> st) & 1u);
+  __syncwarp();
+  if (lane == 0) g_mparity[warp] = parity;
+  __syncthreads();
+}
+
 // r64 = b - A64 x over this CTA's slices (same scheduling as spmv_pairs).
 template <bool NARROW>
 __device__ __noinline__ void spmv_residual(const PcgParams &P) {
@@ -409,8 +587,12 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp(P);
     part[0] = 0.0;
-    if (P.dcol) spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
-    else spmv_pairs<V, V2, false>(P, A, zc, zn, q, bt);
+    if (kMixed && P.dcol && P.staged)
+      spmv_staged(P, (const float *)A, (const float2 *)zc, (float2 *)zn, (float *)q, (float)bt);
+    else if (P.dcol)
+      spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
+    else
+      spmv_pairs<V, V2, false>(P, A, zc, zn, q, bt);
     for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
     write_partials(P, phase, part, 1);
     t1 = stamp(P);
@@ -575,6 +757,13 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
 
 __device__ __forceinline__ void pcg_body(const PcgParams &P) {
   unsigned int phase = 0;
+  if (threadIdx.x == 0) g_abort = 0;
+  if (P.staged && (threadIdx.x & 31) == 0) {
+    for (int st = 0; st < kStages; ++st) mbar_init(&g_mbar[threadIdx.x >> 5][st]);
+    g_mparity[threadIdx.x >> 5] = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
   // only block 0 judges the wall limit; its verdict travels through a partial slot
   const unsigned long long t_start = globaltimer();
   Outcome o;
@@ -659,12 +848,38 @@ __global__ void sell_prepare_kernel(int64_t n, const int64_t *rp, const int *ci,
 
 }  // namespace
 
+namespace {
+// Opt the PCG kernels into kStageSmem bytes of dynamic shared memory (once per
+// device); false when the device refuses, in which case they run unstaged.
+bool staged_smem_ready() {
+  static std::mutex mu;
+  static int state[64] = {0};  // 0 unknown, 1 ready, -1 refused
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return false;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (state[dev] == 0) {
+    const bool ok =
+        cudaFuncSetAttribute((const void *)pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kStageSmem) == cudaSuccess &&
+        cudaFuncSetAttribute((const void *)pcg_batch_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    state[dev] = ok ? 1 : -1;
+  }
+  return state[dev] == 1;
+}
+}  // namespace
+
 int pcg_grid_size(int *grid) {
   int dev = 0, sms = 0, per_sm = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return FFG_CUDA_ERROR;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, kThreads, 0) !=
+  const size_t smem = staged_smem_ready() ? kStageSmem : 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pcg_kernel, kThreads, smem) !=
       cudaSuccess)
     return FFG_CUDA_ERROR;
   if (per_sm < 1) return FFG_CUDA_ERROR;
@@ -807,6 +1022,7 @@ PcgParams make_params(const DeviceSell &A, const double *b, double *x,
   P.cta0 = 0;
   P.ncta = A.grid;
   P.n_slices = (int)A.n_slices;
+  P.staged = 0;
   return P;
 }
 }  // namespace
@@ -818,13 +1034,15 @@ int pcg_launch(const DeviceSell &A, const double *b, double *x, const ffg_solver
     return FFG_INVALID_INPUT;
   }
   PcgParams P = make_params(A, b, x, opts, w);
+  P.staged = staged_smem_ready() ? 1 : 0;
   if (cudaMemsetAsync(w.barrier, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaMemsetAsync(w.control, 0, 64, stream) != cudaSuccess) return FFG_CUDA_ERROR;
   if (cudaMemsetAsync(w.result, 0, kResultDoubles * sizeof(double), stream) != cudaSuccess)
     return FFG_CUDA_ERROR;
   void *args[] = {&P};
   cudaError_t e = cudaLaunchCooperativeKernel((const void *)pcg_kernel, dim3(w.grid),
-                                              dim3(kThreads), args, 0, stream);
+                                              dim3(kThreads), args,
+                                              P.staged ? kStageSmem : 0, stream);
   if (e != cudaSuccess) {
     msg = std::string("cooperative launch failed: ") + cudaGetErrorString(e);
     cudaGetLastError();
@@ -847,14 +1065,16 @@ int pcg_launch_batch(int count, const DeviceSell *const *A, const double *const 
       return FFG_INVALID_INPUT;
     }
   static_assert(sizeof(PcgBatch) <= 32000, "kernel parameter block too large");
+  const int staged = staged_smem_ready() ? 1 : 0;
   PcgBatch B;
   for (int c0 = 0; c0 < count; c0 += kMaxBatch) {
     const int m = std::min(kMaxBatch, count - c0);
     for (int i = 0; i < m; ++i) {
       B.sys[i] = make_params(*A[c0 + i], b[c0 + i], x[c0 + i], opts, *w[c0 + i]);
+      B.sys[i].staged = staged;
       w[c0 + i]->control_host[0] = 0;
     }
-    pcg_batch_kernel<<<m, kThreads, 0, stream>>>(B);
+    pcg_batch_kernel<<<m, kThreads, staged ? kStageSmem : 0, stream>>>(B);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       msg = std::string("batch launch failed: ") + cudaGetErrorString(e);
