@@ -35,11 +35,11 @@ WORKLOAD = "p2_tetra_poisson_48cube_x6_jittered_lognormal"
 TOL = 1e-10
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pcg_kernel
 # launch on the 48^3 workload, from an ncu capture of
-# `bench.py --steps 1 --warmup 3 --no-cpu --no-e2e --no-fp64`, and the
+# `bench.py --steps 1 --warmup 3 --no-cpu --no-e2e --no-fp64 --serving-requests 0`, and the
 # algorithmic bytes of that launch; the live launch's traffic is scaled by
 # its own algorithmic bytes.
-PCG_TRAFFIC_BYTES = 105.395462e9 + 15.132652e9
-PCG_TRAFFIC_ALG_BYTES = 158143482268.0
+PCG_TRAFFIC_BYTES = 102.357361e9 + 3.228644e9
+PCG_TRAFFIC_ALG_BYTES = 159235912804.0
 
 
 def parse():
