@@ -368,11 +368,23 @@ def run_ours(args):
                        "ms_per_step": ems / args.steps}
 
     # serving: a Poisson stream of P1/P2 requests through the continuous-batching
-    # server (one stream per rank); latency from arrival to solution on the host
+    # server; with N GPUs the stream is N times longer and faster and each rank
+    # serves its share (no exchange on the data path); latency from arrival to
+    # solution on the host
     if args.serving_requests > 0:
-        from fortfem_b200 import serving
-        sv = serving.run_stream(args.serving_requests, args.serving_rate, seed=4 + rank,
-                                device=local)
+        from fortfem_b200 import replicas, serving
+        reqs = serving.poisson_stream(args.serving_requests * world, args.serving_rate * world,
+                                      seed=4)
+        share = replicas.partition_requests(reqs, world)[rank]
+        res, wall, setup = serving.run_requests(share, device=local)
+        rows = replicas.gather_lists([(r.rid, r.latency, r.converged, r.iterations,
+                                       r.true_relative_residual, r.mode, r.batch_size,
+                                       r.device_seconds) for r in res])
+        res_all = [serving.Result(i, lat, cv, it, tr, mode, bs, None, dev)
+                   for i, lat, cv, it, tr, mode, bs, dev in rows]
+        res_all.sort(key=lambda r: r.rid)
+        sv = serving.summarize(reqs, res_all, replicas.max_over_ranks(wall),
+                               replicas.max_over_ranks(setup), args.serving_rate * world)
         sv.pop("results")
         line["serving"] = {k: sv[k] for k in (
             "requests", "rate_per_s", "wall_s", "setup_s", "latency_ms", "latency_ms_by_mode",
@@ -381,7 +393,8 @@ def run_ours(args):
         line["serving"]["workload"] = ("70% P1 unit square n ~ logU[32,1024] squares/side, "
                                        "30% P2 Kuhn box n ~ logU[8,40]; lognormal cell "
                                        "coefficient, GRF source (RFF, corr. length 0.1), "
-                                       "Poisson arrivals; tolerance 1e-10 true residual")
+                                       "Poisson arrivals; tolerance 1e-10 true residual; "
+                                       "stream split over ranks by estimated work")
 
     if rank == 0 and world == 1 and not args.no_cpu:
         n_iter = line.get("fp64_gpu", {}).get("iterations")

@@ -380,18 +380,23 @@ class DeviceEngine:
         self.meshes.clear()
 
 
-def run_stream(count: int = 512, rate: float = 20.0, seed: int = 4, small_rows: int = 32768,
-               max_batch: int = 48, streams: int = 2, keep_solutions: bool = False,
-               device: int = 0) -> dict:
-    """Serve a Poisson stream end to end on one GPU; returns latency statistics."""
-    reqs = poisson_stream(count, rate, seed)
+def run_requests(reqs: List[Request], small_rows: int = 32768, max_batch: int = 48,
+                 streams: int = 2, keep_solutions: bool = False, device: int = 0):
+    """Serve `reqs` (arrival times relative to now) on one GPU; returns
+    (results, wall seconds, setup seconds)."""
     eng = DeviceEngine(device, keep_solutions=keep_solutions, streams=streams)
     setup = eng.prepare(reqs)
     sch = Scheduler(small_rows=small_rows, max_batch=max_batch, streams=streams)
     t0 = time.perf_counter()
-    res = serve(reqs, eng, sch)
+    res = serve(reqs, eng, sch) if reqs else []
     wall = time.perf_counter() - t0
     eng.close()
+    return res, wall, setup
+
+
+def summarize(reqs: List[Request], res: List[Result], wall: float, setup: float,
+              rate: float) -> dict:
+    """Latency percentiles (overall and per mode), convergence and throughput."""
     dofs = sum(free_dofs(r.key) for r in reqs)
     by_id = {r.rid: r for r in reqs}
     by_mode = {}
@@ -401,7 +406,7 @@ def run_stream(count: int = 512, rate: float = 20.0, seed: int = 4, small_rows: 
             by_mode[mode] = {"requests": len(lat), **percentiles(lat),
                              "device_s": float(sum(r.device_seconds for r in res
                                                    if r.mode == mode))}
-    return {"requests": count, "rate_per_s": rate, "wall_s": wall, "setup_s": setup,
+    return {"requests": len(reqs), "rate_per_s": rate, "wall_s": wall, "setup_s": setup,
             "latency_ms": percentiles([r.latency for r in res]), "latency_ms_by_mode": by_mode,
             "converged": sum(r.converged for r in res),
             "max_true_relative_residual": max(r.true_relative_residual for r in res),
@@ -410,6 +415,15 @@ def run_stream(count: int = 512, rate: float = 20.0, seed: int = 4, small_rows: 
             "free_dofs_per_s": dofs / wall,
             "whole_device": sum(r.mode == "whole_device" for r in res),
             "mean_batch": float(np.mean([r.batch_size for r in res])), "results": res}
+
+
+def run_stream(count: int = 512, rate: float = 20.0, seed: int = 4, small_rows: int = 32768,
+               max_batch: int = 48, streams: int = 2, keep_solutions: bool = False,
+               device: int = 0) -> dict:
+    """Serve a Poisson stream end to end on one GPU; returns latency statistics."""
+    reqs = poisson_stream(count, rate, seed)
+    res, wall, setup = run_requests(reqs, small_rows, max_batch, streams, keep_solutions, device)
+    return summarize(reqs, res, wall, setup, rate)
 
 
 if __name__ == "__main__":
