@@ -194,10 +194,12 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
                                        double *__restrict__ elem, double *__restrict__ cell_rhs,
                                        int *err) {
   extern __shared__ double sm[];
-  const int nb = D.nb;
-  double *K = sm;                      // nb * nb
+  const int nb = D.nb, fdc = D.fdc;
+  double *K = sm;                      // nb * nb, column-major
   double *F = K + (size_t)nb * nb;     // nb
   double *lf = F + nb;                 // 3 * nql: det J^-1 f_q
+  double *tmp = lf + 3 * nql;          // nb * fdc: one face block of K T or T^T K
+  double *B = tmp + (size_t)nb * fdc;  // fdc * fdc: the face block of T in use
   __shared__ double geo[12];
   __shared__ double Ji_s[9];
   __shared__ double det_s;
@@ -253,25 +255,42 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
     const int8_t *sg = edge_sign + 6 * (size_t)c;
     const uint8_t *fp = face_perm + 4 * (size_t)c;
     double *O = elem + nn * c;
+    // T^T K T with T block diagonal: +-1 on edge moments, a dense fdc x fdc
+    // block per face (T[st+m][st+r] = B[r*fdc+m]), identity on cell moments.
+    // Face blocks first: columns (K <- K T), then rows (K <- T^T K), one face
+    // at a time through `tmp`; the edge signs are applied on the way out.
+    for (int f = 0; f < 4 && fdc > 0; ++f) {
+      const int st = D.edge_end + f * fdc;
+      const double *Bg = face_blocks + (size_t)fp[f] * fdc * fdc;
+      for (int q = threadIdx.x; q < fdc * fdc; q += blockDim.x) B[q] = Bg[q];
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x) {
+        const int i = q % nb, r = q / nb;
+        double acc = 0.0;
+        for (int m = 0; m < fdc; ++m) acc += K[i + (size_t)nb * (st + m)] * B[r * fdc + m];
+        tmp[q] = acc;
+      }
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x)
+        K[(q % nb) + (size_t)nb * (st + q / nb)] = tmp[q];
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x) {
+        const int r = q % fdc, j = q / fdc;
+        double acc = 0.0;
+        for (int m = 0; m < fdc; ++m) acc += B[r * fdc + m] * K[(st + m) + (size_t)nb * j];
+        tmp[q] = acc;
+      }
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x)
+        K[(st + q % fdc) + (size_t)nb * (q / fdc)] = tmp[q];
+      __syncthreads();
+    }
     for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
       const int i = (int)(idx % nb), j = (int)(idx / nb);
-      int si, ni, sj, nj;
-      const double *ci, *cj;
-      double di, dj;
-      ned_block(D, sg, fp, face_blocks, i, si, ni, ci, di);
-      ned_block(D, sg, fp, face_blocks, j, sj, nj, cj, dj);
-      double s = 0.0;
-      for (int m = 0; m < ni; ++m) {
-        const double tm = ci ? ci[m] : di;
-        if (tm == 0.0) continue;
-        double inner = 0.0;
-        for (int n = 0; n < nj; ++n) {
-          const double tn = cj ? cj[n] : dj;
-          inner += K[(si + m) + (size_t)nb * (sj + n)] * tn;
-        }
-        s += tm * inner;
-      }
-      O[idx] = s;
+      double v = K[idx];
+      if (i < D.edge_end && sg[i / D.k] == -1 && ((i % D.k) % 2) == 0) v = -v;
+      if (j < D.edge_end && sg[j / D.k] == -1 && ((j % D.k) % 2) == 0) v = -v;
+      O[idx] = v;
     }
     for (int i = threadIdx.x; i < nb; i += blockDim.x) {
       int si, ni;
@@ -395,8 +414,9 @@ int launch_cell_geometry(const Topology &t, const ElementTables &tab, const Devi
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 
-size_t nedelec_smem_bytes(const ElementTables &tab) {
-  return sizeof(double) * ((size_t)tab.nb * tab.nb + tab.nb + 3 * (size_t)tab.nq_load);
+size_t nedelec_smem_bytes(const ElementTables &tab, int fdc) {
+  return sizeof(double) * ((size_t)tab.nb * tab.nb + tab.nb + 3 * (size_t)tab.nq_load +
+                           (size_t)tab.nb * fdc + (size_t)fdc * fdc);
 }
 
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
@@ -408,7 +428,7 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   D.fdc = t.degree * (t.degree - 1);
   D.edge_end = 6 * t.degree;
   D.face_end = D.edge_end + 4 * D.fdc;
-  const size_t smem = nedelec_smem_bytes(tab);
+  const size_t smem = nedelec_smem_bytes(tab, D.fdc);
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(nedelec_element_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
