@@ -138,7 +138,8 @@ static double ipow(double x, int n) {
   return r;
 }
 
-// Candidate monomial space of evaluate_runtime_candidates (order <= 5,
+// Candidate monomial space of evaluate_runtime_candidates (order <= 5; order 6
+// uses the same construction, see gen_nedelec_tables.py;
 // tetra_nedelec_arbitrary_order.f90:318-396) times the exact dual-basis
 // coefficients (evaluate_tetra_nedelec_first_kind, :75-106).
 bool nedelec_eval(int k, const double *pt, double *val, double *curl) {

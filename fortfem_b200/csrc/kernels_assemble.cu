@@ -154,6 +154,7 @@ __global__ void p1_geometry_kernel(int n_cells, const int *__restrict__ tris,
 // reversed edges, dense face blocks per face permutation, identity on cells.
 struct NedDims {
   int k, nb, fdc, edge_end, face_end;
+  int kglobal;  // the nb x nb matrix does not fit in shared memory: work in `elem`
 };
 
 __device__ __forceinline__ void ned_block(const NedDims &D, const int8_t *sg, const uint8_t *fp,
@@ -195,8 +196,10 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
                                        int *err) {
   extern __shared__ double sm[];
   const int nb = D.nb, fdc = D.fdc;
-  double *K = sm;                      // nb * nb, column-major
-  double *F = K + (size_t)nb * nb;     // nb
+  // K (nb x nb, column-major) lives in shared memory, or (order 6: 373 KB) in
+  // the cell's slice of `elem`, where the finished matrix is written anyway
+  double *K = D.kglobal ? nullptr : sm;
+  double *F = D.kglobal ? sm : sm + (size_t)nb * nb;  // nb
   double *lf = F + nb;                 // 3 * nql: det J^-1 f_q
   double *tmp = lf + 3 * nql;          // nb * fdc: one face block of K T or T^T K
   double *B = tmp + (size_t)nb * fdc;  // fdc * fdc: the face block of T in use
@@ -205,6 +208,7 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
   __shared__ double det_s;
   __shared__ int ok_s;
   for (int c = blockIdx.x; c < n_cells; c += gridDim.x) {
+    if (D.kglobal) K = elem + (size_t)nb * nb * c;
     if (threadIdx.x == 0) {
       double J[9], Ji[9], v0[3];
       tet_jacobian(cells, verts, c, J, v0);
@@ -414,9 +418,9 @@ int launch_cell_geometry(const Topology &t, const ElementTables &tab, const Devi
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 
-size_t nedelec_smem_bytes(const ElementTables &tab, int fdc) {
-  return sizeof(double) * ((size_t)tab.nb * tab.nb + tab.nb + 3 * (size_t)tab.nq_load +
-                           (size_t)tab.nb * fdc + (size_t)fdc * fdc);
+size_t nedelec_smem_bytes(const ElementTables &tab, int fdc, bool kglobal) {
+  return sizeof(double) * ((kglobal ? 0 : (size_t)tab.nb * tab.nb) + tab.nb +
+                           3 * (size_t)tab.nq_load + (size_t)tab.nb * fdc + (size_t)fdc * fdc);
 }
 
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
@@ -428,7 +432,8 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   D.fdc = t.degree * (t.degree - 1);
   D.edge_end = 6 * t.degree;
   D.face_end = D.edge_end + 4 * D.fdc;
-  const size_t smem = nedelec_smem_bytes(tab, D.fdc);
+  D.kglobal = nedelec_smem_bytes(tab, D.fdc, false) > 200 * 1024 ? 1 : 0;
+  const size_t smem = nedelec_smem_bytes(tab, D.fdc, D.kglobal != 0);
   if (smem > 48 * 1024) {
     if (cudaFuncSetAttribute(nedelec_element_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)

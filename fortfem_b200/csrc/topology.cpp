@@ -124,7 +124,7 @@ int build_lagrange(Topology &t, std::string &msg) {
 
 int build_nedelec(Topology &t, std::string &msg) {
   const int k = t.degree;
-  if (k < 1 || k > 5) { msg = "Nedelec order must be 1..5"; return FFG_INVALID_INPUT; }
+  if (k < 1 || k > 6) { msg = "Nedelec order must be 1..6"; return FFG_INVALID_INPUT; }
   t.nb = nedelec_dof_count(k);
   const int fdc = k * (k - 1), cdc = k * (k - 1) * (k - 2) / 2;
   t.gd.assign((size_t)t.nb * t.n_cells, 0);

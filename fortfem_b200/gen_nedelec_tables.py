@@ -1,8 +1,8 @@
 """Exact-rational generator for the first-kind tetrahedral Nedelec tables.
 
-Writes ``fortfem_b200/csrc/nedelec_tables.inc``: for orders 1..5 the dual-basis
+Writes ``fortfem_b200/csrc/nedelec_tables.inc``: for orders 1..6 the dual-basis
 coefficient matrix C = M^-1 of the monomial candidate space, and for orders
-2..5 the 6 face basis-to-local transforms.  Everything is computed with Python
+2..6 the 6 face basis-to-local transforms.  Everything is computed with Python
 ``fractions`` and rounded to the nearest double only when written.
 
 The definitions restate the reference:
@@ -16,6 +16,12 @@ The definitions restate the reference:
   the exact generator ``tools/codegen/app/gen_tetra_nedelec_coefficients.f90:50-200``;
 * face transform = L C^-1 of the face moment matrices under a vertex
   permutation -- ``src/elements/tetra_face_moment_transforms.f90:296-383``.
+
+Order 6 uses the same monomial construction as orders <= 5.  The reference
+switches to Koornwinder/Dubiner modes of fortnum (not vendored) at order 6, so
+its order-6 basis differs from this one by a change of basis inside each edge,
+face and cell block; only basis-invariant quantities (energies, solutions)
+compare across the two.
 
 Order 1..4 tables are pinned against the reference's generated tables by
 ``tests/golden/nedelec_tables.json`` (see ``tests/golden/make_golden.py``).
@@ -32,7 +38,7 @@ REF_VERTS = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)]
 EDGES = [(0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3)]
 FACES = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
 PERMUTATIONS = [(1, 2, 3), (1, 3, 2), (2, 1, 3), (2, 3, 1), (3, 1, 2), (3, 2, 1)]
-MAX_ORDER = 5
+MAX_ORDER = 6
 
 
 def dof_count(k: int) -> int:
@@ -160,6 +166,95 @@ def face_integral(poly, f, ma, mb):
     return total
 
 
+# ------------------------------------------- orthogonal moment weights (k >= 6)
+# From order 6 the reference weights face moments by triangle_dubiner and
+# volume moments by tetrahedron_koornwinder (tetra_nedelec_arbitrary_order.f90:
+# 642-668) instead of monomials.  They are restated here with the standard
+# collapsed-coordinate definitions on the reference triangle / tetrahedron
+# (Dubiner 1991, Koornwinder 1975; Jacobi polynomials P_n^(alpha,0)), built
+# exactly as polynomials with rational coefficients.
+
+def jacobi(n: int, alpha: int):
+    """Coefficients of P_n^(alpha,0)(t) in powers of t (exact)."""
+    from math import comb
+    out = [Fraction(0)] * (n + 1)
+    for s_ in range(n + 1):
+        c = Fraction(comb(n + alpha, n - s_) * comb(n, s_))
+        # ((t-1)/2)^s ((t+1)/2)^(n-s)
+        p = poly1_mul(poly1_pow_affine(Fraction(-1, 2), Fraction(1, 2), s_),
+                      poly1_pow_affine(Fraction(1, 2), Fraction(1, 2), n - s_))
+        for i, x in enumerate(p):
+            out[i] += c * x
+    return out
+
+
+def _polyn_mul(p, q):
+    r = {}
+    for e1, a in p.items():
+        for e2, b in q.items():
+            key = tuple(x + y for x, y in zip(e1, e2))
+            r[key] = r.get(key, Fraction(0)) + a * b
+    return {k_: v for k_, v in r.items() if v != 0}
+
+
+def _polyn_pow(p, n, dim):
+    r = {(0,) * dim: Fraction(1)}
+    for _ in range(n):
+        r = _polyn_mul(r, p)
+    return r
+
+
+def _polyn_add(p, q, scale=Fraction(1)):
+    r = dict(p)
+    for k_, v in q.items():
+        r[k_] = r.get(k_, Fraction(0)) + scale * v
+    return {k_: v for k_, v in r.items() if v != 0}
+
+
+def _collapsed(coef_t, num, den, degree, dim):
+    """den^degree * P(num/den) for P = sum coef_t[i] t^i (num, den linear polys)."""
+    out = {}
+    for i, c in enumerate(coef_t):
+        if c:
+            term = _polyn_mul(_polyn_pow(num, i, dim), _polyn_pow(den, degree - i, dim))
+            out = _polyn_add(out, term, c)
+    return out
+
+
+def dubiner(p: int, q: int):
+    """Dubiner polynomial psi_pq(x, y) on the triangle (0,0),(1,0),(0,1)."""
+    one_minus_y = {(0, 0): Fraction(1), (0, 1): Fraction(-1)}
+    a_num = {(1, 0): Fraction(2), (0, 0): Fraction(-1), (0, 1): Fraction(1)}  # 2x - 1 + y
+    A = _collapsed(jacobi(p, 0), a_num, one_minus_y, p, 2)
+    B = _collapsed(jacobi(q, 2 * p + 1), {(0, 1): Fraction(2), (0, 0): Fraction(-1)},
+                   {(0, 0): Fraction(1)}, q, 2)
+    return _polyn_mul(A, B)
+
+
+def koornwinder(p: int, q: int, r: int):
+    """Koornwinder polynomial phi_pqr(x, y, z) on the unit tetrahedron."""
+    e = lambda x, y, z: (x, y, z)  # noqa: E731
+    one_yz = {e(0, 0, 0): Fraction(1), e(0, 1, 0): Fraction(-1), e(0, 0, 1): Fraction(-1)}
+    a_num = {e(1, 0, 0): Fraction(2), e(0, 0, 0): Fraction(-1), e(0, 1, 0): Fraction(1),
+             e(0, 0, 1): Fraction(1)}                                    # 2x - 1 + y + z
+    one_z = {e(0, 0, 0): Fraction(1), e(0, 0, 1): Fraction(-1)}
+    b_num = {e(0, 1, 0): Fraction(2), e(0, 0, 0): Fraction(-1), e(0, 0, 1): Fraction(1)}  # 2y-1+z
+    A = _collapsed(jacobi(p, 0), a_num, one_yz, p, 3)
+    B = _collapsed(jacobi(q, 2 * p + 1), b_num, one_z, q, 3)
+    C = _collapsed(jacobi(r, 2 * p + 2 * q + 2), {e(0, 0, 1): Fraction(2), e(0, 0, 0): Fraction(-1)},
+                   {e(0, 0, 0): Fraction(1)}, r, 3)
+    return _polyn_mul(_polyn_mul(A, B), C)
+
+
+def face_weight(k: int, a: int, b: int):
+    """Face moment weight in face coordinates: u^a v^b (k <= 5) or Dubiner (k >= 6)."""
+    return {(a, b): Fraction(1)} if k <= 5 else dubiner(a, b)
+
+
+def volume_weight(k: int, a: int, b: int, c: int):
+    return {(a, b, c): Fraction(1)} if k <= 5 else koornwinder(a, b, c)
+
+
 def moment_matrix(k: int):
     cands = candidates(k)
     n = len(cands)
@@ -184,12 +279,14 @@ def moment_matrix(k: int):
             for d in range(k - 1):
                 for ma in range(d + 1):
                     mb = d - ma
+                    w = face_weight(k, ma, mb)
                     row = []
-                    for cand in cands:
+                    for ci, cand in enumerate(cands):
                         s = Fraction(0)
                         for comp in range(3):
                             if t[comp] and cand[comp]:
-                                s += t[comp] * face_integral(cand[comp], f, ma, mb)
+                                for (wa, wb), wc in w.items():
+                                    s += t[comp] * wc * _face_int(k, ci, comp, f, wa, wb, cand)
                         row.append(s)
                     rows.append(row)
     for comp in range(3):
@@ -197,15 +294,27 @@ def moment_matrix(k: int):
             for a in range(d + 1):
                 for b in range(d - a + 1):
                     c = d - a - b
+                    w = volume_weight(k, a, b, c)
                     row = []
                     for cand in cands:
                         s = Fraction(0)
                         for (pa, pb, pc), coef in cand[comp].items():
-                            s += coef * tet_monomial(pa + a, pb + b, pc + c)
+                            for (wa, wb, wc), wv in w.items():
+                                s += coef * wv * tet_monomial(pa + wa, pb + wb, pc + wc)
                         row.append(s)
                     rows.append(row)
     assert len(rows) == n
     return rows
+
+
+_FACE_CACHE = {}
+
+
+def _face_int(k, ci, comp, f, ma, mb, cand):
+    key = (k, ci, comp, f, ma, mb)
+    if key not in _FACE_CACHE:
+        _FACE_CACHE[key] = face_integral(cand[comp], f, ma, mb)
+    return _FACE_CACHE[key]
 
 
 def exact_inverse(M):
@@ -252,17 +361,21 @@ def face_moment_matrix(k: int, perm):
     n = len(idx)
     M = [[Fraction(0)] * n for _ in range(n)]
     for col, (bc, bx, by) in enumerate(idx):
-        # mapped = off + aff @ (u, v); poly = mapped_x^bx mapped_y^by
-        px = affine2_pow(off[0], aff[0][0], aff[0][1], bx)
-        py = affine2_pow(off[1], aff[1][0], aff[1][1], by)
-        pm = poly2_mul(px, py)
+        # mapped = off + aff @ (u, v); poly = weight(bx, by) at the mapped point
+        pm = {}
+        for (wx, wy), wc in face_weight(k, bx, by).items():
+            px = affine2_pow(off[0], aff[0][0], aff[0][1], wx)
+            py = affine2_pow(off[1], aff[1][0], aff[1][1], wy)
+            for key, x in poly2_mul(px, py).items():
+                pm[key] = pm.get(key, Fraction(0)) + wc * x
         for row, (mc, mx, my) in enumerate(idx):
             scale = aff[bc][mc]
             if scale == 0:
                 continue
             s = Fraction(0)
-            for (i, j), x in pm.items():
-                s += x * tri_monomial(i + mx, j + my)
+            for (wx, wy), wc in face_weight(k, mx, my).items():
+                for (i, j), x in pm.items():
+                    s += wc * x * tri_monomial(i + wx, j + wy)
             M[row][col] = scale * s
     return M
 

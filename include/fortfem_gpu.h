@@ -208,7 +208,7 @@ void ffg_build_topology(int family, int degree, int n_vertices, int n_cells, con
 /* Build the topology of an assemble + constrain + solve problem once per mesh
  * (DoF numbering in the reference's first-appearance order, the CSC pattern,
  * the constrained set and the element-to-CSC slot maps) and keep it in HBM.
- * family: FFG_TETRA_LAGRANGE (degree 1..4), FFG_TETRA_NEDELEC (order 1..5) or
+ * family: FFG_TETRA_LAGRANGE (degree 1..4), FFG_TETRA_NEDELEC (order 1..6) or
  * FFG_TRIANGLE_P1 (degree 1; vertices are then 2-D).  For Lagrange the rule
  * and quadrature degree select the element and load quadrature; Nedelec uses
  * the reference rules (order 1: the 4-point rule; order k >= 2: Duffy 2k for

@@ -69,6 +69,27 @@ def test_nedelec_csc_matches_oracle(k):
     assert rel_frob(A.val, val) <= (1e-11 if k == 5 else FROB)
 
 
+# order 6: the element matrix (216 x 216) is built in global memory instead of
+# shared memory; a 6-cell mesh keeps the oracle's quadrature loop short
+def test_nedelec_order6_csc_and_load_match_oracle():
+    k = 6
+    v, t = jittered_box(1, 0.0, 11)
+    rng = np.random.default_rng(6)
+    cc = rng.uniform(0.5, 2.0, len(t))
+    cm = rng.uniform(0.5, 2.0, len(t))
+    A, st = ff.assemble_tetra_nedelec_curl_mass_csc(v, t, 1.7, 0.9, order=k, cell_curl=cc,
+                                                    cell_mass=cm)
+    assert st.code == 0
+    n, cp, ri, val = oracle.nedelec_csc(v, t, k, 1.7, 0.9, cc, cm)
+    assert A.nrow == n == 1014 and np.array_equal(A.col_ptr, cp) and np.array_equal(A.row_idx, ri)
+    assert rel_frob(A.val, val) <= 1e-10
+    pts = oracle.nedelec_load_points(v, t, k)
+    src = np.stack([np.sin(pts[..., 1]), pts[..., 0] * pts[..., 2], np.cos(pts[..., 0])], -1)
+    rhs, st = ff.assemble_tetra_nedelec_vector_load_samples(v, t, k, src)
+    assert st.code == 0
+    assert rel_frob(rhs, oracle.nedelec_load_samples(v, t, k, src)) <= 1e-10
+
+
 @pytest.mark.parametrize("k", [1, 2, 3, 4])
 def test_nedelec_load_matches_oracle(k):
     v, t = jittered_box(2, 0.1, 3)

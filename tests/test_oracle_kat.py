@@ -192,7 +192,10 @@ def _constant_field_dofs(k, verts, tets, dm, field):
                     yd = d - xd
                     mono += 1
                     dof = off + f * fdc + comp * fdc // 2 + mono - 1
-                    dofs[dof] = (field @ tang) * fact(xd) * fact(yd) / fact(xd + yd + 2)
+                    if k <= 5:
+                        dofs[dof] = (field @ tang) * fact(xd) * fact(yd) / fact(xd + yd + 2)
+                    else:  # orthogonal (Dubiner) weights: only the constant one integrates
+                        dofs[dof] = 0.5 * (field @ tang) if d == 0 else 0.0
     base = 6 * k + 4 * fdc
     for c, tet in enumerate(tets):
         J = np.stack([verts[tet[1]] - verts[tet[0]], verts[tet[2]] - verts[tet[0]],
@@ -204,7 +207,10 @@ def _constant_field_dofs(k, verts, tets, dm, field):
                 for xd in range(d + 1):
                     for yd in range(d - xd + 1):
                         zd = d - xd - yd
-                        dofs[gd[c, loc]] = rf[comp] * fact(xd) * fact(yd) * fact(zd) / fact(d + 3)
+                        if k <= 5:
+                            dofs[gd[c, loc]] = rf[comp] * fact(xd) * fact(yd) * fact(zd) / fact(d + 3)
+                        else:  # orthogonal (Koornwinder) weights
+                            dofs[gd[c, loc]] = rf[comp] / 6.0 if d == 0 else 0.0
                         loc += 1
     return dofs
 
@@ -226,7 +232,7 @@ def test_nedelec_energy_kats():
     n, cp, ri, val = oracle.nedelec_csc(verts, tets, 1, 2.0, 0.0)
     y = oracle.csc_matvec(n, cp, ri, val, dofs)
     assert abs(dofs @ y - 28.0 / 3.0) < 3e-12
-    for k in range(2, 6):
+    for k in range(2, 7):
         dm = oracle.nedelec_dof_map(k, tets)
         dofs = _constant_field_dofs(k, verts, tets, dm, field)
         n, cp, ri, val = oracle.nedelec_csc(verts, tets, k, 4.0, 1.5)
