@@ -54,13 +54,12 @@ constexpr int kPartialBatch = 8;   // partial loads in flight per lane
 constexpr int kResultDoubles = 16;
 constexpr int kMinWindow = 256;  // iterations before a plateau forces a reliable update
 constexpr unsigned long long kBarrierLimitNs = 4000000000ull;  // 4 s per barrier wait
-// Staged FP32 SpMV: every warp streams its slices through kStages shared-memory
-// buffers of kChunkCols columns (32 rows each): FP32 values then int16 offsets.
-// Measured on the 48^3 P2 system: 2 x 10 columns (120 KB per CTA) beats
-// 2 x 6/8/12/14/16 and 3 x 8 (wider stages take L1 the gathers need).
-constexpr int kChunkCols = 10;
-constexpr int kStageVal = kChunkCols * 32 * 4;                // 1280 B
-constexpr int kStageBytes = kStageVal + kChunkCols * 32 * 2;  // + 640 B
+// Staged SpMV: every warp streams its slices through kStages shared-memory
+// buffers of kStageBytes (32 rows by as many columns as fit: values, then
+// column indices).  Measured on the 48^3 P2 system (FP32 + int16): 2 x 10
+// columns (120 KB per CTA) beats 2 x 6/8/12/14/16 and 3 x 8 (wider stages
+// take L1 the gathers need).
+constexpr int kStageBytes = 10 * 32 * (4 + 2);                 // 1920 B
 constexpr int kStages = 2;                                   // chunks in flight per warp
 constexpr int kStageSmem = kWarps * kStages * kStageBytes;   // 120 KB per CTA
 constexpr unsigned long long kCopyLimitNs = 1000000000ull;   // 1 s per copy wait
@@ -340,36 +339,54 @@ __device__ bool mbar_wait(const PcgParams &P, unsigned long long *m, unsigned pa
   return false;
 }
 
-// Chunk c of slice s into stage buffer `buf` (values, then offsets).  Slice
-// offsets are multiples of 32 entries and chunks multiples of kChunkCols
-// columns, so both sources are 64-byte aligned and both sizes multiples of 64.
-__device__ __forceinline__ void issue_chunk(const PcgParams &P, const float *val, int s, int c,
+// Stage layout of one (value type, index type) pair: kStageBytes per stage
+// holds COLS columns of 32 rows, values first.  FP32 + int16: 10 columns,
+// FP32 + int32: 7, FP64 + int16: 6, FP64 + int32: 5.
+template <typename V, bool NARROW>
+struct StageShape {
+  static constexpr int kEntry = (int)sizeof(V) + (NARROW ? 2 : 4);
+  static constexpr int COLS = kStageBytes / (32 * kEntry);
+  static constexpr int VAL = COLS * 32 * (int)sizeof(V);
+};
+
+// Chunk c of slice s into stage buffer `buf` (values, then indices).  Slice
+// offsets are multiples of 32 entries and chunks multiples of COLS columns,
+// so both sources are 64-byte aligned and both sizes multiples of 64.
+template <typename V, bool NARROW>
+__device__ __forceinline__ void issue_chunk(const PcgParams &P, const V *val, int s, int c,
                                             unsigned char *buf, unsigned long long *m) {
-  const int64_t e0 = P.soff[s] + (int64_t)c * kChunkCols * 32;
+  using SS = StageShape<V, NARROW>;
+  const int64_t e0 = P.soff[s] + (int64_t)c * SS::COLS * 32;
   const int len = (int)((P.soff[s + 1] - P.soff[s]) / 32);
-  const int cols = min(kChunkCols, len - c * kChunkCols);
-  const unsigned nv = (unsigned)cols * 32u * 4u, nc = (unsigned)cols * 32u * 2u;
+  const int cols = min(SS::COLS, len - c * SS::COLS);
+  const unsigned nv = (unsigned)cols * 32u * (unsigned)sizeof(V);
+  const unsigned nc = (unsigned)cols * 32u * (NARROW ? 2u : 4u);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   mbar_expect(m, nv + nc);
   bulk_load(buf, val + e0, nv, m);
-  bulk_load(buf + kStageVal, P.dcol + e0, nc, m);
+  if (NARROW) bulk_load(buf + SS::VAL, P.dcol + e0, nc, m);
+  else bulk_load(buf + SS::VAL, P.col + e0, nc, m);
 }
 
+template <int COLS>
 __device__ __forceinline__ int slice_chunks(const PcgParams &P, int s) {
   const int len = (int)((P.soff[s + 1] - P.soff[s]) / 32);
-  return (len + kChunkCols - 1) / kChunkCols;
+  return (len + COLS - 1) / COLS;
 }
 
-// Mixed-mode SpMV with int16 offsets, q = A (z + beta p) and p = z + beta p,
-// like spmv_pairs, with the operator streamed by the bulk-copy engine: warp w
-// takes slices s0 + w, s0 + w + 32, ... and keeps one chunk of kChunkCols
-// columns in flight while it gathers and sums the other, so the bytes in
-// flight per SM are set by shared memory rather than by registers.  The copies
-// mark their L2 lines evict-first, which keeps the iteration vectors in L2.
-// Each row is still summed by one lane in column order.
-__device__ __noinline__ void spmv_staged(const PcgParams &P, const float *__restrict__ val,
-                                         const float2 *__restrict__ zc, float2 *__restrict__ zn,
-                                         float *__restrict__ q, float beta) {
+// SpMV q = A (z + beta p) and p = z + beta p, like spmv_pairs, with the
+// operator streamed by the bulk-copy engine: warp w takes slices s0 + w,
+// s0 + w + 32, ... and keeps one chunk of COLS columns in flight while it
+// gathers and sums the other, so the bytes in flight per SM are set by shared
+// memory rather than by registers.  The copies mark their L2 lines
+// evict-first, which keeps the iteration vectors in L2.  Each row is still
+// summed by one lane in column order.
+template <typename V, typename V2, bool NARROW>
+__device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict__ val,
+                                         const V2 *__restrict__ zc, V2 *__restrict__ zn,
+                                         V *__restrict__ q, V beta) {
+  using SS = StageShape<V, NARROW>;
+  constexpr int COLS = SS::COLS;
   extern __shared__ __align__(1024) unsigned char stage_smem[];
   unsigned long long(&mbar)[kWarps][kStages] = g_mbar;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -378,16 +395,16 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const float *__rest
   unsigned char *wbuf = stage_smem + (size_t)warp * kStages * kStageBytes;
   // producer cursor: next chunk to copy (slices with no columns are skipped)
   int ps = s0 + warp, pc = 0;
-  while (ps < s1 && slice_chunks(P, ps) == 0) ps += kWarps;
+  while (ps < s1 && slice_chunks<COLS>(P, ps) == 0) ps += kWarps;
   auto advance = [&]() {
-    if (++pc >= slice_chunks(P, ps)) {
+    if (++pc >= slice_chunks<COLS>(P, ps)) {
       pc = 0;
-      do ps += kWarps; while (ps < s1 && slice_chunks(P, ps) == 0);
+      do ps += kWarps; while (ps < s1 && slice_chunks<COLS>(P, ps) == 0);
     }
   };
   unsigned pending = 0;  // stages with a copy issued and not yet waited for
   for (int k = 0; k < kStages && ps < s1; ++k) {
-    if (lane == 0) issue_chunk(P, val, ps, pc, wbuf + k * kStageBytes, &mbar[warp][k]);
+    if (lane == 0) issue_chunk<V, NARROW>(P, val, ps, pc, wbuf + k * kStageBytes, &mbar[warp][k]);
     pending |= 1u << k;
     advance();
   }
@@ -396,8 +413,8 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const float *__rest
   for (int cs = s0 + warp; cs < s1; cs += kWarps) {
     const int len = (int)((P.soff[cs + 1] - P.soff[cs]) / 32);
     const int row = cs * kSliceRows + lane;
-    float acc = 0.0f;
-    for (int c = 0; c * kChunkCols < len; ++c, ++seq) {
+    V acc = 0;
+    for (int c = 0; c * COLS < len; ++c, ++seq) {
       const int st = (int)(seq % kStages);
       if (ok) {
         const bool got = mbar_wait(P, &mbar[warp][st], (parity >> st) & 1u);
@@ -407,14 +424,16 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const float *__rest
           parity ^= 1u << st;
         }
       }
-      const int cols = min(kChunkCols, len - c * kChunkCols);
-      const float *vb = reinterpret_cast<const float *>(wbuf + st * kStageBytes);
-      const int16_t *cb = reinterpret_cast<const int16_t *>(wbuf + st * kStageBytes + kStageVal);
+      const int cols = min(COLS, len - c * COLS);
+      const V *vb = reinterpret_cast<const V *>(wbuf + st * kStageBytes);
+      const unsigned char *ib = wbuf + st * kStageBytes + SS::VAL;
       if (ok) {
 #pragma unroll
-        for (int j = 0; j < kChunkCols; ++j) {
+        for (int j = 0; j < COLS; ++j) {
           if (j < cols) {
-            const float2 a = zc[row + (int)cb[j * 32 + lane]];
+            const int cidx = NARROW ? row + (int)reinterpret_cast<const int16_t *>(ib)[j * 32 + lane]
+                                    : reinterpret_cast<const int *>(ib)[j * 32 + lane];
+            const V2 a = zc[cidx];
             acc += vb[j * 32 + lane] * (a.x + beta * a.y);
           }
         }
@@ -422,14 +441,15 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const float *__rest
       __syncwarp();
       if (ps < s1) {
         if (ok) {
-          if (lane == 0) issue_chunk(P, val, ps, pc, wbuf + st * kStageBytes, &mbar[warp][st]);
+          if (lane == 0)
+            issue_chunk<V, NARROW>(P, val, ps, pc, wbuf + st * kStageBytes, &mbar[warp][st]);
           pending |= 1u << st;
         }
         advance();
       }
     }
     if (row < P.n && ok) {
-      const float2 a = zc[row];
+      const V2 a = zc[row];
       zn[row].y = a.x + beta * a.y;
       q[row] = acc;
     }
@@ -587,8 +607,10 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp(P);
     part[0] = 0.0;
-    if (kMixed && P.dcol && P.staged)
-      spmv_staged(P, (const float *)A, (const float2 *)zc, (float2 *)zn, (float *)q, (float)bt);
+    if (P.staged && P.dcol)
+      spmv_staged<V, V2, true>(P, A, zc, zn, q, bt);
+    else if (P.staged)
+      spmv_staged<V, V2, false>(P, A, zc, zn, q, bt);
     else if (P.dcol)
       spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
     else
