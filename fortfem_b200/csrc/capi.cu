@@ -134,9 +134,24 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   t.n_vertices = n_vertices;
   if (n_cells < 1 || n_vertices < 1 || !cells) { msg = "empty mesh"; return FFG_INVALID_INPUT; }
   t.cells.assign(cells, cells + (size_t)t.vpc * n_cells);
-  if ((st = build_dofs(t, msg))) return st;
-  if ((st = build_constraints(t, boundary_mode, mask, msg))) return st;
-  if ((st = build_pattern(t, msg))) return st;
+  int grid = 0;
+  if ((st = pcg_grid_size(&grid))) return st;
+  // Lagrange and P1 topologies are built on the device; Nedelec on the host
+  const bool on_device = family == FFG_TETRA_LAGRANGE || family == FFG_TRIANGLE_P1;
+  if (on_device) {
+    if (!validate_cells(t, msg)) return FFG_INVALID_INPUT;
+    if (family == FFG_TRIANGLE_P1 && (t.vpc != 3 || degree != 1)) {
+      msg = "P1 triangles only";
+      return FFG_INVALID_INPUT;
+    }
+    if ((st = build_topology_device(t, boundary_mode, mask, grid, P->dt, &P->csc_col_ptr,
+                                    &P->csc_row, P->S, msg)))
+      return st;
+  } else {
+    if ((st = build_dofs(t, msg))) return st;
+    if ((st = build_constraints(t, boundary_mode, mask, msg))) return st;
+    if ((st = build_pattern(t, msg))) return st;
+  }
   P->rule = rule;
   P->qdeg = qdeg;
   if ((st = build_tables(t, rule, qdeg, P->tab, msg))) return st;
@@ -144,27 +159,25 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   P->samples_per_cell = P->tab.nq_load;
   // device topology
   DeviceTopology &dt = P->dt;
-  if ((st = upload(&dt.cells, t.cells))) return st;
-  if ((st = upload(&dt.gd, t.gd))) return st;
-  if (family == FFG_TETRA_NEDELEC) {
+  if (!on_device) {
+    if ((st = upload(&dt.cells, t.cells))) return st;
+    if ((st = upload(&dt.gd, t.gd))) return st;
     if ((st = upload(&dt.edge_sign, t.edge_sign))) return st;
     if ((st = upload(&dt.face_perm, t.face_perm))) return st;
     if (!P->tab.face_blocks.empty() && (st = upload(&dt.face_blocks, P->tab.face_blocks))) return st;
+    if ((st = upload(&dt.free_index, t.free_index))) return st;
+    if ((st = upload(&dt.inc_ptr, t.inc_ptr))) return st;
+    if ((st = upload(&dt.inc_cell, t.inc_cell))) return st;
+    if ((st = upload(&dt.inc_local, t.inc_local))) return st;
+    if ((st = upload(&dt.slot, t.slot))) return st;
+    // constrained CSC pattern (assembly) and the solver's SELL layout
+    if ((st = upload(&P->csc_col_ptr, t.col_ptr))) return st;
+    if ((st = upload(&P->csc_row, t.row_idx))) return st;
+    build_sell(t.col_ptr, t.row_idx, kSellSigma, P->hsell);
+    if ((st = upload_sell(P->hsell, grid, P->S))) return st;
   }
-  if ((st = upload(&dt.free_index, t.free_index))) return st;
-  if ((st = upload(&dt.inc_ptr, t.inc_ptr))) return st;
-  if ((st = upload(&dt.inc_cell, t.inc_cell))) return st;
-  if ((st = upload(&dt.inc_local, t.inc_local))) return st;
-  if ((st = upload(&dt.slot, t.slot))) return st;
   if (!P->tab.ref.empty() && (st = upload(&dt.ref, P->tab.ref))) return st;
   if (!P->tab.load_basis.empty() && (st = upload(&dt.load_basis, P->tab.load_basis))) return st;
-  // constrained CSC pattern (assembly) and the solver's SELL layout
-  if ((st = upload(&P->csc_col_ptr, t.col_ptr))) return st;
-  if ((st = upload(&P->csc_row, t.row_idx))) return st;
-  int grid = 0;
-  if ((st = pcg_grid_size(&grid))) return st;
-  build_sell(t.col_ptr, t.row_idx, kSellSigma, P->hsell);
-  if ((st = upload_sell(P->hsell, grid, P->S))) return st;
   const int64_t nfree = t.n_free();
   // per-step buffers
   const size_t nc = (size_t)n_cells;

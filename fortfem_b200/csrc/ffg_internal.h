@@ -56,6 +56,8 @@ struct Topology {
 // Build the DoF numbering of a family (first-appearance order of the
 // reference).  Returns FFG_OK or FFG_INVALID_INPUT.
 int build_dofs(Topology &t, std::string &msg);
+// Cell vertices in range and distinct.
+bool validate_cells(const Topology &t, std::string &msg);
 // Constrained set: boundary_mode FFG_BOUNDARY_NONE / _ALL / _MASK.
 int build_constraints(Topology &t, int boundary_mode, const uint8_t *mask, std::string &msg);
 // Free numbering, CSC pattern of the free x free block, incidence lists and slots.
@@ -191,6 +193,14 @@ struct DeviceTopology {
   double *load_basis = nullptr;
   double *face_blocks = nullptr;
 };
+
+// Lagrange / P1 topology built on the device (topology_gpu.cu): the arrays of
+// build_dofs + build_constraints + build_pattern + build_sell, equal entry for
+// entry, written straight into the device structures; the host Topology gets
+// gd, constrained, free_dofs, col_ptr, row_idx, n_dofs and max_column.
+int build_topology_device(Topology &t, int boundary_mode, const uint8_t *mask, int grid,
+                          DeviceTopology &dt, int64_t **csc_col_ptr, int **csc_row,
+                          DeviceSell &S, std::string &msg);
 
 struct AssemblyInputs {
   const double *vertices = nullptr;  // device

@@ -186,6 +186,8 @@ int build_nedelec(Topology &t, std::string &msg) {
 
 }  // namespace
 
+bool validate_cells(const Topology &t, std::string &msg) { return check_cells(t, msg); }
+
 int build_dofs(Topology &t, std::string &msg) {
   if (!check_cells(t, msg)) return FFG_INVALID_INPUT;
   switch (t.family) {
