@@ -74,6 +74,11 @@ SIGNATURES = {
     "ffg_unit_square_mesh": (None, [i32, vp, vp, pi32]),
     "ffg_assemble_tetra_lagrange_stiffness_csc": (
         None, [i32, vp, i32, vp, i32, i32, i32, f64, f64, vp, vp, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_assemble_tetra_lagrange_stiffness_csc_jvp": (
+        None, [i32, vp, i32, vp, i32, i32, i32, f64, f64, vp, f64, f64, i64, pi32, pi64, vp, vp,
+               vp, pi32]),
+    "ffg_assemble_tetra_lagrange_stiffness_csc_vjp": (
+        None, [i32, vp, i32, vp, i32, i32, i32, f64, f64, i64, vp, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_lagrange_scalar_load_samples": (
         None, [i32, vp, i32, vp, i32, i32, i32, vp, i32, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curl_mass_csc": (

@@ -200,6 +200,49 @@ def assemble_tetra_lagrange_stiffness_csc(mesh_vertices, tetrahedra, degree, qua
                      "Tetrahedral H1 sparse assembly failed")
 
 
+def assemble_tetra_lagrange_stiffness_csc_jvp(mesh_vertices, tetrahedra, degree, quadrature_degree,
+                                              stiffness_coefficient, mass_coefficient,
+                                              mesh_vertices_dot, stiffness_coefficient_dot,
+                                              mass_coefficient_dot, rule=K.FFG_RULE_DUFFY):
+    """assemble_tetra_lagrange_stiffness_csc_jvp
+    (src/assembly/assembly_tetra_lagrange_arbitrary_order_3d.f90:336-391): the
+    tangent of the stiffness + mass CSC along (mesh_vertices_dot,
+    stiffness_coefficient_dot, mass_coefficient_dot), on the primal pattern.
+    Returns (CscMatrix, Status)."""
+    where = "Tetrahedral H1 JVP assembly failed"
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    vd = _f64(mesh_vertices_dot)
+    if vd.size != v.size:
+        return None, Status.of(K.FFG_INVALID_INPUT, where)
+    vd = vd.reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    args = [len(v), _ptr(v), len(t), _ptr(t), int(degree), int(rule), int(quadrature_degree),
+            float(stiffness_coefficient), float(mass_coefficient), _ptr(vd),
+            float(stiffness_coefficient_dot), float(mass_coefficient_dot)]
+    return _csc_call("ffg_assemble_tetra_lagrange_stiffness_csc_jvp", args, where)
+
+
+def assemble_tetra_lagrange_stiffness_csc_vjp(mesh_vertices, tetrahedra, degree, quadrature_degree,
+                                              stiffness_coefficient, mass_coefficient,
+                                              matrix_values_bar, rule=K.FFG_RULE_DUFFY):
+    """assemble_tetra_lagrange_stiffness_csc_vjp (same file :393-471).
+    matrix_values_bar: one cotangent per entry of the primal CSC.  Returns
+    (mesh_vertices_bar (n_vertices, 3), stiffness_coefficient_bar,
+    mass_coefficient_bar, Status); the adjoints are zero on failure."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    vb_in = _f64(matrix_values_bar).ravel()
+    vbar = np.zeros_like(v)
+    sb = C.c_double(0.0)
+    mb = C.c_double(0.0)
+    st = C.c_int(0)
+    K.load().ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
+        len(v), _ptr(v), len(t), _ptr(t), int(degree), int(rule), int(quadrature_degree),
+        float(stiffness_coefficient), float(mass_coefficient), C.c_int64(vb_in.size), _ptr(vb_in),
+        _ptr(vbar), C.byref(sb), C.byref(mb), C.byref(st))
+    return vbar, sb.value, mb.value, Status.of(st.value, "Tetrahedral H1 VJP failed")
+
+
 def assemble_tetra_lagrange_scalar_load_samples(mesh_vertices, tetrahedra, degree,
                                                 quadrature_degree, source_values,
                                                 rule=K.FFG_RULE_DUFFY):

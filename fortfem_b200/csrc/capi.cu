@@ -864,6 +864,114 @@ void ffg_assemble_tetra_lagrange_stiffness_csc(int nv, const double *verts, int 
            cell_stiffness, cell_mass, cap, n_dofs, nnz, col_ptr, row_ind, values, status);
 }
 
+void ffg_assemble_tetra_lagrange_stiffness_csc_jvp(
+    int nv, const double *verts, int nt, const int *tets, int degree, int rule, int qdeg,
+    double stiffness, double mass, const double *verts_dot, double stiffness_dot,
+    double mass_dot, int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_ind,
+    double *values_dot, int *status) {
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  if (!verts || !verts_dot) { *status = FFG_INVALID_INPUT; return; }
+  int st = create_problem(FFG_TETRA_LAGRANGE, degree, nv, nt, tets, rule, qdeg, FFG_BOUNDARY_NONE,
+                          nullptr, P, msg);
+  if (st) { *status = st; return; }
+  const Topology &t = P->topo;
+  if (n_dofs) *n_dofs = (int)t.n_dofs;
+  if (nnz) *nnz = t.nnz();
+  if (cap < t.nnz() || !col_ptr || !row_ind || !values_dot) { *status = FFG_CAPACITY; return; }
+  double *vdot = nullptr;
+  const size_t vbytes = sizeof(double) * 3 * (size_t)nv;
+  if ((st = dalloc(&vdot, 3 * (size_t)nv))) { *status = st; return; }
+  if (!P->csc_val && (st = dalloc(&P->csc_val, (size_t)std::max<int64_t>(t.nnz(), 1)))) {
+    cudaFree(vdot);
+    *status = st;
+    return;
+  }
+  AssemblyInputs in;
+  in.vertices = P->in_vertices;
+  int herr = 0;
+  if (cudaMemcpy(P->in_vertices, verts, vbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(vdot, verts_dot, vbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(P->err, 0, sizeof(int)) != cudaSuccess) {
+    st = FFG_CUDA_ERROR;
+  } else if (!(st = launch_lagrange_geometry_jvp(t, P->dt, P->in_vertices, vdot, stiffness, mass,
+                                                 stiffness_dot, mass_dot, P->geo, P->geo_stride,
+                                                 P->err, 0)) &&
+             !(st = launch_columns(t, P->tab, P->dt, in, P->geo, P->geo_stride, nullptr, nullptr,
+                                   P->csc_col_ptr, P->csc_row, nullptr, P->csc_val, P->rhs, 0))) {
+    if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = FFG_CUDA_ERROR;
+    else if (herr)
+      st = herr;
+    else if (cudaMemcpy(values_dot, P->csc_val, sizeof(double) * (size_t)t.nnz(),
+                        cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = FFG_CUDA_ERROR;
+  }
+  cudaFree(vdot);
+  if (st) { *status = st; return; }
+  std::memcpy(col_ptr, t.col_ptr.data(), sizeof(int64_t) * t.col_ptr.size());
+  std::memcpy(row_ind, t.row_idx.data(), sizeof(int) * t.row_idx.size());
+  *status = FFG_OK;
+}
+
+void ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
+    int nv, const double *verts, int nt, const int *tets, int degree, int rule, int qdeg,
+    double stiffness, double mass, int64_t nnz, const double *values_bar, double *verts_bar,
+    double *stiffness_bar, double *mass_bar, int *status) {
+  // outputs start at zero, as the reference's do, whatever the outcome
+  if (verts_bar && nv > 0) std::memset(verts_bar, 0, sizeof(double) * 3 * (size_t)nv);
+  if (stiffness_bar) *stiffness_bar = 0.0;
+  if (mass_bar) *mass_bar = 0.0;
+  if (!verts || !values_bar || !verts_bar || !stiffness_bar || !mass_bar) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  int st = create_problem(FFG_TETRA_LAGRANGE, degree, nv, nt, tets, rule, qdeg, FFG_BOUNDARY_NONE,
+                          nullptr, P, msg);
+  if (st) { *status = st; return; }
+  const Topology &t = P->topo;
+  if (nnz != t.nnz()) { *status = FFG_INVALID_INPUT; return; }
+  double *vb = nullptr, *dvbar = nullptr, *coef = nullptr;
+  const size_t vcount = 3 * (size_t)nv;
+  if ((st = dalloc(&vb, (size_t)std::max<int64_t>(nnz, 1))) || (st = dalloc(&dvbar, vcount)) ||
+      (st = dalloc(&coef, 2))) {
+    for (double *p : {vb, dvbar, coef})
+      if (p) cudaFree(p);
+    *status = st;
+    return;
+  }
+  double hc[2] = {0.0, 0.0};
+  int herr = 0;
+  if (cudaMemcpy(P->in_vertices, verts, sizeof(double) * vcount, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(vb, values_bar, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemset(P->err, 0, sizeof(int)) != cudaSuccess) {
+    st = FFG_CUDA_ERROR;
+  } else if (!(st = lagrange_vjp(t, P->dt, P->csc_col_ptr, P->csc_row, P->in_vertices, vb,
+                                 stiffness, mass, dvbar, coef, P->err, 0))) {
+    if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = FFG_CUDA_ERROR;
+    else if (herr)
+      st = herr;
+    else if (cudaMemcpy(verts_bar, dvbar, sizeof(double) * vcount, cudaMemcpyDeviceToHost) !=
+                 cudaSuccess ||
+             cudaMemcpy(hc, coef, sizeof(hc), cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = FFG_CUDA_ERROR;
+  }
+  for (double *p : {vb, dvbar, coef}) cudaFree(p);
+  if (st) {
+    std::memset(verts_bar, 0, sizeof(double) * vcount);
+    *status = st;
+    return;
+  }
+  *stiffness_bar = hc[0];
+  *mass_bar = hc[1];
+  *status = FFG_OK;
+}
+
 void ffg_assemble_tetra_lagrange_scalar_load_samples(int nv, const double *verts, int nt,
                                                      const int *tets, int degree, int rule,
                                                      int qdeg, const double *samples, int n_dofs,

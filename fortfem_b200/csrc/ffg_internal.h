@@ -229,4 +229,18 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    cudaStream_t s);
 int geo_stride_for(const Topology &t, const ElementTables &tab);
 
+// Forward / reverse mode of the Lagrange stiffness + mass assembly (kernels_ad.cu).
+// The JVP writes the tangent of the seven contraction weights of every cell
+// into `geo` (load samples zero); launch_columns then yields the tangent CSC
+// values.  The VJP reads the CSC cotangent values_bar (device, on the pattern
+// col_ptr/row_idx) and writes the vertex adjoints (3 n_vertices) and the
+// stiffness and mass adjoints (2), all device arrays; it returns once done.
+int launch_lagrange_geometry_jvp(const Topology &t, const DeviceTopology &dt,
+                                 const double *vertices, const double *vertices_dot, double ca,
+                                 double cb, double ca_dot, double cb_dot, double *geo, int stride,
+                                 int *err, cudaStream_t s);
+int lagrange_vjp(const Topology &t, const DeviceTopology &dt, const int64_t *col_ptr,
+                 const int *row_idx, const double *vertices, const double *values_bar, double ca,
+                 double cb, double *vertices_bar, double *coef_bar, int *err, cudaStream_t s);
+
 }  // namespace ffg

@@ -127,6 +127,27 @@ void ffg_assemble_tetra_lagrange_stiffness_csc(
     const double *cell_stiffness, const double *cell_mass, int64_t nnz_capacity, int *n_dofs,
     int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values, int *status);
 
+/* assemble_tetra_lagrange_stiffness_csc_jvp, same file :336-391: the tangent
+ * of the stiffness + mass CSC along (vertices_dot, stiffness_dot, mass_dot),
+ * on the primal matrix's pattern (col_ptr/row_ind as the primal call gives).
+ * vertices_dot has the shape of vertices.  Capacity as the primal call. */
+void ffg_assemble_tetra_lagrange_stiffness_csc_jvp(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int degree,
+    int rule, int quadrature_degree, double stiffness_coefficient, double mass_coefficient,
+    const double *vertices_dot, double stiffness_coefficient_dot, double mass_coefficient_dot,
+    int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_ind,
+    double *values_dot, int *status);
+
+/* assemble_tetra_lagrange_stiffness_csc_vjp, same file :393-471: the adjoints
+ * of the vertices (3*n_vertices), the stiffness and the mass coefficient for
+ * a cotangent values_bar on the primal CSC pattern (nnz entries, nnz equal to
+ * the primal matrix's, else FFG_INVALID_INPUT).  Outputs are zeroed first. */
+void ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int degree,
+    int rule, int quadrature_degree, double stiffness_coefficient, double mass_coefficient,
+    int64_t nnz, const double *values_bar, double *vertices_bar,
+    double *stiffness_coefficient_bar, double *mass_coefficient_bar, int *status);
+
 /* assemble_tetra_lagrange_scalar_load_samples, same file :473-528.
  * source_values holds n_q values per cell (n_q of the rule), cell-major. */
 void ffg_assemble_tetra_lagrange_scalar_load_samples(

@@ -53,6 +53,22 @@ int or_lagrange_csc(int n_vertices, const double *vertices, int n_tets, const in
                     const double *cell_stiffness, const double *cell_mass,
                     int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
                     int *row_idx, double *values);
+/* forward (JVP) and reverse (VJP) mode of the element and the CSC assembly */
+int or_lagrange_element_jvp(const double *vertices, int degree, int rule, int quadrature_degree,
+                            double stiffness, double mass, const double *vertices_dot,
+                            double stiffness_dot, double mass_dot, double *matrix_dot);
+int or_lagrange_element_vjp(const double *vertices, int degree, int rule, int quadrature_degree,
+                            double stiffness, double mass, const double *matrix_bar,
+                            double *vertices_bar, double *stiffness_bar, double *mass_bar);
+int or_lagrange_csc_jvp(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                        int degree, int rule, int quadrature_degree, double stiffness, double mass,
+                        const double *vertices_dot, double stiffness_dot, double mass_dot,
+                        int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+                        int *row_idx, double *values_dot);
+int or_lagrange_csc_vjp(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                        int degree, int rule, int quadrature_degree, double stiffness, double mass,
+                        int64_t nnz, const double *values_bar, double *vertices_bar,
+                        double *stiffness_bar, double *mass_bar);
 int or_lagrange_load_samples(int n_vertices, const double *vertices, int n_tets, const int *tets,
                              int degree, int rule, int quadrature_degree,
                              const double *source_values /* n_q x T */, double *rhs);

@@ -193,6 +193,65 @@ def lagrange_csc(vertices, tets, p, rule=0, q=None, stiffness=1.0, mass=0.0, cel
     return n, cp, ri, v
 
 
+def lagrange_element_jvp(vertices, p, vertices_dot, stiffness, mass, stiffness_dot, mass_dot,
+                         rule=0, q=None):
+    if q is None:
+        q = 2 * p + 4
+    nb = lagrange_dof_count(p)
+    m = np.zeros(nb * nb)
+    _check(_call("or_lagrange_element_jvp", _arr(vertices, np.float64), p, rule, q,
+                 float(stiffness), float(mass), _arr(vertices_dot, np.float64),
+                 float(stiffness_dot), float(mass_dot), m), "lagrange_element_jvp")
+    return m.reshape(nb, nb, order="F")
+
+
+def lagrange_element_vjp(vertices, p, matrix_bar, stiffness, mass, rule=0, q=None):
+    """(vertices_bar (4,3), stiffness_bar, mass_bar) of one element."""
+    if q is None:
+        q = 2 * p + 4
+    vb = np.zeros(12)
+    sb = C.c_double(0.0); mb = C.c_double(0.0)
+    _check(_call("or_lagrange_element_vjp", _arr(vertices, np.float64), p, rule, q,
+                 float(stiffness), float(mass),
+                 _arr(np.asarray(matrix_bar).ravel(order="F"), np.float64), vb, C.byref(sb),
+                 C.byref(mb)), "lagrange_element_vjp")
+    return vb.reshape(4, 3), sb.value, mb.value
+
+
+def lagrange_csc_jvp(vertices, tets, p, vertices_dot, stiffness, mass, stiffness_dot, mass_dot,
+                     rule=0, q=None):
+    """(n, col_ptr, row_idx, values_dot) of assemble_tetra_lagrange_stiffness_csc_jvp."""
+    if q is None:
+        q = 2 * p + 4
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    nnz = int(_call("or_lagrange_csc_nnz", p, len(tets), tets, restype=C.c_int64))
+    if nnz < 0:
+        raise OracleError("lagrange_csc_nnz failed")
+    nd = C.c_int(0); nz = C.c_int64(0)
+    _, n = lagrange_dof_map(p, tets)
+    cp = np.zeros(n + 1, np.int64); ri = np.zeros(nnz, np.int32); v = np.zeros(nnz)
+    _check(_call("or_lagrange_csc_jvp", len(vertices), vertices, len(tets), tets, p, rule, q,
+                 float(stiffness), float(mass), _arr(vertices_dot, np.float64),
+                 float(stiffness_dot), float(mass_dot), C.c_int64(nnz), C.byref(nd), C.byref(nz),
+                 cp, ri, v), "lagrange_csc_jvp")
+    return n, cp, ri, v
+
+
+def lagrange_csc_vjp(vertices, tets, p, values_bar, stiffness, mass, rule=0, q=None):
+    """(vertices_bar (n_vertices,3), stiffness_bar, mass_bar) of
+    assemble_tetra_lagrange_stiffness_csc_vjp."""
+    if q is None:
+        q = 2 * p + 4
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    values_bar = _arr(values_bar, np.float64)
+    vb = np.zeros(vertices.size)
+    sb = C.c_double(0.0); mb = C.c_double(0.0)
+    _check(_call("or_lagrange_csc_vjp", len(vertices), vertices, len(tets), tets, p, rule, q,
+                 float(stiffness), float(mass), C.c_int64(values_bar.size), values_bar, vb,
+                 C.byref(sb), C.byref(mb)), "lagrange_csc_vjp")
+    return vb.reshape(-1, 3), sb.value, mb.value
+
+
 def lagrange_quadrature_points(vertices, tets, rule=0, q=0):
     vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
     nq = 4 if rule == 1 else _call("or_tetra_duffy_count", q)

@@ -610,6 +610,224 @@ int or_lagrange_csc(int nv, const double *verts, int nt, const int *tets, int p,
                              row_idx, values);
 }
 
+// ------------------------------------------------- forward / reverse mode
+// fortnum det3_jvp / inv3_jvp / det3_vjp / inv3_vjp (not vendored) restated
+// from their definitions: d(det J) = det tr(J^-1 dJ), d(J^-1) = -J^-1 dJ J^-1,
+// and the adjoints Jbar += detbar det J^-T, Jbar = -J^-T Jibar J^-T.
+namespace {
+void mat3_mul(const double *A, const double *B, double *C) {  // column-major C = A B
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += A[r + 3 * k] * B[k + 3 * c];
+      C[r + 3 * c] = s;
+    }
+}
+}  // namespace
+
+// assemble_tetra_lagrange_stiffness_element_jvp,
+// assembly_tetra_lagrange_arbitrary_order_3d.f90:107-180: the same point loop
+// as the primal element, differentiated term by term.
+int or_lagrange_element_jvp(const double *v, int p, int rule, int q, double stiff, double mass,
+                            const double *vdot, double stiff_dot, double mass_dot, double *Md) {
+  if (p < 1 || p > 4) return 1;
+  double J[9], Jd[9], Ji[9], Jid[9], T[9];
+  tetra_jacobian(v, J);
+  tetra_jacobian(vdot, Jd);
+  const double det = det3(J);
+  if (!valid_jacobian(J, det)) return 1;
+  inv3(J, det, Ji);
+  mat3_mul(Ji, Jd, T);
+  const double det_dot = det * (T[0] + T[4] + T[8]);
+  double U[9];
+  mat3_mul(T, Ji, U);
+  for (int i = 0; i < 9; ++i) Jid[i] = -U[i];
+  Rule R;
+  if (!make_rule(rule, q, R)) return 1;
+  const int nb = or_lagrange_dof_count(p);
+  std::vector<double> val(nb), grad(3 * nb), pg(3 * nb), pgd(3 * nb);
+  std::fill(Md, Md + (size_t)nb * nb, 0.0);
+  for (size_t pt = 0; pt < R.w.size(); ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    if (or_lagrange_evaluate(p, P, val.data(), grad.data())) return 1;
+    for (int d = 0; d < nb; ++d)
+      for (int i = 0; i < 3; ++i) {
+        double s = 0.0, t = 0.0;
+        for (int k = 0; k < 3; ++k) {
+          s += Ji[k + 3 * i] * grad[3 * d + k];
+          t += Jid[k + 3 * i] * grad[3 * d + k];
+        }
+        pg[3 * d + i] = s;
+        pgd[3 * d + i] = t;
+      }
+    const double w = R.w[pt];
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row) {
+        double ge = 0.0, gd = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          ge += pg[3 * row + i] * pg[3 * col + i];
+          gd += pgd[3 * row + i] * pg[3 * col + i] + pg[3 * row + i] * pgd[3 * col + i];
+        }
+        const double me = val[row] * val[col];
+        Md[row + (size_t)nb * col] +=
+            w * (det_dot * (stiff * ge + mass * me) +
+                 det * (stiff_dot * ge + stiff * gd + mass_dot * me));
+      }
+  }
+  return 0;
+}
+
+// assemble_tetra_lagrange_stiffness_element_vjp, same file :182-274.
+int or_lagrange_element_vjp(const double *v, int p, int rule, int q, double stiff, double mass,
+                            const double *Mb, double *vbar, double *stiff_bar, double *mass_bar) {
+  for (int i = 0; i < 12; ++i) vbar[i] = 0.0;
+  *stiff_bar = 0.0;
+  *mass_bar = 0.0;
+  if (p < 1 || p > 4) return 1;
+  const int nb = or_lagrange_dof_count(p);
+  double J[9], Ji[9];
+  tetra_jacobian(v, J);
+  const double det = det3(J);
+  if (!valid_jacobian(J, det)) return 1;
+  inv3(J, det, Ji);
+  Rule R;
+  if (!make_rule(rule, q, R)) return 1;
+  std::vector<double> val(nb), grad(3 * nb), pg(3 * nb), pgb(3 * nb);
+  double det_bar = 0.0, Jib[9] = {0};
+  for (size_t pt = 0; pt < R.w.size(); ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    if (or_lagrange_evaluate(p, P, val.data(), grad.data())) return 1;
+    for (int d = 0; d < nb; ++d)
+      for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s += Ji[k + 3 * i] * grad[3 * d + k];
+        pg[3 * d + i] = s;
+      }
+    std::fill(pgb.begin(), pgb.end(), 0.0);
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row) {
+        const double seed = R.w[pt] * Mb[row + (size_t)nb * col];
+        double ge = 0.0;
+        for (int i = 0; i < 3; ++i) ge += pg[3 * row + i] * pg[3 * col + i];
+        const double me = val[row] * val[col];
+        det_bar += seed * (stiff * ge + mass * me);
+        *stiff_bar += seed * det * ge;
+        *mass_bar += seed * det * me;
+        for (int i = 0; i < 3; ++i) {
+          pgb[3 * row + i] += seed * det * stiff * pg[3 * col + i];
+          pgb[3 * col + i] += seed * det * stiff * pg[3 * row + i];
+        }
+      }
+    // inverse_jacobian_bar += matmul(gradients, transpose(physical_gradients_bar))
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) {
+        double s = 0.0;
+        for (int d = 0; d < nb; ++d) s += grad[3 * d + r] * pgb[3 * d + c];
+        Jib[r + 3 * c] += s;
+      }
+  }
+  // Jbar = -J^-T Jib J^-T + det_bar det J^-T
+  double JiT[9], A[9], B[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) JiT[r + 3 * c] = Ji[c + 3 * r];
+  mat3_mul(JiT, Jib, A);
+  mat3_mul(A, JiT, B);
+  double Jb[9];
+  for (int i = 0; i < 9; ++i) Jb[i] = -B[i] + det_bar * det * JiT[i];
+  // tetra_jacobian_vjp: J(:,c) = v(:,c+1) - v(:,0)
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      vbar[r + 3 * (c + 1)] += Jb[r + 3 * c];
+      vbar[r] -= Jb[r + 3 * c];
+    }
+  return 0;
+}
+
+// assemble_tetra_lagrange_stiffness_csc_jvp, same file :336-391: element
+// tangents scattered through csc_from_triplet, so the pattern is the primal's.
+int or_lagrange_csc_jvp(int nv, const double *verts, int nt, const int *tets, int p, int rule,
+                        int q, double stiff, double mass, const double *vdot, double stiff_dot,
+                        double mass_dot, int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+                        int *row_idx, double *values) {
+  if (nt < 1) return 1;
+  for (int64_t i = 0; i < 4LL * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int nb = or_lagrange_dof_count(p);
+  std::vector<int> gd((size_t)nb * nt);
+  int ng = 0;
+  if (or_lagrange_dof_map(p, nt, tets, gd.data(), &ng)) return 1;
+  *n_dofs = ng;
+  const int64_t ntrip = (int64_t)nt * nb * nb;
+  std::vector<int> rows(ntrip), cols(ntrip);
+  std::vector<double> tv(ntrip), M((size_t)nb * nb);
+  int64_t e = 0;
+  for (int c = 0; c < nt; ++c) {
+    double v[12], vd[12];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) {
+        v[3 * n + d] = verts[3 * tets[4 * c + n] + d];
+        vd[3 * n + d] = vdot[3 * tets[4 * c + n] + d];
+      }
+    if (or_lagrange_element_jvp(v, p, rule, q, stiff, mass, vd, stiff_dot, mass_dot, M.data()))
+      return 1;
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row, ++e) {
+        rows[e] = gd[(size_t)nb * c + row];
+        cols[e] = gd[(size_t)nb * c + col];
+        tv[e] = M[row + (size_t)nb * col];
+      }
+  }
+  return or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tv.data(), cap, nnz, col_ptr,
+                             row_idx, values);
+}
+
+// assemble_tetra_lagrange_stiffness_csc_vjp, same file :393-471, with
+// csc_value_bar_at (:836-851) reading each element entry's cotangent from the
+// merged pattern; vertex and coefficient adjoints accumulate in cell order.
+int or_lagrange_csc_vjp(int nv, const double *verts, int nt, const int *tets, int p, int rule,
+                        int q, double stiff, double mass, int64_t nnz, const double *values_bar,
+                        double *verts_bar, double *stiff_bar, double *mass_bar) {
+  for (int64_t i = 0; i < 3LL * nv; ++i) verts_bar[i] = 0.0;
+  *stiff_bar = 0.0;
+  *mass_bar = 0.0;
+  if (nt < 1) return 1;
+  for (int64_t i = 0; i < 4LL * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int64_t pat = or_lagrange_csc_nnz(p, nt, tets);
+  if (pat < 0 || pat != nnz) return 1;
+  int ng = 0, nd = 0;
+  const int nb = or_lagrange_dof_count(p);
+  std::vector<int> gd((size_t)nb * nt);
+  if (or_lagrange_dof_map(p, nt, tets, gd.data(), &ng)) return 1;
+  std::vector<int64_t> cp(ng + 1);
+  std::vector<int> ri(nnz);
+  std::vector<double> vals(nnz);
+  int64_t got = 0;
+  if (or_lagrange_csc(nv, verts, nt, tets, p, rule, q, stiff, mass, nullptr, nullptr, nnz, &nd,
+                      &got, cp.data(), ri.data(), vals.data()))
+    return 1;
+  std::vector<double> Mb((size_t)nb * nb);
+  for (int c = 0; c < nt; ++c) {
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row) {
+        const int gr = gd[(size_t)nb * c + row], gc = gd[(size_t)nb * c + col];
+        double b = 0.0;
+        for (int64_t k = cp[gc]; k < cp[gc + 1]; ++k)
+          if (ri[k] == gr) { b = values_bar[k]; break; }
+        Mb[row + (size_t)nb * col] = b;
+      }
+    double v[12], vb[12], sb = 0.0, mb = 0.0;
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * c + n] + d];
+    if (or_lagrange_element_vjp(v, p, rule, q, stiff, mass, Mb.data(), vb, &sb, &mb)) return 1;
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) verts_bar[3 * tets[4 * c + n] + d] += vb[3 * n + d];
+    *stiff_bar += sb;
+    *mass_bar += mb;
+  }
+  return 0;
+}
+
 // assemble_tetra_lagrange_scalar_load_samples,
 // assembly_tetra_lagrange_arbitrary_order_3d.f90:473-528.  rhs has n_dofs entries.
 int or_lagrange_load_samples(int nv, const double *verts, int nt, const int *tets, int p, int rule,

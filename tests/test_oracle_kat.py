@@ -317,3 +317,56 @@ def test_emitted_tables_are_rounded_exact_values():
         Cm = coefficients(k)
         n = len(Cm)
         assert vals == [float(Cm[r][c]) for c in range(n) for r in range(n)]
+
+
+# ---------------------------------------------------------------- JVP / VJP
+# test/test_tetra_lagrange_element_ad.f90:9-79 and
+# test/test_tetra_lagrange_stiffness_csc_ad.f90:10-91: central differences of
+# complete reassembly (step 2e-7, relative 5e-8) and the adjoint identity
+# <Kbar, Kdot> = <vbar, vdot> + kbar kdot + mbar mdot (2e-10 / 3e-10).
+AD_STEP = 2.0e-7
+AD_COEF = (1.7, 0.8, 0.13, -0.09)  # stiffness, mass and their tangents
+AD_VDOT = [[0.01, -0.02, 0.015], [-0.03, 0.01, 0.02], [0.025, -0.015, 0.005],
+           [-0.01, 0.03, -0.02], [0.02, -0.01, 0.025]]
+
+
+def test_lagrange_element_jvp_vjp_kat():
+    v = np.array([[0.1, -0.2, 0.3], [1.3, -0.1, 0.25], [0.25, 0.9, 0.35], [0.0, 0.1, 1.4]])
+    vd = np.array(AD_VDOT[:4])
+    k, m, kd, md = AD_COEF
+    p, q, h = 2, 6, AD_STEP
+    kdot = oracle.lagrange_element_jvp(v, p, vd, k, m, kd, md, q=q)
+    plus = oracle.lagrange_element(v + h * vd, p, q=q, stiffness=k + h * kd, mass=m + h * md)
+    minus = oracle.lagrange_element(v - h * vd, p, q=q, stiffness=k - h * kd, mass=m - h * md)
+    err = np.abs(kdot - (plus - minus) / (2 * h)).max() / max(1.0, np.abs(kdot).max())
+    assert err < 5e-8
+    nb = kdot.shape[0]
+    r, c = np.meshgrid(np.arange(1, nb + 1), np.arange(1, nb + 1), indexing="ij")
+    kbar = 0.002 * r - 0.0015 * c
+    vbar, sbar, mbar = oracle.lagrange_element_vjp(v, p, kbar, k, m, q=q)
+    lhs = np.sum(kbar * kdot)
+    rhs = np.sum(vbar * vd) + sbar * kd + mbar * md
+    assert abs(lhs - rhs) < 2e-10 * max(1.0, abs(lhs), abs(rhs))
+
+
+def test_lagrange_csc_jvp_vjp_kat():
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1]], float)
+    t = np.array([[0, 1, 2, 3], [1, 2, 3, 4]], np.int32)
+    vd = np.array(AD_VDOT)
+    k, m, kd, md = AD_COEF
+    p, q, h = 2, 6, AD_STEP
+    n, cp, ri, vdot = oracle.lagrange_csc_jvp(v, t, p, vd, k, m, kd, md, q=q)
+    n0, cp0, ri0, _ = oracle.lagrange_csc(v, t, p, q=q, stiffness=k, mass=m)
+    assert n == n0 and np.array_equal(cp, cp0) and np.array_equal(ri, ri0)
+    _, _, _, plus = oracle.lagrange_csc(v + h * vd, t, p, q=q, stiffness=k + h * kd,
+                                        mass=m + h * md)
+    _, _, _, minus = oracle.lagrange_csc(v - h * vd, t, p, q=q, stiffness=k - h * kd,
+                                         mass=m - h * md)
+    err = np.abs(vdot - (plus - minus) / (2 * h)).max() / max(1.0, np.abs(vdot).max())
+    assert err < 5e-8
+    e = np.arange(1, len(vdot) + 1, dtype=float)
+    vbar_in = 0.003 * e - 0.00001 * e ** 2
+    vbar, sbar, mbar = oracle.lagrange_csc_vjp(v, t, p, vbar_in, k, m, q=q)
+    lhs = vbar_in @ vdot
+    rhs = np.sum(vbar * vd) + sbar * kd + mbar * md
+    assert abs(lhs - rhs) < 3e-10 * max(1.0, abs(lhs), abs(rhs))
