@@ -11,6 +11,7 @@ from .api import (CscMatrix, FortfemError, Problem, SolverOptions, SolverStats, 
                   assemble_scalar_p1_csc, assemble_tetra_lagrange_scalar_load_samples,
                   assemble_tetra_lagrange_stiffness_csc, assemble_tetra_lagrange_stiffness_csc_jvp,
                   assemble_tetra_lagrange_stiffness_csc_vjp, assemble_tetra_nedelec_curl_mass_csc,
+                  assemble_tetra_nedelec_curl_mass_csc_jvp, assemble_tetra_nedelec_curl_mass_csc_vjp,
                   assemble_tetra_nedelec_vector_load_samples, build_topology,
                   generate_structured_tetra_box_mesh, solve_scalar_p1, solve_sparse,
                   solve_tetra_lagrange_diffusion_reaction, solve_tetra_lagrange_poisson,

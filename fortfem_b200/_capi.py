@@ -83,6 +83,10 @@ SIGNATURES = {
         None, [i32, vp, i32, vp, i32, i32, i32, vp, i32, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curl_mass_csc": (
         None, [i32, vp, i32, vp, i32, f64, f64, vp, vp, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_assemble_tetra_nedelec_curl_mass_csc_jvp": (
+        None, [i32, vp, i32, vp, i32, f64, f64, vp, f64, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_assemble_tetra_nedelec_curl_mass_csc_vjp": (
+        None, [i32, vp, i32, vp, i32, f64, f64, i64, vp, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_vector_load_samples": (
         None, [i32, vp, i32, vp, i32, vp, i32, vp, pi32]),
     "ffg_assemble_scalar_p1_csc": (

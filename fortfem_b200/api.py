@@ -281,6 +281,45 @@ def assemble_tetra_nedelec_curl_mass_csc(mesh_vertices, tetrahedra, curl_coeffic
                      "Tetrahedral Nedelec assembly failed")
 
 
+def assemble_tetra_nedelec_curl_mass_csc_jvp(mesh_vertices, tetrahedra, order, curl_coefficient,
+                                             mass_coefficient, mesh_vertices_dot,
+                                             curl_coefficient_dot, mass_coefficient_dot):
+    """assemble_tetra_nedelec_curl_mass_csc_jvp
+    (src/assembly/assembly_tetra_nedelec_3d.f90:2114-2181): the tangent of the
+    curl + mass CSC along (mesh_vertices_dot, curl_coefficient_dot,
+    mass_coefficient_dot), on the primal pattern.  Returns (CscMatrix, Status)."""
+    where = "Tetrahedral Nedelec curl-mass JVP assembly failed"
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    vd = _f64(mesh_vertices_dot)
+    if vd.size != v.size:
+        return None, Status.of(K.FFG_INVALID_INPUT, where)
+    vd = vd.reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    args = [len(v), _ptr(v), len(t), _ptr(t), int(order), float(curl_coefficient),
+            float(mass_coefficient), _ptr(vd), float(curl_coefficient_dot),
+            float(mass_coefficient_dot)]
+    return _csc_call("ffg_assemble_tetra_nedelec_curl_mass_csc_jvp", args, where)
+
+
+def assemble_tetra_nedelec_curl_mass_csc_vjp(mesh_vertices, tetrahedra, order, curl_coefficient,
+                                             mass_coefficient, matrix_values_bar):
+    """assemble_tetra_nedelec_curl_mass_csc_vjp (same file :2183-2287).
+    Returns (mesh_vertices_bar (n_vertices, 3), curl_coefficient_bar,
+    mass_coefficient_bar, Status); the adjoints are zero on failure."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    vb_in = _f64(matrix_values_bar).ravel()
+    vbar = np.zeros_like(v)
+    cb = C.c_double(0.0)
+    mb = C.c_double(0.0)
+    st = C.c_int(0)
+    K.load().ffg_assemble_tetra_nedelec_curl_mass_csc_vjp(
+        len(v), _ptr(v), len(t), _ptr(t), int(order), float(curl_coefficient),
+        float(mass_coefficient), C.c_int64(vb_in.size), _ptr(vb_in), _ptr(vbar), C.byref(cb),
+        C.byref(mb), C.byref(st))
+    return vbar, cb.value, mb.value, Status.of(st.value, "Tetrahedral Nedelec curl-mass VJP failed")
+
+
 def assemble_tetra_nedelec_vector_load_samples(mesh_vertices, tetrahedra, order, source_values):
     """assemble_tetra_nedelec_vector_load_samples (assembly_tetra_nedelec_3d.f90:128-185).
     source_values: (T, n_q, 3) at the order's load points.  Returns (rhs, Status)."""

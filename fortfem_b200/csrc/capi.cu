@@ -864,16 +864,18 @@ void ffg_assemble_tetra_lagrange_stiffness_csc(int nv, const double *verts, int 
            cell_stiffness, cell_mass, cap, n_dofs, nnz, col_ptr, row_ind, values, status);
 }
 
-void ffg_assemble_tetra_lagrange_stiffness_csc_jvp(
-    int nv, const double *verts, int nt, const int *tets, int degree, int rule, int qdeg,
-    double stiffness, double mass, const double *verts_dot, double stiffness_dot,
-    double mass_dot, int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_ind,
-    double *values_dot, int *status) {
+// Tangent (JVP) of a stiffness/curl + mass CSC on the primal pattern: the
+// element kernels run on the tangent weights, the column gather is the primal's.
+static void tangent_csc(int family, int degree, int nv, const double *verts, int nt,
+                        const int *cells, int rule, int qdeg, double ca, double cb,
+                        const double *verts_dot, double ca_dot, double cb_dot, int64_t cap,
+                        int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_ind,
+                        double *values_dot, int *status) {
   std::shared_ptr<Problem> P;
   std::string msg;
   if (!verts || !verts_dot) { *status = FFG_INVALID_INPUT; return; }
-  int st = create_problem(FFG_TETRA_LAGRANGE, degree, nv, nt, tets, rule, qdeg, FFG_BOUNDARY_NONE,
-                          nullptr, P, msg);
+  int st = create_problem(family, degree, nv, nt, cells, rule, qdeg, FFG_BOUNDARY_NONE, nullptr, P,
+                          msg);
   if (st) { *status = st; return; }
   const Topology &t = P->topo;
   if (n_dofs) *n_dofs = (int)t.n_dofs;
@@ -889,23 +891,33 @@ void ffg_assemble_tetra_lagrange_stiffness_csc_jvp(
   }
   AssemblyInputs in;
   in.vertices = P->in_vertices;
+  in.coef_a = ca;
+  in.coef_b = cb;
+  in.vertices_dot = vdot;
+  in.coef_a_dot = ca_dot;
+  in.coef_b_dot = cb_dot;
   int herr = 0;
   if (cudaMemcpy(P->in_vertices, verts, vbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(vdot, verts_dot, vbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(P->err, 0, sizeof(int)) != cudaSuccess) {
     st = FFG_CUDA_ERROR;
-  } else if (!(st = launch_lagrange_geometry_jvp(t, P->dt, P->in_vertices, vdot, stiffness, mass,
-                                                 stiffness_dot, mass_dot, P->geo, P->geo_stride,
-                                                 P->err, 0)) &&
-             !(st = launch_columns(t, P->tab, P->dt, in, P->geo, P->geo_stride, nullptr, nullptr,
-                                   P->csc_col_ptr, P->csc_row, nullptr, P->csc_val, P->rhs, 0))) {
-    if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-      st = FFG_CUDA_ERROR;
-    else if (herr)
-      st = herr;
-    else if (cudaMemcpy(values_dot, P->csc_val, sizeof(double) * (size_t)t.nnz(),
-                        cudaMemcpyDeviceToHost) != cudaSuccess)
-      st = FFG_CUDA_ERROR;
+  } else {
+    st = family == FFG_TETRA_LAGRANGE
+             ? launch_lagrange_geometry_jvp(t, P->dt, P->in_vertices, vdot, ca, cb, ca_dot, cb_dot,
+                                            P->geo, P->geo_stride, P->err, 0)
+             : launch_nedelec(t, P->tab, P->dt, in, P->elem, P->cell_rhs, P->err, 0);
+    if (!st)
+      st = launch_columns(t, P->tab, P->dt, in, P->geo, P->geo_stride, P->cell_rhs, P->elem,
+                          P->csc_col_ptr, P->csc_row, nullptr, P->csc_val, P->rhs, 0);
+    if (!st) {
+      if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = FFG_CUDA_ERROR;
+      else if (herr)
+        st = herr;
+      else if (cudaMemcpy(values_dot, P->csc_val, sizeof(double) * (size_t)t.nnz(),
+                          cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = FFG_CUDA_ERROR;
+    }
   }
   cudaFree(vdot);
   if (st) { *status = st; return; }
@@ -914,22 +926,23 @@ void ffg_assemble_tetra_lagrange_stiffness_csc_jvp(
   *status = FFG_OK;
 }
 
-void ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
-    int nv, const double *verts, int nt, const int *tets, int degree, int rule, int qdeg,
-    double stiffness, double mass, int64_t nnz, const double *values_bar, double *verts_bar,
-    double *stiffness_bar, double *mass_bar, int *status) {
-  // outputs start at zero, as the reference's do, whatever the outcome
+// Adjoint (VJP) of a stiffness/curl + mass CSC: vertex and coefficient
+// adjoints of a cotangent on the primal pattern; outputs start at zero.
+static void adjoint_csc(int family, int degree, int nv, const double *verts, int nt,
+                        const int *cells, int rule, int qdeg, double ca, double cb, int64_t nnz,
+                        const double *values_bar, double *verts_bar, double *ca_bar,
+                        double *cb_bar, int *status) {
   if (verts_bar && nv > 0) std::memset(verts_bar, 0, sizeof(double) * 3 * (size_t)nv);
-  if (stiffness_bar) *stiffness_bar = 0.0;
-  if (mass_bar) *mass_bar = 0.0;
-  if (!verts || !values_bar || !verts_bar || !stiffness_bar || !mass_bar) {
+  if (ca_bar) *ca_bar = 0.0;
+  if (cb_bar) *cb_bar = 0.0;
+  if (!verts || !values_bar || !verts_bar || !ca_bar || !cb_bar) {
     *status = FFG_INVALID_INPUT;
     return;
   }
   std::shared_ptr<Problem> P;
   std::string msg;
-  int st = create_problem(FFG_TETRA_LAGRANGE, degree, nv, nt, tets, rule, qdeg, FFG_BOUNDARY_NONE,
-                          nullptr, P, msg);
+  int st = create_problem(family, degree, nv, nt, cells, rule, qdeg, FFG_BOUNDARY_NONE, nullptr, P,
+                          msg);
   if (st) { *status = st; return; }
   const Topology &t = P->topo;
   if (nnz != t.nnz()) { *status = FFG_INVALID_INPUT; return; }
@@ -950,16 +963,22 @@ void ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
           cudaSuccess ||
       cudaMemset(P->err, 0, sizeof(int)) != cudaSuccess) {
     st = FFG_CUDA_ERROR;
-  } else if (!(st = lagrange_vjp(t, P->dt, P->csc_col_ptr, P->csc_row, P->in_vertices, vb,
-                                 stiffness, mass, dvbar, coef, P->err, 0))) {
-    if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-      st = FFG_CUDA_ERROR;
-    else if (herr)
-      st = herr;
-    else if (cudaMemcpy(verts_bar, dvbar, sizeof(double) * vcount, cudaMemcpyDeviceToHost) !=
-                 cudaSuccess ||
-             cudaMemcpy(hc, coef, sizeof(hc), cudaMemcpyDeviceToHost) != cudaSuccess)
-      st = FFG_CUDA_ERROR;
+  } else {
+    st = family == FFG_TETRA_LAGRANGE
+             ? lagrange_vjp(t, P->dt, P->csc_col_ptr, P->csc_row, P->in_vertices, vb, ca, cb,
+                            dvbar, coef, P->err, 0)
+             : nedelec_vjp(t, P->tab, P->dt, P->csc_col_ptr, P->csc_row, P->in_vertices, vb, ca,
+                           cb, P->elem, dvbar, coef, P->err, 0);
+    if (!st) {
+      if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = FFG_CUDA_ERROR;
+      else if (herr)
+        st = herr;
+      else if (cudaMemcpy(verts_bar, dvbar, sizeof(double) * vcount, cudaMemcpyDeviceToHost) !=
+                   cudaSuccess ||
+               cudaMemcpy(hc, coef, sizeof(hc), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = FFG_CUDA_ERROR;
+    }
   }
   for (double *p : {vb, dvbar, coef}) cudaFree(p);
   if (st) {
@@ -967,9 +986,43 @@ void ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
     *status = st;
     return;
   }
-  *stiffness_bar = hc[0];
-  *mass_bar = hc[1];
+  *ca_bar = hc[0];
+  *cb_bar = hc[1];
   *status = FFG_OK;
+}
+
+void ffg_assemble_tetra_lagrange_stiffness_csc_jvp(
+    int nv, const double *verts, int nt, const int *tets, int degree, int rule, int qdeg,
+    double stiffness, double mass, const double *verts_dot, double stiffness_dot,
+    double mass_dot, int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_ind,
+    double *values_dot, int *status) {
+  tangent_csc(FFG_TETRA_LAGRANGE, degree, nv, verts, nt, tets, rule, qdeg, stiffness, mass,
+              verts_dot, stiffness_dot, mass_dot, cap, n_dofs, nnz, col_ptr, row_ind, values_dot,
+              status);
+}
+
+void ffg_assemble_tetra_lagrange_stiffness_csc_vjp(
+    int nv, const double *verts, int nt, const int *tets, int degree, int rule, int qdeg,
+    double stiffness, double mass, int64_t nnz, const double *values_bar, double *verts_bar,
+    double *stiffness_bar, double *mass_bar, int *status) {
+  adjoint_csc(FFG_TETRA_LAGRANGE, degree, nv, verts, nt, tets, rule, qdeg, stiffness, mass, nnz,
+              values_bar, verts_bar, stiffness_bar, mass_bar, status);
+}
+
+void ffg_assemble_tetra_nedelec_curl_mass_csc_jvp(
+    int nv, const double *verts, int nt, const int *tets, int order, double curl, double mass,
+    const double *verts_dot, double curl_dot, double mass_dot, int64_t cap, int *n_dofs,
+    int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values_dot, int *status) {
+  tangent_csc(FFG_TETRA_NEDELEC, order, nv, verts, nt, tets, 0, 0, curl, mass, verts_dot, curl_dot,
+              mass_dot, cap, n_dofs, nnz, col_ptr, row_ind, values_dot, status);
+}
+
+void ffg_assemble_tetra_nedelec_curl_mass_csc_vjp(
+    int nv, const double *verts, int nt, const int *tets, int order, double curl, double mass,
+    int64_t nnz, const double *values_bar, double *verts_bar, double *curl_bar, double *mass_bar,
+    int *status) {
+  adjoint_csc(FFG_TETRA_NEDELEC, order, nv, verts, nt, tets, 0, 0, curl, mass, nnz, values_bar,
+              verts_bar, curl_bar, mass_bar, status);
 }
 
 void ffg_assemble_tetra_lagrange_scalar_load_samples(int nv, const double *verts, int nt,

@@ -208,6 +208,10 @@ struct AssemblyInputs {
   const double *cell_a = nullptr, *cell_b = nullptr;  // device, nullable
   const double *samples = nullptr;                    // device, nullable
   const double *g = nullptr;                          // device constrained values, nullable
+  // forward mode: with vertices_dot set, the Nedelec element kernel writes the
+  // tangent element matrices along (vertices_dot, coef_a_dot, coef_b_dot)
+  const double *vertices_dot = nullptr;               // device, nullable
+  double coef_a_dot = 0.0, coef_b_dot = 0.0;
 };
 
 // Per-cell geometry/coefficient block and element right-hand sides.
@@ -229,7 +233,9 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    cudaStream_t s);
 int geo_stride_for(const Topology &t, const ElementTables &tab);
 
-// Forward / reverse mode of the Lagrange stiffness + mass assembly (kernels_ad.cu).
+// Forward / reverse mode of the Lagrange stiffness + mass and the Nedelec
+// curl + mass assembly (kernels_ad.cu; the Nedelec forward mode runs through
+// launch_nedelec with AssemblyInputs::vertices_dot).
 // The JVP writes the tangent of the seven contraction weights of every cell
 // into `geo` (load samples zero); launch_columns then yields the tangent CSC
 // values.  The VJP reads the CSC cotangent values_bar (device, on the pattern
@@ -242,5 +248,12 @@ int launch_lagrange_geometry_jvp(const Topology &t, const DeviceTopology &dt,
 int lagrange_vjp(const Topology &t, const DeviceTopology &dt, const int64_t *col_ptr,
                  const int *row_idx, const double *vertices, const double *values_bar, double ca,
                  double cb, double *vertices_bar, double *coef_bar, int *err, cudaStream_t s);
+// Reverse mode of the Nedelec curl + mass assembly, same outputs; `elem`
+// (n_cells * nb * nb) is the work space of orders whose element matrix does
+// not fit in shared memory.
+int nedelec_vjp(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                const int64_t *col_ptr, const int *row_idx, const double *vertices,
+                const double *values_bar, double ca, double cb, double *elem,
+                double *vertices_bar, double *coef_bar, int *err, cudaStream_t s);
 
 }  // namespace ffg

@@ -1,12 +1,20 @@
 // Forward (JVP) and reverse (VJP) mode of the tetrahedral Lagrange stiffness
 // + mass CSC assembly: assemble_tetra_lagrange_stiffness_csc_jvp and _vjp
 // (src/assembly/assembly_tetra_lagrange_arbitrary_order_3d.f90:336-391 and
-// :393-471, element routines :107-180 and :182-274).
+// :393-471, element routines :107-180 and :182-274), and of the Nedelec curl
+// + mass CSC assembly, assemble_tetra_nedelec_curl_mass_csc_jvp and _vjp
+// (src/assembly/assembly_tetra_nedelec_3d.f90:2114-2181 and :2183-2287,
+// element routines :645-719 and :721-806).
 //
 // Both reuse the contraction the primal assembly runs on: every element
 // matrix is K = sum_s geo_s R^s with seven reference tensors R^s (six
 // symmetric pairs (a,b) of the gradient term, weight kappa det (J^-1 J^-T)_ab,
-// and the mass term, weight m det).
+// and the mass term, weight m det); Nedelec has twelve (curl pairs, weight
+// (c/det) (J^T J)_ab, and mass pairs, weight m det (J^-1 J^-T)_ab) and the
+// orientation transform T around them.  The reference integrates the
+// derivatives at quadrature degree 2k+2 where its primal uses 2k or the
+// 4-point rule; every one of these rules integrates the polynomial
+// integrands exactly, so the tensors serve both.
 //
 // JVP: K is linear in geo, so the tangent element matrix is sum_s geo'_s R^s
 // with geo' the derivative of the seven weights along (v', kappa', m').  One
@@ -40,6 +48,20 @@ __device__ __forceinline__ void pair_of(int s, int &a, int &b) {
   // symmetric pair order shared with basis.cpp: (0,0),(1,1),(2,2),(0,1),(0,2),(1,2)
   a = s < 3 ? s : (s == 5 ? 1 : 0);
   b = s < 3 ? s : (s == 3 ? 1 : 2);
+}
+
+// Binary search of `row` in the sorted CSC column `col`; 0 when absent.
+__device__ __forceinline__ double csc_value_at(const int64_t *__restrict__ col_ptr,
+                                               const int *__restrict__ row_idx,
+                                               const double *__restrict__ values, int row,
+                                               int col) {
+  const int64_t end = col_ptr[col + 1];
+  int64_t lo = col_ptr[col], hi = end;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (row_idx[mid] < row) lo = mid + 1; else hi = mid;
+  }
+  return (lo < end && row_idx[lo] == row) ? values[lo] : 0.0;
 }
 
 // geo'_s for one cell: d(kappa det G_ab) and d(m det), G = J^-1 J^-T, with
@@ -111,13 +133,7 @@ __global__ void lagrange_cell_vjp_kernel(int n_cells, const int *__restrict__ ce
   for (int idx = lane; idx < nn; idx += 32) {
     const int row = free_index[ge[idx % nb]], col = free_index[ge[idx / nb]];
     if (row < 0 || col < 0) continue;
-    const int64_t end = col_ptr[col + 1];
-    int64_t lo = col_ptr[col], hi = end;
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) >> 1;
-      if (row_idx[mid] < row) lo = mid + 1; else hi = mid;
-    }
-    const double b = (lo < end && row_idx[lo] == row) ? values_bar[lo] : 0.0;
+    const double b = csc_value_at(col_ptr, row_idx, values_bar, row, col);
 #pragma unroll
     for (int s = 0; s < 7; ++s) Q[s] += b * __ldg(ref + (size_t)s * nn + idx);
   }
@@ -183,6 +199,154 @@ __global__ void lagrange_cell_vjp_kernel(int n_cells, const int *__restrict__ ce
   }
   out[12] = det * gq;
   out[13] = det * Q[6];
+}
+
+struct NedVjpDims {
+  int k, nb, fdc, edge_end;
+  int oglobal;  // the nb x nb cotangent lives in `elem`, not in shared memory
+};
+
+// One CTA per cell (grid-stride).  The oriented cotangent Obar (the
+// reference's dense_bar at the cell's global DoFs, :2222-2250) is gathered
+// from the CSC, mapped back to the element basis as T Obar T^T (edge signs;
+// per face (Obar T^T) then T (.) through the face block), contracted with
+// the twelve reference tensors, and the cell's geometry adjoints follow from
+// K = (c/det) sum_s C^s (J^T J)_s + m det sum_s V^s (J^-1 J^-T)_s.
+__global__ void nedelec_cell_vjp_kernel(int n_cells, const int *__restrict__ cells,
+                                        const double *__restrict__ verts,
+                                        const int *__restrict__ gd,
+                                        const int *__restrict__ free_index, NedVjpDims D,
+                                        const int64_t *__restrict__ col_ptr,
+                                        const int *__restrict__ row_idx,
+                                        const double *__restrict__ values_bar,
+                                        const double *__restrict__ ref,
+                                        const int8_t *__restrict__ edge_sign,
+                                        const uint8_t *__restrict__ face_perm,
+                                        const double *__restrict__ face_blocks, double ca,
+                                        double cb, double *__restrict__ elem,
+                                        double *__restrict__ cell_bar, int *err) {
+  extern __shared__ double sm[];
+  const int nb = D.nb, fdc = D.fdc;
+  const size_t nn = (size_t)nb * nb;
+  double *O = D.oglobal ? nullptr : sm;
+  double *tmp = D.oglobal ? sm : sm + nn;  // nb * fdc
+  double *B = tmp + (size_t)nb * fdc;      // fdc * fdc
+  __shared__ double part[12][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int c = blockIdx.x; c < n_cells; c += gridDim.x) {
+    if (D.oglobal) O = elem + nn * c;
+    const int *ge = gd + (size_t)nb * c;
+    const int8_t *sg = edge_sign + 6 * (size_t)c;
+    for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+      const int i = (int)(idx % nb), j = (int)(idx / nb);
+      const int row = free_index[ge[i]], col = free_index[ge[j]];
+      double v = (row < 0 || col < 0) ? 0.0 : csc_value_at(col_ptr, row_idx, values_bar, row, col);
+      if (i < D.edge_end && sg[i / D.k] == -1 && ((i % D.k) % 2) == 0) v = -v;
+      if (j < D.edge_end && sg[j / D.k] == -1 && ((j % D.k) % 2) == 0) v = -v;
+      O[idx] = v;
+    }
+    __syncthreads();
+    // face blocks: T[st+m][st+r] = B[r*fdc+m], so (O T^T)[i][st+r] =
+    // sum_m O[i][st+m] B[m*fdc+r] and (T O)[st+r][j] = sum_m B[m*fdc+r] O[st+m][j]
+    for (int f = 0; f < 4 && fdc > 0; ++f) {
+      const int st = D.edge_end + f * fdc;
+      const double *Bg = face_blocks + (size_t)face_perm[4 * (size_t)c + f] * fdc * fdc;
+      for (int q = threadIdx.x; q < fdc * fdc; q += blockDim.x) B[q] = Bg[q];
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x) {
+        const int i = q % nb, r = q / nb;
+        double acc = 0.0;
+        for (int m = 0; m < fdc; ++m) acc += O[i + (size_t)nb * (st + m)] * B[m * fdc + r];
+        tmp[q] = acc;
+      }
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x)
+        O[(q % nb) + (size_t)nb * (st + q / nb)] = tmp[q];
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x) {
+        const int r = q % fdc, j = q / fdc;
+        double acc = 0.0;
+        for (int m = 0; m < fdc; ++m) acc += B[m * fdc + r] * O[(st + m) + (size_t)nb * j];
+        tmp[q] = acc;
+      }
+      __syncthreads();
+      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x)
+        O[(st + q % fdc) + (size_t)nb * (q / fdc)] = tmp[q];
+      __syncthreads();
+    }
+    double Q[12];
+#pragma unroll
+    for (int s = 0; s < 12; ++s) Q[s] = 0.0;
+    for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+      const double o = O[idx];
+#pragma unroll
+      for (int s = 0; s < 12; ++s) Q[s] += o * __ldg(ref + s * nn + idx);
+    }
+#pragma unroll
+    for (int s = 0; s < 12; ++s) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) Q[s] += __shfl_xor_sync(0xffffffffu, Q[s], off);
+      if (lane == 0) part[s][warp] = Q[s];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < 12; ++s) {
+        double a = 0.0;
+        for (int w = 0; w < nwarps; ++w) a += part[s][w];
+        Q[s] = a;
+      }
+      double J[9], Ji[9], v0[3];
+      tet_jacobian(cells, verts, c, J, v0);
+      const double det = det3(J);
+      double *out = cell_bar + (size_t)kCellBar * c;
+      if (!valid_jacobian(J, det)) {
+        atomicCAS(err, 0, FFG_INVALID_INPUT);
+        for (int i = 0; i < kCellBar; ++i) out[i] = 0.0;
+      } else {
+        inv3(J, det, Ji);
+        double hq = 0.0, gq = 0.0, Dm[9], Cm[9];
+        for (int s = 0; s < 6; ++s) {
+          int a, b;
+          pair_of(s, a, b);
+          const double H = J[3 * a] * J[3 * b] + J[3 * a + 1] * J[3 * b + 1] + J[3 * a + 2] * J[3 * b + 2];
+          const double G = Ji[a] * Ji[b] + Ji[a + 3] * Ji[b + 3] + Ji[a + 6] * Ji[b + 6];
+          hq += H * Q[s];
+          gq += G * Q[6 + s];
+          const double wd = ca / det * Q[s], wc = cb * det * Q[6 + s];
+          if (a == b) {
+            Dm[a + 3 * a] = wd;
+            Cm[a + 3 * a] = wc;
+          } else {
+            Dm[a + 3 * b] = Dm[b + 3 * a] = 0.5 * wd;
+            Cm[a + 3 * b] = Cm[b + 3 * a] = 0.5 * wc;
+          }
+        }
+        const double det_bar = -ca * hq / (det * det) + cb * gq;
+        // Jbar = 2 J D - J^-T (2 C J^-1) J^-T + det_bar det J^-T
+        double Jib[9], A[9], Jb[9];
+        for (int k = 0; k < 3; ++k)
+          for (int a = 0; a < 3; ++a)
+            Jib[a + 3 * k] = 2.0 * (Cm[a] * Ji[3 * k] + Cm[a + 3] * Ji[1 + 3 * k] + Cm[a + 6] * Ji[2 + 3 * k]);
+        for (int k = 0; k < 3; ++k)
+          for (int r = 0; r < 3; ++r)
+            A[r + 3 * k] = Ji[3 * r] * Jib[3 * k] + Ji[1 + 3 * r] * Jib[1 + 3 * k] + Ji[2 + 3 * r] * Jib[2 + 3 * k];
+        for (int k = 0; k < 3; ++k)
+          for (int r = 0; r < 3; ++r)
+            Jb[r + 3 * k] = 2.0 * (J[r] * Dm[3 * k] + J[r + 3] * Dm[1 + 3 * k] + J[r + 6] * Dm[2 + 3 * k]) -
+                            (A[r] * Ji[k] + A[r + 3] * Ji[k + 3] + A[r + 6] * Ji[k + 6]) +
+                            det_bar * det * Ji[k + 3 * r];
+        for (int r = 0; r < 3; ++r) {
+          out[r] = -(Jb[r] + Jb[r + 3] + Jb[r + 6]);
+          out[3 + r] = Jb[r];
+          out[6 + r] = Jb[r + 3];
+          out[9 + r] = Jb[r + 6];
+        }
+        out[12] = hq / det;
+        out[13] = det * gq;
+      }
+    }
+    __syncthreads();
+  }
 }
 
 __global__ void iota_kernel(int64_t n, int *v) {
@@ -271,41 +435,98 @@ int launch_lagrange_geometry_jvp(const Topology &t, const DeviceTopology &dt,
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 
+namespace {
+
+// Scratch of the reverse mode: per-cell adjoints and the sorted incidences.
+struct VjpScratch {
+  Scratch cell_bar, keys, inc, inc_in, temp;
+  int alloc(int64_t nc) {
+    int st;
+    if ((st = cell_bar.alloc(sizeof(double) * kCellBar * nc))) return st;
+    if ((st = keys.alloc(sizeof(int) * 4 * nc))) return st;
+    if ((st = inc.alloc(sizeof(int) * 4 * nc))) return st;
+    return inc_in.alloc(sizeof(int) * 4 * nc);
+  }
+};
+
+// Vertex-owner gather of the per-cell adjoints and the coefficient sums.
+int finish_vjp(const Topology &t, const DeviceTopology &dt, VjpScratch &w, double *vertices_bar,
+               double *coef_bar, cudaStream_t s) {
+  const int64_t n_inc = 4 * (int64_t)t.n_cells;
+  iota_kernel<<<blocks_for(n_inc, 256), 256, 0, s>>>(n_inc, (int *)w.inc_in.p);
+  int end_bit = 1;
+  while (end_bit < 31 && (1LL << end_bit) < (int64_t)t.n_vertices) ++end_bit;
+  size_t temp_bytes = 0;
+  if (cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dt.cells, (int *)w.keys.p,
+                                      (const int *)w.inc_in.p, (int *)w.inc.p, n_inc, 0, end_bit,
+                                      s) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  int st;
+  if ((st = w.temp.alloc(temp_bytes))) return st;
+  if (cub::DeviceRadixSort::SortPairs(w.temp.p, temp_bytes, dt.cells, (int *)w.keys.p,
+                                      (const int *)w.inc_in.p, (int *)w.inc.p, n_inc, 0, end_bit,
+                                      s) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  vertex_gather_kernel<<<blocks_for(t.n_vertices, 128), 128, 0, s>>>(
+      t.n_vertices, n_inc, (const int *)w.keys.p, (const int *)w.inc.p,
+      (const double *)w.cell_bar.p, vertices_bar);
+  coefficient_sum_kernel<<<1, 1024, 0, s>>>(t.n_cells, (const double *)w.cell_bar.p, coef_bar);
+  if (cudaGetLastError() != cudaSuccess) return FFG_CUDA_ERROR;
+  // the scratch buffers are released on return: let the stream pass them first
+  return cudaStreamSynchronize(s) == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+}  // namespace
+
 int lagrange_vjp(const Topology &t, const DeviceTopology &dt, const int64_t *col_ptr,
                  const int *row_idx, const double *vertices, const double *values_bar, double ca,
                  double cb, double *vertices_bar, double *coef_bar, int *err, cudaStream_t s) {
   if (t.family != FFG_TETRA_LAGRANGE) return FFG_INVALID_INPUT;
-  const int64_t nc = t.n_cells, n_inc = 4 * nc;
-  Scratch cell_bar, keys, inc, inc_in, temp;
+  VjpScratch w;
   int st;
-  if ((st = cell_bar.alloc(sizeof(double) * kCellBar * nc))) return st;
-  if ((st = keys.alloc(sizeof(int) * n_inc))) return st;
-  if ((st = inc.alloc(sizeof(int) * n_inc))) return st;
-  if ((st = inc_in.alloc(sizeof(int) * n_inc))) return st;
+  if ((st = w.alloc(t.n_cells))) return st;
   const int warps_per_block = 8;
-  lagrange_cell_vjp_kernel<<<blocks_for(nc, warps_per_block), 32 * warps_per_block, 0, s>>>(
+  lagrange_cell_vjp_kernel<<<blocks_for(t.n_cells, warps_per_block), 32 * warps_per_block, 0, s>>>(
       t.n_cells, dt.cells, vertices, dt.gd, dt.free_index, t.nb, col_ptr, row_idx, values_bar,
-      dt.ref, ca, cb, (double *)cell_bar.p, err);
-  iota_kernel<<<blocks_for(n_inc, 256), 256, 0, s>>>(n_inc, (int *)inc_in.p);
-  int end_bit = 1;
-  while (end_bit < 31 && (1LL << end_bit) < (int64_t)t.n_vertices) ++end_bit;
-  size_t temp_bytes = 0;
-  if (cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, dt.cells, (int *)keys.p,
-                                      (const int *)inc_in.p, (int *)inc.p, n_inc, 0, end_bit,
-                                      s) != cudaSuccess)
-    return FFG_CUDA_ERROR;
-  if ((st = temp.alloc(temp_bytes))) return st;
-  if (cub::DeviceRadixSort::SortPairs(temp.p, temp_bytes, dt.cells, (int *)keys.p,
-                                      (const int *)inc_in.p, (int *)inc.p, n_inc, 0, end_bit,
-                                      s) != cudaSuccess)
-    return FFG_CUDA_ERROR;
-  vertex_gather_kernel<<<blocks_for(t.n_vertices, 128), 128, 0, s>>>(
-      t.n_vertices, n_inc, (const int *)keys.p, (const int *)inc.p, (const double *)cell_bar.p,
-      vertices_bar);
-  coefficient_sum_kernel<<<1, 1024, 0, s>>>(t.n_cells, (const double *)cell_bar.p, coef_bar);
+      dt.ref, ca, cb, (double *)w.cell_bar.p, err);
   if (cudaGetLastError() != cudaSuccess) return FFG_CUDA_ERROR;
-  // the scratch buffers are released on return: let the stream pass them first
-  return cudaStreamSynchronize(s) == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+  return finish_vjp(t, dt, w, vertices_bar, coef_bar, s);
+}
+
+int nedelec_vjp(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
+                const int64_t *col_ptr, const int *row_idx, const double *vertices,
+                const double *values_bar, double ca, double cb, double *elem,
+                double *vertices_bar, double *coef_bar, int *err, cudaStream_t s) {
+  if (t.family != FFG_TETRA_NEDELEC || tab.n_terms != 12) return FFG_INVALID_INPUT;
+  NedVjpDims D;
+  D.k = t.degree;
+  D.nb = t.nb;
+  D.fdc = t.degree * (t.degree - 1);
+  D.edge_end = 6 * t.degree;
+  auto smem_for = [&](bool oglobal) {
+    return sizeof(double) * ((oglobal ? 0 : (size_t)D.nb * D.nb) + (size_t)D.nb * D.fdc +
+                             (size_t)D.fdc * D.fdc);
+  };
+  D.oglobal = smem_for(false) > 200 * 1024 ? 1 : 0;
+  const size_t smem = smem_for(D.oglobal != 0);
+  if (D.oglobal && !elem) return FFG_INVALID_INPUT;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(nedelec_cell_vjp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return FFG_CUDA_ERROR;
+  VjpScratch w;
+  int st;
+  if ((st = w.alloc(t.n_cells))) return st;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * 8);
+  nedelec_cell_vjp_kernel<<<grid, 256, smem, s>>>(
+      t.n_cells, dt.cells, vertices, dt.gd, dt.free_index, D, col_ptr, row_idx, values_bar,
+      dt.ref, dt.edge_sign, dt.face_perm, dt.face_blocks, ca, cb, elem, (double *)w.cell_bar.p,
+      err);
+  if (cudaGetLastError() != cudaSuccess) return FFG_CUDA_ERROR;
+  return finish_vjp(t, dt, w, vertices_bar, coef_bar, s);
 }
 
 }  // namespace ffg

@@ -148,7 +148,8 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
                                        const uint8_t *__restrict__ face_perm,
                                        const double *__restrict__ face_blocks,
                                        double *__restrict__ elem, double *__restrict__ cell_rhs,
-                                       int *err) {
+                                       int *err, const double *__restrict__ verts_dot,
+                                       double ca_dot, double cb_dot) {
   extern __shared__ double sm[];
   const int nb = D.nb, fdc = D.fdc;
   // K (nb x nb, column-major) lives in shared memory, or (order 6: 373 KB) in
@@ -173,12 +174,40 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
       inv3(J, ok_s ? det : 1.0, Ji);
       const double cw = ca * (cell_a ? cell_a[c] : 1.0);
       const double mw = cb * (cell_b ? cell_b[c] : 1.0);
-      for (int s = 0; s < 6; ++s) {
-        const int a = kPa[s], b = kPb[s];
-        const double JtJ = J[3 * a] * J[3 * b] + J[3 * a + 1] * J[3 * b + 1] + J[3 * a + 2] * J[3 * b + 2];
-        const double G = Ji[a] * Ji[b] + Ji[a + 3] * Ji[b + 3] + Ji[a + 6] * Ji[b + 6];
-        geo[s] = ok_s ? cw / det * JtJ : 0.0;
-        geo[6 + s] = ok_s ? mw * det * G : 0.0;
+      if (!verts_dot) {
+        for (int s = 0; s < 6; ++s) {
+          const int a = kPa[s], b = kPb[s];
+          const double JtJ = J[3 * a] * J[3 * b] + J[3 * a + 1] * J[3 * b + 1] + J[3 * a + 2] * J[3 * b + 2];
+          const double G = Ji[a] * Ji[b] + Ji[a + 3] * Ji[b + 3] + Ji[a + 6] * Ji[b + 6];
+          geo[s] = ok_s ? cw / det * JtJ : 0.0;
+          geo[6 + s] = ok_s ? mw * det * G : 0.0;
+        }
+      } else {
+        // tangent weights: d(c/det J^T J) and d(m det J^-1 J^-T), with
+        // d det = det tr(J^-1 dJ) and d J^-1 = -J^-1 dJ J^-1
+        double Jd[9], T[9], Jid[9], w0[3];
+        tet_jacobian(cells, verts_dot, c, Jd, w0);
+        for (int col = 0; col < 3; ++col)
+          for (int r = 0; r < 3; ++r)
+            T[r + 3 * col] = Ji[r] * Jd[3 * col] + Ji[r + 3] * Jd[3 * col + 1] + Ji[r + 6] * Jd[3 * col + 2];
+        for (int col = 0; col < 3; ++col)
+          for (int r = 0; r < 3; ++r)
+            Jid[r + 3 * col] = -(T[r] * Ji[3 * col] + T[r + 3] * Ji[3 * col + 1] + T[r + 6] * Ji[3 * col + 2]);
+        const double dd = det * (T[0] + T[4] + T[8]);
+        const double cwd = ca_dot * (cell_a ? cell_a[c] : 1.0);
+        const double mwd = cb_dot * (cell_b ? cell_b[c] : 1.0);
+        for (int s = 0; s < 6; ++s) {
+          const int a = kPa[s], b = kPb[s];
+          double JtJ = 0.0, dJtJ = 0.0, G = 0.0, dG = 0.0;
+          for (int r = 0; r < 3; ++r) {
+            JtJ += J[3 * a + r] * J[3 * b + r];
+            dJtJ += Jd[3 * a + r] * J[3 * b + r] + J[3 * a + r] * Jd[3 * b + r];
+            G += Ji[a + 3 * r] * Ji[b + 3 * r];
+            dG += Jid[a + 3 * r] * Ji[b + 3 * r] + Ji[a + 3 * r] * Jid[b + 3 * r];
+          }
+          geo[s] = ok_s ? cwd / det * JtJ - cw * dd / (det * det) * JtJ + cw / det * dJtJ : 0.0;
+          geo[6 + s] = ok_s ? mwd * det * G + mw * dd * G + mw * det * dG : 0.0;
+        }
       }
       for (int i = 0; i < 9; ++i) Ji_s[i] = Ji[i];
       det_s = ok_s ? det : 0.0;
@@ -401,7 +430,7 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   nedelec_element_kernel<<<grid, 256, smem, s>>>(
       t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
       tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem,
-      cell_rhs, err);
+      cell_rhs, err, in.vertices_dot, in.coef_a_dot, in.coef_b_dot);
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 

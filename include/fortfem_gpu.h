@@ -163,6 +163,26 @@ void ffg_assemble_tetra_nedelec_curl_mass_csc(
     const double *cell_mass, int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
     int *row_ind, double *values, int *status);
 
+/* assemble_tetra_nedelec_curl_mass_csc_jvp, assembly_tetra_nedelec_3d.f90:2114-2181:
+ * the tangent of the curl + mass CSC along (vertices_dot, curl_dot, mass_dot) on
+ * the primal pattern.  The reference differentiates at quadrature degree 2k+2
+ * where its primal uses 2k (order 1: the 4-point rule); both are exact for
+ * these integrands, so the values agree to rounding. */
+void ffg_assemble_tetra_nedelec_curl_mass_csc_jvp(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int order,
+    double curl_coefficient, double mass_coefficient, const double *vertices_dot,
+    double curl_coefficient_dot, double mass_coefficient_dot, int64_t nnz_capacity, int *n_dofs,
+    int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values_dot, int *status);
+
+/* assemble_tetra_nedelec_curl_mass_csc_vjp, same file :2183-2287: vertex, curl
+ * and mass adjoints of a cotangent on the primal CSC pattern (nnz entries).
+ * Outputs are zeroed first. */
+void ffg_assemble_tetra_nedelec_curl_mass_csc_vjp(
+    int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int order,
+    double curl_coefficient, double mass_coefficient, int64_t nnz, const double *values_bar,
+    double *vertices_bar, double *curl_coefficient_bar, double *mass_coefficient_bar,
+    int *status);
+
 /* assemble_tetra_nedelec_vector_load_samples, assembly_tetra_nedelec_3d.f90:128-185
  * (order 1 uses the 4-point rule and edge signs, :2002-2040); source_values
  * holds 3*n_q values per cell. */

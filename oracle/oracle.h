@@ -134,6 +134,20 @@ int or_nedelec_csc(int n_vertices, const double *vertices, int n_tets, const int
                    double curl, double mass, const double *cell_curl, const double *cell_mass,
                    int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_idx,
                    double *values);
+/* forward (JVP) and reverse (VJP) mode of the element and the CSC assembly */
+int or_nedelec_element_jvp(const double *vertices, int order, int quadrature_degree, double curl,
+                           double mass, const double *vertices_dot, double curl_dot,
+                           double mass_dot, double *matrix_dot);
+int or_nedelec_element_vjp(const double *vertices, int order, int quadrature_degree, double curl,
+                           double mass, const double *matrix_bar, double *vertices_bar,
+                           double *curl_bar, double *mass_bar);
+int or_nedelec_csc_jvp(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                       int order, double curl, double mass, const double *vertices_dot,
+                       double curl_dot, double mass_dot, int64_t nnz_capacity, int *n_dofs,
+                       int64_t *nnz, int64_t *col_ptr, int *row_idx, double *values_dot);
+int or_nedelec_csc_vjp(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                       int order, double curl, double mass, int64_t nnz, const double *values_bar,
+                       double *vertices_bar, double *curl_bar, double *mass_bar);
 int or_nedelec_load_samples(int n_vertices, const double *vertices, int n_tets, const int *tets,
                             int order, const double *source_values /* 3 x n_q x T */, double *rhs);
 int or_nedelec_load_points(int n_vertices, const double *vertices, int n_tets, const int *tets,

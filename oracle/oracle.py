@@ -473,6 +473,57 @@ def nedelec_csc(vertices, tets, k, curl=1.0, mass=1.0, cell_curl=None, cell_mass
     return n, cp, ri, v
 
 
+def nedelec_element_jvp(vertices, k, vertices_dot, curl, mass, curl_dot, mass_dot, q=None):
+    if q is None:
+        q = 2 * k + 2
+    nb = nedelec_dof_count(k)
+    m = np.zeros(nb * nb)
+    _check(_call("or_nedelec_element_jvp", _arr(vertices, np.float64), k, q, float(curl),
+                 float(mass), _arr(vertices_dot, np.float64), float(curl_dot), float(mass_dot), m),
+           "nedelec_element_jvp")
+    return m.reshape(nb, nb, order="F")
+
+
+def nedelec_element_vjp(vertices, k, matrix_bar, curl, mass, q=None):
+    """(vertices_bar (4,3), curl_bar, mass_bar) of one element."""
+    if q is None:
+        q = 2 * k + 2
+    vb = np.zeros(12)
+    cb = C.c_double(0.0); mb = C.c_double(0.0)
+    _check(_call("or_nedelec_element_vjp", _arr(vertices, np.float64), k, q, float(curl),
+                 float(mass), _arr(np.asarray(matrix_bar).ravel(order="F"), np.float64), vb,
+                 C.byref(cb), C.byref(mb)), "nedelec_element_vjp")
+    return vb.reshape(4, 3), cb.value, mb.value
+
+
+def nedelec_csc_jvp(vertices, tets, k, vertices_dot, curl, mass, curl_dot, mass_dot):
+    """(n, col_ptr, row_idx, values_dot) of assemble_tetra_nedelec_curl_mass_csc_jvp."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    nnz = int(_call("or_nedelec_csc_nnz", k, len(tets), tets, restype=C.c_int64))
+    if nnz < 0:
+        raise OracleError("nedelec_csc_nnz")
+    n = nedelec_dof_map(k, tets)["n_global"]
+    nd = C.c_int(0); nz = C.c_int64(0)
+    cp = np.zeros(n + 1, np.int64); ri = np.zeros(nnz, np.int32); v = np.zeros(nnz)
+    _check(_call("or_nedelec_csc_jvp", len(vertices), vertices, len(tets), tets, k, float(curl),
+                 float(mass), _arr(vertices_dot, np.float64), float(curl_dot), float(mass_dot),
+                 C.c_int64(nnz), C.byref(nd), C.byref(nz), cp, ri, v), "nedelec_csc_jvp")
+    return n, cp, ri, v
+
+
+def nedelec_csc_vjp(vertices, tets, k, values_bar, curl, mass):
+    """(vertices_bar (n_vertices,3), curl_bar, mass_bar) of
+    assemble_tetra_nedelec_curl_mass_csc_vjp."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    values_bar = _arr(values_bar, np.float64)
+    vb = np.zeros(vertices.size)
+    cb = C.c_double(0.0); mb = C.c_double(0.0)
+    _check(_call("or_nedelec_csc_vjp", len(vertices), vertices, len(tets), tets, k, float(curl),
+                 float(mass), C.c_int64(values_bar.size), values_bar, vb, C.byref(cb),
+                 C.byref(mb)), "nedelec_csc_vjp")
+    return vb.reshape(-1, 3), cb.value, mb.value
+
+
 def nedelec_load_points(vertices, tets, k):
     vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
     nq = 4 if k == 1 else _call("or_tetra_duffy_count", 2 * k + 2)

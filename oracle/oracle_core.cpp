@@ -615,7 +615,7 @@ int or_lagrange_csc(int nv, const double *verts, int nt, const int *tets, int p,
 // from their definitions: d(det J) = det tr(J^-1 dJ), d(J^-1) = -J^-1 dJ J^-1,
 // and the adjoints Jbar += detbar det J^-T, Jbar = -J^-T Jibar J^-T.
 namespace {
-void mat3_mul(const double *A, const double *B, double *C) {  // column-major C = A B
+static void mat3_mul(const double *A, const double *B, double *C) {  // column-major C = A B
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 3; ++r) {
       double s = 0.0;

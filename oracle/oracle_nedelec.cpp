@@ -504,6 +504,258 @@ int or_nedelec_csc(int nv, const double *verts, int nt, const int *tets, int k, 
                              row_idx, values);
 }
 
+// ------------------------------------------------- forward / reverse mode
+namespace {
+static void mat3_mul(const double *A, const double *B, double *C) {  // column-major C = A B
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += A[r + 3 * k] * B[k + 3 * c];
+      C[r + 3 * c] = s;
+    }
+}
+
+// oriented = T^T M T (forward) or T M T^T (reverse), n x n column-major
+static void sandwich(int n, const double *T, const double *M, bool forward, double *out) {
+  std::vector<double> X((size_t)n * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int l = 0; l < n; ++l)
+        s += M[i + (size_t)n * l] * (forward ? T[l + (size_t)n * j] : T[j + (size_t)n * l]);
+      X[i + (size_t)n * j] = s;
+    }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int l = 0; l < n; ++l)
+        s += (forward ? T[l + (size_t)n * i] : T[i + (size_t)n * l]) * X[l + (size_t)n * j];
+      out[i + (size_t)n * j] = s;
+    }
+}
+}  // namespace
+
+// assemble_tetra_nedelec_curl_mass_element_jvp, assembly_tetra_nedelec_3d.f90:645-719,
+// with map_tetra_nedelec_covariant_jvp (src/elements/tetra_piola_maps.f90:59-105)
+// at zero reference tangents: values' = dJ^-T v, curls' = dJ c / det - J c ddet / det^2.
+int or_nedelec_element_jvp(const double *v, int k, int q, double cw, double mw, const double *vdot,
+                           double cw_dot, double mw_dot, double *Md) {
+  if (k < 1 || q < 0) return 1;
+  double J[9], Jd[9], Ji[9], Jid[9], T[9], U[9], det;
+  if (!tetra_geometry(v, J, &det)) return 1;
+  tetra_jacobian(vdot, Jd);
+  inv3(J, det, Ji);
+  mat3_mul(Ji, Jd, T);
+  const double det_dot = det * (T[0] + T[4] + T[8]);
+  mat3_mul(T, Ji, U);
+  for (int i = 0; i < 9; ++i) Jid[i] = -U[i];
+  RuleN R;
+  make_rule(0, q, R);
+  const int n = or_nedelec_dof_count(k);
+  std::vector<double> rv(3 * n), rc(3 * n), pv(3 * n), pc(3 * n), pvd(3 * n), pcd(3 * n);
+  std::fill(Md, Md + (size_t)n * n, 0.0);
+  for (size_t pt = 0; pt < R.w.size(); ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    if (or_nedelec_evaluate(k, P, rv.data(), rc.data())) return 1;
+    covariant(J, det, Ji, n, rv.data(), rc.data(), pv.data(), pc.data());
+    for (int b = 0; b < n; ++b)
+      for (int i = 0; i < 3; ++i) {
+        double s = 0.0, jc = 0.0, jdc = 0.0;
+        for (int m = 0; m < 3; ++m) {
+          s += Jid[m + 3 * i] * rv[3 * b + m];
+          jc += J[i + 3 * m] * rc[3 * b + m];
+          jdc += Jd[i + 3 * m] * rc[3 * b + m];
+        }
+        pvd[3 * b + i] = s;
+        pcd[3 * b + i] = jdc / det - jc * det_dot / (det * det);
+      }
+    const double w = R.w[pt];
+    for (int col = 0; col < n; ++col)
+      for (int row = 0; row < n; ++row) {
+        double ce = 0.0, me = 0.0, cd = 0.0, md = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          ce += pc[3 * row + i] * pc[3 * col + i];
+          me += pv[3 * row + i] * pv[3 * col + i];
+          cd += pcd[3 * row + i] * pc[3 * col + i] + pc[3 * row + i] * pcd[3 * col + i];
+          md += pvd[3 * row + i] * pv[3 * col + i] + pv[3 * row + i] * pvd[3 * col + i];
+        }
+        Md[row + (size_t)n * col] +=
+            w * (det_dot * (cw * ce + mw * me) +
+                 det * (cw_dot * ce + cw * cd + mw_dot * me + mw * md));
+      }
+  }
+  return 0;
+}
+
+// assemble_tetra_nedelec_curl_mass_element_vjp, same file :721-806, with
+// map_tetra_nedelec_covariant_vjp (tetra_piola_maps.f90:107-167) per point.
+int or_nedelec_element_vjp(const double *v, int k, int q, double cw, double mw, const double *Mb,
+                           double *vbar, double *cw_bar, double *mw_bar) {
+  for (int i = 0; i < 12; ++i) vbar[i] = 0.0;
+  *cw_bar = 0.0;
+  *mw_bar = 0.0;
+  if (k < 1 || q < 0) return 1;
+  double J[9], Ji[9], det;
+  if (!tetra_geometry(v, J, &det)) return 1;
+  inv3(J, det, Ji);
+  RuleN R;
+  make_rule(0, q, R);
+  const int n = or_nedelec_dof_count(k);
+  std::vector<double> rv(3 * n), rc(3 * n), pv(3 * n), pc(3 * n), vb(3 * n), cb(3 * n);
+  double Jb[9] = {0}, det_bar = 0.0;
+  double JiT[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) JiT[r + 3 * c] = Ji[c + 3 * r];
+  for (size_t pt = 0; pt < R.w.size(); ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    if (or_nedelec_evaluate(k, P, rv.data(), rc.data())) return 1;
+    covariant(J, det, Ji, n, rv.data(), rc.data(), pv.data(), pc.data());
+    std::fill(vb.begin(), vb.end(), 0.0);
+    std::fill(cb.begin(), cb.end(), 0.0);
+    for (int col = 0; col < n; ++col)
+      for (int row = 0; row < n; ++row) {
+        const double seed = R.w[pt] * Mb[row + (size_t)n * col];
+        double ce = 0.0, me = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          ce += pc[3 * row + i] * pc[3 * col + i];
+          me += pv[3 * row + i] * pv[3 * col + i];
+        }
+        det_bar += seed * (cw * ce + mw * me);
+        *cw_bar += seed * det * ce;
+        *mw_bar += seed * det * me;
+        for (int i = 0; i < 3; ++i) {
+          cb[3 * row + i] += seed * det * cw * pc[3 * col + i];
+          cb[3 * col + i] += seed * det * cw * pc[3 * row + i];
+          vb[3 * row + i] += seed * det * mw * pv[3 * col + i];
+          vb[3 * col + i] += seed * det * mw * pv[3 * row + i];
+        }
+      }
+    // map_tetra_nedelec_covariant_vjp: values = J^-T rv, curls = J rc / det
+    double Jib[9], A[9], B[9];
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) {
+        double s = 0.0;
+        for (int b = 0; b < n; ++b) s += rv[3 * b + r] * vb[3 * b + c];
+        Jib[r + 3 * c] = s;
+      }
+    mat3_mul(JiT, Jib, A);
+    mat3_mul(A, JiT, B);
+    double local[9], db = 0.0;
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r) {
+        double s = 0.0;
+        for (int b = 0; b < n; ++b) s += (cb[3 * b + r] / det) * rc[3 * b + c];
+        local[r + 3 * c] = -B[r + 3 * c] + s;
+      }
+    for (int b = 0; b < n; ++b)
+      for (int i = 0; i < 3; ++i) {
+        double mc = 0.0;
+        for (int m = 0; m < 3; ++m) mc += J[i + 3 * m] * rc[3 * b + m];
+        db += cb[3 * b + i] * mc;
+      }
+    db = -db / (det * det);
+    for (int i = 0; i < 9; ++i) Jb[i] += local[i] + db * det * JiT[i];
+  }
+  for (int i = 0; i < 9; ++i) Jb[i] += det_bar * det * JiT[i];
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      vbar[r + 3 * (c + 1)] += Jb[r + 3 * c];
+      vbar[r] -= Jb[r + 3 * c];
+    }
+  return 0;
+}
+
+// assemble_tetra_nedelec_curl_mass_csc_jvp, same file :2114-2181: the element
+// tangent at quadrature degree 2k+2, oriented T^T K' T, through csc_from_triplet.
+int or_nedelec_csc_jvp(int nv, const double *verts, int nt, const int *tets, int k, double cw,
+                       double mw, const double *vdot, double cw_dot, double mw_dot, int64_t cap,
+                       int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_idx,
+                       double *values) {
+  if (k < 1 || nt < 1) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int nb = or_nedelec_dof_count(k);
+  int ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  *n_dofs = ng;
+  const int64_t ntrip = (int64_t)nt * nb * nb;
+  std::vector<int> rows(ntrip), cols(ntrip);
+  std::vector<double> tv(ntrip), K((size_t)nb * nb), T((size_t)nb * nb), O((size_t)nb * nb);
+  int64_t e = 0;
+  for (int t = 0; t < nt; ++t) {
+    double v[12], vd[12];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) {
+        v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+        vd[3 * n + d] = vdot[3 * tets[4 * t + n] + d];
+      }
+    if (or_nedelec_element_jvp(v, k, 2 * k + 2, cw, mw, vd, cw_dot, mw_dot, K.data())) return 1;
+    if (or_nedelec_transform(k, eo.data() + 6 * t, fp.data() + 12 * t, T.data())) return 1;
+    sandwich(nb, T.data(), K.data(), true, O.data());
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row, ++e) {
+        rows[e] = gd[(size_t)nb * t + row];
+        cols[e] = gd[(size_t)nb * t + col];
+        tv[e] = O[row + (size_t)nb * col];
+      }
+  }
+  return or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tv.data(), cap, nnz, col_ptr,
+                             row_idx, values);
+}
+
+// assemble_tetra_nedelec_curl_mass_csc_vjp, same file :2183-2287: the oriented
+// cotangent read from the merged pattern, T Obar T^T, element VJP at 2k+2.
+int or_nedelec_csc_vjp(int nv, const double *verts, int nt, const int *tets, int k, double cw,
+                       double mw, int64_t nnz, const double *values_bar, double *verts_bar,
+                       double *cw_bar, double *mw_bar) {
+  for (int64_t i = 0; i < 3LL * nv; ++i) verts_bar[i] = 0.0;
+  *cw_bar = 0.0;
+  *mw_bar = 0.0;
+  if (k < 1 || nt < 1) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int64_t pat = or_nedelec_csc_nnz(k, nt, tets);
+  if (pat < 0 || pat != nnz) return 1;
+  const int nb = or_nedelec_dof_count(k);
+  int ng = 0, nd = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  std::vector<int64_t> cp(ng + 1);
+  std::vector<int> ri(nnz);
+  std::vector<double> vals(nnz);
+  int64_t got = 0;
+  if (or_nedelec_csc(nv, verts, nt, tets, k, cw, mw, nullptr, nullptr, nnz, &nd, &got, cp.data(),
+                     ri.data(), vals.data()))
+    return 1;
+  std::vector<double> Ob((size_t)nb * nb), T((size_t)nb * nb), Eb((size_t)nb * nb);
+  for (int t = 0; t < nt; ++t) {
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row) {
+        const int gr = gd[(size_t)nb * t + row], gc = gd[(size_t)nb * t + col];
+        double b = 0.0;
+        for (int64_t x = cp[gc]; x < cp[gc + 1]; ++x)
+          if (ri[x] == gr) { b = values_bar[x]; break; }
+        Ob[row + (size_t)nb * col] = b;
+      }
+    if (or_nedelec_transform(k, eo.data() + 6 * t, fp.data() + 12 * t, T.data())) return 1;
+    sandwich(nb, T.data(), Ob.data(), false, Eb.data());
+    double v[12], vb[12], cb = 0.0, mb = 0.0;
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+    if (or_nedelec_element_vjp(v, k, 2 * k + 2, cw, mw, Eb.data(), vb, &cb, &mb)) return 1;
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) verts_bar[3 * tets[4 * t + n] + d] += vb[3 * n + d];
+    *cw_bar += cb;
+    *mw_bar += mb;
+  }
+  return 0;
+}
+
 static int nedelec_load_rule(int k, RuleN &R) {
   // order 1: the 4-point rule (assemble_tetra_nedelec_load_element :2516-2553);
   // order >= 2: Duffy with q = 2k+2 (assemble_tetra_nedelec_load_element_order :547)

@@ -370,3 +370,49 @@ def test_lagrange_csc_jvp_vjp_kat():
     lhs = vbar_in @ vdot
     rhs = np.sum(vbar * vd) + sbar * kd + mbar * md
     assert abs(lhs - rhs) < 3e-10 * max(1.0, abs(lhs), abs(rhs))
+
+
+# test/test_tetra_nedelec_element_ad.f90 (order 2, quadrature degree 6) and
+# test/test_tetra_nedelec_curl_mass_csc_ad.f90 (order 2, two cells): the same
+# identities with curl 1.7, mass -0.8 and tangents 0.13, -0.09; orders 1 and 3
+# through the same checks.
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_nedelec_element_jvp_vjp_kat(k):
+    v = np.array([[0.1, -0.2, 0.3], [1.3, -0.1, 0.25], [0.25, 0.9, 0.35], [0.0, 0.1, 1.4]])
+    vd = np.array(AD_VDOT[:4])
+    c, m, cd, md = 1.7, -0.8, 0.13, -0.09
+    q, h = 6, AD_STEP
+    kdot = oracle.nedelec_element_jvp(v, k, vd, c, m, cd, md, q=q)
+    plus = oracle.nedelec_element(v + h * vd, k, q=q, curl=c + h * cd, mass=m + h * md)
+    minus = oracle.nedelec_element(v - h * vd, k, q=q, curl=c - h * cd, mass=m - h * md)
+    err = np.abs(kdot - (plus - minus) / (2 * h)).max() / max(1.0, np.abs(kdot).max())
+    assert err < 5e-8
+    nb = kdot.shape[0]
+    r, cc = np.meshgrid(np.arange(1, nb + 1), np.arange(1, nb + 1), indexing="ij")
+    kbar = 0.002 * r - 0.0015 * cc
+    vbar, cbar, mbar = oracle.nedelec_element_vjp(v, k, kbar, c, m, q=q)
+    lhs = np.sum(kbar * kdot)
+    rhs = np.sum(vbar * vd) + cbar * cd + mbar * md
+    assert abs(lhs - rhs) < 2e-10 * max(1.0, abs(lhs), abs(rhs))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_nedelec_csc_jvp_vjp_kat(k):
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1]], float)
+    t = np.array([[0, 1, 2, 3], [1, 2, 3, 4]], np.int32)
+    vd = np.array(AD_VDOT)
+    c, m, cd, md = 1.7, -0.8, 0.13, -0.09
+    h = AD_STEP
+    n, cp, ri, vdot = oracle.nedelec_csc_jvp(v, t, k, vd, c, m, cd, md)
+    n0, cp0, ri0, _ = oracle.nedelec_csc(v, t, k, c, m)
+    assert n == n0 and np.array_equal(cp, cp0) and np.array_equal(ri, ri0)
+    _, _, _, plus = oracle.nedelec_csc(v + h * vd, t, k, c + h * cd, m + h * md)
+    _, _, _, minus = oracle.nedelec_csc(v - h * vd, t, k, c - h * cd, m - h * md)
+    err = np.abs(vdot - (plus - minus) / (2 * h)).max() / max(1.0, np.abs(vdot).max())
+    assert err < 5e-8
+    e = np.arange(1, len(vdot) + 1, dtype=float)
+    vbar_in = 0.003 * e - 0.00001 * e ** 2
+    vbar, cbar, mbar = oracle.nedelec_csc_vjp(v, t, k, vbar_in, c, m)
+    lhs = vbar_in @ vdot
+    rhs = np.sum(vbar * vd) + cbar * cd + mbar * md
+    assert abs(lhs - rhs) < 3e-10 * max(1.0, abs(lhs), abs(rhs))
