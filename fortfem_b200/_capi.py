@@ -39,6 +39,10 @@ FFG_OPTIONS_VERSION = 1
 FFG_NOALLOC_MAX_ROWS = 65536
 FFG_BATCH_CTA_PER_SYSTEM = 0
 FFG_BATCH_WHOLE_DEVICE = 1
+FFG_POINT_REFERENCE = 0
+FFG_POINT_PHYSICAL = 1
+FFG_PROBE_AVERAGE = 0
+FFG_PROBE_FIRST = 1
 
 STATUS_TEXT = {
     FFG_OK: "ok", FFG_INVALID_INPUT: "invalid input", FFG_CAPACITY: "capacity too small",
@@ -87,6 +91,10 @@ SIGNATURES = {
         None, [i32, vp, i32, vp, i32, f64, f64, vp, f64, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curl_mass_csc_vjp": (
         None, [i32, vp, i32, vp, i32, f64, f64, i64, vp, vp, vp, vp, pi32]),
+    "ffg_problem_evaluate": (
+        None, [i32, vp, vp, i32, vp, vp, i32, vp, vp, vp, i32, vp, pi32]),
+    "ffg_problem_probe": (
+        None, [i32, vp, vp, i32, vp, i32, vp, vp, vp, i32, vp, pi32]),
     "ffg_assemble_tetra_nedelec_vector_load_samples": (
         None, [i32, vp, i32, vp, i32, vp, i32, vp, pi32]),
     "ffg_assemble_scalar_p1_csc": (

@@ -614,6 +614,79 @@ class Problem:
             raise FortfemError(st.value, "ffg_problem_reduced_system")
         return CscMatrix(self.n_free, self.n_free, cp, ri, val), rhs, free
 
+    def evaluate(self, vertices, solution, cells, points, physical=False):
+        """Batched evaluation at (cell, point) queries (ffg_problem_evaluate):
+        Lagrange (values (n,), gradients (n, 3)), Nedelec (fields (n, 3),
+        curls (n, 3)), and the per-query status (0 or FFG_INVALID_INPUT)."""
+        v = _f64(vertices)
+        u = _f64(solution)
+        if u.size != self.n_dofs:
+            raise FortfemError(K.FFG_INVALID_INPUT, "solution size")
+        c = _i32(cells).ravel()
+        x = _f64(points).reshape(-1, 3)
+        if len(x) != len(c):
+            raise FortfemError(K.FFG_INVALID_INPUT, "one point per cell")
+        wv = 3 if self.family == K.FFG_TETRA_NEDELEC else 1
+        vals = np.zeros((len(c), wv))
+        ders = np.zeros((len(c), 3))
+        qst = np.zeros(len(c), np.int32)
+        st = C.c_int(0)
+        K.load().ffg_problem_evaluate(self.handle, _ptr(v), _ptr(u), len(c), _ptr(c), _ptr(x),
+                                      K.FFG_POINT_PHYSICAL if physical else K.FFG_POINT_REFERENCE,
+                                      _ptr(vals), _ptr(ders), _ptr(qst), 0, None, C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_evaluate")
+        return (vals[:, 0] if wv == 1 else vals), ders, qst
+
+    def probe(self, vertices, solution, points, mode="average"):
+        """Point probes without a cell hint (ffg_problem_probe): values,
+        derivatives (gradient / curl) and the number of contributing cells per
+        point (0: outside the mesh; -1: rejected as the reference's probe)."""
+        v = _f64(vertices)
+        u = _f64(solution)
+        if u.size != self.n_dofs:
+            raise FortfemError(K.FFG_INVALID_INPUT, "solution size")
+        x = _f64(points).reshape(-1, 3)
+        wv = 3 if self.family == K.FFG_TETRA_NEDELEC else 1
+        vals = np.zeros((len(x), wv))
+        ders = np.zeros((len(x), 3))
+        cnt = np.zeros(len(x), np.int32)
+        st = C.c_int(0)
+        m = {"average": K.FFG_PROBE_AVERAGE, "first": K.FFG_PROBE_FIRST}[mode]
+        K.load().ffg_problem_probe(self.handle, _ptr(v), _ptr(u), len(x), _ptr(x), m, _ptr(vals),
+                                   _ptr(ders), _ptr(cnt), 0, None, C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_probe")
+        return (vals[:, 0] if wv == 1 else vals), ders, cnt
+
+
+def evaluate_tetra_lagrange_solution(vertices, tetrahedra, degree, solution, tetrahedron,
+                                     reference_point):
+    """evaluate_tetra_lagrange_solution
+    (src/solvers/fortfem_tetra_lagrange_solver_3d.f90:131-150), zero-based
+    tetrahedron index.  Returns (value, gradient (3,), status code)."""
+    v = _f64(vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    with Problem(K.FFG_TETRA_LAGRANGE, degree, t, len(v), boundary="none") as p:
+        u = _f64(solution)
+        if u.size != p.n_dofs:
+            return 0.0, np.zeros(3), K.FFG_INVALID_INPUT
+        try:
+            val, grad, qst = p.evaluate(v, u, [tetrahedron], [reference_point])
+        except FortfemError as e:
+            return 0.0, np.zeros(3), e.code
+        return float(val[0]), grad[0], int(qst[0])
+
+
+def probe_tetra_nedelec_solution(vertices, tetrahedra, order, solution, points, mode="average"):
+    """evaluate_box_solution_order (src/solvers/fortfem_magnetic_box_3d.f90:269-343,
+    mode "average") or probe_box_az / probe_box_curl (:345-440, mode "first")
+    at every point: (fields (n, 3), curls (n, 3), counts)."""
+    v = _f64(vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    with Problem(K.FFG_TETRA_NEDELEC, order, t, len(v), boundary="none") as p:
+        return p.probe(v, solution, points, mode)
+
 
 def _samples(source, points, width):
     if source is None:

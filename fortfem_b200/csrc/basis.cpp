@@ -142,45 +142,61 @@ static double ipow(double x, int n) {
 // uses the same construction, see gen_nedelec_tables.py;
 // tetra_nedelec_arbitrary_order.f90:318-396) times the exact dual-basis
 // coefficients (evaluate_tetra_nedelec_first_kind, :75-106).
-bool nedelec_eval(int k, const double *pt, double *val, double *curl) {
-  if (k < 1 || k > FFG_NEDELEC_TABLE_MAX_ORDER) return false;
-  const int n = nedelec_dof_count(k);
-  std::vector<double> cv(3 * n, 0.0), cc(3 * n, 0.0);
-  int i = 0;
-  auto term = [&](int cand, int comp, double coef, int a, int b, int c) {
-    int pw[3] = {a, b, c};
-    cv[3 * cand + comp] += coef * ipow(pt[0], a) * ipow(pt[1], b) * ipow(pt[2], c);
-    double der[3];
-    for (int d = 0; d < 3; ++d) {
-      if (pw[d] == 0) { der[d] = 0.0; continue; }
-      int r[3] = {a, b, c};
-      r[d] -= 1;
-      der[d] = coef * pw[d] * ipow(pt[0], r[0]) * ipow(pt[1], r[1]) * ipow(pt[2], r[2]);
-    }
-    double *cu = &cc[3 * cand];
-    if (comp == 0) { cu[1] += der[2]; cu[2] -= der[1]; }
-    if (comp == 1) { cu[0] -= der[2]; cu[2] += der[0]; }
-    if (comp == 2) { cu[0] += der[1]; cu[1] -= der[0]; }
+void nedelec_candidate_terms(int k, std::vector<int> &terms) {
+  terms.clear();
+  auto add = [&](int c0, int s0, int a0, int b0, int z0, int c1, int s1, int a1, int b1, int z1) {
+    terms.insert(terms.end(), {c0, s0, a0, b0, z0, c1, s1, a1, b1, z1});
   };
   for (int comp = 0; comp < 3; ++comp)
     for (int d = 0; d < k; ++d)
       for (int a = 0; a <= d; ++a)
-        for (int b = 0; b <= d - a; ++b) term(i++, comp, 1.0, a, b, d - a - b);
-  int d = k - 1;
+        for (int b = 0; b <= d - a; ++b) add(comp, 1, a, b, d - a - b, -1, 0, 0, 0, 0);
+  const int d = k - 1;
   for (int fam = 0; fam < 2; ++fam)
     for (int a = 0; a <= d; ++a)
       for (int b = 0; b <= d - a; ++b) {
-        int c = d - a - b;
-        if (fam == 0) { term(i, 0, -1.0, a, b + 1, c); term(i, 1, 1.0, a + 1, b, c); }
-        else { term(i, 0, -1.0, a, b, c + 1); term(i, 2, 1.0, a + 1, b, c); }
-        ++i;
+        const int c = d - a - b;
+        if (fam == 0)
+          add(0, -1, a, b + 1, c, 1, 1, a + 1, b, c);
+        else
+          add(0, -1, a, b, c + 1, 2, 1, a + 1, b, c);
       }
   for (int b = 0; b <= d; ++b) {
-    int c = d - b;
-    term(i, 1, -1.0, 0, b, c + 1);
-    term(i, 2, 1.0, 0, b + 1, c);
-    ++i;
+    const int c = d - b;
+    add(1, -1, 0, b, c + 1, 2, 1, 0, b + 1, c);
   }
+}
+
+const double *nedelec_coefficients(int k) {
+  return (k >= 1 && k <= FFG_NEDELEC_TABLE_MAX_ORDER) ? kNedelecCoefficientTables[k] : nullptr;
+}
+
+bool nedelec_eval(int k, const double *pt, double *val, double *curl) {
+  if (k < 1 || k > FFG_NEDELEC_TABLE_MAX_ORDER) return false;
+  const int n = nedelec_dof_count(k);
+  std::vector<int> terms;
+  nedelec_candidate_terms(k, terms);
+  std::vector<double> cv(3 * n, 0.0), cc(3 * n, 0.0);
+  for (int cand = 0; cand < n; ++cand)
+    for (int t = 0; t < 2; ++t) {
+      const int *tm = &terms[10 * (size_t)cand + 5 * t];
+      const int comp = tm[0];
+      if (comp < 0) continue;
+      const double coef = tm[1];
+      const int pw[3] = {tm[2], tm[3], tm[4]};
+      cv[3 * cand + comp] += coef * ipow(pt[0], pw[0]) * ipow(pt[1], pw[1]) * ipow(pt[2], pw[2]);
+      double der[3];
+      for (int dd = 0; dd < 3; ++dd) {
+        if (pw[dd] == 0) { der[dd] = 0.0; continue; }
+        int r[3] = {pw[0], pw[1], pw[2]};
+        r[dd] -= 1;
+        der[dd] = coef * pw[dd] * ipow(pt[0], r[0]) * ipow(pt[1], r[1]) * ipow(pt[2], r[2]);
+      }
+      double *cu = &cc[3 * cand];
+      if (comp == 0) { cu[1] += der[2]; cu[2] -= der[1]; }
+      if (comp == 1) { cu[0] -= der[2]; cu[2] += der[0]; }
+      if (comp == 2) { cu[0] += der[1]; cu[1] -= der[0]; }
+    }
   const double *C = kNedelecCoefficientTables[k];
   for (int bf = 0; bf < n; ++bf)
     for (int a = 0; a < 3; ++a) {

@@ -79,13 +79,15 @@ struct Problem {
   int *err = nullptr;
   int *err_host = nullptr;   // pinned: degenerate-cell flag of a deferred check
   bool batch_pending = false;  // enqueued by ffg_problem_solve_batch, not yet collected
+  EvalTables eval;           // evaluator tables, built on the first evaluate / probe
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   ~Problem() {
     void *ptrs[] = {dt.cells, dt.gd, dt.edge_sign, dt.face_perm, dt.free_index, dt.inc_ptr,
                     dt.inc_cell, dt.inc_local, dt.slot, dt.ref, dt.load_basis, dt.face_blocks,
                     csc_col_ptr, csc_row, csc_val, geo, cell_rhs, elem, rhs, x, full, in_vertices,
-                    in_cell_a, in_cell_b, in_samples, in_g, free_dofs, err};
+                    in_cell_a, in_cell_b, in_samples, in_g, free_dofs, err, eval.lag_idx,
+                    eval.terms, eval.coef};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     free_sell(S);
@@ -529,6 +531,166 @@ void ffg_problem_phase_times(int handle, double *seconds, int *status) {
   if (!P) { *status = FFG_BAD_HANDLE; return; }
   if (!seconds) { *status = FFG_INVALID_INPUT; return; }
   for (int i = 0; i < 6; ++i) seconds[i] = P->work.phase_seconds[i];
+  *status = FFG_OK;
+}
+
+static int ensure_eval_tables(Problem &P) {
+  const Topology &t = P.topo;
+  if (t.family == FFG_TETRA_LAGRANGE && !P.eval.lag_idx) {
+    std::vector<int> idx;
+    std::vector<double> nodes;
+    lagrange_indices(t.degree, idx, nodes);
+    return upload(&P.eval.lag_idx, idx);
+  }
+  if (t.family == FFG_TETRA_NEDELEC && !P.eval.terms) {
+    std::vector<int> terms;
+    nedelec_candidate_terms(t.degree, terms);
+    const double *C = nedelec_coefficients(t.degree);
+    if (!C) return FFG_INVALID_INPUT;
+    std::vector<double> coef(C, C + (size_t)t.nb * t.nb);
+    int st = upload(&P.eval.terms, terms);
+    return st ? st : upload(&P.eval.coef, coef);
+  }
+  return FFG_OK;
+}
+
+// Host or device staging of the evaluation inputs; outputs copied back when
+// the caller passed host arrays.
+struct EvalStaging {
+  double *vertices = nullptr, *u = nullptr, *points = nullptr, *values = nullptr,
+         *derivs = nullptr;
+  int *cells = nullptr, *flags = nullptr;
+  ~EvalStaging() {
+    void *ptrs[] = {vertices, u, points, values, derivs, cells, flags};
+    for (void *p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+void ffg_problem_evaluate(int handle, const double *vertices, const double *solution,
+                          int n_queries, const int *cells, const double *points, int point_kind,
+                          double *values, double *derivatives, int *query_status, int memory,
+                          void *stream, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const Topology &t = P->topo;
+  if (t.family == FFG_TRIANGLE_P1 || n_queries < 0 || !vertices || !solution ||
+      (n_queries > 0 && (!cells || !points || !values || !derivatives)) ||
+      (point_kind != FFG_POINT_REFERENCE && point_kind != FFG_POINT_PHYSICAL)) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  int st = ensure_eval_tables(*P);
+  if (st) { *status = st; return; }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int wv = t.family == FFG_TETRA_NEDELEC ? 3 : 1;
+  const size_t nq = (size_t)n_queries;
+  EvalStaging S;
+  const double *dv = vertices, *du = solution, *dp = points;
+  const int *dc = cells;
+  double *dval = values, *dder = derivatives;
+  int *dstat = query_status;
+  if (memory == 0) {
+    const size_t vb = sizeof(double) * 3 * (size_t)t.n_vertices;
+    if ((st = dalloc(&S.vertices, 3 * (size_t)t.n_vertices)) || (st = dalloc(&S.u, t.n_dofs)) ||
+        (st = dalloc(&S.points, 3 * nq)) || (st = dalloc(&S.cells, nq)) ||
+        (st = dalloc(&S.values, wv * nq)) || (st = dalloc(&S.derivs, 3 * nq)) ||
+        (st = dalloc(&S.flags, nq))) {
+      *status = st;
+      return;
+    }
+    if (cudaMemcpyAsync(S.vertices, vertices, vb, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(S.u, solution, sizeof(double) * t.n_dofs, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        (nq && cudaMemcpyAsync(S.points, points, sizeof(double) * 3 * nq, cudaMemcpyHostToDevice,
+                               s) != cudaSuccess) ||
+        (nq && cudaMemcpyAsync(S.cells, cells, sizeof(int) * nq, cudaMemcpyHostToDevice, s) !=
+                   cudaSuccess)) {
+      *status = FFG_CUDA_ERROR;
+      return;
+    }
+    dv = S.vertices; du = S.u; dp = S.points; dc = S.cells;
+    dval = S.values; dder = S.derivs; dstat = S.flags;
+  }
+  if (cudaMemsetAsync(P->err, 0, sizeof(int), s) != cudaSuccess) { *status = FFG_CUDA_ERROR; return; }
+  st = evaluate_solution(t, P->dt, P->eval, dv, du, n_queries, dc, dp,
+                         point_kind == FFG_POINT_PHYSICAL ? 1 : 0, dval, dder, dstat, P->err, s);
+  if (st) { *status = st; return; }
+  int herr = 0;
+  if (cudaMemcpyAsync(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  if (memory == 0 && nq) {
+    if (cudaMemcpyAsync(values, S.values, sizeof(double) * wv * nq, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(derivatives, S.derivs, sizeof(double) * 3 * nq, cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess ||
+        (query_status && cudaMemcpyAsync(query_status, S.flags, sizeof(int) * nq,
+                                         cudaMemcpyDeviceToHost, s) != cudaSuccess)) {
+      *status = FFG_CUDA_ERROR;
+      return;
+    }
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) { *status = FFG_CUDA_ERROR; return; }
+  *status = herr ? herr : FFG_OK;
+}
+
+void ffg_problem_probe(int handle, const double *vertices, const double *solution, int n_points,
+                       const double *points, int mode, double *values, double *derivatives,
+                       int *counts, int memory, void *stream, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const Topology &t = P->topo;
+  if (t.family == FFG_TRIANGLE_P1 || n_points < 0 || !vertices || !solution ||
+      (n_points > 0 && (!points || !values || !derivatives || !counts)) ||
+      (mode != FFG_PROBE_AVERAGE && mode != FFG_PROBE_FIRST)) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  int st = ensure_eval_tables(*P);
+  if (st) { *status = st; return; }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int wv = t.family == FFG_TETRA_NEDELEC ? 3 : 1;
+  const size_t np = (size_t)n_points;
+  EvalStaging S;
+  const double *dv = vertices, *du = solution, *dp = points;
+  double *dval = values, *dder = derivatives;
+  int *dcnt = counts;
+  if (memory == 0) {
+    if ((st = dalloc(&S.vertices, 3 * (size_t)t.n_vertices)) || (st = dalloc(&S.u, t.n_dofs)) ||
+        (st = dalloc(&S.points, 3 * np)) || (st = dalloc(&S.values, wv * np)) ||
+        (st = dalloc(&S.derivs, 3 * np)) || (st = dalloc(&S.flags, np))) {
+      *status = st;
+      return;
+    }
+    if (cudaMemcpyAsync(S.vertices, vertices, sizeof(double) * 3 * (size_t)t.n_vertices,
+                        cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(S.u, solution, sizeof(double) * t.n_dofs, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        (np && cudaMemcpyAsync(S.points, points, sizeof(double) * 3 * np, cudaMemcpyHostToDevice,
+                               s) != cudaSuccess)) {
+      *status = FFG_CUDA_ERROR;
+      return;
+    }
+    dv = S.vertices; du = S.u; dp = S.points;
+    dval = S.values; dder = S.derivs; dcnt = S.flags;
+  }
+  st = probe_solution(t, P->dt, P->eval, dv, du, n_points, dp, mode == FFG_PROBE_FIRST ? 1 : 0,
+                      dval, dder, dcnt, s);
+  if (st) { *status = st; return; }
+  if (memory == 0 && np) {
+    if (cudaMemcpyAsync(values, S.values, sizeof(double) * wv * np, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(derivatives, S.derivs, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess ||
+        cudaMemcpyAsync(counts, S.flags, sizeof(int) * np, cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess) {
+      *status = FFG_CUDA_ERROR;
+      return;
+    }
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) { *status = FFG_CUDA_ERROR; return; }
   *status = FFG_OK;
 }
 

@@ -76,6 +76,13 @@ void lagrange_indices(int p, std::vector<int> &idx, std::vector<double> &nodes);
 void lagrange_eval(int p, const std::vector<int> &idx, const double *pt, double *val, double *grad);
 int nedelec_dof_count(int k);
 bool nedelec_eval(int k, const double *pt, double *val, double *curl);
+// The candidate vector monomials of the order-k first-kind space
+// (tetra_nedelec_arbitrary_order.f90:318-396): per candidate two terms of
+// (component, sign, x power, y power, z power), component -1 for an unused
+// term.  The basis is the candidates times nedelec_coefficients(k)
+// (candidate-major, n x n column-major by basis function).
+void nedelec_candidate_terms(int k, std::vector<int> &terms);
+const double *nedelec_coefficients(int k);
 const double *face_transform_table(int k, int perm_index);
 
 // Reference tensors for the per-cell contraction.
@@ -255,5 +262,29 @@ int nedelec_vjp(const Topology &t, const ElementTables &tab, const DeviceTopolog
                 const int64_t *col_ptr, const int *row_idx, const double *vertices,
                 const double *values_bar, double ca, double cb, double *elem,
                 double *vertices_bar, double *coef_bar, int *err, cudaStream_t s);
+
+// --------------------------------------------------- evaluation and probes
+// Device tables of the solution evaluators (kernels_probe.cu), built on first use.
+struct EvalTables {
+  int *lag_idx = nullptr;  // Lagrange: 4 barycentric indices per basis function
+  int *terms = nullptr;    // Nedelec: nedelec_candidate_terms
+  double *coef = nullptr;  // Nedelec: nedelec_coefficients
+};
+// Value and derivative (Lagrange gradient / Nedelec curl) of the solution u
+// (device, n_dofs) at n_queries (cell, point) pairs, points reference or
+// physical; values hold 1 (Lagrange) or 3 (Nedelec) entries per query,
+// derivs 3, qstatus (nullable) 0 or FFG_INVALID_INPUT per query.  err is set
+// when the Lagrange mesh holds a degenerate cell.  Asynchronous on s.
+int evaluate_solution(const Topology &t, const DeviceTopology &dt, const EvalTables &et,
+                      const double *vertices, const double *u, int n_queries, const int *qcell,
+                      const double *qpoint, int physical, double *values, double *derivs,
+                      int *qstatus, int *err, cudaStream_t s);
+// Point location over all cells and the evaluation there: the average over
+// the containing cells, or the first containing cell when first_only;
+// counts per point (0 none, -1 rejected by the basis's point test).
+// Returns once done.
+int probe_solution(const Topology &t, const DeviceTopology &dt, const EvalTables &et,
+                   const double *vertices, const double *u, int n_points, const double *points,
+                   int first_only, double *values, double *derivs, int *counts, cudaStream_t s);
 
 }  // namespace ffg

@@ -336,6 +336,46 @@ void ffg_problem_solve_batch(int count, const int *handles, const double *const 
  * assembly to the end of the batch's solve). */
 void ffg_problem_batch_stats(int handle, ffg_solver_stats *stats, int *status);
 
+/* ------------------------------------------------- evaluation and probes */
+
+#define FFG_POINT_REFERENCE 0 /* points are reference coordinates of the query's cell */
+#define FFG_POINT_PHYSICAL 1  /* physical points, mapped back by the cell's inverse
+                                 Jacobian (invert_tetra_affine_map,
+                                 src/geometry/tetra_affine_map.f90:15-33) */
+#define FFG_PROBE_AVERAGE 0   /* mean over every containing cell, in cell order */
+#define FFG_PROBE_FIRST 1     /* the first containing cell */
+
+/* Batched solution evaluation on a problem's mesh (tetrahedral families).
+ * Lagrange: evaluate_tetra_lagrange_solution_prepared and _at_point
+ * (src/solvers/fortfem_tetra_lagrange_solver_3d.f90:491-528, :305-325) -
+ * values[q] and the physical gradient derivatives[3q..3q+2]; the call fails
+ * with FFG_INVALID_INPUT when a cell of the mesh is degenerate, as the
+ * reference's evaluator initialisation does (:437-489).  Nedelec: the field
+ * values[3q..] and curl derivatives[3q..] of the oriented local DoFs on the
+ * query's cell (the per-cell evaluation of evaluate_box_solution_order,
+ * src/solvers/fortfem_magnetic_box_3d.f90:313-334).  solution holds n_dofs
+ * entries (all DoFs, as ffg_problem_solve returns them).  query_status
+ * (nullable) receives 0, or FFG_INVALID_INPUT for a cell index out of range,
+ * a degenerate cell or a point outside the reference cell (the basis
+ * evaluation's -64 eps test).  memory = 1: every array is device memory and
+ * the work runs on `stream`; the call returns when it is done. */
+void ffg_problem_evaluate(int handle, const double *vertices, const double *solution,
+                          int n_queries, const int *cells, const double *points, int point_kind,
+                          double *values, double *derivatives, int *query_status, int memory,
+                          void *stream, int *status);
+
+/* Point probes without a cell hint: evaluate_box_solution_order
+ * (fortfem_magnetic_box_3d.f90:269-343, FFG_PROBE_AVERAGE) and probe_box_az /
+ * probe_box_curl (:345-440, FFG_PROBE_FIRST).  A cell contains a point when
+ * det > 0 and the point's reference coordinates are >= -1e-12 with sum <=
+ * 1 + 1e-12.  Outputs as ffg_problem_evaluate; counts[q] is the number of
+ * cells that contributed (0: the point lies in no cell, values zero; -1: the
+ * basis evaluation rejected it on a containing cell, where the reference's
+ * probe fails).  Lagrange problems are probed the same way. */
+void ffg_problem_probe(int handle, const double *vertices, const double *solution, int n_points,
+                       const double *points, int mode, double *values, double *derivatives,
+                       int *counts, int memory, void *stream, int *status);
+
 /* Release a problem handle (fortfem_factor_free, src/bindings/fortfem_capi_solver.f90:108-124). */
 void ffg_problem_free(int handle, int *status);
 

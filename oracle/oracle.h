@@ -79,6 +79,20 @@ int or_lagrange_dirichlet_faithful(int degree, int n_vertices, const double *ver
 int or_lagrange_dirichlet(int degree, int n_vertices, const double *vertices, int n_tets,
                           const int *tets, uint8_t *constrained, double *node_points);
 
+/* ---- solution probes (evaluation at reference / physical points, point location) ---- */
+int or_lagrange_evaluate_solution(int n_vertices, const double *vertices, int n_tets,
+                                  const int *tets, int degree, int n_dofs, const double *solution,
+                                  int cell, const double *reference_point, double *value,
+                                  double *gradient);
+int or_lagrange_evaluate_solution_at_point(int n_vertices, const double *vertices, int n_tets,
+                                           const int *tets, int degree, int n_dofs,
+                                           const double *solution, int cell, const double *point,
+                                           double *value, double *gradient);
+/* mode 0: average over every containing cell; 1: the first containing cell */
+int or_lagrange_probe(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                      int degree, int n_dofs, const double *solution, const double *point,
+                      int mode, double *value, double *gradient, int *count);
+
 /* ---- P1 triangles ---- */
 int or_p1_dense_matrix(int n_vertices, const double *vertices, int n_triangles, const int *triangles,
                        double mass, double stiffness, double *matrix /* n x n col-major */);
@@ -148,6 +162,13 @@ int or_nedelec_csc_jvp(int n_vertices, const double *vertices, int n_tets, const
 int or_nedelec_csc_vjp(int n_vertices, const double *vertices, int n_tets, const int *tets,
                        int order, double curl, double mass, int64_t nnz, const double *values_bar,
                        double *vertices_bar, double *curl_bar, double *mass_bar);
+int or_nedelec_evaluate_solution(int n_vertices, const double *vertices, int n_tets,
+                                 const int *tets, int order, int n_dofs, const double *solution,
+                                 int cell, const double *reference_point, double *value /*3*/,
+                                 double *curl /*3*/);
+int or_nedelec_probe(int n_vertices, const double *vertices, int n_tets, const int *tets, int order,
+                     int n_dofs, const double *solution, const double *point, int mode,
+                     double *value /*3*/, double *curl /*3*/, int *count);
 int or_nedelec_load_samples(int n_vertices, const double *vertices, int n_tets, const int *tets,
                             int order, const double *source_values /* 3 x n_q x T */, double *rhs);
 int or_nedelec_load_points(int n_vertices, const double *vertices, int n_tets, const int *tets,

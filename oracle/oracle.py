@@ -548,3 +548,49 @@ def pec_mask(k, tets, faithful=False):
     con = np.zeros(n, np.uint8)
     _check(_call("or_pec_mask", k, len(tets), tets, int(faithful), con), "pec_mask")
     return con.astype(bool)
+
+
+# ------------------------------------------------------------ solution probes
+
+def lagrange_evaluate_solution(vertices, tets, p, solution, cell, point, physical=False):
+    """(value, gradient) of evaluate_tetra_lagrange_solution (reference point)
+    or evaluate_tetra_lagrange_solution_at_point (physical point); None when
+    the reference rejects the query."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    u = _arr(solution, np.float64)
+    val = C.c_double(0.0); g = np.zeros(3)
+    name = "or_lagrange_evaluate_solution_at_point" if physical else "or_lagrange_evaluate_solution"
+    st = _call(name, len(vertices), vertices, len(tets), tets, p, len(u), u, int(cell),
+               _arr(point, np.float64), C.byref(val), g)
+    return None if st else (val.value, g)
+
+
+def lagrange_probe(vertices, tets, p, solution, point, mode=0):
+    """(value, gradient, count) of the all-cell point probe."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    u = _arr(solution, np.float64)
+    val = C.c_double(0.0); g = np.zeros(3); cnt = C.c_int(0)
+    _call("or_lagrange_probe", len(vertices), vertices, len(tets), tets, p, len(u), u,
+          _arr(point, np.float64), int(mode), C.byref(val), g, C.byref(cnt))
+    return val.value, g, cnt.value
+
+
+def nedelec_evaluate_solution(vertices, tets, k, solution, cell, point):
+    """(value, curl) at a reference point of one cell; None when rejected."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    u = _arr(solution, np.float64)
+    v = np.zeros(3); c = np.zeros(3)
+    st = _call("or_nedelec_evaluate_solution", len(vertices), vertices, len(tets), tets, k, len(u),
+               u, int(cell), _arr(point, np.float64), v, c)
+    return None if st else (v, c)
+
+
+def nedelec_probe(vertices, tets, k, solution, point, mode=0):
+    """(value, curl, count) of evaluate_box_solution_order (mode 0) or the
+    first-containing-cell probes (mode 1)."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    u = _arr(solution, np.float64)
+    v = np.zeros(3); c = np.zeros(3); cnt = C.c_int(0)
+    _call("or_nedelec_probe", len(vertices), vertices, len(tets), tets, k, len(u), u,
+          _arr(point, np.float64), int(mode), v, c, C.byref(cnt))
+    return v, c, cnt.value

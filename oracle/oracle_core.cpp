@@ -973,6 +973,140 @@ int or_lagrange_dirichlet(int p, int nv, const double *verts, int nt, const int 
   return lagrange_dirichlet_impl(p, nv, verts, nt, tets, constrained, node_points, false);
 }
 
+// ---------------------------------------------------------- solution probes
+// evaluate_tetra_lagrange_solution, src/solvers/fortfem_tetra_lagrange_solver_3d.f90:131-150:
+// initialize_tetra_lagrange_solution_evaluator (:437-489: every cell valid,
+// solution sized to the DoF map) then evaluate_tetra_lagrange_solution_prepared
+// (:491-528: value = sum u_i phi_i, gradient = J^-T sum u_i grad phi_i).
+int or_lagrange_evaluate_solution(int nv, const double *verts, int nt, const int *tets, int p,
+                                  int n_dofs, const double *u, int cell, const double *xi,
+                                  double *value, double *grad) {
+  *value = 0.0;
+  grad[0] = grad[1] = grad[2] = 0.0;
+  if (nt < 1 || p < 1 || p > 4) return 1;
+  for (int64_t i = 0; i < 4LL * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int nb = or_lagrange_dof_count(p);
+  std::vector<int> gd((size_t)nb * nt);
+  int ng = 0;
+  if (or_lagrange_dof_map(p, nt, tets, gd.data(), &ng)) return 1;
+  for (int c = 0; c < nt; ++c) {
+    double v[12], J[9];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * c + n] + d];
+    tetra_jacobian(v, J);
+    if (!valid_jacobian(J, det3(J))) return 1;
+  }
+  if (cell < 0 || cell >= nt || n_dofs != ng) return 1;
+  // evaluate_tetra_lagrange rejects barycentric coordinates below -64 eps (:88-89)
+  const double bary[4] = {1.0 - (xi[0] + xi[1] + xi[2]), xi[0], xi[1], xi[2]};
+  for (double b : bary)
+    if (b < -64.0 * kEps) return 1;
+  std::vector<double> val(nb), g(3 * nb);
+  if (or_lagrange_evaluate(p, xi, val.data(), g.data())) return 1;
+  double v[12], J[9], Ji[9];
+  for (int n = 0; n < 4; ++n)
+    for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * cell + n] + d];
+  tetra_jacobian(v, J);
+  inv3(J, det3(J), Ji);
+  double rg[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < nb; ++d) {
+    const double ud = u[gd[(size_t)nb * cell + d]];
+    *value += ud * val[d];
+    for (int a = 0; a < 3; ++a) rg[a] += ud * g[3 * d + a];
+  }
+  // matmul(transpose(inverse_jacobian), reference_gradient)
+  for (int i = 0; i < 3; ++i) grad[i] = Ji[3 * i] * rg[0] + Ji[3 * i + 1] * rg[1] + Ji[3 * i + 2] * rg[2];
+  return 0;
+}
+
+// evaluate_tetra_lagrange_solution_at_point, same file :305-325, with
+// invert_tetra_affine_map (src/geometry/tetra_affine_map.f90:15-33).
+int or_lagrange_evaluate_solution_at_point(int nv, const double *verts, int nt, const int *tets,
+                                           int p, int n_dofs, const double *u, int cell,
+                                           const double *point, double *value, double *grad) {
+  *value = 0.0;
+  grad[0] = grad[1] = grad[2] = 0.0;
+  if (cell < 0 || cell >= nt) return 1;
+  for (int n = 0; n < 4; ++n)
+    if (tets[4 * cell + n] < 0 || tets[4 * cell + n] >= nv) return 1;
+  double v[12], J[9], Ji[9];
+  for (int n = 0; n < 4; ++n)
+    for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * cell + n] + d];
+  tetra_jacobian(v, J);
+  const double det = det3(J);
+  if (!valid_jacobian(J, det)) return 1;
+  inv3(J, det, Ji);
+  double xi[3];
+  for (int i = 0; i < 3; ++i) {
+    double s = 0.0;
+    for (int k = 0; k < 3; ++k) s += Ji[i + 3 * k] * (point[k] - v[k]);
+    xi[i] = s;
+  }
+  return or_lagrange_evaluate_solution(nv, verts, nt, tets, p, n_dofs, u, cell, xi, value, grad);
+}
+
+// Point probe over all cells for a Lagrange solution, the loop of
+// evaluate_box_solution_order (src/solvers/fortfem_magnetic_box_3d.f90:269-343)
+// with the scalar basis: every cell with det > 0 whose reference coordinates
+// of the point are >= -1e-12 with sum <= 1 + 1e-12 contributes (value,
+// gradient); mode 0 averages them in cell order, mode 1 takes the first.
+// *count is the number of contributing cells (0: none; -1: a contributing
+// cell rejected by the basis evaluation's -64 eps test).
+int or_lagrange_probe(int nv, const double *verts, int nt, const int *tets, int p, int n_dofs,
+                      const double *u, const double *point, int mode, double *value,
+                      double *grad, int *count) {
+  *value = 0.0;
+  grad[0] = grad[1] = grad[2] = 0.0;
+  *count = 0;
+  const int nb = or_lagrange_dof_count(p);
+  std::vector<int> gd((size_t)nb * nt);
+  int ng = 0;
+  if (or_lagrange_dof_map(p, nt, tets, gd.data(), &ng) || n_dofs != ng) return 1;
+  std::vector<double> val(nb), g(3 * nb);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  int found = 0;
+  for (int c = 0; c < nt; ++c) {
+    double v[12], J[9], Ji[9];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * c + n] + d];
+    tetra_jacobian(v, J);
+    const double det = det3(J);
+    if (det <= 0.0) continue;
+    inv3(J, det, Ji);
+    double xi[3];
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s += Ji[i + 3 * k] * (point[k] - v[k]);
+      xi[i] = s;
+    }
+    if (xi[0] < -1.0e-12 || xi[1] < -1.0e-12 || xi[2] < -1.0e-12) continue;
+    if (xi[0] + xi[1] + xi[2] > 1.0 + 1.0e-12) continue;
+    if (1.0 - (xi[0] + xi[1] + xi[2]) < -64.0 * kEps || xi[0] < -64.0 * kEps ||
+        xi[1] < -64.0 * kEps || xi[2] < -64.0 * kEps) {
+      *count = -1;
+      return 1;
+    }
+    or_lagrange_evaluate(p, xi, val.data(), g.data());
+    double val_c = 0.0, rg[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < nb; ++d) {
+      const double ud = u[gd[(size_t)nb * c + d]];
+      val_c += ud * val[d];
+      for (int a = 0; a < 3; ++a) rg[a] += ud * g[3 * d + a];
+    }
+    acc[0] += val_c;
+    for (int i = 0; i < 3; ++i)
+      acc[1 + i] += Ji[3 * i] * rg[0] + Ji[3 * i + 1] * rg[1] + Ji[3 * i + 2] * rg[2];
+    ++found;
+    if (mode == 1) break;
+  }
+  *count = found;
+  if (found < 1) return 1;
+  *value = acc[0] / found;
+  for (int i = 0; i < 3; ++i) grad[i] = acc[1 + i] / found;
+  return 0;
+}
+
 // --------------------------------------------------------------- P1 triangles
 // assemble_scalar_p1_matrix, src/fortfem_forms_simple.f90:1678-1728 (dense).
 static int p1_local(const double *verts, const int *tri, double mass, double stiff, double *local) {

@@ -756,6 +756,126 @@ int or_nedelec_csc_vjp(int nv, const double *verts, int nt, const int *tets, int
   return 0;
 }
 
+// ---------------------------------------------------------- solution probes
+namespace {
+// The oriented field of a solution on one cell at reference point xi: local
+// DoFs T u(gd), basis values / curls, covariant map (the body of
+// evaluate_box_solution_order, fortfem_magnetic_box_3d.f90:313-334).
+int nedelec_cell_field(int k, const double *J, double det, const double *Ji, const int *gd,
+                       const int *eo, const int *fp, const double *u, const double *xi,
+                       double *value, double *curl) {
+  const int n = or_nedelec_dof_count(k);
+  std::vector<double> T((size_t)n * n), ld(n), rv(3 * n), rc(3 * n), pv(3 * n), pc(3 * n);
+  if (or_nedelec_transform(k, eo, fp, T.data())) return 1;
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += T[i + (size_t)n * j] * u[gd[j]];
+    ld[i] = s;
+  }
+  if (or_nedelec_evaluate(k, xi, rv.data(), rc.data())) return 1;
+  covariant(J, det, Ji, n, rv.data(), rc.data(), pv.data(), pc.data());
+  for (int a = 0; a < 3; ++a) {
+    double s = 0.0, t = 0.0;
+    for (int i = 0; i < n; ++i) {
+      s += pv[3 * i + a] * ld[i];
+      t += pc[3 * i + a] * ld[i];
+    }
+    value[a] = s;
+    curl[a] = t;
+  }
+  return 0;
+}
+}  // namespace
+
+// Field and curl of a Nedelec solution at a reference point of one cell (the
+// per-cell evaluation of evaluate_box_solution_order); the cell must pass
+// tetra_geometry's test.
+int or_nedelec_evaluate_solution(int nv, const double *verts, int nt, const int *tets, int k,
+                                 int n_dofs, const double *u, int cell, const double *xi,
+                                 double *value, double *curl) {
+  for (int a = 0; a < 3; ++a) value[a] = curl[a] = 0.0;
+  if (k < 1 || nt < 1 || cell < 0 || cell >= nt) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int nb = or_nedelec_dof_count(k);
+  int ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  if (n_dofs != ng) return 1;
+  double v[12], J[9], Ji[9], det;
+  for (int n = 0; n < 4; ++n)
+    for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * cell + n] + d];
+  if (!tetra_geometry(v, J, &det)) return 1;
+  inv3(J, det, Ji);
+  return nedelec_cell_field(k, J, det, Ji, gd.data() + (size_t)nb * cell, eo.data() + 6 * cell,
+                            fp.data() + 12 * cell, u, xi, value, curl);
+}
+
+// evaluate_box_solution_order, src/solvers/fortfem_magnetic_box_3d.f90:269-343
+// (mode 0: the average over every containing cell, in cell order) and
+// probe_box_az / probe_box_curl, :345-440 (mode 1: the first containing
+// cell).  A cell contains the point when det > 0 and its reference
+// coordinates are >= -1e-12 with sum <= 1 + 1e-12.  *count = number of
+// contributing cells; -1 when evaluate_tetra_nedelec_first_kind rejects the
+// point on a containing cell (its -64 eps test), which fails the probe.
+int or_nedelec_probe(int nv, const double *verts, int nt, const int *tets, int k, int n_dofs,
+                     const double *u, const double *point, int mode, double *value, double *curl,
+                     int *count) {
+  for (int a = 0; a < 3; ++a) value[a] = curl[a] = 0.0;
+  *count = 0;
+  if (k < 1 || nt < 1) return 1;
+  const int nb = or_nedelec_dof_count(k);
+  int ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  if (n_dofs != ng) return 1;
+  double acc_v[3] = {0.0, 0.0, 0.0}, acc_c[3] = {0.0, 0.0, 0.0};
+  int found = 0;
+  const double tol = 64.0 * kEps;
+  for (int c = 0; c < nt; ++c) {
+    double v[12], J[9], Ji[9];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * c + n] + d];
+    tetra_jacobian(v, J);
+    const double det = det3(J);
+    if (det <= 0.0) continue;
+    inv3(J, det, Ji);
+    double xi[3];
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.0;
+      for (int q = 0; q < 3; ++q) s += Ji[i + 3 * q] * (point[q] - v[q]);
+      xi[i] = s;
+    }
+    if (xi[0] < -1.0e-12 || xi[1] < -1.0e-12 || xi[2] < -1.0e-12) continue;
+    if (xi[0] + xi[1] + xi[2] > 1.0 + 1.0e-12) continue;
+    if (xi[0] < -tol || xi[1] < -tol || xi[2] < -tol || xi[0] + xi[1] + xi[2] > 1.0 + tol) {
+      *count = -1;
+      return 1;
+    }
+    double fv[3], fc[3];
+    if (nedelec_cell_field(k, J, det, Ji, gd.data() + (size_t)nb * c, eo.data() + 6 * c,
+                           fp.data() + 12 * c, u, xi, fv, fc))
+      return 1;
+    for (int a = 0; a < 3; ++a) {
+      acc_v[a] += fv[a];
+      acc_c[a] += fc[a];
+    }
+    ++found;
+    if (mode == 1) break;
+  }
+  *count = found;
+  if (found < 1) return 1;
+  for (int a = 0; a < 3; ++a) {
+    value[a] = acc_v[a] / found;
+    curl[a] = acc_c[a] / found;
+  }
+  return 0;
+}
+
 static int nedelec_load_rule(int k, RuleN &R) {
   // order 1: the 4-point rule (assemble_tetra_nedelec_load_element :2516-2553);
   // order >= 2: Duffy with q = 2k+2 (assemble_tetra_nedelec_load_element_order :547)

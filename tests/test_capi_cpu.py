@@ -30,6 +30,14 @@ def test_library_exports_every_header_symbol():
     assert sorted(K.exported_symbols()) == syms
 
 
+def test_python_constants_match_header():
+    text = open(os.path.join(ROOT, "include", "fortfem_gpu.h")).read()
+    defines = re.findall(r"#define\s+(FFG_[A-Z0-9_]+)\s+(-?\d+)", text)
+    assert len(defines) > 20
+    for name, value in defines:
+        assert getattr(K, name) == int(value), name
+
+
 def test_no_device_is_reported_not_faked():
     count = C.c_int(-1)
     st = C.c_int(0)

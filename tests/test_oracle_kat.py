@@ -416,3 +416,109 @@ def test_nedelec_csc_jvp_vjp_kat(k):
     lhs = vbar_in @ vdot
     rhs = np.sum(vbar * vd) + cbar * cd + mbar * md
     assert abs(lhs - rhs) < 3e-10 * max(1.0, abs(lhs), abs(rhs))
+
+
+# ---------------------------------------------------------- solution probes
+# test/test_tetra_lagrange_poisson_p_convergence.f90:11-19 (four cells around
+# an interior vertex), :133-157 (affine Dirichlet data reproduced to 1e-12 by
+# evaluate_tetra_lagrange_solution) and :159-181 (reaction with source 2 and
+# no essential boundary gives the constant 2, zero gradient).
+PROBE_TETS = np.array([[0, 1, 2, 4], [0, 3, 1, 4], [0, 2, 3, 4], [1, 3, 2, 4]], np.int32)
+PROBE_VERTS = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0.25, 0.25, 0.25]], float)
+
+
+def _oracle_lagrange_solve(p, stiffness, mass, source, boundary_fn):
+    v, t = PROBE_VERTS, PROBE_TETS
+    q = 2 * p + 4
+    n, cp, ri, val = oracle.lagrange_csc(v, t, p, 0, q, stiffness, mass)
+    pts = oracle.lagrange_quadrature_points(v, t, 0, q)
+    rhs = oracle.lagrange_load_samples(v, t, p, source(pts), 0, q)
+    con, nodes = oracle.lagrange_dirichlet(p, v, t)
+    if boundary_fn is None:
+        con[:] = False
+    g = np.where(con, boundary_fn(nodes) if boundary_fn else 0.0, 0.0)
+    nf, rcp, rri, rv, rr, free = oracle.reduce_constrained(n, cp, ri, val, rhs, con, g)
+    dense = oracle.csc_to_scipy(nf, rcp, rri, rv).toarray()
+    u = g.copy()
+    u[free] = np.linalg.solve(dense, rr)
+    return u
+
+
+def test_lagrange_evaluate_affine_and_reaction_kat():
+    affine = lambda x: 1.0 + x[..., 0] + 2.0 * x[..., 1] - 3.0 * x[..., 2]
+    u = _oracle_lagrange_solve(1, 1.0, 0.0, lambda x: 0.0 * x[..., 0], affine)
+    value, grad = oracle.lagrange_evaluate_solution(PROBE_VERTS, PROBE_TETS, 1, u, 0,
+                                                    [0.2, 0.3, 0.1])
+    assert abs(value - affine(np.array([0.225, 0.325, 0.025]))) < 1e-12
+    assert np.abs(grad - [1.0, 2.0, -3.0]).max() < 1e-12
+    u = _oracle_lagrange_solve(1, 0.0, 1.0, lambda x: 2.0 + 0.0 * x[..., 0], None)
+    value, grad = oracle.lagrange_evaluate_solution(PROBE_VERTS, PROBE_TETS, 1, u, 3,
+                                                    [0.2, 0.1, 0.3])
+    assert abs(value - 2.0) < 1e-12 and np.abs(grad).max() < 1e-12
+
+
+def lagrange_node_points(v, t, p):
+    """Physical location of every global Lagrange DoF (the cell's affine map of
+    its reference nodes)."""
+    gd, n = oracle.lagrange_dof_map(p, t)
+    _, ref_nodes = oracle.lagrange_indices(p)
+    out = np.zeros((n, 3))
+    for c in range(len(t)):
+        J = (v[t[c, 1:]] - v[t[c, 0]]).T
+        out[gd[c]] = v[t[c, 0]] + ref_nodes @ J.T
+    return out
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_lagrange_probe_reproduces_its_space(p):
+    # nodal interpolation of a degree-p polynomial is exact: every evaluation
+    # route returns the polynomial and its gradient
+    v, t = oracle.box_mesh([2, 2, 2])
+    f = lambda x: (1.0 + x[..., 0] - 2 * x[..., 1] + 0.5 * x[..., 2]) ** p
+    df = lambda x: p * (1.0 + x[0] - 2 * x[1] + 0.5 * x[2]) ** (p - 1) * np.array([1, -2, 0.5])
+    u = f(lagrange_node_points(v, t, p))
+    rng = np.random.default_rng(p)
+    for _ in range(5):
+        x = rng.uniform(0.05, 0.95, 3)
+        for mode in (0, 1):
+            val, g, cnt = oracle.lagrange_probe(v, t, p, u, x, mode)
+            assert cnt >= 1
+            assert abs(val - f(x)) < 1e-12 * max(1, abs(f(x)))
+            assert np.abs(g - df(x)).max() < 1e-10 * max(1, np.abs(df(x)).max())
+    # a vertex of the box lies in several cells; mode 0 counts them all
+    val, g, cnt = oracle.lagrange_probe(v, t, p, u, [0.5, 0.5, 0.5], 0)
+    assert cnt > 1 and abs(val - f(np.array([0.5, 0.5, 0.5]))) < 1e-12
+    # outside the mesh: no cell
+    assert oracle.lagrange_probe(v, t, p, u, [1.5, 0.5, 0.5], 0)[2] == 0
+
+
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_nedelec_probe_reproduces_its_space(k):
+    # the L2 projection of a field of the order-k space is the field itself:
+    # k = 1 holds a + b x x (curl 2b); order k holds every degree-(k-1) field
+    v, t = oracle.box_mesh([2, 2, 2])
+    a, b = np.array([0.3, -0.7, 1.1]), np.array([0.5, 0.2, -0.4])
+
+    def field(x):
+        extra = {1: np.zeros(3), 2: np.array([x[1], 0.0, x[0]]),
+                 3: np.array([x[1] * x[2], 0.0, x[0] ** 2])}[k]
+        return a + np.cross(b, x) + extra
+
+    def curl(x):
+        extra = {1: np.zeros(3), 2: np.array([0.0, -1.0, -1.0]),
+                 3: np.array([0.0, x[1] - 2 * x[0], -x[2]])}[k]
+        return 2 * b + extra
+
+    n, cp, ri, val = oracle.nedelec_csc(v, t, k, 0.0, 1.0)
+    pts = oracle.nedelec_load_points(v, t, k)
+    samples = np.array([[field(x) for x in cell] for cell in pts])
+    rhs = oracle.nedelec_load_samples(v, t, k, samples)
+    u = np.linalg.solve(oracle.csc_to_scipy(n, cp, ri, val).toarray(), rhs)
+    rng = np.random.default_rng(k)
+    for _ in range(4):
+        x = rng.uniform(0.05, 0.95, 3)
+        for mode in (0, 1):
+            fv, fc, cnt = oracle.nedelec_probe(v, t, k, u, x, mode)
+            assert cnt >= 1
+            assert np.abs(fv - field(x)).max() < 1e-9
+            assert np.abs(fc - curl(x)).max() < 1e-8
