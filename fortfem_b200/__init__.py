@@ -12,6 +12,7 @@ from .api import (CscMatrix, FortfemError, Problem, SolverOptions, SolverStats, 
                   assemble_tetra_lagrange_stiffness_csc, assemble_tetra_lagrange_stiffness_csc_jvp,
                   assemble_tetra_lagrange_stiffness_csc_vjp, assemble_tetra_nedelec_curl_mass_csc,
                   assemble_tetra_nedelec_curl_mass_csc_jvp, assemble_tetra_nedelec_curl_mass_csc_vjp,
+                  assemble_tetra_nedelec_curvilinear_pml_csc, assemble_tetra_nedelec_pml_csc,
                   assemble_tetra_nedelec_vector_load_samples, build_topology,
                   evaluate_tetra_lagrange_solution, probe_tetra_nedelec_solution,
                   generate_structured_tetra_box_mesh, solve_scalar_p1, solve_sparse,

@@ -91,6 +91,10 @@ SIGNATURES = {
         None, [i32, vp, i32, vp, i32, f64, f64, vp, f64, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curl_mass_csc_vjp": (
         None, [i32, vp, i32, vp, i32, f64, f64, i64, vp, vp, vp, vp, pi32]),
+    "ffg_assemble_tetra_nedelec_pml_csc": (
+        None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_assemble_tetra_nedelec_curvilinear_pml_csc": (
+        None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_problem_evaluate": (
         None, [i32, vp, vp, i32, vp, vp, i32, vp, vp, vp, i32, vp, pi32]),
     "ffg_problem_probe": (

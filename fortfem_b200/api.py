@@ -320,6 +320,49 @@ def assemble_tetra_nedelec_curl_mass_csc_vjp(mesh_vertices, tetrahedra, order, c
     return vbar, cb.value, mb.value, Status.of(st.value, "Tetrahedral Nedelec curl-mass VJP failed")
 
 
+def _pml_call(fn, v, t, order, stretch_pairs, wave_number, where):
+    lib = K.load()
+    nd = C.c_int(0)
+    nz = C.c_int64(0)
+    st = C.c_int(0)
+    args = [len(v), _ptr(v), len(t), _ptr(t), int(order), _ptr(stretch_pairs), float(wave_number)]
+    getattr(lib, fn)(*args, C.c_int64(0), C.byref(nd), C.byref(nz), None, None, None, C.byref(st))
+    if st.value not in (K.FFG_OK, K.FFG_CAPACITY):
+        return None, Status.of(st.value, where)
+    n = nd.value
+    cp = np.zeros(n + 1, np.int64)
+    ri = np.zeros(nz.value, np.int32)
+    val = np.zeros(2 * nz.value)
+    getattr(lib, fn)(*args, C.c_int64(nz.value), C.byref(nd), C.byref(nz), _ptr(cp), _ptr(ri),
+                     _ptr(val), C.byref(st))
+    if st.value:
+        return None, Status.of(st.value, where)
+    return CscMatrix(n, n, cp, ri, val.view(np.complex128)), Status()
+
+
+def assemble_tetra_nedelec_pml_csc(mesh_vertices, tetrahedra, order, stretch, wave_number):
+    """assemble_tetra_nedelec_pml_csc (src/assembly/assembly_tetra_nedelec_3d.f90:1613-1685):
+    stretch (T, 3) complex per cell.  Returns (CscMatrix with complex values, Status)."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    s = np.ascontiguousarray(np.asarray(stretch, np.complex128).reshape(len(t), 3))
+    return _pml_call("ffg_assemble_tetra_nedelec_pml_csc", v, t, order, s.view(np.float64),
+                     wave_number, "Complex tetrahedral Nedelec PML assembly failed")
+
+
+def assemble_tetra_nedelec_curvilinear_pml_csc(mesh_vertices, tetrahedra, order, stretch,
+                                               wave_number):
+    """assemble_tetra_nedelec_curvilinear_pml_csc (same file :1372-1444): stretch
+    (T, 3, 3) complex, stretch[t] the cell's matrix.  Returns (CscMatrix, Status)."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    s = np.asarray(stretch, np.complex128).reshape(len(t), 3, 3)
+    s = np.ascontiguousarray(np.transpose(s, (0, 2, 1)))  # column-major per cell
+    return _pml_call("ffg_assemble_tetra_nedelec_curvilinear_pml_csc", v, t, order,
+                     s.view(np.float64), wave_number,
+                     "Curvilinear tetrahedral Nedelec PML assembly failed")
+
+
 def assemble_tetra_nedelec_vector_load_samples(mesh_vertices, tetrahedra, order, source_values):
     """assemble_tetra_nedelec_vector_load_samples (assembly_tetra_nedelec_3d.f90:128-185).
     source_values: (T, n_q, 3) at the order's load points.  Returns (rhs, Status)."""

@@ -1205,6 +1205,92 @@ void ffg_assemble_tetra_nedelec_curl_mass_csc(int nv, const double *verts, int n
            cap, n_dofs, nnz, col_ptr, row_ind, values, status);
 }
 
+// Complex PML curl-curl CSC: the Nedelec element kernel on the real and on
+// the imaginary parts of the PML weights, each gathered by the column kernel.
+static void pml_csc(bool curvilinear, int nv, const double *verts, int nt, const int *tets,
+                    int order, const double *stretch, double wave, int64_t cap, int *n_dofs,
+                    int64_t *nnz, int64_t *col_ptr, int *row_ind, double *values, int *status) {
+  if (!verts || !stretch || !(wave > 0.0)) { *status = FFG_INVALID_INPUT; return; }
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  int st = create_problem(FFG_TETRA_NEDELEC, order, nv, nt, tets, 0, 0, FFG_BOUNDARY_NONE, nullptr,
+                          P, msg);
+  if (st) { *status = st; return; }
+  const Topology &t = P->topo;
+  if (n_dofs) *n_dofs = (int)t.n_dofs;
+  if (nnz) *nnz = t.nnz();
+  if (cap < t.nnz() || !col_ptr || !row_ind || !values) { *status = FFG_CAPACITY; return; }
+  const size_t sw = curvilinear ? 18 : 6;
+  const size_t nc = (size_t)nt, nz = (size_t)std::max<int64_t>(t.nnz(), 1);
+  double *dstretch = nullptr, *geo_re = nullptr, *geo_im = nullptr, *val_re = nullptr,
+         *val_im = nullptr, *out = nullptr;
+  auto release = [&]() {
+    for (double *p : {dstretch, geo_re, geo_im, val_re, val_im, out})
+      if (p) cudaFree(p);
+  };
+  if ((st = dalloc(&dstretch, sw * nc)) || (st = dalloc(&geo_re, 12 * nc)) ||
+      (st = dalloc(&geo_im, 12 * nc)) || (st = dalloc(&val_re, nz)) ||
+      (st = dalloc(&val_im, nz)) || (st = dalloc(&out, 2 * nz))) {
+    release();
+    *status = st;
+    return;
+  }
+  int herr = 0;
+  if (cudaMemcpy(P->in_vertices, verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemcpy(dstretch, stretch, sizeof(double) * sw * nc, cudaMemcpyHostToDevice) !=
+          cudaSuccess ||
+      cudaMemset(P->err, 0, sizeof(int)) != cudaSuccess) {
+    st = FFG_CUDA_ERROR;
+  } else {
+    st = launch_pml_weights(t, P->dt, P->in_vertices, dstretch, curvilinear, wave, geo_re, geo_im,
+                            P->err, 0);
+    for (int part = 0; part < 2 && !st; ++part) {
+      AssemblyInputs in;
+      in.vertices = P->in_vertices;
+      in.geo_override = part == 0 ? geo_re : geo_im;
+      st = launch_nedelec(t, P->tab, P->dt, in, P->elem, P->cell_rhs, P->err, 0);
+      if (!st)
+        st = launch_columns(t, P->tab, P->dt, in, P->geo, P->geo_stride, P->cell_rhs, P->elem,
+                            P->csc_col_ptr, P->csc_row, nullptr, part == 0 ? val_re : val_im,
+                            P->rhs, 0);
+    }
+    if (!st) st = launch_interleave(t.nnz(), val_re, val_im, out, 0);
+    if (!st) {
+      if (cudaMemcpy(&herr, P->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = FFG_CUDA_ERROR;
+      else if (herr)
+        st = herr;
+      else if (cudaMemcpy(values, out, sizeof(double) * 2 * (size_t)t.nnz(),
+                          cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = FFG_CUDA_ERROR;
+    }
+  }
+  release();
+  if (st) { *status = st; return; }
+  std::memcpy(col_ptr, t.col_ptr.data(), sizeof(int64_t) * t.col_ptr.size());
+  std::memcpy(row_ind, t.row_idx.data(), sizeof(int) * t.row_idx.size());
+  *status = FFG_OK;
+}
+
+void ffg_assemble_tetra_nedelec_pml_csc(int nv, const double *verts, int nt, const int *tets,
+                                        int order, const double *stretch, double wave_number,
+                                        int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+                                        int *row_ind, double *values, int *status) {
+  pml_csc(false, nv, verts, nt, tets, order, stretch, wave_number, cap, n_dofs, nnz, col_ptr,
+          row_ind, values, status);
+}
+
+void ffg_assemble_tetra_nedelec_curvilinear_pml_csc(int nv, const double *verts, int nt,
+                                                    const int *tets, int order,
+                                                    const double *stretch, double wave_number,
+                                                    int64_t cap, int *n_dofs, int64_t *nnz,
+                                                    int64_t *col_ptr, int *row_ind,
+                                                    double *values, int *status) {
+  pml_csc(true, nv, verts, nt, tets, order, stretch, wave_number, cap, n_dofs, nnz, col_ptr,
+          row_ind, values, status);
+}
+
 void ffg_assemble_tetra_nedelec_vector_load_samples(int nv, const double *verts, int nt,
                                                     const int *tets, int order,
                                                     const double *samples, int n_dofs, double *rhs,

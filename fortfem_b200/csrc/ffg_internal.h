@@ -219,6 +219,9 @@ struct AssemblyInputs {
   // tangent element matrices along (vertices_dot, coef_a_dot, coef_b_dot)
   const double *vertices_dot = nullptr;               // device, nullable
   double coef_a_dot = 0.0, coef_b_dot = 0.0;
+  // Nedelec: 12 contraction weights per cell supplied by the caller (device,
+  // nullable); replaces the curl / mass weights computed from the geometry
+  const double *geo_override = nullptr;
 };
 
 // Per-cell geometry/coefficient block and element right-hand sides.
@@ -262,6 +265,20 @@ int nedelec_vjp(const Topology &t, const ElementTables &tab, const DeviceTopolog
                 const int64_t *col_ptr, const int *row_idx, const double *vertices,
                 const double *values_bar, double ca, double cb, double *elem,
                 double *vertices_bar, double *coef_bar, int *err, cudaStream_t s);
+
+// ------------------------------------------------------------ complex PML
+// The twelve Nedelec contraction weights of the complex PML forms per cell,
+// real and imaginary parts (12 doubles per cell each): curl pairs
+// (1/det) (J^T Cc J)_ab, mass pairs -k^2 det (J^-1 Cm J^-T)_ab, with
+// (Cc, Cm) the Cartesian (stretch: 3 complex per cell) or curvilinear
+// (stretch: 3x3 complex per cell, column-major) PML tensors.  Complex
+// values are (re, im) pairs.  err: degenerate cell or invalid stretch.
+int launch_pml_weights(const Topology &t, const DeviceTopology &dt, const double *vertices,
+                       const double *stretch, bool curvilinear, double wave_number,
+                       double *geo_re, double *geo_im, int *err, cudaStream_t s);
+// values[2i] = re[i], values[2i+1] = im[i]
+int launch_interleave(int64_t n, const double *re, const double *im, double *values,
+                      cudaStream_t s);
 
 // --------------------------------------------------- evaluation and probes
 // Device tables of the solution evaluators (kernels_probe.cu), built on first use.

@@ -149,7 +149,8 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
                                        const double *__restrict__ face_blocks,
                                        double *__restrict__ elem, double *__restrict__ cell_rhs,
                                        int *err, const double *__restrict__ verts_dot,
-                                       double ca_dot, double cb_dot) {
+                                       double ca_dot, double cb_dot,
+                                       const double *__restrict__ geo_in) {
   extern __shared__ double sm[];
   const int nb = D.nb, fdc = D.fdc;
   // K (nb x nb, column-major) lives in shared memory, or (order 6: 373 KB) in
@@ -174,7 +175,10 @@ __global__ void nedelec_element_kernel(int n_cells, const int *__restrict__ cell
       inv3(J, ok_s ? det : 1.0, Ji);
       const double cw = ca * (cell_a ? cell_a[c] : 1.0);
       const double mw = cb * (cell_b ? cell_b[c] : 1.0);
-      if (!verts_dot) {
+      if (geo_in) {
+        // caller-computed weights (the complex PML tensors, one part at a time)
+        for (int s = 0; s < 12; ++s) geo[s] = ok_s ? geo_in[12 * (size_t)c + s] : 0.0;
+      } else if (!verts_dot) {
         for (int s = 0; s < 6; ++s) {
           const int a = kPa[s], b = kPb[s];
           const double JtJ = J[3 * a] * J[3 * b] + J[3 * a + 1] * J[3 * b + 1] + J[3 * a + 2] * J[3 * b + 2];
@@ -430,7 +434,7 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   nedelec_element_kernel<<<grid, 256, smem, s>>>(
       t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
       tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem,
-      cell_rhs, err, in.vertices_dot, in.coef_a_dot, in.coef_b_dot);
+      cell_rhs, err, in.vertices_dot, in.coef_a_dot, in.coef_b_dot, in.geo_override);
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 

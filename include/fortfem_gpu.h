@@ -183,6 +183,32 @@ void ffg_assemble_tetra_nedelec_curl_mass_csc_vjp(
     double *vertices_bar, double *curl_coefficient_bar, double *mass_coefficient_bar,
     int *status);
 
+/* assemble_tetra_nedelec_pml_csc, assembly_tetra_nedelec_3d.f90:1613-1685 (element
+ * :826-887): the complex curl-curl minus k^2 mass operator with the Cartesian PML
+ * tensors of cartesian_curl_curl_pml_coefficients (src/boundary/cartesian_helmholtz_pml.f90:94-108).
+ * stretch: 3 complex values per tetrahedron as (re, im) pairs (6 doubles per
+ * cell); values: nnz complex entries as (re, im) pairs (2 * nnz doubles, the
+ * layout of C99 double complex and of Fortran complex(dp), csc_z_t%val).
+ * The reference integrates at degree 2k+2, the primal curl-mass at 2k (order 1:
+ * the 4-point rule); both are exact for these integrands. */
+void ffg_assemble_tetra_nedelec_pml_csc(int n_vertices, const double *vertices, int n_tetrahedra,
+                                        const int *tetrahedra, int order, const double *stretch,
+                                        double wave_number, int64_t nnz_capacity, int *n_dofs,
+                                        int64_t *nnz, int64_t *col_ptr, int *row_ind,
+                                        double *values, int *status);
+
+/* assemble_tetra_nedelec_curvilinear_pml_csc, same file :1372-1444 (element
+ * :1092-1153), tensors of curvilinear_curl_curl_pml_coefficients
+ * (src/boundary/curvilinear_helmholtz_pml.f90:113-131): stretch is a complex
+ * 3x3 matrix per tetrahedron, column-major as the Fortran stretch(:, :, t),
+ * (re, im) pairs (18 doubles per cell). */
+void ffg_assemble_tetra_nedelec_curvilinear_pml_csc(int n_vertices, const double *vertices,
+                                                    int n_tetrahedra, const int *tetrahedra,
+                                                    int order, const double *stretch,
+                                                    double wave_number, int64_t nnz_capacity,
+                                                    int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+                                                    int *row_ind, double *values, int *status);
+
 /* assemble_tetra_nedelec_vector_load_samples, assembly_tetra_nedelec_3d.f90:128-185
  * (order 1 uses the 4-point rule and edge signs, :2002-2040); source_values
  * holds 3*n_q values per cell. */

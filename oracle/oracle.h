@@ -162,6 +162,20 @@ int or_nedelec_csc_jvp(int n_vertices, const double *vertices, int n_tets, const
 int or_nedelec_csc_vjp(int n_vertices, const double *vertices, int n_tets, const int *tets,
                        int order, double curl, double mass, int64_t nnz, const double *values_bar,
                        double *vertices_bar, double *curl_bar, double *mass_bar);
+/* complex PML variants: stretch 3 (Cartesian) or 9 (curvilinear, column-major)
+ * complex values per cell as (re, im) pairs; matrices / values complex
+ * (re, im) interleaved, element matrices column-major */
+int or_nedelec_pml_element(const double *vertices, int order, int quadrature_degree,
+                           const double *stretch, double wave_number, double *matrix);
+int or_nedelec_curvilinear_pml_element(const double *vertices, int order, int quadrature_degree,
+                                       const double *stretch, double wave_number, double *matrix);
+int or_nedelec_pml_csc(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                       int order, const double *stretch, double wave_number, int64_t nnz_capacity,
+                       int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_idx, double *values);
+int or_nedelec_curvilinear_pml_csc(int n_vertices, const double *vertices, int n_tets,
+                                   const int *tets, int order, const double *stretch,
+                                   double wave_number, int64_t nnz_capacity, int *n_dofs,
+                                   int64_t *nnz, int64_t *col_ptr, int *row_idx, double *values);
 int or_nedelec_evaluate_solution(int n_vertices, const double *vertices, int n_tets,
                                  const int *tets, int order, int n_dofs, const double *solution,
                                  int cell, const double *reference_point, double *value /*3*/,

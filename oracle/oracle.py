@@ -594,3 +594,41 @@ def nedelec_probe(vertices, tets, k, solution, point, mode=0):
     _call("or_nedelec_probe", len(vertices), vertices, len(tets), tets, k, len(u), u,
           _arr(point, np.float64), int(mode), v, c, C.byref(cnt))
     return v, c, cnt.value
+
+
+# ------------------------------------------------------------------ complex PML
+
+def _cplx_in(stretch):
+    a = np.ascontiguousarray(stretch, dtype=np.complex128)
+    return np.ascontiguousarray(a.view(np.float64).ravel())
+
+
+def nedelec_pml_element(vertices, k, stretch, wave_number, q=None, curvilinear=False):
+    """Complex element matrix of assemble_tetra_nedelec_pml_element (stretch (3,))
+    or the curvilinear variant (stretch (3, 3))."""
+    if q is None:
+        q = 2 * k + 2
+    nb = nedelec_dof_count(k)
+    m = np.zeros(2 * nb * nb)
+    s = np.asarray(stretch, np.complex128)
+    if curvilinear:
+        s = s.ravel(order="F")
+    name = "or_nedelec_curvilinear_pml_element" if curvilinear else "or_nedelec_pml_element"
+    _check(_call(name, _arr(vertices, np.float64), k, q, _cplx_in(s), float(wave_number), m), name)
+    return m.view(np.complex128).reshape(nb, nb, order="F")
+
+
+def nedelec_pml_csc(vertices, tets, k, stretch, wave_number, curvilinear=False):
+    """(n, col_ptr, row_idx, complex values): stretch (T, 3) or (T, 3, 3)."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    s = np.asarray(stretch, np.complex128)
+    if curvilinear:
+        s = np.transpose(s, (0, 2, 1))  # column-major per cell
+    nnz = int(_call("or_nedelec_csc_nnz", k, len(tets), tets, restype=C.c_int64))
+    n = nedelec_dof_map(k, tets)["n_global"]
+    nd = C.c_int(0); nz = C.c_int64(0)
+    cp = np.zeros(n + 1, np.int64); ri = np.zeros(nnz, np.int32); v = np.zeros(2 * nnz)
+    name = "or_nedelec_curvilinear_pml_csc" if curvilinear else "or_nedelec_pml_csc"
+    _check(_call(name, len(vertices), vertices, len(tets), tets, k, _cplx_in(s),
+                 float(wave_number), C.c_int64(nnz), C.byref(nd), C.byref(nz), cp, ri, v), name)
+    return n, cp, ri, v.view(np.complex128)

@@ -10,7 +10,9 @@
 
 #include <algorithm>
 #include <array>
+#include <cfloat>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -874,6 +876,203 @@ int or_nedelec_probe(int nv, const double *verts, int nt, const int *tets, int k
     curl[a] = acc_c[a] / found;
   }
   return 0;
+}
+
+// ---------------------------------------------------------- complex PML
+namespace {
+using cplx = std::complex<double>;
+
+// cartesian_curl_curl_pml_coefficients (src/boundary/cartesian_helmholtz_pml.f90:94-108)
+// through cartesian_scalar_helmholtz_pml_coefficients (:30-48): mass = the H1
+// tensor diag(s2 s3/s1, s1 s3/s2, s1 s2/s3), curl = its inverse.
+bool cartesian_pml(const cplx *s, cplx *cc, cplx *mc) {
+  for (int a = 0; a < 3; ++a)
+    if (std::abs(s[a]) <= DBL_MIN) return false;
+  mc[0] = s[1] * s[2] / s[0];
+  mc[1] = s[0] * s[2] / s[1];
+  mc[2] = s[0] * s[1] / s[2];
+  for (int a = 0; a < 3; ++a) cc[a] = 1.0 / mc[a];
+  return true;
+}
+
+// curvilinear_curl_curl_pml_coefficients (src/boundary/curvilinear_helmholtz_pml.f90:113-131)
+// with inverse_and_determinant (:202-216): curl = S^T S / det S, mass = det S S^-1 S^-T.
+// S, cc, mc column-major 3x3.
+bool curvilinear_pml(const cplx *S, cplx *cc, cplx *mc) {
+  auto m = [&](int r, int c) { return S[r + 3 * c]; };
+  const cplx det = m(0, 0) * (m(1, 1) * m(2, 2) - m(1, 2) * m(2, 1)) -
+                   m(0, 1) * (m(1, 0) * m(2, 2) - m(1, 2) * m(2, 0)) +
+                   m(0, 2) * (m(1, 0) * m(2, 1) - m(1, 1) * m(2, 0));
+  double mx = 0.0;
+  for (int i = 0; i < 9; ++i) {
+    if (!std::isfinite(S[i].real()) || !std::isfinite(S[i].imag())) return false;
+    mx = std::max(mx, std::abs(S[i]));
+  }
+  if (!std::isfinite(det.real()) || !std::isfinite(det.imag())) return false;
+  const double sc = std::max(1.0, mx);
+  if (std::abs(det) <= 64.0 * kEps * sc * sc * sc) return false;
+  cplx cof[9], inv[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      const int r1 = (r + 1) % 3, r2 = (r + 2) % 3, c1 = (c + 1) % 3, c2 = (c + 2) % 3;
+      cof[r + 3 * c] = m(r1, c1) * m(r2, c2) - m(r1, c2) * m(r2, c1);
+    }
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) inv[r + 3 * c] = cof[c + 3 * r] / det;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      cplx a = 0.0, b = 0.0;
+      for (int q = 0; q < 3; ++q) {
+        a += S[q + 3 * r] * S[q + 3 * c];      // (S^T S)(r, c)
+        b += inv[r + 3 * q] * inv[c + 3 * q];  // (S^-1 S^-T)(r, c)
+      }
+      cc[r + 3 * c] = a / det;
+      mc[r + 3 * c] = det * b;
+    }
+  return true;
+}
+
+// The element loops of assemble_tetra_nedelec_pml_element (assembly_tetra_nedelec_3d.f90:826-887,
+// diagonal tensors) and assemble_tetra_nedelec_curvilinear_pml_element (:1092-1153,
+// full tensors): K += det w (curl_i . Cc curl_j - k^2 v_i . Cm v_j).
+int pml_element(const double *v, int k, int q, const cplx *cc, const cplx *mc, bool full,
+                double wave, cplx *M) {
+  double J[9], Ji[9], det;
+  if (!tetra_geometry(v, J, &det)) return 1;
+  inv3(J, det, Ji);
+  RuleN R;
+  make_rule(0, q, R);
+  const int n = or_nedelec_dof_count(k);
+  std::vector<double> rv(3 * n), rc(3 * n), pv(3 * n), pc(3 * n);
+  std::fill(M, M + (size_t)n * n, cplx(0.0, 0.0));
+  auto apply = [&](const cplx *C, const double *x, cplx *y) {
+    for (int a = 0; a < 3; ++a) {
+      if (!full) { y[a] = C[a] * x[a]; continue; }
+      y[a] = C[a] * x[0] + C[a + 3] * x[1] + C[a + 6] * x[2];
+    }
+  };
+  for (size_t pt = 0; pt < R.w.size(); ++pt) {
+    double P[3] = {R.x[pt], R.y[pt], R.z[pt]};
+    if (or_nedelec_evaluate(k, P, rv.data(), rc.data())) return 1;
+    covariant(J, det, Ji, n, rv.data(), rc.data(), pv.data(), pc.data());
+    const double pw = det * R.w[pt];
+    for (int col = 0; col < n; ++col) {
+      cplx ccj[3], mcj[3];
+      apply(cc, &pc[3 * col], ccj);
+      apply(mc, &pv[3 * col], mcj);
+      for (int row = 0; row < n; ++row) {
+        cplx a = 0.0, b = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          a += pc[3 * row + i] * ccj[i];
+          b += pv[3 * row + i] * mcj[i];
+        }
+        M[row + (size_t)n * col] += pw * (a - wave * wave * b);
+      }
+    }
+  }
+  return 0;
+}
+
+// assemble_tetra_nedelec_pml_csc (:1613-1685) / _curvilinear_pml_csc (:1372-1444):
+// element at quadrature degree 2k+2, oriented T^T K T, csc_from_triplet on the
+// real and imaginary parts (the same triplet order for both).
+int pml_csc(int nv, const double *verts, int nt, const int *tets, int k, const double *stretch,
+            bool full, double wave, int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+            int *row_idx, double *values) {
+  if (k < 1 || nt < 1 || !(wave > 0.0)) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  const int nb = or_nedelec_dof_count(k);
+  int ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  *n_dofs = ng;
+  const int64_t ntrip = (int64_t)nt * nb * nb;
+  std::vector<int> rows(ntrip), cols(ntrip);
+  std::vector<double> tre(ntrip), tim(ntrip), T((size_t)nb * nb), X((size_t)nb * nb);
+  std::vector<cplx> K((size_t)nb * nb);
+  const int sw = full ? 9 : 3;
+  int64_t e = 0;
+  for (int t = 0; t < nt; ++t) {
+    double v[12];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+    cplx S[9], cc[9], mc[9];
+    for (int i = 0; i < sw; ++i)
+      S[i] = cplx(stretch[2 * (sw * (size_t)t + i)], stretch[2 * (sw * (size_t)t + i) + 1]);
+    if (!(full ? curvilinear_pml(S, cc, mc) : cartesian_pml(S, cc, mc))) return 1;
+    if (pml_element(v, k, 2 * k + 2, cc, mc, full, wave, K.data())) return 1;
+    if (or_nedelec_transform(k, eo.data() + 6 * t, fp.data() + 12 * t, T.data())) return 1;
+    std::vector<double> Kr((size_t)nb * nb), Kim((size_t)nb * nb), Or((size_t)nb * nb),
+        Oi((size_t)nb * nb);
+    for (size_t i = 0; i < K.size(); ++i) {
+      Kr[i] = K[i].real();
+      Kim[i] = K[i].imag();
+    }
+    sandwich(nb, T.data(), Kr.data(), true, Or.data());
+    sandwich(nb, T.data(), Kim.data(), true, Oi.data());
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row, ++e) {
+        rows[e] = gd[(size_t)nb * t + row];
+        cols[e] = gd[(size_t)nb * t + col];
+        tre[e] = Or[row + (size_t)nb * col];
+        tim[e] = Oi[row + (size_t)nb * col];
+      }
+  }
+  std::vector<double> vre, vim;
+  int64_t z = 0;
+  int st = or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tre.data(), 0, &z, nullptr,
+                               nullptr, nullptr);
+  *nnz = z;
+  if (z > cap || !col_ptr) return -2;
+  vre.resize(z);
+  vim.resize(z);
+  st = or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tre.data(), cap, nnz, col_ptr,
+                           row_idx, vre.data());
+  if (st) return st;
+  st = or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tim.data(), cap, nnz, col_ptr,
+                           row_idx, vim.data());
+  if (st) return st;
+  for (int64_t i = 0; i < z; ++i) {
+    values[2 * i] = vre[i];
+    values[2 * i + 1] = vim[i];
+  }
+  return 0;
+}
+}  // namespace
+
+int or_nedelec_pml_element(const double *v, int k, int q, const double *stretch, double wave,
+                           double *M) {
+  if (k < 1 || q < 0 || !(wave > 0.0)) return 1;
+  cplx S[3], cc[3], mc[3];
+  for (int a = 0; a < 3; ++a) S[a] = cplx(stretch[2 * a], stretch[2 * a + 1]);
+  if (!cartesian_pml(S, cc, mc)) return 1;
+  return pml_element(v, k, q, cc, mc, false, wave, reinterpret_cast<cplx *>(M));
+}
+
+int or_nedelec_curvilinear_pml_element(const double *v, int k, int q, const double *stretch,
+                                       double wave, double *M) {
+  if (k < 1 || q < 0 || !(wave > 0.0)) return 1;
+  cplx S[9], cc[9], mc[9];
+  for (int a = 0; a < 9; ++a) S[a] = cplx(stretch[2 * a], stretch[2 * a + 1]);
+  if (!curvilinear_pml(S, cc, mc)) return 1;
+  return pml_element(v, k, q, cc, mc, true, wave, reinterpret_cast<cplx *>(M));
+}
+
+int or_nedelec_pml_csc(int nv, const double *verts, int nt, const int *tets, int k,
+                       const double *stretch, double wave, int64_t cap, int *n_dofs, int64_t *nnz,
+                       int64_t *col_ptr, int *row_idx, double *values) {
+  return pml_csc(nv, verts, nt, tets, k, stretch, false, wave, cap, n_dofs, nnz, col_ptr, row_idx,
+                 values);
+}
+
+int or_nedelec_curvilinear_pml_csc(int nv, const double *verts, int nt, const int *tets, int k,
+                                   const double *stretch, double wave, int64_t cap, int *n_dofs,
+                                   int64_t *nnz, int64_t *col_ptr, int *row_idx, double *values) {
+  return pml_csc(nv, verts, nt, tets, k, stretch, true, wave, cap, n_dofs, nnz, col_ptr, row_idx,
+                 values);
 }
 
 static int nedelec_load_rule(int k, RuleN &R) {

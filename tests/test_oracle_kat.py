@@ -522,3 +522,51 @@ def test_nedelec_probe_reproduces_its_space(k):
             assert cnt >= 1
             assert np.abs(fv - field(x)).max() < 1e-9
             assert np.abs(fc - curl(x)).max() < 1e-8
+
+
+# ------------------------------------------------------------------ complex PML
+# test/test_tetra_nedelec_pml_element.f90: unit stretch reduces to curl-curl
+# minus k^2 mass (orders 1-4, 2e-12); an absorbing anisotropic stretch gives a
+# complex-symmetric element with a nonzero imaginary part.
+PML_TET = np.array([[0, 0, 0], [1.2, 0, 0], [0.1, 0.9, 0], [0, 0.2, 1.1]])
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_pml_element_unit_stretch_kat(k):
+    wave = 1.7
+    m = oracle.nedelec_pml_element(PML_TET, k, np.ones(3), wave, q=10)
+    ref = oracle.nedelec_element(PML_TET, k, q=10, curl=1.0, mass=-wave ** 2)
+    assert np.abs(m - ref).max() < 2e-12
+    # the same with the curvilinear tensor form and S = I
+    mc = oracle.nedelec_pml_element(PML_TET, k, np.eye(3), wave, q=10, curvilinear=True)
+    assert np.abs(mc - ref).max() < 2e-12
+
+
+def test_pml_element_absorbing_kat():
+    s = np.array([1 + 0.8j, 1.0, 1.0])
+    m = oracle.nedelec_pml_element(PML_TET, 2, s, 1.7, q=10)
+    assert np.abs(m - m.T).max() < 2e-12
+    assert np.abs(m.imag).max() > 1e-3
+    # a diagonal curvilinear stretch is the Cartesian one
+    mc = oracle.nedelec_pml_element(PML_TET, 2, np.diag(s), 1.7, q=10, curvilinear=True)
+    assert np.abs(mc - m).max() < 1e-12 * np.abs(m).max()
+
+
+# test/test_tetra_nedelec_pml_sparse.f90:21-52: order-1 global PML mass has the
+# exact constant-field energy -k^2/3 sum_a m_a f_a^2 on two unit cells.
+def test_pml_csc_constant_field_energy_kat():
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0, 0, -1]], float)
+    t = np.array([[0, 1, 2, 3], [0, 2, 1, 4]], np.int32)
+    s = np.array([[1 + 0.6j, 1.0, 1.0]] * 2)
+    n, cp, ri, val = oracle.nedelec_pml_csc(v, t, 1, s, 1.3)
+    dm = oracle.nedelec_dof_map(1, t)
+    edges = dm["edges"]
+    field = np.array([1.0, 2.0, -1.0])
+    dofs = np.array([field @ (v[b] - v[a]) for a, b in edges.T], complex) \
+        if edges.shape[0] == 2 else np.array([field @ (v[b] - v[a]) for a, b in edges], complex)
+    A = oracle.csc_to_scipy(n, cp, ri, val)
+    energy = dofs @ (A @ dofs)
+    mass = np.array([s[0, 1] * s[0, 2] / s[0, 0], s[0, 0] * s[0, 2] / s[0, 1],
+                     s[0, 0] * s[0, 1] / s[0, 2]])
+    expected = -1.3 ** 2 / 3.0 * np.sum(mass * field ** 2)
+    assert abs(energy - expected) < 3e-12
