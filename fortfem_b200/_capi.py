@@ -43,6 +43,7 @@ FFG_POINT_REFERENCE = 0
 FFG_POINT_PHYSICAL = 1
 FFG_PROBE_AVERAGE = 0
 FFG_PROBE_FIRST = 1
+FFG_DIST_WORK_DOUBLES = 1024
 
 STATUS_TEXT = {
     FFG_OK: "ok", FFG_INVALID_INPUT: "invalid input", FFG_CAPACITY: "capacity too small",
@@ -95,6 +96,17 @@ SIGNATURES = {
         None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curvilinear_pml_csc": (
         None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_problem_assemble": (
+        None, [i32, vp, f64, f64, vp, vp, vp, vp, i32, vp, pi32]),
+    "ffg_problem_sell_permutation": (None, [i32, vp, pi32]),
+    "ffg_problem_system_arrays": (None, [i32, vp, vp, i32, vp, pi32]),
+    "ffg_problem_sell_spmv": (None, [i32, vp, vp, vp, pi32]),
+    "ffg_dist_start": (None, [i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, pi32]),
+    "ffg_dist_update": (None, [i64, vp, f64, vp, vp, vp, vp, vp, vp, vp, vp, vp, pi32]),
+    "ffg_dist_dot": (None, [i64, vp, vp, vp, vp, vp, vp, pi32]),
+    "ffg_dist_direction": (None, [i64, vp, f64, vp, vp, vp, pi32]),
+    "ffg_dist_gather": (None, [i64, vp, vp, vp, vp, pi32]),
+    "ffg_dist_scatter": (None, [i64, vp, vp, vp, vp, pi32]),
     "ffg_problem_evaluate": (
         None, [i32, vp, vp, i32, vp, vp, i32, vp, vp, vp, i32, vp, pi32]),
     "ffg_problem_probe": (

@@ -25,7 +25,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
           "-I" + os.path.join(HERE, "..", "include")]
 SOURCES = ["topology.cpp", "basis.cpp", "kernels_assemble.cu", "kernels_pcg.cu", "capi.cu",
            "noalloc.cu", "topology_gpu.cu", "kernels_ad.cu",
-           "kernels_probe.cu", "kernels_pml.cu"]
+           "kernels_probe.cu", "kernels_pml.cu",
+           "kernels_dist.cu"]
 
 
 def _headers():

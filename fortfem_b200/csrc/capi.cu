@@ -694,6 +694,53 @@ void ffg_problem_probe(int handle, const double *vertices, const double *solutio
   *status = FFG_OK;
 }
 
+void ffg_problem_assemble(int handle, const double *vertices, double ca, double cb,
+                          const double *cell_a, const double *cell_b, const double *samples,
+                          const double *g, int memory, void *stream, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if ((memory != 0 && memory != 1) || P->batch_pending) { *status = FFG_INVALID_INPUT; return; }
+  std::string msg;
+  *status = assemble(*P, vertices, ca, cb, cell_a, cell_b, samples, g, memory, true,
+                     (cudaStream_t)stream, msg);
+}
+
+void ffg_problem_sell_permutation(int handle, int *perm, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const int64_t n = P->topo.n_free();
+  if (!perm) { *status = FFG_INVALID_INPUT; return; }
+  if (n > 0 &&
+      cudaMemcpy(perm, P->S.perm, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  *status = FFG_OK;
+}
+
+void ffg_problem_system_arrays(int handle, double *rhs, double *dinv, int memory, void *stream,
+                               int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (memory != 0 && memory != 1) { *status = FFG_INVALID_INPUT; return; }
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = sizeof(double) * (size_t)P->topo.n_free();
+  const cudaMemcpyKind kind = memory == 0 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  if (bytes && ((rhs && cudaMemcpyAsync(rhs, P->rhs, bytes, kind, s) != cudaSuccess) ||
+                (dinv && cudaMemcpyAsync(dinv, P->S.dinv64, bytes, kind, s) != cudaSuccess))) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  *status = cudaStreamSynchronize(s) == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+void ffg_problem_sell_spmv(int handle, const double *x, double *y, void *stream, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (!x || !y) { *status = FFG_INVALID_INPUT; return; }
+  *status = sell_spmv64(P->S, x, y, (cudaStream_t)stream);
+}
+
 void ffg_problem_free(int handle, int *status) {
   std::lock_guard<std::mutex> lock(g_mutex);
   auto it = g_problems.find(handle);

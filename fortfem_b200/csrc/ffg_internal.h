@@ -280,6 +280,9 @@ int launch_pml_weights(const Topology &t, const DeviceTopology &dt, const double
 int launch_interleave(int64_t n, const double *re, const double *im, double *values,
                       cudaStream_t s);
 
+// FP64 y = A x on the SELL layout (vectors in the SELL row order).
+int sell_spmv64(const DeviceSell &A, const double *x, double *y, cudaStream_t s);
+
 // --------------------------------------------------- evaluation and probes
 // Device tables of the solution evaluators (kernels_probe.cu), built on first use.
 struct EvalTables {

@@ -402,6 +402,64 @@ void ffg_problem_probe(int handle, const double *vertices, const double *solutio
                        const double *points, int mode, double *values, double *derivatives,
                        int *counts, int memory, void *stream, int *status);
 
+/* ------------------------------------------- one system over several GPUs */
+
+/* No counterpart in the reference (its solve is serial).  Building blocks of
+ * the row-block Jacobi-PCG that solves one system sharded over several GPUs
+ * (fortfem_b200/sharding.py): every rank owns a set of rows, assembles the
+ * cells that touch them (a ghost layer included) as its own problem, and the
+ * host loop exchanges the search direction of the ghost rows and all-reduces
+ * the dot products between these launches.  Vectors live in device memory in
+ * the SELL row order of the rank's problem (ffg_problem_sell_permutation);
+ * `owned` (uint8, one per row) selects the rows whose dot products count. */
+
+/* Assemble the constrained system into the problem's device operator and
+ * right-hand side without solving (arguments as ffg_problem_solve). */
+void ffg_problem_assemble(int handle, const double *vertices, double coef_a, double coef_b,
+                          const double *cell_a, const double *cell_b, const double *source_samples,
+                          const double *constrained_values, int memory, void *stream, int *status);
+
+/* perm[i] = free-DoF index (position in ffg_build_topology's free list) of
+ * SELL row i; n_free entries, host memory. */
+void ffg_problem_sell_permutation(int handle, int *perm, int *status);
+
+/* Copy the assembled right-hand side and the Jacobi inverse diagonal (SELL
+ * order, n_free each; either pointer may be null) to host (memory = 0) or
+ * device (memory = 1) arrays. */
+void ffg_problem_system_arrays(int handle, double *rhs, double *dinv, int memory, void *stream,
+                               int *status);
+
+/* y = A x with the assembled FP64 operator, device vectors in SELL order. */
+void ffg_problem_sell_spmv(int handle, const double *x, double *y, void *stream, int *status);
+
+/* Device work array for the reductions below: FFG_DIST_WORK_DOUBLES doubles. */
+#define FFG_DIST_WORK_DOUBLES 1024
+
+/* r = b - ax, z = D^-1 r, p = z on owned rows; dots (device, 3) = (r,r), (r,z), (b,b)
+ * over owned rows, summed in a fixed order. */
+void ffg_dist_start(int64_t n, const uint8_t *owned, const double *b, const double *ax,
+                    const double *dinv, double *r, double *z, double *p, double *work,
+                    double *dots, void *stream, int *status);
+
+/* x += alpha p, r -= alpha q, z = D^-1 r on owned rows; dots (device, 2) = (r,r), (r,z). */
+void ffg_dist_update(int64_t n, const uint8_t *owned, double alpha, const double *p,
+                     const double *q, const double *dinv, double *x, double *r, double *z,
+                     double *work, double *dots, void *stream, int *status);
+
+/* dot (device, 1) = (a, b) over owned rows. */
+void ffg_dist_dot(int64_t n, const uint8_t *owned, const double *a, const double *b,
+                  double *work, double *dot, void *stream, int *status);
+
+/* p = z + beta p on owned rows. */
+void ffg_dist_direction(int64_t n, const uint8_t *owned, double beta, const double *z, double *p,
+                        void *stream, int *status);
+
+/* dst[i] = src[idx[i]] (pack a halo) and dst[idx[i]] = src[i] (unpack), i < m. */
+void ffg_dist_gather(int64_t m, const int *idx, const double *src, double *dst, void *stream,
+                     int *status);
+void ffg_dist_scatter(int64_t m, const int *idx, const double *src, double *dst, void *stream,
+                      int *status);
+
 /* Release a problem handle (fortfem_factor_free, src/bindings/fortfem_capi_solver.f90:108-124). */
 void ffg_problem_free(int handle, int *status);
 
