@@ -130,8 +130,9 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
   if (g_abort) return false;
   if (P.ncta == 1) return true;
   if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(P.bar, 1u);
+    // arrival with release semantics: the CTA's writes before the
+    // __syncthreads above are ordered before it (bar.sync, then release)
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(P.bar) : "memory");
     const unsigned int target = phase * (unsigned int)P.ncta;
     const unsigned long long t0 = globaltimer();
     int good = 1;
@@ -144,9 +145,8 @@ __device__ bool grid_barrier(const PcgParams &P, unsigned int &phase) {
         good = 0;
         break;
       }
-      __nanosleep(20);
     }
-    __threadfence();
+    // the acquire load that saw the count orders the reads that follow
     ok = good && ld_volatile_int(P.control) == 0;
   }
   __syncthreads();
@@ -513,6 +513,18 @@ __device__ __forceinline__ void for_rows(const PcgParams &P, F f) {
   for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) f((int)r);
 }
 
+// The same rows split evenly over the CTAs (32-row multiples).  The slice
+// ranges balance stored entries, which suits the SpMV; a purely row-wise
+// phase that follows a grid barrier balances better on equal row counts.
+template <class F>
+__device__ __forceinline__ void for_rows_even(const PcgParams &P, F f) {
+  const int64_t per = ((P.n + (int64_t)P.ncta * kSliceRows - 1) / ((int64_t)P.ncta * kSliceRows)) *
+                      kSliceRows;
+  const int64_t r0 = (int64_t)cta_of(P) * per;
+  const int64_t r1 = min(r0 + per, P.n);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) f((int)r);
+}
+
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
 template <typename V>
@@ -641,7 +653,7 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     t0 = stamp(P);
     part[0] = part[1] = 0.0;
     part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
-    for_rows(P, [&](int row) {
+    for_rows_even(P, [&](int row) {
       V2 a = zn[row];
       P.x[row] = P.x[row] + xs * (double)a.y;
       const V rr = r[row] - al * q[row];
