@@ -25,6 +25,7 @@ FFG_NOT_READY = -9
 FFG_TETRA_LAGRANGE = 1
 FFG_TETRA_NEDELEC = 2
 FFG_TRIANGLE_P1 = 3
+FFG_TRIANGLE_LAGRANGE = 4
 
 FFG_RULE_DUFFY = 0
 FFG_RULE_DEGREE_TWO = 1
@@ -113,6 +114,10 @@ SIGNATURES = {
         None, [i32, vp, vp, i32, vp, i32, vp, vp, vp, i32, vp, pi32]),
     "ffg_assemble_tetra_nedelec_vector_load_samples": (
         None, [i32, vp, i32, vp, i32, vp, i32, vp, pi32]),
+    "ffg_assemble_triangle_lagrange_csc": (
+        None, [i32, vp, i32, vp, i32, i32, f64, f64, vp, vp, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_assemble_triangle_lagrange_load_samples": (
+        None, [i32, vp, i32, vp, i32, i32, vp, i32, vp, pi32]),
     "ffg_assemble_scalar_p1_csc": (
         None, [i32, vp, i32, vp, f64, f64, vp, i64, pi64, vp, vp, vp, pi32]),
     "ffg_solve_sparse": (

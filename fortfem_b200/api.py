@@ -383,6 +383,73 @@ def assemble_tetra_nedelec_vector_load_samples(mesh_vertices, tetrahedra, order,
         p.close()
 
 
+def assemble_triangle_lagrange_csc(vertices, triangles, degree, quadrature_degree=None,
+                                   stiffness_coefficient=1.0, mass_coefficient=0.0,
+                                   cell_stiffness=None, cell_mass=None):
+    """kappa grad u . grad v + m u v on arbitrary-order triangle Lagrange elements
+    (the basis of src/elements/triangle_lagrange_arbitrary_order.f90:29-127)
+    in CSC.  quadrature_degree defaults to 2 degree.  Returns (CscMatrix, Status)."""
+    v = _f64(vertices).reshape(-1, 2)
+    t = _i32(triangles).reshape(-1, 3)
+    q = 2 * degree if quadrature_degree is None else quadrature_degree
+    args = [len(v), _ptr(v), len(t), _ptr(t), int(degree), int(q), float(stiffness_coefficient),
+            float(mass_coefficient), _ptr(_opt(cell_stiffness, len(t))),
+            _ptr(_opt(cell_mass, len(t)))]
+    return _csc_call("ffg_assemble_triangle_lagrange_csc", args,
+                     "Triangle Lagrange assembly failed")
+
+
+def assemble_triangle_lagrange_load_samples(vertices, triangles, degree, source_values,
+                                            quadrature_degree=None):
+    """The load of source samples at the rule's points (T, n_q).  Returns (rhs, Status)."""
+    v = _f64(vertices).reshape(-1, 2)
+    t = _i32(triangles).reshape(-1, 3)
+    q = 2 * degree if quadrature_degree is None else quadrature_degree
+    p = Problem(K.FFG_TRIANGLE_LAGRANGE, degree, t, len(v), quadrature_degree=q, boundary="none")
+    try:
+        src = _f64(source_values)
+        if src.size != p.samples_per_cell * len(t):
+            return None, Status.of(K.FFG_INVALID_INPUT, "Triangle Lagrange load failed")
+        rhs = np.zeros(p.n_dofs)
+        st = C.c_int(0)
+        K.load().ffg_assemble_triangle_lagrange_load_samples(
+            len(v), _ptr(v), len(t), _ptr(t), int(degree), int(q), _ptr(src), p.n_dofs,
+            _ptr(rhs), C.byref(st))
+        return (rhs if st.value == 0 else None), Status.of(st.value, "Triangle Lagrange load failed")
+    finally:
+        p.close()
+
+
+def solve_triangle_lagrange(vertices, triangles, degree, source, stiffness_coefficient=1.0,
+                            mass_coefficient=0.0, boundary_value=None, options=None,
+                            quadrature_degree=None):
+    """-div(kappa grad u) + m u = f on arbitrary-order triangles with u = g on
+    the boundary edges (boundary_value a vectorised g(x, y) or per-DoF
+    values; None: no essential boundary).  Returns (solution, Status, SolverStats)."""
+    v = _f64(vertices).reshape(-1, 2)
+    t = _i32(triangles).reshape(-1, 3)
+    q = 2 * degree if quadrature_degree is None else quadrature_degree
+    bmode = "all" if boundary_value is not None else "none"
+    with Problem(K.FFG_TRIANGLE_LAGRANGE, degree, t, len(v), quadrature_degree=q,
+                 boundary=bmode) as p:
+        pts = p.sample_points(v)
+        samples = None
+        if source is not None:
+            samples = np.asarray(source(pts[..., 0], pts[..., 1]), np.float64) if callable(source) \
+                else _f64(source)
+        g = None
+        if boundary_value is not None:
+            if callable(boundary_value):
+                dp = p.dof_points(v)
+                g = np.where(p.constrained(), boundary_value(dp[:, 0], dp[:, 1]), 0.0)
+            else:
+                g = _f64(boundary_value)
+        sol, stats = p.solve(v, stiffness_coefficient, mass_coefficient, None, None, samples, g,
+                             options)
+        return sol, Status.of(0 if stats.converged else K.FFG_NOT_CONVERGED,
+                              "Triangle Lagrange solve failed"), stats
+
+
 def assemble_scalar_p1_csc(vertices, triangles, mass_coefficient=0.0, stiffness_coefficient=1.0,
                            cell_stiffness=None):
     """assemble_scalar_p1_matrix (src/fortfem_forms_simple.f90:1678-1728) scattered into CSC."""
@@ -452,7 +519,7 @@ def build_topology(family: int, degree: int, cells, n_vertices: int, boundary="n
     """Host-only topology (ffg_build_topology): returns dict with global_dofs
     (cells x n_b), constrained mask, and the constrained CSC pattern."""
     cells = _i32(cells)
-    vpc = 3 if family == K.FFG_TRIANGLE_P1 else 4
+    vpc = 3 if family in (K.FFG_TRIANGLE_P1, K.FFG_TRIANGLE_LAGRANGE) else 4
     nc = cells.size // vpc
     if isinstance(boundary, str):
         mode, mask = _BOUNDARY[boundary], None
@@ -468,6 +535,8 @@ def build_topology(family: int, degree: int, cells, n_vertices: int, boundary="n
         raise FortfemError(st.value, "ffg_build_topology")
     if family == K.FFG_TRIANGLE_P1:
         nb = 3
+    elif family == K.FFG_TRIANGLE_LAGRANGE:
+        nb = (degree + 1) * (degree + 2) // 2
     elif family == K.FFG_TETRA_LAGRANGE:
         nb = (degree + 1) * (degree + 2) * (degree + 3) // 6
     else:
@@ -503,8 +572,9 @@ class Problem:
         self.degree = degree
         self.cells = _i32(cells)
         self.n_vertices = int(n_vertices)
-        self.dim = 2 if family == K.FFG_TRIANGLE_P1 else 3
-        vpc = 3 if family == K.FFG_TRIANGLE_P1 else 4
+        triangles = family in (K.FFG_TRIANGLE_P1, K.FFG_TRIANGLE_LAGRANGE)
+        self.dim = 2 if triangles else 3
+        vpc = 3 if triangles else 4
         n_cells = self.cells.size // vpc
         self.n_cells = n_cells
         if isinstance(boundary, str):

@@ -130,6 +130,136 @@ void lagrange_eval(int p, const std::vector<int> &idx, const double *pt, double 
   }
 }
 
+int triangle_lagrange_dof_count(int p) { return (p + 1) * (p + 2) / 2; }
+
+// Barycentric powers (first = 1 - x - y, second = x, third = y) and nodes in
+// the order of initialize_triangle_lagrange_basis
+// (src/elements/triangle_lagrange_arbitrary_order.f90:52-68).
+void triangle_lagrange_indices(int p, std::vector<int> &pw, std::vector<double> &nodes) {
+  pw.clear();
+  nodes.clear();
+  for (int a = 0; a <= p; ++a)
+    for (int b = 0; b <= p - a; ++b) {
+      const int c = p - a - b;
+      pw.insert(pw.end(), {a, b, c});
+      nodes.insert(nodes.end(), {(double)b / p, (double)c / p});
+    }
+}
+
+namespace {
+double factorial(int n) {
+  double r = 1.0;
+  for (int i = 2; i <= n; ++i) r *= (double)i;
+  return r;
+}
+double ipow_n(double x, int n) {
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+// Bernstein polynomials of the barycentric powers and their (x, y) gradients
+// (evaluate_bernstein_polynomials, triangle_lagrange_arbitrary_order.f90:143-198).
+void triangle_bernstein(int p, const std::vector<int> &pw, double x, double y, double *val,
+                        double *grad) {
+  const int n = (int)pw.size() / 3;
+  const double bary[3] = {1.0 - x - y, x, y};
+  for (int d = 0; d < n; ++d) {
+    const int e[3] = {pw[3 * d], pw[3 * d + 1], pw[3 * d + 2]};
+    const double coef = factorial(p) / (factorial(e[0]) * factorial(e[1]) * factorial(e[2]));
+    val[d] = coef * ipow_n(bary[0], e[0]) * ipow_n(bary[1], e[1]) * ipow_n(bary[2], e[2]);
+    double der[3];
+    for (int k = 0; k < 3; ++k) {
+      if (e[k] == 0) { der[k] = 0.0; continue; }
+      int r[3] = {e[0], e[1], e[2]};
+      r[k] -= 1;
+      der[k] = (double)e[k] * ipow_n(bary[0], r[0]) * ipow_n(bary[1], r[1]) * ipow_n(bary[2], r[2]);
+    }
+    grad[2 * d] = coef * (-der[0] + der[1]);
+    grad[2 * d + 1] = coef * (-der[0] + der[2]);
+  }
+}
+}  // namespace
+
+// The nodal basis is the Bernstein basis times the inverse of its Vandermonde
+// matrix at the nodes (triangle_lagrange_arbitrary_order.f90:70-88; the
+// reference inverts with fortnum's dense_solve, here Gauss-Jordan with
+// partial pivoting).  C[m + n b] is the weight of Bernstein polynomial m in
+// basis function b.
+bool triangle_lagrange_coefficients(int p, std::vector<double> &C) {
+  std::vector<int> pw;
+  std::vector<double> nodes;
+  triangle_lagrange_indices(p, pw, nodes);
+  const int n = (int)pw.size() / 3;
+  std::vector<double> V((size_t)n * n), row(n), g(2 * (size_t)n);
+  for (int d = 0; d < n; ++d) {
+    triangle_bernstein(p, pw, nodes[2 * d], nodes[2 * d + 1], row.data(), g.data());
+    for (int m = 0; m < n; ++m) V[d + (size_t)n * m] = row[m];
+  }
+  C.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) C[i + (size_t)n * i] = 1.0;
+  for (int col = 0; col < n; ++col) {
+    int piv = col;
+    for (int r = col + 1; r < n; ++r)
+      if (std::fabs(V[r + (size_t)n * col]) > std::fabs(V[piv + (size_t)n * col])) piv = r;
+    if (V[piv + (size_t)n * col] == 0.0) return false;
+    if (piv != col)
+      for (int k = 0; k < n; ++k) {
+        std::swap(V[col + (size_t)n * k], V[piv + (size_t)n * k]);
+        std::swap(C[col + (size_t)n * k], C[piv + (size_t)n * k]);
+      }
+    const double inv = 1.0 / V[col + (size_t)n * col];
+    for (int k = 0; k < n; ++k) {
+      V[col + (size_t)n * k] *= inv;
+      C[col + (size_t)n * k] *= inv;
+    }
+    for (int r = 0; r < n; ++r) {
+      if (r == col) continue;
+      const double f = V[r + (size_t)n * col];
+      if (f == 0.0) continue;
+      for (int k = 0; k < n; ++k) {
+        V[r + (size_t)n * k] -= f * V[col + (size_t)n * k];
+        C[r + (size_t)n * k] -= f * C[col + (size_t)n * k];
+      }
+    }
+  }
+  return true;
+}
+
+// Values and (x, y) gradients of the nodal triangle basis at (x, y).
+void triangle_lagrange_eval(int p, const std::vector<int> &pw, const std::vector<double> &C,
+                            double x, double y, double *val, double *grad) {
+  const int n = (int)pw.size() / 3;
+  std::vector<double> bv(n), bg(2 * (size_t)n);
+  triangle_bernstein(p, pw, x, y, bv.data(), bg.data());
+  for (int b = 0; b < n; ++b) {
+    double v = 0.0, gx = 0.0, gy = 0.0;
+    for (int m = 0; m < n; ++m) {
+      const double c = C[m + (size_t)n * b];
+      v += c * bv[m];
+      gx += c * bg[2 * m];
+      gy += c * bg[2 * m + 1];
+    }
+    val[b] = v;
+    grad[2 * b] = gx;
+    grad[2 * b + 1] = gy;
+  }
+}
+
+// triangle_duffy_quadrature (src/quadrature/triangle_duffy_quadrature.f90:12-45):
+// (q + 3) / 2 Gauss points per direction, x = t_a, y = (1 - t_a) t_b.
+void triangle_rule(int q, std::vector<double> &x, std::vector<double> &y, std::vector<double> &w) {
+  const int m = (q + 3) / 2;
+  std::vector<double> t(m), tw(m);
+  gauss_legendre01(m, t.data(), tw.data());
+  x.clear(); y.clear(); w.clear();
+  for (int a = 0; a < m; ++a)
+    for (int b = 0; b < m; ++b) {
+      x.push_back(t[a]);
+      y.push_back((1.0 - t[a]) * t[b]);
+      w.push_back(tw[a] * tw[b] * (1.0 - t[a]));
+    }
+}
+
 int nedelec_dof_count(int k) { return k * (k + 2) * (k + 3) / 2; }
 
 static double ipow(double x, int n) {
@@ -223,6 +353,58 @@ int build_tables(const Topology &t, int rule, int qdeg, ElementTables &tab, std:
   if (t.family == FFG_TRIANGLE_P1) {
     tab.n_terms = 0;
     tab.nq_load = 1;
+    return FFG_OK;
+  }
+  if (t.family == FFG_TRIANGLE_LAGRANGE) {
+    // K = sum_ab kappa |det| (J^-1 J^-T)_ab R^ab + m |det| R^mass, pairs
+    // (0,0), (1,1), (0,1); one Duffy rule of degree qdeg for matrix and load
+    if (qdeg < 0) { msg = "bad quadrature degree"; return FFG_INVALID_INPUT; }
+    std::vector<int> pw;
+    std::vector<double> nodes, C, qx, qy, qw;
+    triangle_lagrange_indices(t.degree, pw, nodes);
+    if (!triangle_lagrange_coefficients(t.degree, C)) {
+      msg = "singular triangle Vandermonde matrix";
+      return FFG_INVALID_INPUT;
+    }
+    triangle_rule(qdeg, qx, qy, qw);
+    const int nq = (int)qw.size();
+    std::vector<double> val((size_t)nq * nb), grad((size_t)nq * nb * 2);
+    for (int q = 0; q < nq; ++q)
+      triangle_lagrange_eval(t.degree, pw, C, qx[q], qy[q], &val[(size_t)q * nb],
+                             &grad[(size_t)q * nb * 2]);
+    const int pa[3] = {0, 1, 0}, pb[3] = {0, 1, 1};
+    tab.n_terms = 4;
+    tab.ref.assign((size_t)4 * nb * nb, 0.0);
+    for (int s = 0; s < 3; ++s) {
+      const int a = pa[s], b = pb[s];
+      double *M = &tab.ref[(size_t)s * nb * nb];
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) {
+          double acc = 0.0;
+          for (int q = 0; q < nq; ++q) {
+            const double *g = &grad[(size_t)q * nb * 2];
+            double v = g[2 * i + a] * g[2 * j + b];
+            if (a != b) v += g[2 * i + b] * g[2 * j + a];
+            acc += qw[q] * v;
+          }
+          M[i + (size_t)nb * j] = acc;
+        }
+    }
+    double *Mm = &tab.ref[(size_t)3 * nb * nb];
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        double acc = 0.0;
+        for (int q = 0; q < nq; ++q) acc += qw[q] * val[(size_t)q * nb + i] * val[(size_t)q * nb + j];
+        Mm[i + (size_t)nb * j] = acc;
+      }
+    tab.nq_load = nq;
+    tab.load_basis.assign((size_t)nq * nb, 0.0);
+    tab.load_xi.assign((size_t)nq * 3, 0.0);
+    for (int q = 0; q < nq; ++q) {
+      for (int i = 0; i < nb; ++i) tab.load_basis[(size_t)q * nb + i] = qw[q] * val[(size_t)q * nb + i];
+      tab.load_xi[3 * q] = qx[q];
+      tab.load_xi[3 * q + 1] = qy[q];
+    }
     return FFG_OK;
   }
   if (t.family == FFG_TETRA_LAGRANGE) {
@@ -331,6 +513,7 @@ int geo_stride_for(const Topology &t, const ElementTables &tab) {
     case FFG_TETRA_LAGRANGE: return 7 + tab.nq_load;
     case FFG_TETRA_NEDELEC: return 12;
     case FFG_TRIANGLE_P1: return 10;
+    case FFG_TRIANGLE_LAGRANGE: return 4 + tab.nq_load;
   }
   return 0;
 }

@@ -130,8 +130,8 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   Topology &t = P->topo;
   t.family = family;
   t.degree = degree;
-  t.vpc = (family == FFG_TRIANGLE_P1) ? 3 : 4;
-  P->dim = (family == FFG_TRIANGLE_P1) ? 2 : 3;
+  t.vpc = (family == FFG_TRIANGLE_P1 || family == FFG_TRIANGLE_LAGRANGE) ? 3 : 4;
+  P->dim = (family == FFG_TRIANGLE_P1 || family == FFG_TRIANGLE_LAGRANGE) ? 2 : 3;
   t.n_cells = n_cells;
   t.n_vertices = n_vertices;
   if (n_cells < 1 || n_vertices < 1 || !cells) { msg = "empty mesh"; return FFG_INVALID_INPUT; }
@@ -473,7 +473,7 @@ void ffg_build_topology(int family, int degree, int n_vertices, int n_cells, con
   Topology t;
   t.family = family;
   t.degree = degree;
-  t.vpc = (family == FFG_TRIANGLE_P1) ? 3 : 4;
+  t.vpc = (family == FFG_TRIANGLE_P1 || family == FFG_TRIANGLE_LAGRANGE) ? 3 : 4;
   t.n_cells = n_cells;
   t.n_vertices = n_vertices;
   std::string msg;
@@ -574,7 +574,7 @@ void ffg_problem_evaluate(int handle, const double *vertices, const double *solu
   auto P = find_problem(handle);
   if (!P) { *status = FFG_BAD_HANDLE; return; }
   const Topology &t = P->topo;
-  if (t.family == FFG_TRIANGLE_P1 || n_queries < 0 || !vertices || !solution ||
+  if (t.family == FFG_TRIANGLE_P1 || t.family == FFG_TRIANGLE_LAGRANGE || n_queries < 0 || !vertices || !solution ||
       (n_queries > 0 && (!cells || !points || !values || !derivatives)) ||
       (point_kind != FFG_POINT_REFERENCE && point_kind != FFG_POINT_PHYSICAL)) {
     *status = FFG_INVALID_INPUT;
@@ -642,7 +642,7 @@ void ffg_problem_probe(int handle, const double *vertices, const double *solutio
   auto P = find_problem(handle);
   if (!P) { *status = FFG_BAD_HANDLE; return; }
   const Topology &t = P->topo;
-  if (t.family == FFG_TRIANGLE_P1 || n_points < 0 || !vertices || !solution ||
+  if (t.family == FFG_TRIANGLE_P1 || t.family == FFG_TRIANGLE_LAGRANGE || n_points < 0 || !vertices || !solution ||
       (n_points > 0 && (!points || !values || !derivatives || !counts)) ||
       (mode != FFG_PROBE_AVERAGE && mode != FFG_PROBE_FIRST)) {
     *status = FFG_INVALID_INPUT;
@@ -772,6 +772,17 @@ void ffg_problem_sample_points(int handle, const double *vertices, double *point
       points[3 * (size_t)c + 2] = 0.0;
       continue;
     }
+    if (t.family == FFG_TRIANGLE_LAGRANGE) {
+      const double *a = vertices + 2 * (size_t)v[0], *b = vertices + 2 * (size_t)v[1],
+                   *d = vertices + 2 * (size_t)v[2];
+      for (int q = 0; q < tab.nq_load; ++q) {
+        const double *xi = &tab.load_xi[3 * q];
+        for (int r = 0; r < 2; ++r)
+          points[3 * ((size_t)tab.nq_load * c + q) + r] = a[r] + (b[r] - a[r]) * xi[0] + (d[r] - a[r]) * xi[1];
+        points[3 * ((size_t)tab.nq_load * c + q) + 2] = 0.0;
+      }
+      continue;
+    }
     const double *p0 = vertices + 3 * (size_t)v[0];
     for (int q = 0; q < tab.nq_load; ++q) {
       const double *xi = &tab.load_xi[3 * q];
@@ -795,6 +806,24 @@ void ffg_problem_dof_points(int handle, const double *vertices, double *points, 
       points[3 * (size_t)i] = vertices[2 * (size_t)i];
       points[3 * (size_t)i + 1] = vertices[2 * (size_t)i + 1];
       points[3 * (size_t)i + 2] = 0.0;
+    }
+    *status = FFG_OK;
+    return;
+  }
+  if (t.family == FFG_TRIANGLE_LAGRANGE) {
+    std::vector<int> pw;
+    std::vector<double> nodes;
+    triangle_lagrange_indices(t.degree, pw, nodes);
+    for (int c = 0; c < t.n_cells; ++c) {
+      const int *v = t.cells.data() + 3 * (size_t)c;
+      const double *a = vertices + 2 * (size_t)v[0], *b = vertices + 2 * (size_t)v[1],
+                   *d = vertices + 2 * (size_t)v[2];
+      for (int l = 0; l < t.nb; ++l) {
+        const int g = t.gd[(size_t)t.nb * c + l];
+        for (int r = 0; r < 2; ++r)
+          points[3 * (size_t)g + r] = a[r] + (b[r] - a[r]) * nodes[2 * l] + (d[r] - a[r]) * nodes[2 * l + 1];
+        points[3 * (size_t)g + 2] = 0.0;
+      }
     }
     *status = FFG_OK;
     return;
@@ -1343,6 +1372,23 @@ void ffg_assemble_tetra_nedelec_vector_load_samples(int nv, const double *verts,
                                                     const double *samples, int n_dofs, double *rhs,
                                                     int *status) {
   full_load(FFG_TETRA_NEDELEC, order, nv, verts, nt, tets, 0, 0, samples, n_dofs, rhs, status);
+}
+
+void ffg_assemble_triangle_lagrange_csc(int nv, const double *verts, int nt, const int *tris,
+                                        int degree, int qdeg, double stiffness, double mass,
+                                        const double *cell_stiffness, const double *cell_mass,
+                                        int64_t cap, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+                                        int *row_ind, double *values, int *status) {
+  full_csc(FFG_TRIANGLE_LAGRANGE, degree, nv, verts, nt, tris, 0, qdeg, stiffness, mass,
+           cell_stiffness, cell_mass, cap, n_dofs, nnz, col_ptr, row_ind, values, status);
+}
+
+void ffg_assemble_triangle_lagrange_load_samples(int nv, const double *verts, int nt,
+                                                 const int *tris, int degree, int qdeg,
+                                                 const double *samples, int n_dofs, double *rhs,
+                                                 int *status) {
+  full_load(FFG_TRIANGLE_LAGRANGE, degree, nv, verts, nt, tris, 0, qdeg, samples, n_dofs, rhs,
+            status);
 }
 
 void ffg_assemble_scalar_p1_csc(int nv, const double *verts, int nt, const int *tris, double mass,

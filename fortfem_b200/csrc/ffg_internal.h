@@ -74,6 +74,11 @@ void gauss_legendre01(int n, double *x, double *w);
 int lagrange_dof_count(int p);
 void lagrange_indices(int p, std::vector<int> &idx, std::vector<double> &nodes);
 void lagrange_eval(int p, const std::vector<int> &idx, const double *pt, double *val, double *grad);
+int triangle_lagrange_dof_count(int p);
+void triangle_lagrange_indices(int p, std::vector<int> &powers, std::vector<double> &nodes);
+bool triangle_lagrange_coefficients(int p, std::vector<double> &C);
+void triangle_lagrange_eval(int p, const std::vector<int> &powers, const std::vector<double> &C,
+                            double x, double y, double *val, double *grad);
 int nedelec_dof_count(int k);
 bool nedelec_eval(int k, const double *pt, double *val, double *curl);
 // The candidate vector monomials of the order-k first-kind space

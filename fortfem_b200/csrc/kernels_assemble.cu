@@ -100,6 +100,46 @@ __global__ void p1_geometry_kernel(int n_cells, const int *__restrict__ tris,
   g[9] = samples ? samples[c] * area / 3.0 : 0.0;
 }
 
+// Arbitrary-order triangles: geo = [k |det| G_00, k |det| G_11, k |det| G_01,
+// m |det|, |det| f_q (n_q)], G = J^-1 J^-T of the affine map (columns v1 - v0,
+// v2 - v0); |det| as the P1 forms take the unsigned area.
+__global__ void triangle_lagrange_geometry_kernel(int n_cells, const int *__restrict__ tris,
+                                                  const double *__restrict__ verts, double ca,
+                                                  double cb, const double *__restrict__ cell_a,
+                                                  const double *__restrict__ cell_b,
+                                                  const double *__restrict__ samples, int nq,
+                                                  double *__restrict__ geo, int stride, int *err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  double x[3], y[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int v = tris[3 * (size_t)c + i];
+    x[i] = verts[2 * (size_t)v];
+    y[i] = verts[2 * (size_t)v + 1];
+  }
+  const double j00 = x[1] - x[0], j10 = y[1] - y[0], j01 = x[2] - x[0], j11 = y[2] - y[0];
+  const double det = j00 * j11 - j01 * j10;
+  const double m = fmax(fmax(fabs(j00), fabs(j10)), fmax(fabs(j01), fabs(j11)));
+  const double sc = fmax(1.0, m);
+  double *g = geo + (size_t)stride * c;
+  if (!(fabs(det) > 64.0 * kEps * sc * sc)) {
+    atomicCAS(err, 0, FFG_INVALID_INPUT);
+    for (int i = 0; i < stride; ++i) g[i] = 0.0;
+    return;
+  }
+  // J^-1 rows: (j11, -j01) / det and (-j10, j00) / det
+  const double i00 = j11 / det, i01 = -j01 / det, i10 = -j10 / det, i11 = j00 / det;
+  const double area = fabs(det);
+  const double kappa = ca * (cell_a ? cell_a[c] : 1.0);
+  const double mass = cb * (cell_b ? cell_b[c] : 1.0);
+  g[0] = kappa * area * (i00 * i00 + i01 * i01);
+  g[1] = kappa * area * (i10 * i10 + i11 * i11);
+  g[2] = kappa * area * (i00 * i10 + i01 * i11);
+  g[3] = mass * area;
+  for (int q = 0; q < nq; ++q) g[4 + q] = samples ? area * samples[(size_t)nq * c + q] : 0.0;
+}
+
 // ------------------------------------------------- K2 Nedelec element matrices
 // One CTA per cell: K = (c/det) sum C^ab (J^T J)_ab + m det sum V^ab (J^-1 J^-T)_ab,
 // then the oriented matrix T^T K T of assemble_arbitrary_order_curl_mass_csc
@@ -338,13 +378,16 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
     const int l = inc_local[p];
     const uint16_t *sl = slot + (size_t)p * nb;
     const int *ge = gd + (size_t)nb * e;
-    double gco[7];
+    // reference-tensor families: 7 weights (tetrahedra) or 4 (triangles)
+    constexpr int NT = FAMILY == FFG_TRIANGLE_LAGRANGE ? 4 : 7;
+    constexpr bool TENSORS = FAMILY == FFG_TETRA_LAGRANGE || FAMILY == FFG_TRIANGLE_LAGRANGE;
+    double gco[NT];
     double F = 0.0;
-    if (FAMILY == FFG_TETRA_LAGRANGE) {
+    if (TENSORS) {
       const double *gg = geo + (size_t)stride * e;
 #pragma unroll
-      for (int s = 0; s < 7; ++s) gco[s] = gg[s];
-      for (int q = 0; q < nq; ++q) F += gg[7 + q] * __ldg(load_basis + (size_t)q * nb + l);
+      for (int s = 0; s < NT; ++s) gco[s] = gg[s];
+      for (int q = 0; q < nq; ++q) F += gg[NT + q] * __ldg(load_basis + (size_t)q * nb + l);
     } else if (FAMILY == FFG_TRIANGLE_P1) {
       F = geo[10 * (size_t)e + 9];
     } else {
@@ -352,11 +395,11 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
     }
     for (int i = 0; i < nb; ++i) {
       double kil;
-      if (FAMILY == FFG_TETRA_LAGRANGE) {
+      if (TENSORS) {
         const size_t off = i + (size_t)nb * l;
         kil = 0.0;
 #pragma unroll
-        for (int s = 0; s < 7; ++s) kil += gco[s] * __ldg(ref + s * nn + off);
+        for (int s = 0; s < NT; ++s) kil += gco[s] * __ldg(ref + s * nn + off);
       } else if (FAMILY == FFG_TRIANGLE_P1) {
         kil = geo[10 * (size_t)e + i + 3 * l];
       } else {
@@ -396,6 +439,10 @@ int launch_cell_geometry(const Topology &t, const ElementTables &tab, const Devi
   const int T = 128;
   if (t.family == FFG_TETRA_LAGRANGE) {
     lagrange_geometry_kernel<<<blocks_for(t.n_cells, T), T, 0, s>>>(
+        t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
+        tab.nq_load, geo, stride, err);
+  } else if (t.family == FFG_TRIANGLE_LAGRANGE) {
+    triangle_lagrange_geometry_kernel<<<blocks_for(t.n_cells, T), T, 0, s>>>(
         t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
         tab.nq_load, geo, stride, err);
   } else if (t.family == FFG_TRIANGLE_P1) {
@@ -466,6 +513,8 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
     FFG_LAUNCH(FFG_TETRA_LAGRANGE);
   else if (t.family == FFG_TRIANGLE_P1)
     FFG_LAUNCH(FFG_TRIANGLE_P1);
+  else if (t.family == FFG_TRIANGLE_LAGRANGE)
+    FFG_LAUNCH(FFG_TRIANGLE_LAGRANGE);
   else
     FFG_LAUNCH(FFG_TETRA_NEDELEC);
 #undef FFG_LAUNCH

@@ -122,6 +122,43 @@ int build_lagrange(Topology &t, std::string &msg) {
   return FFG_OK;
 }
 
+// Arbitrary-order triangles: the first-appearance rule of the tetrahedral
+// map on triangles (a local DoF is keyed by its (vertex, power) pairs of
+// nonzero power, sorted by vertex).
+int build_triangle_lagrange(Topology &t, std::string &msg) {
+  const int p = t.degree;
+  if (p < 1 || p > 6) { msg = "triangle Lagrange degree must be 1..6"; return FFG_INVALID_INPUT; }
+  std::vector<int> pw;
+  std::vector<double> nodes;
+  triangle_lagrange_indices(p, pw, nodes);
+  t.nb = triangle_lagrange_dof_count(p);
+  t.gd.assign((size_t)t.nb * t.n_cells, 0);
+  if (t.n_vertices >= (1 << 29)) { msg = "too many vertices"; return FFG_INVALID_INPUT; }
+  std::unordered_map<Key128, int, Key128Hash> map;
+  map.reserve((size_t)t.n_cells * t.nb / 2 + 64);
+  int next = 0;
+  for (int c = 0; c < t.n_cells; ++c) {
+    const int *v = t.cells.data() + 3 * (size_t)c;
+    for (int l = 0; l < t.nb; ++l) {
+      std::pair<int, int> kv[3];
+      int n = 0;
+      for (int i = 0; i < 3; ++i)
+        if (pw[3 * l + i] != 0) kv[n++] = {v[i], pw[3 * l + i]};
+      std::sort(kv, kv + n);
+      uint64_t a = 0, b = 0;
+      for (int i = 0; i < n; ++i) {
+        uint64_t word = ((uint64_t)(kv[i].first + 1) << 3) | (uint64_t)kv[i].second;
+        if (i < 2) a |= word << (32 * i); else b |= word;
+      }
+      auto it = map.emplace(Key128{a, b}, next);
+      if (it.second) ++next;
+      t.gd[(size_t)t.nb * c + l] = it.first->second;
+    }
+  }
+  t.n_dofs = next;
+  return FFG_OK;
+}
+
 int build_nedelec(Topology &t, std::string &msg) {
   const int k = t.degree;
   if (k < 1 || k > 6) { msg = "Nedelec order must be 1..6"; return FFG_INVALID_INPUT; }
@@ -197,6 +234,9 @@ int build_dofs(Topology &t, std::string &msg) {
     case FFG_TETRA_NEDELEC:
       if (t.vpc != 4) return FFG_INVALID_INPUT;
       return build_nedelec(t, msg);
+    case FFG_TRIANGLE_LAGRANGE:
+      if (t.vpc != 3) return FFG_INVALID_INPUT;
+      return build_triangle_lagrange(t, msg);
     case FFG_TRIANGLE_P1:
       if (t.vpc != 3 || t.degree != 1) { msg = "P1 triangles only"; return FFG_INVALID_INPUT; }
       t.nb = 3;
@@ -227,6 +267,25 @@ int build_constraints(Topology &t, int mode, const uint8_t *mask, std::string &m
         t.constrained[kv.first >> 32] = 1;
         t.constrained[kv.first & 0xffffffffu] = 1;
       }
+    return FFG_OK;
+  }
+  if (t.family == FFG_TRIANGLE_LAGRANGE) {
+    // every DoF on an edge of one triangle (the opposite vertex's power is 0)
+    std::unordered_map<uint64_t, int, U64Hash> cnt;
+    cnt.reserve((size_t)t.n_cells * 2);
+    for (int c = 0; c < t.n_cells; ++c)
+      for (int e = 0; e < 3; ++e) cnt[edge_key(t.cells[3 * c + e], t.cells[3 * c + (e + 1) % 3])]++;
+    std::vector<int> pw;
+    std::vector<double> nodes;
+    triangle_lagrange_indices(t.degree, pw, nodes);
+    for (int c = 0; c < t.n_cells; ++c) {
+      const int *v = t.cells.data() + 3 * (size_t)c;
+      for (int o = 0; o < 3; ++o) {
+        if (cnt[edge_key(v[(o + 1) % 3], v[(o + 2) % 3])] != 1) continue;
+        for (int l = 0; l < t.nb; ++l)
+          if (pw[3 * l + o] == 0) t.constrained[t.gd[(size_t)t.nb * c + l]] = 1;
+      }
+    }
     return FFG_OK;
   }
   // incidence-one faces

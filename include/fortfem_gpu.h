@@ -42,6 +42,7 @@ extern "C" {
 #define FFG_TETRA_LAGRANGE 1
 #define FFG_TETRA_NEDELEC 2
 #define FFG_TRIANGLE_P1 3
+#define FFG_TRIANGLE_LAGRANGE 4 /* arbitrary-order triangle Lagrange, degree 1..6 */
 
 /* Quadrature rules: FFG_RULE_DUFFY uses tetra_duffy_quadrature(degree)
  * (src/quadrature/tetra_duffy_quadrature.f90:12-51); FFG_RULE_DEGREE_TWO is the
@@ -55,7 +56,8 @@ extern "C" {
                                build_dirichlet_data, fortfem_tetra_lagrange_solver_3d.f90:551-610;
                                Nedelec: build_zero_tangential_mask,
                                fortfem_tetra_nedelec_solver_3d.f90:416-458;
-                               P1: find_boundary vertices, mesh_2d.f90:560-603) */
+                               P1: find_boundary vertices, mesh_2d.f90:560-603;
+                               triangle Lagrange: every DoF on an edge of one triangle) */
 #define FFG_BOUNDARY_MASK 2 /* caller-supplied uint8 mask over the global DoFs */
 
 /* Solver precision. */
@@ -215,6 +217,33 @@ void ffg_assemble_tetra_nedelec_curvilinear_pml_csc(int n_vertices, const double
 void ffg_assemble_tetra_nedelec_vector_load_samples(
     int n_vertices, const double *vertices, int n_tetrahedra, const int *tetrahedra, int order,
     const double *source_values, int n_dofs, double *rhs, int *status);
+
+/* kappa grad u . grad v + m u v on arbitrary-order triangle Lagrange elements
+ * (degree 1..6) in CSC.  The reference has the basis
+ * (src/elements/triangle_lagrange_arbitrary_order.f90:29-127: Bernstein
+ * polynomials made nodal by their inverse Vandermonde matrix) but no assembly
+ * routine for it; this one follows its tetrahedral Lagrange assembly
+ * (assembly_tetra_lagrange_arbitrary_order_3d.f90:40-105, 276-334) with the
+ * triangle Duffy rule of quadrature_degree
+ * (src/quadrature/triangle_duffy_quadrature.f90:12-45), |det J| as the area
+ * factor, and the first-appearance DoF numbering of the tetrahedral map
+ * (tetra_lagrange_global_dof_map.f90:13-99) on triangles.  vertices are
+ * [x0,y0,x1,...]; cell_* nullable as above. */
+void ffg_assemble_triangle_lagrange_csc(int n_vertices, const double *vertices, int n_triangles,
+                                        const int *triangles, int degree, int quadrature_degree,
+                                        double stiffness_coefficient, double mass_coefficient,
+                                        const double *cell_stiffness, const double *cell_mass,
+                                        int64_t nnz_capacity, int *n_dofs, int64_t *nnz,
+                                        int64_t *col_ptr, int *row_ind, double *values,
+                                        int *status);
+
+/* The load sum_q w_q |det J| f_q phi_i of the same elements; source_values
+ * holds n_q samples per triangle (the rule's points, cell-major). */
+void ffg_assemble_triangle_lagrange_load_samples(int n_vertices, const double *vertices,
+                                                 int n_triangles, const int *triangles,
+                                                 int degree, int quadrature_degree,
+                                                 const double *source_values, int n_dofs,
+                                                 double *rhs, int *status);
 
 /* assemble_scalar_p1_matrix / assemble_scalar_p1_load scattered into CSC,
  * src/fortfem_forms_simple.f90:1678-1761 (the reference builds it dense). */

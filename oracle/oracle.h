@@ -93,6 +93,30 @@ int or_lagrange_probe(int n_vertices, const double *vertices, int n_tets, const 
                       int degree, int n_dofs, const double *solution, const double *point,
                       int mode, double *value, double *gradient, int *count);
 
+/* ---- arbitrary-order triangle Lagrange (vertices [x0,y0,x1,...]) ---- */
+int or_triangle_lagrange_dof_count(int degree);
+int or_triangle_lagrange_nodes(int degree, double *nodes /*2 x n_b*/, int *powers /*3 x n_b*/);
+int or_triangle_lagrange_evaluate(int degree, double x, double y, double *values,
+                                  double *gradients /*2 x n_b*/);
+int or_triangle_lagrange_dof_map(int degree, int n_tris, const int *tris, int *global_dofs,
+                                 int *n_global);
+int or_triangle_lagrange_element(const double *vertices /*2x3*/, int degree, int quadrature_degree,
+                                 double stiffness, double mass, double *matrix);
+int64_t or_triangle_lagrange_csc_nnz(int degree, int n_tris, const int *tris);
+int or_triangle_lagrange_csc(int n_vertices, const double *vertices, int n_tris, const int *tris,
+                             int degree, int quadrature_degree, double stiffness, double mass,
+                             const double *cell_stiffness, const double *cell_mass,
+                             int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr,
+                             int *row_idx, double *values);
+int or_triangle_lagrange_load_samples(int n_vertices, const double *vertices, int n_tris,
+                                      const int *tris, int degree, int quadrature_degree,
+                                      const double *samples /* n_q x T */, double *rhs);
+int or_triangle_lagrange_points(int n_vertices, const double *vertices, int n_tris,
+                                const int *tris, int degree, int quadrature_degree,
+                                double *sample_points /*2 x n_q x T*/,
+                                double *dof_points /*2 x n_dofs*/);
+int or_triangle_lagrange_boundary(int degree, int n_tris, const int *tris, uint8_t *constrained);
+
 /* ---- P1 triangles ---- */
 int or_p1_dense_matrix(int n_vertices, const double *vertices, int n_triangles, const int *triangles,
                        double mass, double stiffness, double *matrix /* n x n col-major */);

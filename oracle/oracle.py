@@ -632,3 +632,84 @@ def nedelec_pml_csc(vertices, tets, k, stretch, wave_number, curvilinear=False):
     _check(_call(name, len(vertices), vertices, len(tets), tets, k, _cplx_in(s),
                  float(wave_number), C.c_int64(nnz), C.byref(nd), C.byref(nz), cp, ri, v), name)
     return n, cp, ri, v.view(np.complex128)
+
+
+# ------------------------------------------------- arbitrary-order triangle Lagrange
+
+def triangle_lagrange_dof_count(p):
+    return (p + 1) * (p + 2) // 2
+
+
+def triangle_lagrange_nodes(p):
+    nb = triangle_lagrange_dof_count(p)
+    nodes = np.zeros(2 * nb); pw = np.zeros(3 * nb, np.int32)
+    _check(_call("or_triangle_lagrange_nodes", p, nodes, pw), "triangle_lagrange_nodes")
+    return nodes.reshape(nb, 2), pw.reshape(nb, 3)
+
+
+def triangle_lagrange_evaluate(p, x, y):
+    """(values (n_b,), gradients (n_b, 2)); None when the point is rejected."""
+    nb = triangle_lagrange_dof_count(p)
+    v = np.zeros(nb); g = np.zeros(2 * nb)
+    st = _call("or_triangle_lagrange_evaluate", p, float(x), float(y), v, g)
+    return None if st else (v, g.reshape(nb, 2))
+
+
+def triangle_lagrange_dof_map(p, tris):
+    tris = _arr(tris, np.int32)
+    nb = triangle_lagrange_dof_count(p)
+    gd = np.zeros(nb * len(tris), np.int32)
+    n = C.c_int(0)
+    _check(_call("or_triangle_lagrange_dof_map", p, len(tris), tris, gd, C.byref(n)), "dof_map")
+    return gd.reshape(len(tris), nb), n.value
+
+
+def triangle_lagrange_element(vertices, p, q, stiffness=1.0, mass=0.0):
+    nb = triangle_lagrange_dof_count(p)
+    m = np.zeros(nb * nb)
+    _check(_call("or_triangle_lagrange_element", _arr(vertices, np.float64), p, q,
+                 float(stiffness), float(mass), m), "triangle_lagrange_element")
+    return m.reshape(nb, nb, order="F")
+
+
+def triangle_lagrange_csc(vertices, tris, p, q, stiffness=1.0, mass=0.0, cell_stiffness=None,
+                          cell_mass=None):
+    vertices = _arr(vertices, np.float64); tris = _arr(tris, np.int32)
+    cs = None if cell_stiffness is None else _arr(cell_stiffness, np.float64)
+    cm = None if cell_mass is None else _arr(cell_mass, np.float64)
+    nnz = int(_call("or_triangle_lagrange_csc_nnz", p, len(tris), tris, restype=C.c_int64))
+    _, n = triangle_lagrange_dof_map(p, tris)
+    nd = C.c_int(0); nz = C.c_int64(0)
+    cp = np.zeros(n + 1, np.int64); ri = np.zeros(nnz, np.int32); v = np.zeros(nnz)
+    _check(_call("or_triangle_lagrange_csc", len(vertices), vertices, len(tris), tris, p, q,
+                 float(stiffness), float(mass), cs, cm, C.c_int64(nnz), C.byref(nd), C.byref(nz),
+                 cp, ri, v), "triangle_lagrange_csc")
+    return n, cp, ri, v
+
+
+def triangle_lagrange_points(vertices, tris, p, q):
+    """(sample points (T, n_q, 2), DoF points (n_dofs, 2))."""
+    vertices = _arr(vertices, np.float64); tris = _arr(tris, np.int32)
+    nq = _call("or_triangle_duffy_count", q)
+    _, n = triangle_lagrange_dof_map(p, tris)
+    sp = np.zeros(2 * nq * len(tris)); dp = np.zeros(2 * n)
+    _check(_call("or_triangle_lagrange_points", len(vertices), vertices, len(tris), tris, p, q,
+                 sp, dp), "triangle_lagrange_points")
+    return sp.reshape(len(tris), nq, 2), dp.reshape(n, 2)
+
+
+def triangle_lagrange_load_samples(vertices, tris, p, q, samples):
+    vertices = _arr(vertices, np.float64); tris = _arr(tris, np.int32)
+    _, n = triangle_lagrange_dof_map(p, tris)
+    rhs = np.zeros(n)
+    _check(_call("or_triangle_lagrange_load_samples", len(vertices), vertices, len(tris), tris, p,
+                 q, _arr(samples, np.float64), rhs), "triangle_lagrange_load_samples")
+    return rhs
+
+
+def triangle_lagrange_boundary(p, tris):
+    tris = _arr(tris, np.int32)
+    _, n = triangle_lagrange_dof_map(p, tris)
+    out = np.zeros(n, np.uint8)
+    _check(_call("or_triangle_lagrange_boundary", p, len(tris), tris, out), "boundary")
+    return out.astype(bool)

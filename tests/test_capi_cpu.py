@@ -136,3 +136,19 @@ def test_topology_rejects_bad_cells():
         ff.build_topology(K.FFG_TETRA_LAGRANGE, 5, np.array([[0, 1, 2, 3]]), 4)
     with pytest.raises(ff.FortfemError):
         ff.build_topology(K.FFG_TETRA_NEDELEC, 1, np.array([[0, 1, 2, 9]]), 4)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 6])
+def test_triangle_lagrange_topology_bit_exact(p):
+    v, t = oracle.unit_square_mesh(6)
+    topo = ff.build_topology(K.FFG_TRIANGLE_LAGRANGE, p, t, len(v), "all")
+    gd, n = oracle.triangle_lagrange_dof_map(p, t)
+    assert topo["n_dofs"] == n and np.array_equal(topo["global_dofs"], gd)
+    assert np.array_equal(topo["constrained"], oracle.triangle_lagrange_boundary(p, t))
+    # the constrained pattern is the oracle's CSC restricted to free DoFs
+    nn, cp, ri, _ = oracle.triangle_lagrange_csc(v, t, p, 2 * p)
+    A = oracle.csc_to_scipy(nn, cp, ri, np.ones(len(ri))).tocsc()
+    free = np.flatnonzero(~topo["constrained"])
+    R = A[free][:, free].tocsc()
+    R.sort_indices()
+    assert np.array_equal(topo["col_ptr"], R.indptr) and np.array_equal(topo["row_idx"], R.indices)

@@ -570,3 +570,42 @@ def test_pml_csc_constant_field_energy_kat():
                      s[0, 0] * s[0, 1] / s[0, 2]])
     expected = -1.3 ** 2 / 3.0 * np.sum(mass * field ** 2)
     assert abs(energy - expected) < 3e-12
+
+
+# ------------------------------------------------- arbitrary-order triangles
+# test/test_triangle_lagrange_arbitrary_order.f90:16-57 (degrees 0..4):
+# Kronecker nodal values, partition of unity, zero gradient sum, and exact
+# interpolation of every monomial of the degree.
+@pytest.mark.parametrize("p", [0, 1, 2, 3, 4])
+def test_triangle_lagrange_basis_kat(p):
+    nodes, _ = oracle.triangle_lagrange_nodes(p)
+    for d, (x, y) in enumerate(nodes):
+        v, _ = oracle.triangle_lagrange_evaluate(p, x, y)
+        e = np.zeros(len(v)); e[d] = 1.0
+        assert np.abs(v - e).max() < 2e-12
+    x, y = 0.23, 0.31
+    v, g = oracle.triangle_lagrange_evaluate(p, x, y)
+    assert abs(v.sum() - 1.0) < 2e-13 and np.abs(g.sum(axis=0)).max() < 5e-13
+    for a in range(p + 1):
+        for b in range(p - a + 1):
+            c = nodes[:, 0] ** a * nodes[:, 1] ** b
+            assert abs(c @ v - x ** a * y ** b) < 2e-12
+            grad = [a * x ** (a - 1) * y ** b if a else 0.0, b * x ** a * y ** (b - 1) if b else 0.0]
+            assert np.abs(c @ g - grad).max() < 8e-12
+
+
+def test_triangle_lagrange_element_properties():
+    v = np.array([[0.1, 0.2], [1.3, -0.1], [0.4, 0.9]])
+    area = 0.5 * abs(np.linalg.det(np.array([v[1] - v[0], v[2] - v[0]])))
+    # degree 1 is the P1 element of assemble_scalar_p1_matrix (forms_simple.f90:1702-1717)
+    m1 = oracle.triangle_lagrange_element(v, 1, 2, stiffness=1.3, mass=0.7)
+    ref = oracle.p1_dense(v, np.array([[0, 1, 2]], np.int32), mass=0.7, stiffness=1.3)
+    _, pw = oracle.triangle_lagrange_nodes(1)
+    vert = pw.argmax(axis=1)          # local DoF l sits on the vertex with power 1
+    assert np.abs(m1 - ref[np.ix_(vert, vert)]).max() < 1e-13
+    for p in range(1, 7):
+        k = oracle.triangle_lagrange_element(v, p, 2 * p, stiffness=1.0, mass=0.0)
+        m = oracle.triangle_lagrange_element(v, p, 2 * p, stiffness=0.0, mass=1.0)
+        assert np.abs(k.sum(axis=1)).max() < 1e-11          # constants are in the kernel
+        assert abs(m.sum() - area) < 1e-13                   # the mass of 1 is the area
+        assert np.abs(k - k.T).max() < 1e-13 and np.linalg.eigvalsh(m).min() > 0
