@@ -651,14 +651,21 @@ class Problem:
         return v, ca, cb, s, gg
 
     def solve(self, vertices, coef_a=1.0, coef_b=0.0, cell_a=None, cell_b=None, samples=None,
-              constrained_values=None, options: Optional[SolverOptions] = None):
-        """Assemble + constrain + solve with host arrays; returns (solution, SolverStats)."""
+              constrained_values=None, options: Optional[SolverOptions] = None, out=None):
+        """Assemble + constrain + solve with host arrays; returns (solution, SolverStats).
+        `out` (float64, n_dofs, C-contiguous) receives the solution; a page-locked
+        buffer there makes the device-to-host copy a direct DMA."""
         v, ca, cb, s, g = self._inputs(vertices, cell_a, cell_b, samples, constrained_values)
         opts = options or SolverOptions(precision="mixed", tolerance=1e-10, preconditioner="jacobi",
                                         max_iterations=1000000)
         oc = opts.to_c()
         sc = K.SolverStatsC()
-        sol = np.zeros(self.n_dofs)
+        if out is None:
+            sol = np.zeros(self.n_dofs)
+        else:
+            sol = out
+            if sol.dtype != np.float64 or sol.size != self.n_dofs or not sol.flags.c_contiguous:
+                raise FortfemError(K.FFG_INVALID_INPUT, "out must be float64, n_dofs, contiguous")
         st = C.c_int(0)
         K.load().ffg_problem_solve(self.handle, _ptr(v), float(coef_a), float(coef_b), _ptr(ca),
                                    _ptr(cb), _ptr(s), _ptr(g), C.byref(oc), _ptr(sol), C.byref(sc),
