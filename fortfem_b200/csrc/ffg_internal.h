@@ -150,8 +150,9 @@ struct SolveWork {
   double *r64 = nullptr, *partial = nullptr;
   double *rd = nullptr, *qd = nullptr;      // FP64-mode residual and A p
   double2 *zpd0 = nullptr, *zpd1 = nullptr; // FP64-mode (z, p) pairs, double-buffered
-  float *rf = nullptr, *qf = nullptr;       // mixed-mode FP32 residual and A p
-  float2 *zpf0 = nullptr, *zpf1 = nullptr;  // mixed-mode (z, p) pairs
+  float *rf = nullptr, *zf = nullptr;       // mixed-mode FP32 r and z = D^-1 r
+  float *pf = nullptr, *qf = nullptr;       // mixed-mode FP32 p and q = A p
+  float2 *zpf0 = nullptr, *zpf1 = nullptr;  // mixed-mode (z, p) pairs once q = A p is direct
   unsigned int *barrier = nullptr;
   int *control = nullptr;    // [0] error status
   double *result = nullptr;  // device statistics block

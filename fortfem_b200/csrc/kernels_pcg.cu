@@ -12,19 +12,19 @@
 // a given grid.  Grid barriers spin with a time bound and report FFG_TIMEOUT
 // instead of hanging.
 //
-// Iteration (two grid barriers):
+// FP64 mode restates pcg_solve_operator / pcg_iteration_loop
+// (src/solvers/advanced_solvers.f90:831-925), two grid barriers an iteration:
 //   A: p = z + beta p_old on the fly while gathering, q = A p, (p, q)
-//   B: x += alpha p (FP64), r -= alpha q, z = D^-1 r, (r, r), (r, z)
+//   B: x += alpha p, r -= alpha q, z = D^-1 r, (r, r), (r, z)
 // The (z, p) pair of every row is stored interleaved and double-buffered so
 // the gather of iteration k never races with the writes of iteration k+1.
-//
-// FP64 mode restates pcg_solve_operator / pcg_iteration_loop
-// (src/solvers/advanced_solvers.f90:831-925): stop when the recursive residual
-// ||r||_2 <= tol*||r_0||_2 (relative) or tol (absolute), or at breakdown
-// (|p^T A p| < 1e-14 as the reference, or p^T A p <= 0 when selected);
-// Jacobi z = D^-1 r with D^-1 = 1 where |a_ii| <= 1e-14.
+// It stops when the recursive residual ||r||_2 <= tol*||r_0||_2 (relative)
+// or tol (absolute), or at breakdown (|p^T A p| < 1e-14 as the reference, or
+// p^T A p <= 0 when selected); Jacobi z = D^-1 r with D^-1 = 1 where
+// |a_ii| <= 1e-14.
 // Mixed mode: the same CG recurrences in FP32 on a scaled residual with the
-// solution accumulated in FP64; whenever the FP32 residual has fallen by the
+// solution accumulated in FP64, the SpMV gathering z alone (q = A p is
+// carried as A z + beta q_old); whenever the FP32 residual has fallen by the
 // reliable-update factor (or claims convergence) the true FP64 residual
 // b - A x replaces it (the search direction is kept, rescaled), and the solve
 // ends when ||b - A x||_2 <= tol*||b||_2.  A replacement is also forced when
@@ -77,8 +77,8 @@ struct PcgParams {
   const double *b;
   double *x;
   double *r64;
-  float *rf, *qf;
-  float2 *zpf0, *zpf1;
+  float *rf, *zf, *pf, *qf;  // mixed mode: r, z = D^-1 r, p, q = A p
+  float2 *zpf0, *zpf1;       // mixed mode after a switch to direct A p: (z, p) pairs
   double *rd, *qd;
   double2 *zpd0, *zpd1;
   double *partial;  // [2][kSlots][grid]
@@ -244,10 +244,8 @@ __device__ __forceinline__ int grab_slice(int *counter, int lane) {
 // order.  Only per-row results are written here; the dot products are taken
 // afterwards in a fixed row order so that results stay bit-reproducible
 // whatever warp computed which slice.
-template <typename V, typename V2, bool NARROW>
-__device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict__ val,
-                                        const V2 *__restrict__ zc, V2 *__restrict__ zn,
-                                        V *__restrict__ q, V beta) {
+template <typename V, bool NARROW, class G>
+__device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict__ val, const G g) {
   __shared__ int next_slice;
   int s0, s1;
   slice_range(P, s0, s1);
@@ -269,14 +267,9 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
     for (int j = 0; j < len; ++j) {
       const int64_t k = base + (int64_t)j * kSliceRows;
       const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
-      const V2 a = zc[c];
-      acc += __ldcs(val + k) * (a.x + beta * a.y);
+      acc += __ldcs(val + k) * g.column(c);
     }
-    if (row < P.n) {
-      const V2 a = zc[row];
-      zn[row].y = a.x + beta * a.y;
-      q[row] = acc;
-    }
+    if (row < P.n) g.finish(row, acc);
     s = nxt;
     if (s < s1) {
       nxt = grab_slice(&next_slice, lane);
@@ -381,10 +374,9 @@ __device__ __forceinline__ int slice_chunks(const PcgParams &P, int s) {
 // memory rather than by registers.  The copies mark their L2 lines
 // evict-first, which keeps the iteration vectors in L2.  Each row is still
 // summed by one lane in column order.
-template <typename V, typename V2, bool NARROW>
+template <typename V, bool NARROW, class G>
 __device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict__ val,
-                                         const V2 *__restrict__ zc, V2 *__restrict__ zn,
-                                         V *__restrict__ q, V beta) {
+                                         const G g) {
   using SS = StageShape<V, NARROW>;
   constexpr int COLS = SS::COLS;
   extern __shared__ __align__(1024) unsigned char stage_smem[];
@@ -433,8 +425,7 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict
           if (j < cols) {
             const int cidx = NARROW ? row + (int)reinterpret_cast<const int16_t *>(ib)[j * 32 + lane]
                                     : reinterpret_cast<const int *>(ib)[j * 32 + lane];
-            const V2 a = zc[cidx];
-            acc += vb[j * 32 + lane] * (a.x + beta * a.y);
+            acc += vb[j * 32 + lane] * g.column(cidx);
           }
         }
       }
@@ -448,11 +439,7 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict
         advance();
       }
     }
-    if (row < P.n && ok) {
-      const V2 a = zc[row];
-      zn[row].y = a.x + beta * a.y;
-      q[row] = acc;
-    }
+    if (row < P.n && ok) g.finish(row, acc);
   }
   // after a failed wait, give the copies still in flight (bounded) time to
   // land before the stage buffers are given up
@@ -527,17 +514,6 @@ __device__ __forceinline__ void for_rows_even(const PcgParams &P, F f) {
 
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
-template <typename V>
-struct VecOf;
-template <>
-struct VecOf<float> {
-  using V2 = float2;
-};
-template <>
-struct VecOf<double> {
-  using V2 = double2;
-};
-
 struct Outcome {
   int iterations = 0, updates = 0, converged = 0, status = FFG_OK, stagnated = 0, aborted = 0;
   double true_res = 0.0, final_res = 0.0, bnorm = 0.0;
@@ -554,26 +530,63 @@ __device__ __forceinline__ unsigned long long stamp(const PcgParams &P) {
   return (cta_of(P) == 0 && threadIdx.x == 0) ? globaltimer() : 0ull;
 }
 
-// The CG loop in value type V (float: mixed mode, double: FP64 mode).
-// `continuation` runs the FP64 loop after a stagnated mixed solve: its target
-// is the true residual tol*||b|| and its guard is the SPD one.
-template <typename V>
-__device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
-                                unsigned long long t_start, bool continuation, Outcome &o,
-                                Timing &tm) {
-  using V2 = typename VecOf<V>::V2;
-  constexpr bool kMixed = sizeof(V) == 4;
-  const V *A = kMixed ? (const V *)P.v32 : (const V *)P.v64;
-  const V *dinv = kMixed ? (const V *)P.d32 : (const V *)P.d64;
-  V *r = kMixed ? (V *)P.rf : (V *)P.rd;
-  V *q = kMixed ? (V *)P.qf : (V *)P.qd;
-  V2 *zp[2] = {kMixed ? (V2 *)P.zpf0 : (V2 *)P.zpd0, kMixed ? (V2 *)P.zpf1 : (V2 *)P.zpd1};
-  double part[kSlots], red[kSlots];
-  const bool true_target = kMixed || continuation;
-  unsigned long long t0, t1, t2;
+// Gather policies of the SpMV: column(c) is the operand value of column c and
+// finish(row, acc) stores the row's product with the row-wise updates that
+// belong to it.
 
-  // r64 = b - A x, ||r64||, ||b||
-  t0 = stamp(P);
+// FP64 PCG: the operand p = z + beta p_old of column c is formed on the fly
+// from the (z, p_old) pair; finish stores p and q = A p.
+template <typename V, typename V2>
+struct PairGather {
+  const V2 *__restrict__ zc;
+  V2 *__restrict__ zn;
+  V *__restrict__ q;
+  V beta;
+  __device__ __forceinline__ V column(int c) const {
+    const V2 a = zc[c];
+    return a.x + beta * a.y;
+  }
+  __device__ __forceinline__ void finish(int row, V acc) const {
+    const V2 a = zc[row];
+    zn[row].y = a.x + beta * a.y;
+    q[row] = acc;
+  }
+};
+
+// Mixed mode: the SpMV gathers z alone and forms q = A p as A z + beta q_old
+// (p = z + beta p_old), so a column costs 4 bytes of gather instead of the
+// 8 of a (z, p) pair; finish stores p and q of the row.
+struct ZGather {
+  const float *__restrict__ z;
+  float *__restrict__ p;
+  float *__restrict__ q;
+  float beta;
+  __device__ __forceinline__ float column(int c) const { return z[c]; }
+  __device__ __forceinline__ void finish(int row, float acc) const {
+    p[row] = z[row] + beta * p[row];
+    q[row] = acc + beta * q[row];
+  }
+};
+
+// q = A p directly (mixed mode, at a reliable update).
+struct PGather {
+  const float *__restrict__ p;
+  float *__restrict__ q;
+  __device__ __forceinline__ float column(int c) const { return p[c]; }
+  __device__ __forceinline__ void finish(int row, float acc) const { q[row] = acc; }
+};
+
+template <typename V, class G>
+__device__ __forceinline__ void spmv(const PcgParams &P, const V *val, const G &g) {
+  if (P.staged && P.dcol) spmv_staged<V, true>(P, val, g);
+  else if (P.staged) spmv_staged<V, false>(P, val, g);
+  else if (P.dcol) spmv_pairs<V, true>(P, val, g);
+  else spmv_pairs<V, false>(P, val, g);
+}
+
+// r64 = b - A x and the partial sums of (r64, r64) and (b, b), reduced.
+__device__ bool residual_norms(const PcgParams &P, unsigned int &phase, double *red) {
+  double part[kSlots];
   residual(P);
   part[0] = part[1] = 0.0;
   for_rows(P, [&](int row) {
@@ -582,26 +595,43 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     part[1] += bb * bb;
   });
   write_partials(P, phase, part, 2);
-  if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+  if (!grid_barrier(P, phase)) return false;
   read_partials(P, phase, red, 2);
+  return true;
+}
+
+// FP64 Jacobi-PCG, the reference's recurrences.  `continuation` runs it after
+// a stagnated mixed solve: its target is then the true residual tol*||b|| and
+// its guard the SPD one.
+__device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
+                                  unsigned long long t_start, bool continuation, Outcome &o,
+                                  Timing &tm) {
+  const double *A = P.v64;
+  const double *dinv = P.d64;
+  double *r = P.rd;
+  double *q = P.qd;
+  double2 *zp[2] = {P.zpd0, P.zpd1};
+  double part[kSlots], red[kSlots];
+  unsigned long long t0, t1, t2;
+
+  t0 = stamp(P);
+  if (!residual_norms(P, phase, red)) { o.aborted = 1; return; }
   const double bnorm = sqrt(red[1]);
   const double rnorm = sqrt(red[0]);
   o.bnorm = bnorm;
-  double scale = kMixed ? (rnorm > 0.0 ? rnorm : 1.0) : 1.0;
-  const double target = P.relative ? P.tol * (true_target ? bnorm : rnorm) : P.tol;
+  const double target = P.relative ? P.tol * (continuation ? bnorm : rnorm) : P.tol;
   double true_res = rnorm, last_true = rnorm;
-  int stall = 0, since = 0, window = kMinWindow;
+  int stall = 0;
   int converged = (rnorm <= target) ? 1 : 0;
   double rz = 0.0;
   if (!converged) {
-    const double inv = 1.0 / scale;
     part[0] = 0.0;
     for_rows(P, [&](int row) {
-      const V rr = (V)(P.r64[row] * inv);
-      const V z = dinv[row] * rr;
+      const double rr = P.r64[row];
+      const double z = dinv[row] * rr;
       r[row] = rr;
-      zp[0][row] = V2{z, (V)0};
-      part[0] += (double)rr * (double)z;
+      zp[0][row] = double2{z, 0.0};
+      part[0] += rr * z;
     });
     write_partials(P, phase, part, 1);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -609,25 +639,17 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     rz = red[0];
   }
   tm.u += stamp(P) - t0;
-  double beta = 0.0, rr_last = 1.0;
+  double beta = 0.0;
   int cur = 0;
   const int budget = P.max_it - o.iterations;
   for (int it = 1; !converged && it <= budget; ++it) {
-    const V2 *zc = zp[cur];
-    V2 *zn = zp[cur ^ 1];
-    const V bt = (V)beta;
+    const double2 *zc = zp[cur];
+    double2 *zn = zp[cur ^ 1];
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp(P);
     part[0] = 0.0;
-    if (P.staged && P.dcol)
-      spmv_staged<V, V2, true>(P, A, zc, zn, q, bt);
-    else if (P.staged)
-      spmv_staged<V, V2, false>(P, A, zc, zn, q, bt);
-    else if (P.dcol)
-      spmv_pairs<V, V2, true>(P, A, zc, zn, q, bt);
-    else
-      spmv_pairs<V, V2, false>(P, A, zc, zn, q, bt);
-    for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
+    spmv(P, A, PairGather<double, double2>{zc, zn, q, beta});
+    for_rows(P, [&](int row) { part[0] += zn[row].y * q[row]; });
     write_partials(P, phase, part, 1);
     t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -636,33 +658,24 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     tm.a += t1 - t0;
     tm.aw += t2 - t1;
     const double pAp = red[0];
-    const bool breakdown = (!kMixed && !continuation && P.guard == 0)
-                               ? (fabs(pAp) < 1.0e-14)
-                               : !(pAp > 0.0 && is_finite_d(pAp));
-    if (breakdown) {
-      // an FP32 p^T A p that is not positive (cancellation on a near-null
-      // direction of the operator) ends the FP32 phase before x is touched;
-      // the FP64 loop continues from the current x
-      if (kMixed) o.stagnated = 1;
-      break;
-    }
+    const bool breakdown = (!continuation && P.guard == 0) ? (fabs(pAp) < 1.0e-14)
+                                                           : !(pAp > 0.0 && is_finite_d(pAp));
+    if (breakdown) break;
     const double alpha = rz / pAp;
-    const V al = (V)alpha;
-    const double xs = alpha * scale;
-    // B: x += alpha p (FP64), r -= alpha q, z = D^-1 r
+    // B: x += alpha p, r -= alpha q, z = D^-1 r
     t0 = stamp(P);
     part[0] = part[1] = 0.0;
     part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
     for_rows_even(P, [&](int row) {
-      V2 a = zn[row];
-      P.x[row] = P.x[row] + xs * (double)a.y;
-      const V rr = r[row] - al * q[row];
+      double2 a = zn[row];
+      P.x[row] = P.x[row] + alpha * a.y;
+      const double rr = r[row] - alpha * q[row];
       r[row] = rr;
-      const V z = dinv[row] * rr;
+      const double z = dinv[row] * rr;
       a.x = z;
       zn[row] = a;
-      part[0] += (double)rr * (double)rr;
-      part[1] += (double)rr * (double)z;
+      part[0] += rr * rr;
+      part[1] += rr * z;
     });
     write_partials(P, phase, part, 3);
     t1 = stamp(P);
@@ -672,60 +685,14 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
     tm.b += t1 - t0;
     tm.bw += t2 - t1;
     ++o.iterations;
-    double rr = red[0], rz_new = red[1];
-    const double est = sqrt(rr) * scale;
-    if (red[2] != 0.0) { o.status = FFG_TIMEOUT; true_res = est; break; }
-    if (!kMixed) {
-      true_res = est;
-      if (est <= target && !continuation) { converged = 1; break; }
-      if (est <= target) {
-        // the continuation's target is the true residual: check b - A x and,
-        // while it still falls, replace the recursive residual with it
-        t0 = stamp(P);
-        part[0] = 0.0;
-        residual(P);
-        for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
-        write_partials(P, phase, part, 1);
-        if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
-        read_partials(P, phase, red, 1);
-        true_res = sqrt(red[0]);
-        if (true_res <= target) { converged = 1; tm.u += stamp(P) - t0; break; }
-        stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
-        last_true = true_res;
-        if (stall >= 2 || !is_finite_d(true_res)) { tm.u += stamp(P) - t0; break; }
-        ++o.updates;
-        part[0] = 0.0;
-        for_rows(P, [&](int row) {
-          const V rr2 = (V)P.r64[row];
-          r[row] = rr2;
-          const V z = dinv[row] * rr2;
-          V2 a = zn[row];
-          a.x = z;
-          zn[row] = a;
-          part[0] += (double)rr2 * (double)z;
-        });
-        write_partials(P, phase, part, 1);
-        if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
-        read_partials(P, phase, red, 1);
-        tm.u += stamp(P) - t0;
-        rz_new = red[0];
-      }
-    } else {
-      // reliable update: replace the recursive residual with b - A x in FP64
-      // when it has fallen by delta, claims convergence, has grown tenfold
-      // past the last true residual (the FP32 recurrence is diverging; the
-      // search then restarts), or has not triggered within `window`
-      // iterations (an FP32 plateau, judged by the stall test below)
-      const bool grew = !(est < 10.0 * scale);
-      const bool slow = o.iterations - since > window;
-      if (!(est <= target || rr <= P.delta * P.delta * rr_last || grew || slow)) {
-        beta = rz_new / rz;
-        rz = rz_new;
-        cur ^= 1;
-        continue;
-      }
-      if (o.updates >= P.max_updates) break;
-      ++o.updates;
+    double rz_new = red[1];
+    const double est = sqrt(red[0]);
+    true_res = est;
+    if (red[2] != 0.0) { o.status = FFG_TIMEOUT; break; }
+    if (est <= target && !continuation) { converged = 1; break; }
+    if (est <= target) {
+      // the continuation's target is the true residual: check b - A x and,
+      // while it still falls, replace the recursive residual with it
       t0 = stamp(P);
       part[0] = 0.0;
       residual(P);
@@ -735,35 +702,25 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
       read_partials(P, phase, red, 1);
       true_res = sqrt(red[0]);
       if (true_res <= target) { converged = 1; tm.u += stamp(P) - t0; break; }
-      if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
       stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
       last_true = true_res;
-      if (stall >= 2) { o.stagnated = 1; tm.u += stamp(P) - t0; break; }
-      const double ratio = scale / true_res;  // old units -> new units
-      const V rt = (V)ratio;
-      const double inv = 1.0 / true_res;
+      if (stall >= 2 || !is_finite_d(true_res)) { tm.u += stamp(P) - t0; break; }
+      ++o.updates;
       part[0] = 0.0;
       for_rows(P, [&](int row) {
-        const V rr2 = (V)(P.r64[row] * inv);
+        const double rr2 = P.r64[row];
         r[row] = rr2;
-        const V z = dinv[row] * rr2;
-        V2 a = zn[row];
+        const double z = dinv[row] * rr2;
+        double2 a = zn[row];
         a.x = z;
-        a.y = a.y * rt;
         zn[row] = a;
-        part[0] += (double)rr2 * (double)z;
+        part[0] += rr2 * z;
       });
       write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
       tm.u += stamp(P) - t0;
-      rz = rz * ratio * ratio;
       rz_new = red[0];
-      scale = true_res;
-      rr_last = 1.0;
-      window = max(kMinWindow, 4 * (o.iterations - since));
-      since = o.iterations;
-      if (grew) rz = 0.0;  // restart: beta = 0 below
     }
     beta = rz != 0.0 ? rz_new / rz : 0.0;
     rz = rz_new;
@@ -771,11 +728,6 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
   }
   o.converged = converged;
   o.final_res = true_res;
-  if (kMixed && converged) {
-    o.true_res = true_res;
-    return;
-  }
-  if (kMixed && o.stagnated) return;  // the FP64 continuation measures its own residual
   // true FP64 residual of the returned x
   t0 = stamp(P);
   part[0] = 0.0;
@@ -786,7 +738,221 @@ __device__ __noinline__ void cg(const PcgParams &P, unsigned int &phase,
   read_partials(P, phase, red, 1);
   tm.u += stamp(P) - t0;
   o.true_res = sqrt(red[0]);
-  if (kMixed) o.final_res = o.true_res;
+}
+
+// Mixed mode: the PCG recurrences in FP32 on a scaled residual, the solution
+// accumulated in FP64, two grid barriers an iteration:
+//   A: w = A z (gathering z alone), p = z + beta p, q = w + beta q, (p, q)
+//   B: x += alpha p (FP64), r -= alpha q, z = D^-1 r, (r, r), (r, z)
+// q is A p up to the rounding of its recurrence, and every reliable update
+// recomputes it from p.  That rounding grows with the condition number: the
+// first reliable update forced by a plateau, or one whose true residual has
+// not halved (other than after a restart, which the non-monotone residual of
+// CG makes routine early on), switches the solve for good to the direct
+// form, in which A gathers (z, p_old) pairs and forms q = A (z + beta p_old)
+// on the fly.
+__device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
+                                      unsigned long long t_start, Outcome &o, Timing &tm) {
+  const float *dinv = P.d32;
+  float *r = P.rf, *z = P.zf, *p = P.pf, *q = P.qf;
+  float2 *zp[2] = {P.zpf0, P.zpf1};
+  double part[kSlots], red[kSlots];
+  unsigned long long t0, t1, t2;
+
+  t0 = stamp(P);
+  if (!residual_norms(P, phase, red)) { o.aborted = 1; return; }
+  const double bnorm = sqrt(red[1]);
+  const double rnorm = sqrt(red[0]);
+  o.bnorm = bnorm;
+  double scale = rnorm > 0.0 ? rnorm : 1.0;
+  const double target = P.relative ? P.tol * bnorm : P.tol;
+  double true_res = rnorm, last_true = rnorm;
+  int stall = 0, since = 0, window = kMinWindow;
+  int converged = (rnorm <= target) ? 1 : 0;
+  bool direct = false;
+  int cur = 0;
+  double rz = 0.0;
+  if (!converged) {
+    const double inv = 1.0 / scale;
+    part[0] = 0.0;
+    for_rows(P, [&](int row) {
+      const float rr = (float)(P.r64[row] * inv);
+      const float zz = dinv[row] * rr;
+      r[row] = rr;
+      z[row] = zz;
+      p[row] = 0.f;
+      q[row] = 0.f;
+      part[0] += (double)rr * (double)zz;
+    });
+    write_partials(P, phase, part, 1);
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+    read_partials(P, phase, red, 1);
+    rz = red[0];
+  }
+  tm.u += stamp(P) - t0;
+  double beta = 0.0;
+  const int budget = P.max_it - o.iterations;
+  for (int it = 1; !converged && it <= budget; ++it) {
+    // A: q = A p, p = z + beta p, (p, q)
+    t0 = stamp(P);
+    part[0] = 0.0;
+    const float bt = (float)beta;
+    float2 *zn = zp[cur ^ 1];
+    if (direct) {
+      spmv(P, P.v32, PairGather<float, float2>{zp[cur], zn, q, bt});
+      for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
+    } else {
+      spmv(P, P.v32, ZGather{z, p, q, bt});
+      for_rows(P, [&](int row) { part[0] += (double)p[row] * (double)q[row]; });
+    }
+    write_partials(P, phase, part, 1);
+    t1 = stamp(P);
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+    read_partials(P, phase, red, 1);
+    t2 = stamp(P);
+    tm.a += t1 - t0;
+    tm.aw += t2 - t1;
+    const double pAp = red[0];
+    if (!(pAp > 0.0 && is_finite_d(pAp))) {
+      // an FP32 p^T A p that is not positive (cancellation on a near-null
+      // direction of the operator) ends the FP32 phase before x is touched;
+      // the FP64 loop continues from the current x
+      o.stagnated = 1;
+      break;
+    }
+    const double alpha = rz / pAp;
+    const float al = (float)alpha;
+    const double xs = alpha * scale;
+    // B: x += alpha p (FP64), r -= alpha q, z = D^-1 r
+    t0 = stamp(P);
+    part[0] = part[1] = 0.0;
+    part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
+    if (direct) {
+      for_rows_even(P, [&](int row) {
+        float2 a = zn[row];
+        P.x[row] = P.x[row] + xs * (double)a.y;
+        const float rr = r[row] - al * q[row];
+        r[row] = rr;
+        a.x = dinv[row] * rr;
+        zn[row] = a;
+        part[0] += (double)rr * (double)rr;
+        part[1] += (double)rr * (double)a.x;
+      });
+    } else {
+      for_rows_even(P, [&](int row) {
+        P.x[row] = P.x[row] + xs * (double)p[row];
+        const float rr = r[row] - al * q[row];
+        r[row] = rr;
+        const float zz = dinv[row] * rr;
+        z[row] = zz;
+        part[0] += (double)rr * (double)rr;
+        part[1] += (double)rr * (double)zz;
+      });
+    }
+    write_partials(P, phase, part, 3);
+    t1 = stamp(P);
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+    read_partials(P, phase, red, 3);
+    t2 = stamp(P);
+    tm.b += t1 - t0;
+    tm.bw += t2 - t1;
+    ++o.iterations;
+    if (direct) cur ^= 1;
+    const double rr = red[0], rz_new = red[1];
+    const double est = sqrt(rr) * scale;
+    if (red[2] != 0.0) { o.status = FFG_TIMEOUT; true_res = est; break; }
+    // reliable update: replace the recursive residual with b - A x in FP64
+    // when it has fallen by delta, claims convergence, has grown tenfold
+    // past the last true residual (the FP32 recurrence is diverging; the
+    // search then restarts), or has not triggered within `window`
+    // iterations (an FP32 plateau, judged by the stall test below)
+    const bool grew = !(est < 10.0 * scale);
+    const bool slow = o.iterations - since > window;
+    if (!(est <= target || rr <= P.delta * P.delta || grew || slow)) {
+      beta = rz_new / rz;
+      rz = rz_new;
+      continue;
+    }
+    if (o.updates >= P.max_updates) break;
+    ++o.updates;
+    t0 = stamp(P);
+    part[0] = 0.0;
+    residual(P);
+    for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+    write_partials(P, phase, part, 1);
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+    read_partials(P, phase, red, 1);
+    true_res = sqrt(red[0]);
+    if (true_res <= target) { converged = 1; tm.u += stamp(P) - t0; break; }
+    if (!(true_res > 0.0) || !is_finite_d(true_res)) break;
+    stall = (true_res > 0.5 * last_true) ? stall + 1 : 0;
+    last_true = true_res;
+    if (stall >= 2) { o.stagnated = 1; tm.u += stamp(P) - t0; break; }
+    const bool to_direct = !direct && (slow || (stall > 0 && !grew));
+    // r = (b - A x) / ||b - A x|| in the new units and z = D^-1 r; p keeps
+    // the old units and the ratio goes into beta.  The recurrence form takes
+    // q = A p afresh; the direct form (or the switch to it) stores (z, p).
+    const double ratio = scale / true_res;
+    const double inv = 1.0 / true_res;
+    part[0] = 0.0;
+    if (direct) {
+      float2 *zc = zp[cur];
+      for_rows(P, [&](int row) {
+        const float rr2 = (float)(P.r64[row] * inv);
+        const float zz = dinv[row] * rr2;
+        r[row] = rr2;
+        zc[row].x = zz;
+        part[0] += (double)rr2 * (double)zz;
+      });
+    } else if (to_direct) {
+      float2 *zc = zp[cur];
+      for_rows(P, [&](int row) {
+        const float rr2 = (float)(P.r64[row] * inv);
+        const float zz = dinv[row] * rr2;
+        r[row] = rr2;
+        zc[row] = make_float2(zz, p[row]);
+        part[0] += (double)rr2 * (double)zz;
+      });
+      direct = true;
+    } else {
+      spmv(P, P.v32, PGather{p, q});
+      for_rows(P, [&](int row) {
+        const float rr2 = (float)(P.r64[row] * inv);
+        const float zz = dinv[row] * rr2;
+        r[row] = rr2;
+        z[row] = zz;
+        part[0] += (double)rr2 * (double)zz;
+      });
+    }
+    write_partials(P, phase, part, 1);
+    if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+    read_partials(P, phase, red, 1);
+    tm.u += stamp(P) - t0;
+    // p_new = z + beta' (ratio p): beta' against the old (r, z) in new units
+    beta = grew ? 0.0 : red[0] / (rz * ratio);
+    rz = red[0];
+    scale = true_res;
+    window = max(kMinWindow, 4 * (o.iterations - since));
+    since = o.iterations;
+  }
+  o.converged = converged;
+  o.final_res = true_res;
+  if (converged) {
+    o.true_res = true_res;
+    return;
+  }
+  if (o.stagnated) return;  // the FP64 continuation measures its own residual
+  // true FP64 residual of the returned x
+  t0 = stamp(P);
+  part[0] = 0.0;
+  residual(P);
+  for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+  write_partials(P, phase, part, 1);
+  if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
+  read_partials(P, phase, red, 1);
+  tm.u += stamp(P) - t0;
+  o.true_res = sqrt(red[0]);
+  o.final_res = o.true_res;
 }
 
 __device__ __forceinline__ void pcg_body(const PcgParams &P) {
@@ -804,12 +970,12 @@ __device__ __forceinline__ void pcg_body(const PcgParams &P) {
   Timing tm;
   int continued = 0;
   if (P.precision == FFG_PRECISION_FP64) {
-    cg<double>(P, phase, t_start, false, o, tm);
+    cg64(P, phase, t_start, false, o, tm);
   } else {
-    cg<float>(P, phase, t_start, false, o, tm);
+    cg_mixed(P, phase, t_start, o, tm);
     if (!o.aborted && o.stagnated && !o.converged && o.status == FFG_OK) {
       continued = 1;
-      cg<double>(P, phase, t_start, true, o, tm);
+      cg64(P, phase, t_start, true, o, tm);
     }
   }
   if (o.aborted) return;
@@ -988,6 +1154,8 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
   A((void **)&w.zpd0, N * sizeof(double2));
   A((void **)&w.zpd1, N * sizeof(double2));
   A((void **)&w.rf, N * sizeof(float));
+  A((void **)&w.zf, N * sizeof(float));
+  A((void **)&w.pf, N * sizeof(float));
   A((void **)&w.qf, N * sizeof(float));
   A((void **)&w.zpf0, N * sizeof(float2));
   A((void **)&w.zpf1, N * sizeof(float2));
@@ -1013,7 +1181,8 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
 }
 
 void solve_work_free(SolveWork &w) {
-  void *ptrs[] = {w.r64, w.rd, w.qd, w.zpd0, w.zpd1, w.rf, w.qf, w.zpf0, w.zpf1, w.partial,
+  void *ptrs[] = {w.r64, w.rd, w.qd, w.zpd0, w.zpd1, w.rf, w.zf, w.pf, w.qf, w.zpf0, w.zpf1,
+                  w.partial,
                   w.barrier, w.control, w.result};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1038,7 +1207,7 @@ PcgParams make_params(const DeviceSell &A, const double *b, double *x,
   P.b = b;
   P.x = x;
   P.r64 = w.r64;
-  P.rf = w.rf; P.qf = w.qf; P.zpf0 = w.zpf0; P.zpf1 = w.zpf1;
+  P.rf = w.rf; P.zf = w.zf; P.pf = w.pf; P.qf = w.qf; P.zpf0 = w.zpf0; P.zpf1 = w.zpf1;
   P.rd = w.rd; P.qd = w.qd; P.zpd0 = w.zpd0; P.zpd1 = w.zpd1;
   P.partial = w.partial;
   P.bar = w.barrier;
