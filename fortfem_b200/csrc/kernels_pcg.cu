@@ -237,28 +237,22 @@ __device__ __forceinline__ int grab_slice(int *counter, int lane) {
   return __shfl_sync(0xffffffffu, t, 0);
 }
 
-// SELL SpMV over this CTA's slices.  Slices are handed to warps through a
-// shared-memory counter (the CTA's slice range is fixed, so every row is still
-// produced by this CTA), one slice ahead so that the next slice can be
-// prefetched; lane l of the warp owns row 32s+l and accumulates it in a fixed
-// order.  Only per-row results are written here; the dot products are taken
-// afterwards in a fixed row order so that results stay bit-reproducible
-// whatever warp computed which slice.
+// SELL SpMV over this CTA's slices: warp w takes slices s0 + w, s0 + w + 32,
+// ... and prefetches its next slice into L2 while it sums the current one;
+// lane l of the warp owns row 32s+l and accumulates it in a fixed order.
+// Returns the thread's sum of what g.finish returns for its rows: a thread
+// visits the same rows in the same order as for_rows, so a dot product taken
+// here has the bits of one taken by a separate row pass.
 template <typename V, bool NARROW, class G>
-__device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict__ val, const G g) {
-  __shared__ int next_slice;
+__device__ __noinline__ double spmv_pairs(const PcgParams &P, const V *__restrict__ val,
+                                          const G g) {
   int s0, s1;
   slice_range(P, s0, s1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) next_slice = s0 + kWarps;
-  __syncthreads();
-  int s = s0 + warp;
-  int nxt = s < s1 ? grab_slice(&next_slice, lane) : s1;
-  if (lane == 0) {
-    if (s < s1) prefetch_slice<V, NARROW>(P, val, s);
-    if (nxt < s1) prefetch_slice<V, NARROW>(P, val, nxt);
-  }
-  while (s < s1) {
+  double dot = 0.0;
+  if (lane == 0 && s0 + warp < s1) prefetch_slice<V, NARROW>(P, val, s0 + warp);
+  for (int s = s0 + warp; s < s1; s += kWarps) {
+    if (lane == 0 && s + kWarps < s1) prefetch_slice<V, NARROW>(P, val, s + kWarps);
     const int64_t base = P.soff[s] + lane;
     const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
     const int row = s * kSliceRows + lane;
@@ -269,14 +263,10 @@ __device__ __noinline__ void spmv_pairs(const PcgParams &P, const V *__restrict_
       const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
       acc += __ldcs(val + k) * g.column(c);
     }
-    if (row < P.n) g.finish(row, acc);
-    s = nxt;
-    if (s < s1) {
-      nxt = grab_slice(&next_slice, lane);
-      if (lane == 0 && nxt < s1) prefetch_slice<V, NARROW>(P, val, nxt);
-    }
+    if (row < P.n) dot += g.finish(row, acc);
   }
   __syncthreads();
+  return dot;
 }
 
 // ------------------------------------------------------ staged FP32 SpMV
@@ -367,16 +357,16 @@ __device__ __forceinline__ int slice_chunks(const PcgParams &P, int s) {
   return (len + COLS - 1) / COLS;
 }
 
-// SpMV q = A (z + beta p) and p = z + beta p, like spmv_pairs, with the
-// operator streamed by the bulk-copy engine: warp w takes slices s0 + w,
-// s0 + w + 32, ... and keeps one chunk of COLS columns in flight while it
+// The SpMV of spmv_pairs (same slices per warp, same return value) with the
+// operator streamed by the bulk-copy engine: warp w keeps one chunk of COLS
+// columns in flight while it
 // gathers and sums the other, so the bytes in flight per SM are set by shared
 // memory rather than by registers.  The copies mark their L2 lines
 // evict-first, which keeps the iteration vectors in L2.  Each row is still
 // summed by one lane in column order.
 template <typename V, bool NARROW, class G>
-__device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict__ val,
-                                         const G g) {
+__device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restrict__ val,
+                                           const G g) {
   using SS = StageShape<V, NARROW>;
   constexpr int COLS = SS::COLS;
   extern __shared__ __align__(1024) unsigned char stage_smem[];
@@ -402,6 +392,7 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict
   }
   unsigned parity = g_mparity[warp], seq = 0;
   bool ok = true;
+  double dot = 0.0;
   for (int cs = s0 + warp; cs < s1; cs += kWarps) {
     const int len = (int)((P.soff[cs + 1] - P.soff[cs]) / 32);
     const int row = cs * kSliceRows + lane;
@@ -439,7 +430,7 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict
         advance();
       }
     }
-    if (row < P.n && ok) g.finish(row, acc);
+    if (row < P.n && ok) dot += g.finish(row, acc);
   }
   // after a failed wait, give the copies still in flight (bounded) time to
   // land before the stage buffers are given up
@@ -448,6 +439,7 @@ __device__ __noinline__ void spmv_staged(const PcgParams &P, const V *__restrict
   __syncwarp();
   if (lane == 0) g_mparity[warp] = parity;
   __syncthreads();
+  return dot;
 }
 
 // r64 = b - A64 x over this CTA's slices (same scheduling as spmv_pairs).
@@ -512,6 +504,30 @@ __device__ __forceinline__ void for_rows_even(const PcgParams &P, F f) {
   for (int64_t r = r0 + threadIdx.x; r < r1; r += kThreads) f((int)r);
 }
 
+// for_rows_even kRowBatch rows at a time: load(row, u) runs for the batch's
+// rows before step(row, u) runs for any of them, so that their loads are in
+// flight together; each thread still visits its rows in increasing order.
+constexpr int kRowBatch = 4;
+template <class L, class F>
+__device__ __forceinline__ void for_rows_even_batched(const PcgParams &P, L load, F step) {
+  const int64_t per = ((P.n + (int64_t)P.ncta * kSliceRows - 1) / ((int64_t)P.ncta * kSliceRows)) *
+                      kSliceRows;
+  const int64_t r0 = (int64_t)cta_of(P) * per;
+  const int64_t r1 = min(r0 + per, P.n);
+  for (int64_t b = r0 + threadIdx.x; b < r1; b += (int64_t)kRowBatch * kThreads) {
+#pragma unroll
+    for (int u = 0; u < kRowBatch; ++u) {
+      const int64_t row = b + (int64_t)u * kThreads;
+      if (row < r1) load((int)row, u);
+    }
+#pragma unroll
+    for (int u = 0; u < kRowBatch; ++u) {
+      const int64_t row = b + (int64_t)u * kThreads;
+      if (row < r1) step((int)row, u);
+    }
+  }
+}
+
 __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
 struct Outcome {
@@ -532,7 +548,7 @@ __device__ __forceinline__ unsigned long long stamp(const PcgParams &P) {
 
 // Gather policies of the SpMV: column(c) is the operand value of column c and
 // finish(row, acc) stores the row's product with the row-wise updates that
-// belong to it.
+// belong to it, returning the row's term of (p, q).
 
 // FP64 PCG: the operand p = z + beta p_old of column c is formed on the fly
 // from the (z, p_old) pair; finish stores p and q = A p.
@@ -546,10 +562,12 @@ struct PairGather {
     const V2 a = zc[c];
     return a.x + beta * a.y;
   }
-  __device__ __forceinline__ void finish(int row, V acc) const {
+  __device__ __forceinline__ double finish(int row, V acc) const {
     const V2 a = zc[row];
-    zn[row].y = a.x + beta * a.y;
+    const V pn = a.x + beta * a.y;
+    zn[row].y = pn;
     q[row] = acc;
+    return (double)pn * (double)acc;
   }
 };
 
@@ -562,9 +580,12 @@ struct ZGather {
   float *__restrict__ q;
   float beta;
   __device__ __forceinline__ float column(int c) const { return z[c]; }
-  __device__ __forceinline__ void finish(int row, float acc) const {
-    p[row] = z[row] + beta * p[row];
-    q[row] = acc + beta * q[row];
+  __device__ __forceinline__ double finish(int row, float acc) const {
+    const float pn = z[row] + beta * p[row];
+    const float qn = acc + beta * q[row];
+    p[row] = pn;
+    q[row] = qn;
+    return (double)pn * (double)qn;
   }
 };
 
@@ -573,15 +594,18 @@ struct PGather {
   const float *__restrict__ p;
   float *__restrict__ q;
   __device__ __forceinline__ float column(int c) const { return p[c]; }
-  __device__ __forceinline__ void finish(int row, float acc) const { q[row] = acc; }
+  __device__ __forceinline__ double finish(int row, float acc) const {
+    q[row] = acc;
+    return 0.0;
+  }
 };
 
 template <typename V, class G>
-__device__ __forceinline__ void spmv(const PcgParams &P, const V *val, const G &g) {
-  if (P.staged && P.dcol) spmv_staged<V, true>(P, val, g);
-  else if (P.staged) spmv_staged<V, false>(P, val, g);
-  else if (P.dcol) spmv_pairs<V, true>(P, val, g);
-  else spmv_pairs<V, false>(P, val, g);
+__device__ __forceinline__ double spmv(const PcgParams &P, const V *val, const G &g) {
+  if (P.staged && P.dcol) return spmv_staged<V, true>(P, val, g);
+  if (P.staged) return spmv_staged<V, false>(P, val, g);
+  if (P.dcol) return spmv_pairs<V, true>(P, val, g);
+  return spmv_pairs<V, false>(P, val, g);
 }
 
 // r64 = b - A x and the partial sums of (r64, r64) and (b, b), reduced.
@@ -647,9 +671,7 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
     double2 *zn = zp[cur ^ 1];
     // A: p = z + beta p_old, q = A p, (p, q)
     t0 = stamp(P);
-    part[0] = 0.0;
-    spmv(P, A, PairGather<double, double2>{zc, zn, q, beta});
-    for_rows(P, [&](int row) { part[0] += zn[row].y * q[row]; });
+    part[0] = spmv(P, A, PairGather<double, double2>{zc, zn, q, beta});
     write_partials(P, phase, part, 1);
     t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -666,17 +688,28 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
     t0 = stamp(P);
     part[0] = part[1] = 0.0;
     part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
-    for_rows_even(P, [&](int row) {
-      double2 a = zn[row];
-      P.x[row] = P.x[row] + alpha * a.y;
-      const double rr = r[row] - alpha * q[row];
-      r[row] = rr;
-      const double z = dinv[row] * rr;
-      a.x = z;
-      zn[row] = a;
-      part[0] += rr * rr;
-      part[1] += rr * z;
-    });
+    {
+      double2 a[kRowBatch] = {};
+      double xv[kRowBatch] = {}, rv[kRowBatch] = {}, qv[kRowBatch] = {}, dv[kRowBatch] = {};
+      for_rows_even_batched(
+          P,
+          [&](int row, int u) {
+            a[u] = zn[row];
+            xv[u] = P.x[row];
+            rv[u] = r[row];
+            qv[u] = q[row];
+            dv[u] = dinv[row];
+          },
+          [&](int row, int u) {
+            P.x[row] = xv[u] + alpha * a[u].y;
+            const double rr = rv[u] - alpha * qv[u];
+            r[row] = rr;
+            const double z = dv[u] * rr;
+            zn[row].x = z;
+            part[0] += rr * rr;
+            part[1] += rr * z;
+          });
+    }
     write_partials(P, phase, part, 3);
     t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -798,13 +831,8 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     part[0] = 0.0;
     const float bt = (float)beta;
     float2 *zn = zp[cur ^ 1];
-    if (direct) {
-      spmv(P, P.v32, PairGather<float, float2>{zp[cur], zn, q, bt});
-      for_rows(P, [&](int row) { part[0] += (double)zn[row].y * (double)q[row]; });
-    } else {
-      spmv(P, P.v32, ZGather{z, p, q, bt});
-      for_rows(P, [&](int row) { part[0] += (double)p[row] * (double)q[row]; });
-    }
+    part[0] = direct ? spmv(P, P.v32, PairGather<float, float2>{zp[cur], zn, q, bt})
+                     : spmv(P, P.v32, ZGather{z, p, q, bt});
     write_partials(P, phase, part, 1);
     t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -827,27 +855,29 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     t0 = stamp(P);
     part[0] = part[1] = 0.0;
     part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
-    if (direct) {
-      for_rows_even(P, [&](int row) {
-        float2 a = zn[row];
-        P.x[row] = P.x[row] + xs * (double)a.y;
-        const float rr = r[row] - al * q[row];
+    {
+      double xv[kRowBatch] = {};
+      float pv[kRowBatch] = {}, rv[kRowBatch] = {}, qv[kRowBatch] = {}, dv[kRowBatch] = {};
+      auto step = [&](int row, int u) {
+        P.x[row] = xv[u] + xs * (double)pv[u];
+        const float rr = rv[u] - al * qv[u];
         r[row] = rr;
-        a.x = dinv[row] * rr;
-        zn[row] = a;
-        part[0] += (double)rr * (double)rr;
-        part[1] += (double)rr * (double)a.x;
-      });
-    } else {
-      for_rows_even(P, [&](int row) {
-        P.x[row] = P.x[row] + xs * (double)p[row];
-        const float rr = r[row] - al * q[row];
-        r[row] = rr;
-        const float zz = dinv[row] * rr;
-        z[row] = zz;
+        const float zz = dv[u] * rr;
+        if (direct) zn[row].x = zz;
+        else z[row] = zz;
         part[0] += (double)rr * (double)rr;
         part[1] += (double)rr * (double)zz;
-      });
+      };
+      auto load = [&](int row, int u) {
+        xv[u] = P.x[row];
+        rv[u] = r[row];
+        qv[u] = q[row];
+        dv[u] = dinv[row];
+      };
+      if (direct)
+        for_rows_even_batched(P, [&](int row, int u) { load(row, u); pv[u] = zn[row].y; }, step);
+      else
+        for_rows_even_batched(P, [&](int row, int u) { load(row, u); pv[u] = p[row]; }, step);
     }
     write_partials(P, phase, part, 3);
     t1 = stamp(P);
