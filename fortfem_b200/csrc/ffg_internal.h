@@ -139,11 +139,18 @@ struct DeviceSell {
   float *dinv32 = nullptr;
   int *perm = nullptr, *iperm = nullptr;
   int *cta_slice = nullptr;  // grid + 1 slice boundaries of the CTAs
+  int *wslice = nullptr;     // the slices of each warp of the grid, warp by warp
+  int *woff = nullptr;       // grid * 32 + 1 starts of the warps' lists in wslice
   int grid = 0;
 };
 
 // Upload the slice structure (values left zero) and the CTA partition.
 int upload_sell(const HostSell &h, int grid, DeviceSell &d);
+// Work partition of a SELL operator over `grid` CTAs of 32 warps: cs holds
+// grid + 1 CTA slice boundaries, wslice the slices of every warp (warp by
+// warp, CTA-major) and woff (grid * 32 + 1) where each warp's list starts.
+void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector<int> &cs,
+                    std::vector<int> &wslice, std::vector<int> &woff);
 void free_sell(DeviceSell &d);
 
 struct SolveWork {

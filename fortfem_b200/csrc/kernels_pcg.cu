@@ -74,6 +74,7 @@ struct PcgParams {
   const float *d32;
   const double *d64;
   const int *cta_slice;
+  const int *wslice, *woff;  // per-warp slice lists of the cooperative grid
   const double *b;
   double *x;
   double *r64;
@@ -212,6 +213,34 @@ __device__ __forceinline__ void slice_range(const PcgParams &P, int &s0, int &s1
   }
 }
 
+// The slices of one warp, in the order it takes them: the list dealt to it
+// when the whole cooperative grid solves the system, otherwise every 32nd
+// slice of the CTA's range.
+struct WarpSlices {
+  const int *list;
+  int k0, n, first;
+  __device__ __forceinline__ int at(int k) const { return list ? list[k0 + k] : first + k * kWarps; }
+};
+
+__device__ __forceinline__ WarpSlices warp_slices(const PcgParams &P, int warp) {
+  WarpSlices w;
+  if (P.wslice && P.ncta > 1) {
+    const int i = cta_of(P) * kWarps + warp;
+    w.list = P.wslice;
+    w.k0 = P.woff[i];
+    w.n = P.woff[i + 1] - w.k0;
+    w.first = 0;
+  } else {
+    int s0, s1;
+    slice_range(P, s0, s1);
+    w.list = nullptr;
+    w.k0 = 0;
+    w.first = s0 + warp;
+    w.n = w.first < s1 ? (s1 - w.first + kWarps - 1) / kWarps : 0;
+  }
+  return w;
+}
+
 // Asynchronous L2 prefetch of a byte range (16-byte aligned, size a nonzero
 // multiple of 16): the warp's next slice streams into L2 while the current
 // one is processed, so its loads meet L2 rather than HBM latency.
@@ -237,22 +266,21 @@ __device__ __forceinline__ int grab_slice(int *counter, int lane) {
   return __shfl_sync(0xffffffffu, t, 0);
 }
 
-// SELL SpMV over this CTA's slices: warp w takes slices s0 + w, s0 + w + 32,
-// ... and prefetches its next slice into L2 while it sums the current one;
-// lane l of the warp owns row 32s+l and accumulates it in a fixed order.
-// Returns the thread's sum of what g.finish returns for its rows: a thread
-// visits the same rows in the same order as for_rows, so a dot product taken
-// here has the bits of one taken by a separate row pass.
+// SELL SpMV over this CTA's slices: each warp walks its own slices
+// (warp_slices) and prefetches its next slice into L2 while it sums the
+// current one; lane l owns row 32s+l and accumulates it in a fixed order.
+// Returns the thread's sum, in a fixed order, of what g.finish returns for
+// its rows.
 template <typename V, bool NARROW, class G>
 __device__ __noinline__ double spmv_pairs(const PcgParams &P, const V *__restrict__ val,
                                           const G g) {
-  int s0, s1;
-  slice_range(P, s0, s1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const WarpSlices ws = warp_slices(P, warp);
   double dot = 0.0;
-  if (lane == 0 && s0 + warp < s1) prefetch_slice<V, NARROW>(P, val, s0 + warp);
-  for (int s = s0 + warp; s < s1; s += kWarps) {
-    if (lane == 0 && s + kWarps < s1) prefetch_slice<V, NARROW>(P, val, s + kWarps);
+  if (lane == 0 && ws.n > 0) prefetch_slice<V, NARROW>(P, val, ws.at(0));
+  for (int k = 0; k < ws.n; ++k) {
+    const int s = ws.at(k);
+    if (lane == 0 && k + 1 < ws.n) prefetch_slice<V, NARROW>(P, val, ws.at(k + 1));
     const int64_t base = P.soff[s] + lane;
     const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
     const int row = s * kSliceRows + lane;
@@ -372,28 +400,30 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
   extern __shared__ __align__(1024) unsigned char stage_smem[];
   unsigned long long(&mbar)[kWarps][kStages] = g_mbar;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int s0, s1;
-  slice_range(P, s0, s1);
+  const WarpSlices ws = warp_slices(P, warp);
   unsigned char *wbuf = stage_smem + (size_t)warp * kStages * kStageBytes;
-  // producer cursor: next chunk to copy (slices with no columns are skipped)
-  int ps = s0 + warp, pc = 0;
-  while (ps < s1 && slice_chunks<COLS>(P, ps) == 0) ps += kWarps;
+  // producer cursor: chunk pc of the warp's pk-th slice is copied next
+  // (slices with no columns are skipped)
+  int pk = 0, pc = 0;
+  while (pk < ws.n && slice_chunks<COLS>(P, ws.at(pk)) == 0) ++pk;
   auto advance = [&]() {
-    if (++pc >= slice_chunks<COLS>(P, ps)) {
+    if (++pc >= slice_chunks<COLS>(P, ws.at(pk))) {
       pc = 0;
-      do ps += kWarps; while (ps < s1 && slice_chunks<COLS>(P, ps) == 0);
+      do ++pk; while (pk < ws.n && slice_chunks<COLS>(P, ws.at(pk)) == 0);
     }
   };
   unsigned pending = 0;  // stages with a copy issued and not yet waited for
-  for (int k = 0; k < kStages && ps < s1; ++k) {
-    if (lane == 0) issue_chunk<V, NARROW>(P, val, ps, pc, wbuf + k * kStageBytes, &mbar[warp][k]);
+  for (int k = 0; k < kStages && pk < ws.n; ++k) {
+    if (lane == 0)
+      issue_chunk<V, NARROW>(P, val, ws.at(pk), pc, wbuf + k * kStageBytes, &mbar[warp][k]);
     pending |= 1u << k;
     advance();
   }
   unsigned parity = g_mparity[warp], seq = 0;
   bool ok = true;
   double dot = 0.0;
-  for (int cs = s0 + warp; cs < s1; cs += kWarps) {
+  for (int ck = 0; ck < ws.n; ++ck) {
+    const int cs = ws.at(ck);
     const int len = (int)((P.soff[cs + 1] - P.soff[cs]) / 32);
     const int row = cs * kSliceRows + lane;
     V acc = 0;
@@ -421,10 +451,11 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
         }
       }
       __syncwarp();
-      if (ps < s1) {
+      if (pk < ws.n) {
         if (ok) {
           if (lane == 0)
-            issue_chunk<V, NARROW>(P, val, ps, pc, wbuf + st * kStageBytes, &mbar[warp][st]);
+            issue_chunk<V, NARROW>(P, val, ws.at(pk), pc, wbuf + st * kStageBytes,
+                                   &mbar[warp][st]);
           pending |= 1u << st;
         }
         advance();
@@ -1137,16 +1168,12 @@ int upload_sell(const HostSell &h, int grid, DeviceSell &d) {
   A((void **)&d.dinv32, sizeof(float) * N);
   A((void **)&d.perm, sizeof(int) * N);
   A((void **)&d.iperm, sizeof(int) * N);
+  std::vector<int> cs, wslice, woff;
+  sell_partition(h.soff.data(), h.n_slices, grid, cs, wslice, woff);
   A((void **)&d.cta_slice, sizeof(int) * (grid + 1));
+  A((void **)&d.wslice, sizeof(int) * wslice.size());
+  A((void **)&d.woff, sizeof(int) * woff.size());
   if (bad) { cudaGetLastError(); free_sell(d); return FFG_OUT_OF_MEMORY; }
-  // CTA partition: contiguous slice ranges with about equal stored entries
-  std::vector<int> cs(grid + 1, 0);
-  for (int b = 1; b < grid; ++b) {
-    const int64_t target = (int64_t)((double)h.padded * b / grid);
-    const int s = (int)(std::lower_bound(h.soff.begin(), h.soff.end(), target) - h.soff.begin());
-    cs[b] = std::max(cs[b - 1], std::min<int>(s, (int)h.n_slices));
-  }
-  cs[grid] = (int)h.n_slices;
   bool ok = true;
   ok = ok && cudaMemcpy(d.soff, h.soff.data(), sizeof(int64_t) * h.soff.size(), cudaMemcpyHostToDevice) == cudaSuccess;
   if (h.narrow)
@@ -1158,12 +1185,61 @@ int upload_sell(const HostSell &h, int grid, DeviceSell &d) {
   ok = ok && cudaMemcpy(d.perm, h.perm.data(), sizeof(int) * h.n, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(d.iperm, h.iperm.data(), sizeof(int) * h.n, cudaMemcpyHostToDevice) == cudaSuccess;
   ok = ok && cudaMemcpy(d.cta_slice, cs.data(), sizeof(int) * (grid + 1), cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!wslice.empty())
+    ok = ok && cudaMemcpy(d.wslice, wslice.data(), sizeof(int) * wslice.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(d.woff, woff.data(), sizeof(int) * woff.size(), cudaMemcpyHostToDevice) == cudaSuccess;
   return ok ? FFG_OK : FFG_CUDA_ERROR;
+}
+
+// A slice costs its stored entries plus kSliceCost for its row epilogue and
+// copy waits.  CTAs take contiguous slice ranges of about equal cost; inside
+// a CTA the slices are dealt longest first, each to the warp with the least
+// cost so far (lowest warp on ties), and a warp takes its slices in the
+// order dealt.  Dealing by cost rather than round robin matters because
+// slices are sorted by length inside each sigma window, so every 32nd slice
+// lands on a warp-dependent mix of long and short ones.
+void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector<int> &cs,
+                    std::vector<int> &wslice, std::vector<int> &woff) {
+  constexpr int64_t kSliceCost = 128;
+  const int64_t ns = n_slices;
+  auto cost = [&](int64_t s) { return soff[s + 1] - soff[s] + kSliceCost; };
+  std::vector<int64_t> cum((size_t)ns + 1, 0);
+  for (int64_t s = 0; s < ns; ++s) cum[s + 1] = cum[s] + cost(s);
+  cs.assign((size_t)grid + 1, 0);
+  for (int b = 1; b < grid; ++b) {
+    const int64_t target = (int64_t)((double)cum[ns] * b / grid);
+    const int s = (int)(std::lower_bound(cum.begin(), cum.end(), target) - cum.begin());
+    cs[b] = std::max(cs[b - 1], std::min<int>(s, (int)ns));
+  }
+  cs[grid] = (int)ns;
+  wslice.clear();
+  wslice.reserve((size_t)ns);
+  woff.assign((size_t)grid * kWarps + 1, 0);
+  std::vector<std::vector<int>> lists(kWarps);
+  std::vector<int> order;
+  for (int b = 0; b < grid; ++b) {
+    order.resize((size_t)(cs[b + 1] - cs[b]));
+    for (size_t i = 0; i < order.size(); ++i) order[i] = cs[b] + (int)i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return cost(x) > cost(y); });
+    std::vector<int64_t> load(kWarps, 0);
+    for (int s : order) {
+      const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      lists[w].push_back(s);
+      load[w] += cost(s);
+    }
+    for (int w = 0; w < kWarps; ++w) {
+      woff[(size_t)b * kWarps + w] = (int)wslice.size();
+      wslice.insert(wslice.end(), lists[w].begin(), lists[w].end());
+      lists[w].clear();
+    }
+  }
+  woff[(size_t)grid * kWarps] = (int)wslice.size();
 }
 
 void free_sell(DeviceSell &d) {
   void *ptrs[] = {d.soff, d.dcol, d.col, d.val64, d.val32, d.dinv64, d.dinv32, d.perm, d.iperm,
-                  d.cta_slice};
+                  d.cta_slice, d.wslice, d.woff};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d = DeviceSell();
@@ -1234,6 +1310,8 @@ PcgParams make_params(const DeviceSell &A, const double *b, double *x,
   P.d32 = A.dinv32;
   P.d64 = A.dinv64;
   P.cta_slice = A.cta_slice;
+  P.wslice = A.wslice;
+  P.woff = A.woff;
   P.b = b;
   P.x = x;
   P.r64 = w.r64;

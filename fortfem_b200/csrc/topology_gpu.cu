@@ -628,26 +628,26 @@ int build_topology_device(Topology &t, int mode, const uint8_t *mask, int grid,
   Buf<int> colw;
   Buf<double> v64, d64;
   Buf<float> v32, d32;
-  Buf<int> cta;
+  Buf<int> cta, wsl, wof;
   if (narrow) FFG_ALLOC(dcol, P);
   else FFG_ALLOC(colw, P);
   FFG_ALLOC(v64, P); FFG_ALLOC(v32, P); FFG_ALLOC(d64, F); FFG_ALLOC(d32, F);
-  FFG_ALLOC(cta, (size_t)grid + 1);
   FFG_TRY(cudaMemset(v64.p, 0, sizeof(double) * P));
   FFG_TRY(cudaMemset(v32.p, 0, sizeof(float) * P));
   sell_fill_kernel<<<nblk(S.n_slices * kSliceRows), kT>>>(F, S.n_slices, soff.p, perm.p, iperm.p,
                                                            col_ptr.p, row.p, dcol.p, colw.p);
-  // CTA partition: contiguous slice ranges with about equal stored entries
+  // CTA partition and per-warp slice lists
   std::vector<int64_t> hsoff((size_t)S.n_slices + 1);
   FFG_TRY(cudaMemcpy(hsoff.data(), soff.p, sizeof(int64_t) * hsoff.size(), cudaMemcpyDeviceToHost));
-  std::vector<int> cs((size_t)grid + 1, 0);
-  for (int b = 1; b < grid; ++b) {
-    const int64_t target = (int64_t)((double)S.padded * b / grid);
-    const int s = (int)(std::lower_bound(hsoff.begin(), hsoff.end(), target) - hsoff.begin());
-    cs[b] = std::max(cs[b - 1], std::min<int>(s, (int)S.n_slices));
-  }
-  cs[grid] = (int)S.n_slices;
+  std::vector<int> cs, hws, hwo;
+  sell_partition(hsoff.data(), S.n_slices, grid, cs, hws, hwo);
+  FFG_ALLOC(cta, cs.size());
+  FFG_ALLOC(wsl, std::max<size_t>(hws.size(), 1));
+  FFG_ALLOC(wof, hwo.size());
   FFG_TRY(cudaMemcpy(cta.p, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice));
+  if (!hws.empty())
+    FFG_TRY(cudaMemcpy(wsl.p, hws.data(), sizeof(int) * hws.size(), cudaMemcpyHostToDevice));
+  FFG_TRY(cudaMemcpy(wof.p, hwo.data(), sizeof(int) * hwo.size(), cudaMemcpyHostToDevice));
   FFG_TRY(cudaDeviceSynchronize());
   // ---- host copies the library reads later
   t.gd.resize((size_t)nl);
@@ -681,6 +681,8 @@ int build_topology_device(Topology &t, int mode, const uint8_t *mask, int grid,
   S.perm = perm.release();
   S.iperm = iperm.release();
   S.cta_slice = cta.release();
+  S.wslice = wsl.release();
+  S.woff = wof.release();
   return FFG_OK;
 }
 

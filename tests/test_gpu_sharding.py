@@ -4,9 +4,11 @@ owned-row dot products, halo gather/scatter) and reproduces the
 single-system PCG with the same iteration count (+-1 for the summation order
 of the dot products): against the library's own single-GPU FP64 solve (the
 owned rows are assembled bit for bit as in the single-system operator) and
-against the oracle's PCG (the reference's algorithm) within 1e-7 relative -
-CG stopped at a 1e-10 residual leaves differences of tol x condition number
-between runs whose dot products are summed in different orders.  Several ranks share the
+against the oracle's PCG (the reference's algorithm) within 1e-7 relative
+(1e-6 for the curl-curl + mass systems) - two solves stopped at a 1e-10
+relative residual may differ by up to 2 x tol x condition number when their
+dot products are summed in different orders, and the Nedelec systems here
+have condition numbers above 1e3.  Several ranks share the
 one GPU and exchange through gloo in host memory, so no kernel waits on
 another."""
 import os
@@ -28,6 +30,10 @@ from shard_gpu_case import case, oracle_solution  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
+def _rtol(family):
+    return 1e-6 if family == K.FFG_TETRA_NEDELEC else 1e-7
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -46,9 +52,9 @@ def test_one_rank_equals_the_single_system(family, degree, n):
     ref, rst = oracle_solution(family, degree, c)
     assert st.converged == rst["converged"]
     assert abs(st.iterations - rst["iterations"]) <= 1
-    assert np.abs(full - ref).max() <= 1e-7 * np.abs(ref).max()
+    assert np.abs(full - ref).max() <= _rtol(family) * np.abs(ref).max()
     one = single_gpu(family, degree, c)
-    assert np.abs(full - one).max() <= 1e-7 * np.abs(one).max()
+    assert np.abs(full - one).max() <= _rtol(family) * np.abs(one).max()
     assert st.exchanged_values == 0
 
 
@@ -91,7 +97,7 @@ def test_ranks_on_one_gpu_equal_the_single_system(family, degree, n, world, tmp_
     for r in res:
         assert bool(r["converged"]) == rst["converged"]
         assert abs(int(r["iterations"]) - rst["iterations"]) <= 1
-        assert np.abs(r["full"] - ref).max() <= 1e-7 * np.abs(ref).max()
-        assert np.abs(r["full"] - one).max() <= 1e-7 * np.abs(one).max()
+        assert np.abs(r["full"] - ref).max() <= _rtol(family) * np.abs(ref).max()
+        assert np.abs(r["full"] - one).max() <= _rtol(family) * np.abs(one).max()
         assert int(r["exchanged"]) > 0
     assert all(np.array_equal(res[0]["full"], r["full"]) for r in res)
