@@ -159,6 +159,7 @@ struct SolveWork {
   double2 *zpd0 = nullptr, *zpd1 = nullptr; // FP64-mode (z, p) pairs, double-buffered
   float *rf = nullptr, *zf = nullptr;       // mixed-mode FP32 r and z = D^-1 r
   float *pf = nullptr, *qf = nullptr;       // mixed-mode FP32 p and q = A p
+  float *xf = nullptr;                      // mixed-mode FP32 step of x not yet folded in
   float2 *zpf0 = nullptr, *zpf1 = nullptr;  // mixed-mode (z, p) pairs once q = A p is direct
   unsigned int *barrier = nullptr;
   int *control = nullptr;    // [0] error status

@@ -79,6 +79,7 @@ struct PcgParams {
   double *x;
   double *r64;
   float *rf, *zf, *pf, *qf;  // mixed mode: r, z = D^-1 r, p, q = A p
+  float *xf;                 // mixed mode: increment of x since it was last folded in
   float2 *zpf0, *zpf1;       // mixed mode after a switch to direct A p: (z, p) pairs
   double *rd, *qd;
   double2 *zpd0, *zpd1;
@@ -804,10 +805,23 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
   o.true_res = sqrt(red[0]);
 }
 
+// Mixed mode: x += the FP32 increment gathered since the last fold, for every
+// row once, then a grid barrier so that x is whole before it is read.
+__device__ bool fold_x(const PcgParams &P, unsigned int &phase) {
+  for_rows_even(P, [&](int row) {
+    P.x[row] += (double)P.xf[row];
+    P.xf[row] = 0.f;
+  });
+  return grid_barrier(P, phase);
+}
+
 // Mixed mode: the PCG recurrences in FP32 on a scaled residual, the solution
 // accumulated in FP64, two grid barriers an iteration:
 //   A: w = A z (gathering z alone), p = z + beta p, q = w + beta q, (p, q)
-//   B: x += alpha p (FP64), r -= alpha q, z = D^-1 r, (r, r), (r, z)
+//   B: dx += alpha p, r -= alpha q, z = D^-1 r, (r, r), (r, z)
+// The step dx is accumulated in FP32 and added to the FP64 x before every
+// true residual (iterative refinement: each interval between reliable updates
+// solves for a correction whose own FP32 rounding the next interval removes).
 // q is A p up to the rounding of its recurrence, and every reliable update
 // recomputes it from p.  That rounding grows with the condition number: the
 // first reliable update forced by a plateau, or one whose true residual has
@@ -846,6 +860,7 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
       z[row] = zz;
       p[row] = 0.f;
       q[row] = 0.f;
+      P.xf[row] = 0.f;
       part[0] += (double)rr * (double)zz;
     });
     write_partials(P, phase, part, 1);
@@ -855,6 +870,7 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
   }
   tm.u += stamp(P) - t0;
   double beta = 0.0;
+  bool unfolded = false;  // xf holds a step not yet added to x
   const int budget = P.max_it - o.iterations;
   for (int it = 1; !converged && it <= budget; ++it) {
     // A: q = A p, p = z + beta p, (p, q)
@@ -881,16 +897,16 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     }
     const double alpha = rz / pAp;
     const float al = (float)alpha;
-    const double xs = alpha * scale;
-    // B: x += alpha p (FP64), r -= alpha q, z = D^-1 r
+    const float xs = (float)(alpha * scale);
+    // B: dx += alpha p, r -= alpha q, z = D^-1 r
     t0 = stamp(P);
     part[0] = part[1] = 0.0;
     part[2] = (cta_of(P) == 0 && threadIdx.x == 0 && globaltimer() - t_start > P.limit_ns) ? 1.0 : 0.0;
     {
-      double xv[kRowBatch] = {};
-      float pv[kRowBatch] = {}, rv[kRowBatch] = {}, qv[kRowBatch] = {}, dv[kRowBatch] = {};
+      float xv[kRowBatch] = {}, pv[kRowBatch] = {}, rv[kRowBatch] = {}, qv[kRowBatch] = {},
+            dv[kRowBatch] = {};
       auto step = [&](int row, int u) {
-        P.x[row] = xv[u] + xs * (double)pv[u];
+        P.xf[row] = xv[u] + xs * pv[u];
         const float rr = rv[u] - al * qv[u];
         r[row] = rr;
         const float zz = dv[u] * rr;
@@ -900,7 +916,7 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
         part[1] += (double)rr * (double)zz;
       };
       auto load = [&](int row, int u) {
-        xv[u] = P.x[row];
+        xv[u] = P.xf[row];
         rv[u] = r[row];
         qv[u] = q[row];
         dv[u] = dinv[row];
@@ -918,6 +934,7 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     tm.b += t1 - t0;
     tm.bw += t2 - t1;
     ++o.iterations;
+    unfolded = true;
     if (direct) cur ^= 1;
     const double rr = red[0], rz_new = red[1];
     const double est = sqrt(rr) * scale;
@@ -937,6 +954,8 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     if (o.updates >= P.max_updates) break;
     ++o.updates;
     t0 = stamp(P);
+    if (!fold_x(P, phase)) { o.aborted = 1; return; }
+    unfolded = false;
     part[0] = 0.0;
     residual(P);
     for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
@@ -996,6 +1015,7 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     window = max(kMinWindow, 4 * (o.iterations - since));
     since = o.iterations;
   }
+  if (unfolded && !fold_x(P, phase)) { o.aborted = 1; return; }
   o.converged = converged;
   o.final_res = true_res;
   if (converged) {
@@ -1263,6 +1283,7 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
   A((void **)&w.zf, N * sizeof(float));
   A((void **)&w.pf, N * sizeof(float));
   A((void **)&w.qf, N * sizeof(float));
+  A((void **)&w.xf, N * sizeof(float));
   A((void **)&w.zpf0, N * sizeof(float2));
   A((void **)&w.zpf1, N * sizeof(float2));
   A((void **)&w.partial, 2 * kSlots * (size_t)grid * sizeof(double));
@@ -1287,7 +1308,7 @@ int solve_work_alloc(SolveWork &w, int64_t n, int grid) {
 }
 
 void solve_work_free(SolveWork &w) {
-  void *ptrs[] = {w.r64, w.rd, w.qd, w.zpd0, w.zpd1, w.rf, w.zf, w.pf, w.qf, w.zpf0, w.zpf1,
+  void *ptrs[] = {w.r64, w.rd, w.qd, w.zpd0, w.zpd1, w.rf, w.zf, w.pf, w.qf, w.xf, w.zpf0, w.zpf1,
                   w.partial,
                   w.barrier, w.control, w.result};
   for (void *p : ptrs)
@@ -1315,7 +1336,8 @@ PcgParams make_params(const DeviceSell &A, const double *b, double *x,
   P.b = b;
   P.x = x;
   P.r64 = w.r64;
-  P.rf = w.rf; P.zf = w.zf; P.pf = w.pf; P.qf = w.qf; P.zpf0 = w.zpf0; P.zpf1 = w.zpf1;
+  P.rf = w.rf; P.zf = w.zf; P.pf = w.pf; P.qf = w.qf; P.xf = w.xf;
+  P.zpf0 = w.zpf0; P.zpf1 = w.zpf1;
   P.rd = w.rd; P.qd = w.qd; P.zpd0 = w.zpd0; P.zpd1 = w.zpd1;
   P.partial = w.partial;
   P.bar = w.barrier;
