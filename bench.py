@@ -38,8 +38,8 @@ TOL = 1e-10
 # `bench.py --steps 1 --warmup 3 --no-cpu --no-e2e --no-fp64 --serving-requests 0`, and the
 # algorithmic bytes of that launch; the live launch's traffic is scaled by
 # its own algorithmic bytes.
-PCG_TRAFFIC_BYTES = 102.357361e9 + 3.228644e9
-PCG_TRAFFIC_ALG_BYTES = 159235912804.0
+PCG_TRAFFIC_BYTES = 103.621655e9 + 2.646321e9
+PCG_TRAFFIC_ALG_BYTES = 158778363588.0
 
 
 def parse():
