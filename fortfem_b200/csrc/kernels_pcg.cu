@@ -361,16 +361,14 @@ struct StageShape {
   static constexpr int VAL = COLS * 32 * (int)sizeof(V);
 };
 
-// Chunk c of slice s into stage buffer `buf` (values, then indices).  Slice
-// offsets are multiples of 32 entries and chunks multiples of COLS columns,
-// so both sources are 64-byte aligned and both sizes multiples of 64.
+// The chunk of `cols` columns starting at entry e0 into stage buffer `buf`
+// (values, then indices).  Slice offsets are multiples of 32 entries and
+// chunks multiples of COLS columns, so both sources are 64-byte aligned and
+// both sizes multiples of 64.
 template <typename V, bool NARROW>
-__device__ __forceinline__ void issue_chunk(const PcgParams &P, const V *val, int s, int c,
+__device__ __forceinline__ void issue_chunk(const PcgParams &P, const V *val, int64_t e0, int cols,
                                             unsigned char *buf, unsigned long long *m) {
   using SS = StageShape<V, NARROW>;
-  const int64_t e0 = P.soff[s] + (int64_t)c * SS::COLS * 32;
-  const int len = (int)((P.soff[s + 1] - P.soff[s]) / 32);
-  const int cols = min(SS::COLS, len - c * SS::COLS);
   const unsigned nv = (unsigned)cols * 32u * (unsigned)sizeof(V);
   const unsigned nc = (unsigned)cols * 32u * (NARROW ? 2u : 4u);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -380,11 +378,11 @@ __device__ __forceinline__ void issue_chunk(const PcgParams &P, const V *val, in
   else bulk_load(buf + SS::VAL, P.col + e0, nc, m);
 }
 
-template <int COLS>
-__device__ __forceinline__ int slice_chunks(const PcgParams &P, int s) {
-  const int len = (int)((P.soff[s + 1] - P.soff[s]) / 32);
-  return (len + COLS - 1) / COLS;
-}
+// One slice of a warp's list: its index, first entry and length in columns.
+struct SliceRef {
+  int s, len;
+  int64_t e0;
+};
 
 // The SpMV of spmv_pairs (same slices per warp, same return value) with the
 // operator streamed by the bulk-copy engine: warp w keeps one chunk of COLS
@@ -403,20 +401,55 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const WarpSlices ws = warp_slices(P, warp);
   unsigned char *wbuf = stage_smem + (size_t)warp * kStages * kStageBytes;
-  // producer cursor: chunk pc of the warp's pk-th slice is copied next
+  // lane k holds slice k of the warp's list (read once per SpMV), so that the
+  // copy of the next chunk never waits on a load of the slice offsets; a
+  // list longer than 32 reads the rest from memory
+  int my_s = 0, my_len = 0;
+  int64_t my_e0 = 0;
+  if (lane < ws.n) {
+    my_s = ws.at(lane);
+    my_e0 = P.soff[my_s];
+    my_len = (int)((P.soff[my_s + 1] - my_e0) / kSliceRows);
+  }
+  auto slice = [&](int k) {  // k is warp-uniform
+    SliceRef r;
+    if (k < 32) {
+      r.s = __shfl_sync(0xffffffffu, my_s, k);
+      r.len = __shfl_sync(0xffffffffu, my_len, k);
+      r.e0 = __shfl_sync(0xffffffffu, my_e0, k);
+    } else {
+      r.s = ws.at(k);
+      r.e0 = P.soff[r.s];
+      r.len = (int)((P.soff[r.s + 1] - r.e0) / kSliceRows);
+    }
+    return r;
+  };
+  // producer cursor: chunk pc of the warp's pk-th slice (pr) is copied next
   // (slices with no columns are skipped)
   int pk = 0, pc = 0;
-  while (pk < ws.n && slice_chunks<COLS>(P, ws.at(pk)) == 0) ++pk;
-  auto advance = [&]() {
-    if (++pc >= slice_chunks<COLS>(P, ws.at(pk))) {
-      pc = 0;
-      do ++pk; while (pk < ws.n && slice_chunks<COLS>(P, ws.at(pk)) == 0);
+  SliceRef pr{0, 0, 0};
+  auto seek = [&]() {
+    for (; pk < ws.n; ++pk) {
+      pr = slice(pk);
+      if (pr.len > 0) break;
     }
+  };
+  seek();
+  auto advance = [&]() {
+    if (++pc * COLS >= pr.len) {
+      pc = 0;
+      ++pk;
+      seek();
+    }
+  };
+  auto issue = [&](int st) {
+    if (lane == 0)
+      issue_chunk<V, NARROW>(P, val, pr.e0 + (int64_t)pc * COLS * 32, min(COLS, pr.len - pc * COLS),
+                             wbuf + st * kStageBytes, &mbar[warp][st]);
   };
   unsigned pending = 0;  // stages with a copy issued and not yet waited for
   for (int k = 0; k < kStages && pk < ws.n; ++k) {
-    if (lane == 0)
-      issue_chunk<V, NARROW>(P, val, ws.at(pk), pc, wbuf + k * kStageBytes, &mbar[warp][k]);
+    issue(k);
     pending |= 1u << k;
     advance();
   }
@@ -424,9 +457,9 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
   bool ok = true;
   double dot = 0.0;
   for (int ck = 0; ck < ws.n; ++ck) {
-    const int cs = ws.at(ck);
-    const int len = (int)((P.soff[cs + 1] - P.soff[cs]) / 32);
-    const int row = cs * kSliceRows + lane;
+    const SliceRef cr = slice(ck);
+    const int len = cr.len;
+    const int row = cr.s * kSliceRows + lane;
     V acc = 0;
     for (int c = 0; c * COLS < len; ++c, ++seq) {
       const int st = (int)(seq % kStages);
@@ -454,9 +487,7 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
       __syncwarp();
       if (pk < ws.n) {
         if (ok) {
-          if (lane == 0)
-            issue_chunk<V, NARROW>(P, val, ws.at(pk), pc, wbuf + st * kStageBytes,
-                                   &mbar[warp][st]);
+          issue(st);
           pending |= 1u << st;
         }
         advance();
