@@ -1251,7 +1251,7 @@ int upload_sell(const HostSell &h, int grid, DeviceSell &d) {
 // lands on a warp-dependent mix of long and short ones.
 void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector<int> &cs,
                     std::vector<int> &wslice, std::vector<int> &woff) {
-  constexpr int64_t kSliceCost = 128;
+  constexpr int64_t kSliceCost = 256;
   const int64_t ns = n_slices;
   auto cost = [&](int64_t s) { return soff[s + 1] - soff[s] + kSliceCost; };
   std::vector<int64_t> cum((size_t)ns + 1, 0);
