@@ -260,13 +260,6 @@ __device__ __forceinline__ void prefetch_slice(const PcgParams &P, const V *val,
   else prefetch_l2(P.col + e0, (unsigned)((e1 - e0) * sizeof(int)));
 }
 
-// Next slice of this CTA's range for the calling warp (shared counter).
-__device__ __forceinline__ int grab_slice(int *counter, int lane) {
-  int t = 0;
-  if (lane == 0) t = atomicAdd(counter, 1);
-  return __shfl_sync(0xffffffffu, t, 0);
-}
-
 // SELL SpMV over this CTA's slices: each warp walks its own slices
 // (warp_slices) and prefetches its next slice into L2 while it sums the
 // current one; lane l owns row 32s+l and accumulates it in a fixed order.
@@ -285,12 +278,12 @@ __device__ __noinline__ double spmv_pairs(const PcgParams &P, const V *__restric
     const int64_t base = P.soff[s] + lane;
     const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
     const int row = s * kSliceRows + lane;
-    V acc = 0;
+    typename G::Acc acc{};
 #pragma unroll 8
     for (int j = 0; j < len; ++j) {
       const int64_t k = base + (int64_t)j * kSliceRows;
       const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
-      acc += __ldcs(val + k) * g.column(c);
+      g.accumulate(acc, __ldcs(val + k), c);
     }
     if (row < P.n) dot += g.finish(row, acc);
   }
@@ -460,7 +453,7 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
     const SliceRef cr = slice(ck);
     const int len = cr.len;
     const int row = cr.s * kSliceRows + lane;
-    V acc = 0;
+    typename G::Acc acc{};
     for (int c = 0; c * COLS < len; ++c, ++seq) {
       const int st = (int)(seq % kStages);
       if (ok) {
@@ -480,7 +473,7 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
           if (j < cols) {
             const int cidx = NARROW ? row + (int)reinterpret_cast<const int16_t *>(ib)[j * 32 + lane]
                                     : reinterpret_cast<const int *>(ib)[j * 32 + lane];
-            acc += vb[j * 32 + lane] * g.column(cidx);
+            g.accumulate(acc, vb[j * 32 + lane], cidx);
           }
         }
       }
@@ -503,47 +496,6 @@ __device__ __noinline__ double spmv_staged(const PcgParams &P, const V *__restri
   if (lane == 0) g_mparity[warp] = parity;
   __syncthreads();
   return dot;
-}
-
-// r64 = b - A64 x over this CTA's slices (same scheduling as spmv_pairs).
-template <bool NARROW>
-__device__ __noinline__ void spmv_residual(const PcgParams &P) {
-  __shared__ int next_slice;
-  int s0, s1;
-  slice_range(P, s0, s1);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) next_slice = s0 + kWarps;
-  __syncthreads();
-  int s = s0 + warp;
-  int nxt = s < s1 ? grab_slice(&next_slice, lane) : s1;
-  if (lane == 0) {
-    if (s < s1) prefetch_slice<double, NARROW>(P, P.v64, s);
-    if (nxt < s1) prefetch_slice<double, NARROW>(P, P.v64, nxt);
-  }
-  while (s < s1) {
-    const int64_t base = P.soff[s] + lane;
-    const int len = (int)((P.soff[s + 1] - P.soff[s]) / kSliceRows);
-    const int row = s * kSliceRows + lane;
-    double acc = 0.0;
-#pragma unroll 8
-    for (int j = 0; j < len; ++j) {
-      const int64_t k = base + (int64_t)j * kSliceRows;
-      const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
-      acc += __ldcs(P.v64 + k) * P.x[c];
-    }
-    if (row < P.n) P.r64[row] = P.b[row] - acc;
-    s = nxt;
-    if (s < s1) {
-      nxt = grab_slice(&next_slice, lane);
-      if (lane == 0 && nxt < s1) prefetch_slice<double, NARROW>(P, P.v64, nxt);
-    }
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void residual(const PcgParams &P) {
-  if (P.dcol) spmv_residual<true>(P);
-  else spmv_residual<false>(P);
 }
 
 template <class F>
@@ -609,9 +561,10 @@ __device__ __forceinline__ unsigned long long stamp(const PcgParams &P) {
   return (cta_of(P) == 0 && threadIdx.x == 0) ? globaltimer() : 0ull;
 }
 
-// Gather policies of the SpMV: column(c) is the operand value of column c and
-// finish(row, acc) stores the row's product with the row-wise updates that
-// belong to it, returning the row's term of (p, q).
+// Gather policies of the SpMV: accumulate(acc, a, c) adds the stored entry a
+// of column c to the row's accumulator and finish(row, acc) stores the row's
+// results with the row-wise updates that belong to them, returning the row's
+// term of the phase's dot product.
 
 // FP64 PCG: the operand p = z + beta p_old of column c is formed on the fly
 // from the (z, p_old) pair; finish stores p and q = A p.
@@ -621,10 +574,12 @@ struct PairGather {
   V2 *__restrict__ zn;
   V *__restrict__ q;
   V beta;
+  using Acc = V;
   __device__ __forceinline__ V column(int c) const {
     const V2 a = zc[c];
     return a.x + beta * a.y;
   }
+  __device__ __forceinline__ void accumulate(Acc &acc, V v, int c) const { acc += v * column(c); }
   __device__ __forceinline__ double finish(int row, V acc) const {
     const V2 a = zc[row];
     const V pn = a.x + beta * a.y;
@@ -642,7 +597,8 @@ struct ZGather {
   float *__restrict__ p;
   float *__restrict__ q;
   float beta;
-  __device__ __forceinline__ float column(int c) const { return z[c]; }
+  using Acc = float;
+  __device__ __forceinline__ void accumulate(Acc &acc, float v, int c) const { acc += v * z[c]; }
   __device__ __forceinline__ double finish(int row, float acc) const {
     const float pn = z[row] + beta * p[row];
     const float qn = acc + beta * q[row];
@@ -652,14 +608,26 @@ struct ZGather {
   }
 };
 
-// q = A p directly (mixed mode, at a reliable update).
-struct PGather {
+// r64 = b - A x with the FP64 operator, returning the row's term of (r64, r64);
+// with p given, also q = A p (FP64 products, stored in FP32) in the same pass.
+struct ResidualGather {
+  const double *__restrict__ x;
   const float *__restrict__ p;
   float *__restrict__ q;
-  __device__ __forceinline__ float column(int c) const { return p[c]; }
-  __device__ __forceinline__ double finish(int row, float acc) const {
-    q[row] = acc;
-    return 0.0;
+  const double *__restrict__ b;
+  double *__restrict__ r64;
+  struct Acc {
+    double x = 0.0, p = 0.0;
+  };
+  __device__ __forceinline__ void accumulate(Acc &acc, double v, int c) const {
+    acc.x += v * x[c];
+    if (p) acc.p += v * (double)p[c];
+  }
+  __device__ __forceinline__ double finish(int row, const Acc &acc) const {
+    const double r = b[row] - acc.x;
+    r64[row] = r;
+    if (p) q[row] = (float)acc.p;
+    return r * r;
   }
 };
 
@@ -671,14 +639,20 @@ __device__ __forceinline__ double spmv(const PcgParams &P, const V *val, const G
   return spmv_pairs<V, false>(P, val, g);
 }
 
+// r64 = b - A x; returns the thread's share of (r64, r64) (and q = A p when p
+// is given).
+__device__ __forceinline__ double residual(const PcgParams &P, const float *p = nullptr,
+                                           float *q = nullptr) {
+  return spmv(P, P.v64, ResidualGather{P.x, p, q, P.b, P.r64});
+}
+
 // r64 = b - A x and the partial sums of (r64, r64) and (b, b), reduced.
 __device__ bool residual_norms(const PcgParams &P, unsigned int &phase, double *red) {
   double part[kSlots];
-  residual(P);
-  part[0] = part[1] = 0.0;
+  part[0] = residual(P);
+  part[1] = 0.0;
   for_rows(P, [&](int row) {
-    const double bb = P.b[row], rr = P.r64[row];
-    part[0] += rr * rr;
+    const double bb = P.b[row];
     part[1] += bb * bb;
   });
   write_partials(P, phase, part, 2);
@@ -790,9 +764,7 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
       // the continuation's target is the true residual: check b - A x and,
       // while it still falls, replace the recursive residual with it
       t0 = stamp(P);
-      part[0] = 0.0;
-      residual(P);
-      for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+      part[0] = residual(P);
       write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
       read_partials(P, phase, red, 1);
@@ -826,9 +798,7 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
   o.final_res = true_res;
   // true FP64 residual of the returned x
   t0 = stamp(P);
-  part[0] = 0.0;
-  residual(P);
-  for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+  part[0] = residual(P);
   write_partials(P, phase, part, 1);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 1);
@@ -987,9 +957,9 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     t0 = stamp(P);
     if (!fold_x(P, phase)) { o.aborted = 1; return; }
     unfolded = false;
-    part[0] = 0.0;
-    residual(P);
-    for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+    // q = A p comes with the residual (used if the update goes on in the
+    // recurrence form)
+    part[0] = direct ? residual(P) : residual(P, p, q);
     write_partials(P, phase, part, 1);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
     read_partials(P, phase, red, 1);
@@ -1001,8 +971,9 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     if (stall >= 2) { o.stagnated = 1; tm.u += stamp(P) - t0; break; }
     const bool to_direct = !direct && (slow || (stall > 0 && !grew));
     // r = (b - A x) / ||b - A x|| in the new units and z = D^-1 r; p keeps
-    // the old units and the ratio goes into beta.  The recurrence form takes
-    // q = A p afresh; the direct form (or the switch to it) stores (z, p).
+    // the old units and the ratio goes into beta.  The recurrence form goes
+    // on with q = A p from the residual pass; the direct form (or the switch
+    // to it) stores (z, p).
     const double ratio = scale / true_res;
     const double inv = 1.0 / true_res;
     part[0] = 0.0;
@@ -1026,7 +997,6 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
       });
       direct = true;
     } else {
-      spmv(P, P.v32, PGather{p, q});
       for_rows(P, [&](int row) {
         const float rr2 = (float)(P.r64[row] * inv);
         const float zz = dinv[row] * rr2;
@@ -1056,9 +1026,7 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
   if (o.stagnated) return;  // the FP64 continuation measures its own residual
   // true FP64 residual of the returned x
   t0 = stamp(P);
-  part[0] = 0.0;
-  residual(P);
-  for_rows(P, [&](int row) { part[0] += P.r64[row] * P.r64[row]; });
+  part[0] = residual(P);
   write_partials(P, phase, part, 1);
   if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
   read_partials(P, phase, red, 1);
