@@ -38,8 +38,8 @@ TOL = 1e-10
 # `bench.py --steps 1 --warmup 3 --no-cpu --no-e2e --no-fp64 --serving-requests 0`, and the
 # algorithmic bytes of that launch; the live launch's traffic is scaled by
 # its own algorithmic bytes.
-PCG_TRAFFIC_BYTES = 103.896268e9 + 3.543342e9
-PCG_TRAFFIC_ALG_BYTES = 158778363588.0
+PCG_TRAFFIC_BYTES = 101.803065e9 + 3.318534e9
+PCG_TRAFFIC_ALG_BYTES = 159007138196.0
 
 
 def parse():

@@ -49,6 +49,25 @@ def test_batch_matches_alone_and_the_cooperative_path():
     eng.close()
 
 
+def test_one_block_system_with_more_than_32_slices_per_warp():
+    # 18^3 x 6 P2: 42,875 free rows, 1,340 slices, so each of the block's 32
+    # warps walks about 42 slices (past the 32 a warp keeps in registers)
+    eng = S.DeviceEngine(keep_solutions=True)
+    r = S.Request(0, "p2", 18, 211)
+    assert eng.can_host(r.key)
+    mesh = eng.meshes[r.key]
+    assert mesh.problem.n_free > 32 * 32 * 32
+    one = _run(eng, "cta_per_system", [r])[0]
+    assert one.converged and one.true_relative_residual <= 1e-10
+    v, kappa, src = eng._inputs(mesh, r)
+    ref = torch.empty(mesh.problem.n_dofs, dtype=torch.float64, device=eng.device)
+    st = mesh.problem.solve_device(v, ref, 1.0, 0.0, kappa, None, src, None, eng.options)
+    assert st.converged
+    ref = ref.cpu().numpy()
+    assert np.abs(one.solution - ref).max() <= 1e-6 * np.abs(ref).max()
+    eng.close()
+
+
 def test_serving_stream_results_same_alone_and_in_the_mix():
     reqs = S.poisson_stream(40, 2000.0, seed=11, p1_range=(8, 96), p2_range=(4, 14))
     eng = S.DeviceEngine(keep_solutions=True)
