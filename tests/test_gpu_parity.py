@@ -217,6 +217,23 @@ def test_mixed_precision_reaches_true_residual_1e10():
     assert np.abs(sol[free] - x_direct).max() <= 1e-7 * np.abs(x_direct).max()
 
 
+def test_host_solve_into_caller_buffer():
+    import torch
+    v, t = jittered_box(5, 0.1, 17)
+    kappa = np.exp(np.random.default_rng(17).standard_normal(len(t)))
+    with ff.Problem(K.FFG_TETRA_LAGRANGE, 2, t, len(v), rule=K.FFG_RULE_DEGREE_TWO) as prob:
+        pts = prob.sample_points(v)
+        src = np.cos(pts[..., 0]) * pts[..., 1]
+        sol, _ = prob.solve(v, 1.0, 0.0, kappa, None, src)
+        out = torch.zeros(prob.n_dofs, dtype=torch.float64).pin_memory().numpy()
+        sol2, st = prob.solve(v, 1.0, 0.0, kappa, None, src, out=out)
+        assert st.converged and sol2 is out and np.array_equal(out, sol)
+        for bad in (np.zeros(prob.n_dofs, np.float32), np.zeros(prob.n_dofs + 1),
+                    np.zeros(2 * prob.n_dofs)[::2]):
+            with pytest.raises(ff.FortfemError):
+                prob.solve(v, 1.0, 0.0, kappa, None, src, out=bad)
+
+
 def test_p1_unit_square_solve_matches_reference_dense_path():
     v, t = ff.unit_square_mesh(65)
     opts = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
