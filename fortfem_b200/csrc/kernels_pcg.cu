@@ -1,16 +1,17 @@
 // Persistent Jacobi-PCG (sm_100a) on a SELL-32-sigma operator.
 //
 // One cooperative launch runs the whole solve.  Every CTA owns a contiguous
-// range of 32-row slices (balanced by stored entries) and therefore a
-// contiguous range of rows of the permuted system.  In the SpMV a warp walks
-// one slice: lane l accumulates row 32s+l in a fixed order, reading 128
-// contiguous bytes of values and 64 (16-bit column offsets) per step with
-// evict-first streaming loads.  Vector phases walk the CTA's rows with all
-// threads, coalesced.  Dot products are reduced per CTA, written to a
-// per-phase partial buffer and summed by every CTA in the same fixed order,
-// so all CTAs take identical decisions and results are bit-reproducible for
-// a given grid.  Grid barriers spin with a time bound and report FFG_TIMEOUT
-// instead of hanging.
+// range of 32-row slices (balanced by stored entries plus a per-slice cost)
+// and therefore a contiguous range of rows of the permuted system; its
+// slices are dealt to its warps longest first (sell_partition).  In the SpMV
+// a warp walks its slices: the bulk-copy engine streams each slice's values
+// and 16-bit column offsets into shared memory, 10 columns at a time, and
+// lane l accumulates row 32s+l in a fixed order.  Vector phases walk rows
+// with all threads, coalesced.  Dot products are summed per thread in a
+// fixed row order, reduced per CTA, written to a per-phase partial buffer and
+// summed by every CTA in the same fixed order, so all CTAs take identical
+// decisions and results are bit-reproducible for a given grid.  Grid
+// barriers spin with a time bound and report FFG_TIMEOUT instead of hanging.
 //
 // FP64 mode restates pcg_solve_operator / pcg_iteration_loop
 // (src/solvers/advanced_solvers.f90:831-925), two grid barriers an iteration:
@@ -281,9 +282,9 @@ __device__ __noinline__ double spmv_pairs(const PcgParams &P, const V *__restric
     typename G::Acc acc{};
 #pragma unroll 8
     for (int j = 0; j < len; ++j) {
-      const int64_t k = base + (int64_t)j * kSliceRows;
-      const int c = NARROW ? row + (int)__ldcs(P.dcol + k) : __ldcs(P.col + k);
-      g.accumulate(acc, __ldcs(val + k), c);
+      const int64_t e = base + (int64_t)j * kSliceRows;
+      const int c = NARROW ? row + (int)__ldcs(P.dcol + e) : __ldcs(P.col + e);
+      g.accumulate(acc, __ldcs(val + e), c);
     }
     if (row < P.n) dot += g.finish(row, acc);
   }
