@@ -22,6 +22,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -75,12 +76,14 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region; the raw
+    samples go to clocks_<gpu>.csv in $FFG_CLOCKS_DIR (default: the temp dir)."""
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{index}.csv")
+        out = os.environ.get("FFG_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"clocks_{index}.csv")
 
     def start(self):
         try:
