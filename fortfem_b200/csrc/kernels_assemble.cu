@@ -429,6 +429,83 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
   }
 }
 
+// CSC columns of high-order elements (n_b >= 16), one warp per free column:
+// the incidences go in ascending cell order as in column_kernel, and for each
+// one the lanes take the element's local rows i (distinct rows land in
+// distinct slots), adding into the column held in shared memory, so every
+// entry receives its terms in the same order as in column_kernel; the
+// element column, the slot row and the finished column are read and written
+// contiguously.  The lifting is summed per lane and then across the warp in
+// a fixed order.  Shared memory: max_len doubles per warp.
+template <int FAMILY>
+__global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
+                                       const int64_t *__restrict__ col_ptr,
+                                       const int64_t *__restrict__ inc_ptr,
+                                       const int *__restrict__ inc_cell,
+                                       const uint8_t *__restrict__ inc_local,
+                                       const uint16_t *__restrict__ slot,
+                                       const int *__restrict__ gd, int nb,
+                                       const double *__restrict__ geo, int stride,
+                                       const double *__restrict__ ref,
+                                       const double *__restrict__ load_basis, int nq,
+                                       const double *__restrict__ elem,
+                                       const double *__restrict__ cell_rhs,
+                                       const double *__restrict__ g, double *__restrict__ val,
+                                       double *__restrict__ rhs) {
+  extern __shared__ double col_acc[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+  if (j >= n_free) return;
+  const int64_t start = col_ptr[j];
+  const int len = (int)(col_ptr[j + 1] - start);
+  double *A = col_acc + (size_t)warp * max_len;
+  for (int k = lane; k < len; k += 32) A[k] = 0.0;
+  __syncwarp();
+  const size_t nn = (size_t)nb * nb;
+  constexpr int NT = FAMILY == FFG_TRIANGLE_LAGRANGE ? 4 : 7;
+  constexpr bool TENSORS = FAMILY == FFG_TETRA_LAGRANGE || FAMILY == FFG_TRIANGLE_LAGRANGE;
+  double b = 0.0, lift = 0.0;
+  for (int64_t p = inc_ptr[j]; p < inc_ptr[j + 1]; ++p) {
+    const int e = inc_cell[p];
+    const int l = inc_local[p];
+    const uint16_t *sl = slot + (size_t)p * nb;
+    const int *ge = gd + (size_t)nb * e;
+    double gco[NT];
+    double F = 0.0;
+    if (TENSORS) {
+      const double *gg = geo + (size_t)stride * e;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) gco[t] = gg[t];
+      for (int q = 0; q < nq; ++q) F += gg[NT + q] * __ldg(load_basis + (size_t)q * nb + l);
+    } else {
+      F = cell_rhs[(size_t)nb * e + l];
+    }
+    for (int i = lane; i < nb; i += 32) {
+      double kil;
+      if (TENSORS) {
+        const size_t off = i + (size_t)nb * l;
+        kil = 0.0;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) kil += gco[t] * __ldg(ref + t * nn + off);
+      } else {
+        kil = elem[nn * e + i + (size_t)nb * l];
+      }
+      const uint16_t sidx = sl[i];
+      if (sidx == kConstrainedSlot) {
+        if (g) lift += kil * g[ge[i]];
+      } else {
+        A[sidx] += kil;
+      }
+    }
+    b += F;
+    __syncwarp();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lift += __shfl_xor_sync(0xffffffffu, lift, o);
+  for (int k = lane; k < len; k += 32) val[start + k] = A[k];
+  if (lane == 0) rhs[j] = b - lift;
+}
+
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -503,10 +580,22 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
 #define FFG_COLUMN_ARGS                                                                        \
   F, col_ptr, row_idx, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd, t.nb, geo, stride, \
       dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, iperm, soff, v64, v32, d64, d32, rhs
+  // high-order CSC columns: one warp per column (48 KB of columns per block)
+  constexpr int kColSmem = 48 * 1024;
+  const int col_bytes = t.max_column * (int)sizeof(double);
+  const bool by_warp = !sell && t.nb >= 16 && t.family != FFG_TRIANGLE_P1 && t.max_column > 0 &&
+                       col_bytes <= kColSmem;
+  const int wpb = by_warp ? std::max(1, std::min(8, kColSmem / col_bytes)) : 0;
 #define FFG_LAUNCH(FAM)                                                                        \
   do {                                                                                         \
     if (sell)                                                                                  \
       column_kernel<FAM, true><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);                \
+    else if (by_warp && FAM != FFG_TRIANGLE_P1)                                                \
+      csc_column_warp_kernel<FAM><<<(unsigned)((F + wpb - 1) / wpb), 32 * wpb,                 \
+                                    (size_t)wpb * col_bytes, s>>>(                             \
+          F, t.max_column, col_ptr, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd,      \
+          t.nb, geo, stride, dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, v64,    \
+          rhs);                                                                                \
     else                                                                                       \
       column_kernel<FAM, false><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);               \
   } while (0)
