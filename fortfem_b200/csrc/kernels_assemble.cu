@@ -177,10 +177,14 @@ __device__ __forceinline__ void ned_block(const NedDims &D, const int8_t *sg, co
   }
 }
 
-// At most 64 registers: four 256-thread CTAs per SM overlap one another's
-// per-cell barriers (the thread-0 geometry spills a little; measured on the
-// 24^3 x 6 slab system: k = 2 3.8 -> 2.4 ms, k = 3 10.9 -> 7.2 ms).
-__global__ void __launch_bounds__(256, 4) nedelec_element_kernel(int n_cells, const int *__restrict__ cells,
+// At most 64 registers, so that 1024 threads of CTAs share an SM and overlap
+// one another's per-cell barriers (the thread-0 geometry spills a little).
+// THREADS = 128 for orders <= 3 (eight cells in flight per SM), 256 above,
+// where shared memory limits the resident CTAs; measured on the 24^3 x 6
+// slab system (one 256-thread CTA per 96 registers before): order 2 3.8 ->
+// 1.9 ms, order 3 10.9 -> 6.3 ms, order 4 26.2 -> 24.0 ms.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) nedelec_element_kernel(int n_cells, const int *__restrict__ cells,
                                        const double *__restrict__ verts, double ca, double cb,
                                        const double *__restrict__ cell_a,
                                        const double *__restrict__ cell_b,
@@ -547,19 +551,26 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   D.face_end = D.edge_end + 4 * D.fdc;
   D.kglobal = nedelec_smem_bytes(tab, D.fdc, false) > 200 * 1024 ? 1 : 0;
   const size_t smem = nedelec_smem_bytes(tab, D.fdc, D.kglobal != 0);
+  const bool small = D.nb <= 45;  // orders 1-3
   if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(nedelec_element_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-      return FFG_CUDA_ERROR;
+    const cudaError_t e =
+        small ? cudaFuncSetAttribute(nedelec_element_kernel<128>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+              : cudaFuncSetAttribute(nedelec_element_kernel<256>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return FFG_CUDA_ERROR;
   }
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * 8);
-  nedelec_element_kernel<<<grid, 256, smem, s>>>(
-      t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,
-      tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem,
-      cell_rhs, err, in.vertices_dot, in.coef_a_dot, in.coef_b_dot, in.geo_override);
+  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * (small ? 16 : 8));
+#define FFG_NED_ARGS                                                                           \
+  t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,     \
+      tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem, \
+      cell_rhs, err, in.vertices_dot, in.coef_a_dot, in.coef_b_dot, in.geo_override
+  if (small) nedelec_element_kernel<128><<<grid, 128, smem, s>>>(FFG_NED_ARGS);
+  else nedelec_element_kernel<256><<<grid, 256, smem, s>>>(FFG_NED_ARGS);
+#undef FFG_NED_ARGS
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 
