@@ -14,12 +14,14 @@ from .api import (CscMatrix, FortfemError, Problem, SolverOptions, SolverStats, 
                   assemble_tetra_lagrange_stiffness_csc_vjp, assemble_tetra_nedelec_curl_mass_csc,
                   assemble_tetra_nedelec_curl_mass_csc_jvp, assemble_tetra_nedelec_curl_mass_csc_vjp,
                   assemble_tetra_nedelec_curvilinear_pml_csc, assemble_tetra_nedelec_pml_csc,
-                  assemble_tetra_nedelec_vector_load_samples, assemble_triangle_lagrange_csc,
+                  assemble_tetra_nedelec_vector_load_samples,
+                  assemble_tetra_nedelec_weighted_csc, assemble_triangle_lagrange_csc,
                   assemble_triangle_lagrange_load_samples, build_topology,
                   evaluate_tetra_lagrange_solution, probe_tetra_nedelec_solution,
                   generate_structured_tetra_box_mesh, solve_scalar_p1, solve_sparse,
                   solve_tetra_lagrange_diffusion_reaction, solve_tetra_lagrange_poisson,
-                  solve_tetra_nedelec_curl_mass, solve_triangle_lagrange, solver_options, spmv,
+                  solve_tetra_nedelec_curl_mass, solve_tetra_nedelec_weighted_curl_mass,
+                  solve_triangle_lagrange, solver_options, spmv, cell_tensors,
                   unit_square_mesh)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -34,6 +34,8 @@ FFG_BOUNDARY_NONE = 0
 FFG_BOUNDARY_ALL = 1
 FFG_BOUNDARY_MASK = 2
 
+FFG_ASSEMBLY_FP64 = 0
+FFG_ASSEMBLY_TF32X3 = 1
 FFG_PRECISION_FP64 = 0
 FFG_PRECISION_MIXED = 1
 FFG_OPTIONS_VERSION = 1
@@ -93,6 +95,10 @@ SIGNATURES = {
         None, [i32, vp, i32, vp, i32, f64, f64, vp, f64, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curl_mass_csc_vjp": (
         None, [i32, vp, i32, vp, i32, f64, f64, i64, vp, vp, vp, vp, pi32]),
+    "ffg_assemble_tetra_nedelec_weighted_csc": (
+        None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
+    "ffg_problem_set_cell_tensor": (None, [i32, vp, pi32]),
+    "ffg_problem_set_assembly_precision": (None, [i32, i32, pi32]),
     "ffg_assemble_tetra_nedelec_pml_csc": (
         None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curvilinear_pml_csc": (

@@ -281,6 +281,36 @@ def assemble_tetra_nedelec_curl_mass_csc(mesh_vertices, tetrahedra, curl_coeffic
                      "Tetrahedral Nedelec assembly failed")
 
 
+def cell_tensors(coefficient, vertices, tetrahedra) -> np.ndarray:
+    """One symmetric 3 x 3 tensor per cell as the C-ABI takes it (9 doubles per
+    cell, column-major).  `coefficient` is an (n_cells, 3, 3) array, or a
+    tensor_coefficient_3d-style callable f(x, y, z) -> 3 x 3 that is evaluated
+    once per cell at its centroid (the caller declares it cellwise constant)."""
+    v = _f64(vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    if callable(coefficient):
+        cen = v[t].mean(axis=1)
+        ten = np.array([np.asarray(coefficient(*c), dtype=np.float64) for c in cen])
+    else:
+        ten = np.asarray(coefficient, dtype=np.float64)
+    ten = ten.reshape(len(t), 3, 3)
+    return np.ascontiguousarray(np.transpose(ten, (0, 2, 1))).reshape(-1)
+
+
+def assemble_tetra_nedelec_weighted_csc(mesh_vertices, tetrahedra, coefficient, mass_coefficient,
+                                        order=None):
+    """assemble_tetra_nedelec_weighted_csc (src/assembly/assembly_tetra_nedelec_3d.f90:1870-2000)
+    with the tensor coefficient constant on each cell (see cell_tensors).
+    Returns (CscMatrix, Status)."""
+    v = _f64(mesh_vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    ten = cell_tensors(coefficient, v, t)
+    args = [len(v), _ptr(v), len(t), _ptr(t), 1 if order is None else int(order), _ptr(ten),
+            float(mass_coefficient)]
+    return _csc_call("ffg_assemble_tetra_nedelec_weighted_csc", args,
+                     "Weighted tetrahedral Nedelec assembly failed")
+
+
 def assemble_tetra_nedelec_curl_mass_csc_jvp(mesh_vertices, tetrahedra, order, curl_coefficient,
                                              mass_coefficient, mesh_vertices_dot,
                                              curl_coefficient_dot, mass_coefficient_dot):
@@ -734,6 +764,35 @@ class Problem:
             raise FortfemError(st.value, "ffg_problem_reduced_system")
         return CscMatrix(self.n_free, self.n_free, cp, ri, val), rhs, free
 
+    def set_assembly_precision(self, precision: str):
+        """Nedelec orders 3-4: "fp64" (CUDA-core FP64 contraction, the parity
+        path) or "tf32x3" (tensor-core 3xTF32 contraction, FP32 accumulation)
+        for every following assembly (ffg_problem_set_assembly_precision)."""
+        modes = {"fp64": K.FFG_ASSEMBLY_FP64, "tf32x3": K.FFG_ASSEMBLY_TF32X3}
+        if precision not in modes:
+            raise FortfemError(K.FFG_INVALID_INPUT, f"assembly precision {precision!r}")
+        st = C.c_int(0)
+        K.load().ffg_problem_set_assembly_precision(self.handle, modes[precision], C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_set_assembly_precision")
+
+    def set_cell_tensor(self, coefficient, vertices=None):
+        """Nedelec: a symmetric 3 x 3 tensor per cell (array (n_cells, 3, 3), or a
+        callable evaluated at the cell centroids of `vertices`) multiplying the
+        curl coefficient in every following assembly; None clears it
+        (ffg_problem_set_cell_tensor)."""
+        st = C.c_int(0)
+        if coefficient is None:
+            K.load().ffg_problem_set_cell_tensor(self.handle, None, C.byref(st))
+        else:
+            if callable(coefficient) and vertices is None:
+                raise FortfemError(K.FFG_INVALID_INPUT, "set_cell_tensor: vertices needed")
+            ten = cell_tensors(coefficient, vertices if vertices is not None
+                               else np.zeros((self.n_vertices, 3)), self.cells)
+            K.load().ffg_problem_set_cell_tensor(self.handle, _ptr(ten), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_set_cell_tensor")
+
     def evaluate(self, vertices, solution, cells, points, physical=False):
         """Batched evaluation at (cell, point) queries (ffg_problem_evaluate):
         Lagrange (values (n,), gradients (n, 3)), Nedelec (fields (n, 3),
@@ -870,6 +929,26 @@ def solve_tetra_nedelec_curl_mass(vertices, tetrahedra, order, source, curl_coef
                              None, options)
         return sol, Status.of(0 if stats.converged else K.FFG_NOT_CONVERGED,
                               "Tetrahedral Nedelec curl-mass solve failed"), stats
+
+
+def solve_tetra_nedelec_weighted_curl_mass(vertices, tetrahedra, order, curl_coefficient, source,
+                                           mass_coefficient, zero_tangential_boundary=False,
+                                           options=None):
+    """solve_tetra_nedelec_weighted_curl_mass (src/solvers/fortfem_tetra_nedelec_solver_3d.f90:41-95)
+    with the tensor coefficient constant on each cell (array or callable evaluated
+    at the centroids), sparse direct solve replaced by the GPU Jacobi-PCG.
+    Returns (solution, Status, SolverStats)."""
+    where = "Weighted tetrahedral Nedelec curl-mass solve failed"
+    if order < 1 or not mass_coefficient > 0.0:
+        return None, Status.of(K.FFG_INVALID_INPUT, where), None
+    v = _f64(vertices).reshape(-1, 3)
+    t = _i32(tetrahedra).reshape(-1, 4)
+    with Problem(K.FFG_TETRA_NEDELEC, order, t, len(v),
+                 boundary="all" if zero_tangential_boundary else "none") as p:
+        p.set_cell_tensor(coefficient=curl_coefficient, vertices=v)
+        samples = _samples(source, p.sample_points(v), 3)
+        sol, stats = p.solve(v, 1.0, mass_coefficient, None, None, samples, None, options)
+        return sol, Status.of(0 if stats.converged else K.FFG_NOT_CONVERGED, where), stats
 
 
 _BATCH_MODES = {"cta_per_system": K.FFG_BATCH_CTA_PER_SYSTEM,

@@ -76,6 +76,12 @@ struct Problem {
   double *in_vertices = nullptr, *in_cell_a = nullptr, *in_cell_b = nullptr, *in_samples = nullptr,
          *in_g = nullptr;
   int *free_dofs = nullptr;
+  // Nedelec with a per-cell tensor coefficient: the tensors (9 per cell) and
+  // the contraction weights computed from them at every assembly
+  double *cell_tensor = nullptr, *geo_w = nullptr;
+  // Nedelec element contraction: FP64 CUDA cores or 3xTF32 tensor cores
+  int assembly_precision = FFG_ASSEMBLY_FP64;
+  TcPlan tc;
   int *err = nullptr;
   int *err_host = nullptr;   // pinned: degenerate-cell flag of a deferred check
   bool batch_pending = false;  // enqueued by ffg_problem_solve_batch, not yet collected
@@ -86,11 +92,13 @@ struct Problem {
     void *ptrs[] = {dt.cells, dt.gd, dt.edge_sign, dt.face_perm, dt.free_index, dt.inc_ptr,
                     dt.inc_cell, dt.inc_local, dt.slot, dt.ref, dt.load_basis, dt.face_blocks,
                     csc_col_ptr, csc_row, csc_val, geo, cell_rhs, elem, rhs, x, full, in_vertices,
-                    in_cell_a, in_cell_b, in_samples, in_g, free_dofs, err, eval.lag_idx,
+                    in_cell_a, in_cell_b, in_samples, in_g, free_dofs, cell_tensor, geo_w,
+                    err, eval.lag_idx,
                     eval.terms, eval.coef};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     free_sell(S);
+    tc_free_plan(tc);
     solve_work_free(work);
     if (err_host) cudaFreeHost(err_host);
     for (auto &e : ev)
@@ -115,6 +123,14 @@ int device_ready() {
     return FFG_NO_DEVICE;
   }
   return FFG_OK;
+}
+
+// Status of a finished solve: a launch or copy error first, then converged,
+// then the wall limit (FFG_TIMEOUT) apart from plain non-convergence.
+int solve_status(int st, const ffg_solver_stats &s) {
+  if (st) return st;
+  if (s.converged) return FFG_OK;
+  return s.status == FFG_TIMEOUT ? FFG_TIMEOUT : FFG_NOT_CONVERGED;
 }
 
 void report(int verbosity, const std::string &msg) {
@@ -250,14 +266,39 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
     return FFG_OUT_OF_MEMORY;
   if (cudaMemsetAsync(P.err, 0, sizeof(int), s) != cudaSuccess) return FFG_CUDA_ERROR;
   int st;
+  const float *elem32 = nullptr;
+  int ld32 = 0;
   if (t.family == FFG_TETRA_NEDELEC) {
-    st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s);
+    if (P.cell_tensor) {
+      st = launch_weighted_weights(t, P.dt, in, P.cell_tensor, P.geo_w, P.err, s);
+      if (st) return st;
+      in.geo_override = P.geo_w;
+    }
+    if (P.assembly_precision == FFG_ASSEMBLY_TF32X3) {
+      // matrices on the tensor cores (FP32, leading dimension tc.ld), loads in FP64
+      if (!P.tc.tile_n && (st = tc_build_plan(t.degree, P.tab, P.tc))) return st;
+      if (in.samples) {
+        st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s, true);
+      } else {
+        st = cudaMemsetAsync(P.cell_rhs, 0, sizeof(double) * t.nb * (size_t)t.n_cells, s) ==
+                     cudaSuccess
+                 ? FFG_OK
+                 : FFG_CUDA_ERROR;
+      }
+      if (st) return st;
+      float *e32 = reinterpret_cast<float *>(P.elem);
+      st = launch_nedelec_tc(t, P.dt, in, P.tc, e32, P.err, s);
+      elem32 = e32;
+      ld32 = P.tc.ld;
+    } else {
+      st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s);
+    }
   } else {
     st = launch_cell_geometry(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.err, s);
   }
   if (st) return st;
   st = launch_columns(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.elem, P.csc_col_ptr,
-                      P.csc_row, sell ? &P.S : nullptr, P.csc_val, P.rhs, s);
+                      P.csc_row, sell ? &P.S : nullptr, P.csc_val, P.rhs, s, elem32, ld32);
   if (st) return st;
   if (defer_check) {
     // the flag is read with the statistics, after the stream has passed
@@ -749,6 +790,73 @@ void ffg_problem_free(int handle, int *status) {
   *status = FFG_OK;
 }
 
+// A symmetric, finite 3 x 3 tensor per cell (column-major): the weighted
+// Nedelec path takes only symmetric tensors (reluctivities), whose entries
+// agree with their transposes to 1e-12 of the largest entry.
+static bool symmetric_tensors(int64_t n_cells, const double *ten) {
+  for (int64_t c = 0; c < n_cells; ++c) {
+    const double *M = ten + 9 * c;
+    double mx = 0.0;
+    for (int i = 0; i < 9; ++i) {
+      if (!std::isfinite(M[i])) return false;
+      mx = std::max(mx, std::fabs(M[i]));
+    }
+    for (int r = 0; r < 3; ++r)
+      for (int e = r + 1; e < 3; ++e)
+        if (std::fabs(M[r + 3 * e] - M[e + 3 * r]) > 1e-12 * mx) return false;
+  }
+  return true;
+}
+
+void ffg_problem_set_assembly_precision(int handle, int precision, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (P->batch_pending || (precision != FFG_ASSEMBLY_FP64 && precision != FFG_ASSEMBLY_TF32X3)) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  if (precision == FFG_ASSEMBLY_TF32X3 &&
+      (P->topo.family != FFG_TETRA_NEDELEC || !tc_supported_order(P->topo.degree))) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  P->assembly_precision = precision;
+  *status = FFG_OK;
+}
+
+void ffg_problem_set_cell_tensor(int handle, const double *tensors, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (P->topo.family != FFG_TETRA_NEDELEC || P->batch_pending) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  if (!tensors) {
+    if (P->cell_tensor) cudaFree(P->cell_tensor);
+    if (P->geo_w) cudaFree(P->geo_w);
+    P->cell_tensor = P->geo_w = nullptr;
+    *status = FFG_OK;
+    return;
+  }
+  const size_t nc = (size_t)P->topo.n_cells;
+  if (!symmetric_tensors((int64_t)nc, tensors)) { *status = FFG_INVALID_INPUT; return; }
+  int st = FFG_OK;
+  if (!P->cell_tensor && (st = dalloc(&P->cell_tensor, 9 * std::max<size_t>(nc, 1)))) {
+    *status = st;
+    return;
+  }
+  if (!P->geo_w && (st = dalloc(&P->geo_w, 12 * std::max<size_t>(nc, 1)))) {
+    *status = st;
+    return;
+  }
+  if (nc && cudaMemcpy(P->cell_tensor, tensors, sizeof(double) * 9 * nc,
+                       cudaMemcpyHostToDevice) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  *status = FFG_OK;
+}
+
 void ffg_problem_constrained(int handle, uint8_t *mask, int *status) {
   auto P = find_problem(handle);
   if (!P) { *status = FFG_BAD_HANDLE; return; }
@@ -1019,7 +1127,7 @@ void ffg_problem_batch_stats(int handle, ffg_solver_stats *stats, int *status) {
   local.solve_seconds = ts * 1e-3;
   if (st) local.status = st;
   if (stats) *stats = local;
-  *status = st ? st : (local.converged ? FFG_OK : FFG_NOT_CONVERGED);
+  *status = solve_status(st, local);
 }
 
 void ffg_problem_reduced_system(int handle, const double *vertices, double ca, double cb,
@@ -1281,6 +1389,43 @@ void ffg_assemble_tetra_nedelec_curl_mass_csc(int nv, const double *verts, int n
            cap, n_dofs, nnz, col_ptr, row_ind, values, status);
 }
 
+void ffg_assemble_tetra_nedelec_weighted_csc(int nv, const double *verts, int nt,
+                                             const int *tets, int order,
+                                             const double *cell_tensors, double mass,
+                                             int64_t cap, int *n_dofs, int64_t *nnz,
+                                             int64_t *col_ptr, int *row_ind, double *values,
+                                             int *status) {
+  if (!verts || !cell_tensors || nt < 1) { *status = FFG_INVALID_INPUT; return; }
+  if (!symmetric_tensors(nt, cell_tensors)) { *status = FFG_INVALID_INPUT; return; }
+  std::shared_ptr<Problem> P;
+  std::string msg;
+  int st = create_problem(FFG_TETRA_NEDELEC, order, nv, nt, tets, 0, 0, FFG_BOUNDARY_NONE, nullptr,
+                          P, msg);
+  if (st) { *status = st; return; }
+  if (n_dofs) *n_dofs = (int)P->topo.n_dofs;
+  if (nnz) *nnz = P->topo.nnz();
+  if (cap < P->topo.nnz() || !col_ptr || !row_ind || !values) { *status = FFG_CAPACITY; return; }
+  if ((st = dalloc(&P->cell_tensor, 9 * (size_t)nt)) || (st = dalloc(&P->geo_w, 12 * (size_t)nt))) {
+    *status = st;
+    return;
+  }
+  if (cudaMemcpy(P->cell_tensor, cell_tensors, sizeof(double) * 9 * (size_t)nt,
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  st = assemble(*P, verts, 1.0, mass, nullptr, nullptr, nullptr, nullptr, 0, false, 0, msg);
+  if (st) { *status = st; return; }
+  std::memcpy(col_ptr, P->topo.col_ptr.data(), sizeof(int64_t) * P->topo.col_ptr.size());
+  std::memcpy(row_ind, P->topo.row_idx.data(), sizeof(int) * P->topo.row_idx.size());
+  if (cudaMemcpy(values, P->csc_val, sizeof(double) * (size_t)P->topo.nnz(),
+                 cudaMemcpyDeviceToHost) != cudaSuccess) {
+    *status = FFG_CUDA_ERROR;
+    return;
+  }
+  *status = FFG_OK;
+}
+
 // Complex PML curl-curl CSC: the Nedelec element kernel on the real and on
 // the imaginary parts of the PML weights, each gathered by the column kernel.
 static void pml_csc(bool curvilinear, int nv, const double *verts, int nt, const int *tets,
@@ -1463,7 +1608,7 @@ void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row
   cudaFree(dx);
   report(o.verbosity, msg);
   if (stats) *stats = local;
-  *status = st ? st : (local.converged ? FFG_OK : FFG_NOT_CONVERGED);
+  *status = solve_status(st, local);
 }
 
 void ffg_csc_matvec(int n, int64_t nnz, const int64_t *col_ptr, const int *row_ind,

@@ -242,10 +242,33 @@ struct AssemblyInputs {
 int launch_cell_geometry(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                          const AssemblyInputs &in, double *geo, int geo_stride, double *cell_rhs,
                          int *err, cudaStream_t s);
+// 3xTF32 tensor-core contraction of Nedelec element matrices (orders 3, 4):
+// tile plan and B operand images of one order, in device memory.
+struct TcPlan {
+  int order = 0, n_tiles = 0, ld = 0;  // ld: leading dimension of the FP32 element matrices
+  int *tile_n = nullptr, *tile_pair0 = nullptr, *pair_code = nullptr, *boff = nullptr;
+  float *bimage = nullptr, *face_t = nullptr;
+  size_t image_bytes = 0;
+};
+bool tc_supported_order(int k);
+int tc_build_plan(int k, const ElementTables &tab, TcPlan &plan);
+void tc_free_plan(TcPlan &plan);
+// Oriented element matrices T^T K T in FP32 (n_cells x nb x plan.ld, column-major).
+int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const AssemblyInputs &in,
+                      const TcPlan &plan, float *elem, int *err, cudaStream_t s);
+
+// Tensor-weighted Nedelec: the twelve contraction weights of every cell from
+// its symmetric 3 x 3 tensor (column-major, 9 per cell, device) and the
+// scalar curl / mass coefficients of `in`, for the element kernel's
+// caller-weight mode.
+int launch_weighted_weights(const Topology &t, const DeviceTopology &dt, const AssemblyInputs &in,
+                            const double *tensor, double *geo, int *err, cudaStream_t s);
 // Nedelec: oriented element matrices (n_cells * nb * nb) and oriented element loads.
+// load_only: the element loads alone (the matrices come from the tensor-core
+// kernel).
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
-                   cudaStream_t s);
+                   cudaStream_t s, bool load_only = false);
 // Column-owner gather into the constrained operator.  With `sell` set the
 // values go to the slices (FP64 + FP32 copy, Jacobi diagonal, rhs in the
 // SELL numbering); otherwise to the CSC value array `csc_val` with the rhs in
@@ -254,7 +277,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    const AssemblyInputs &in, const double *geo, int geo_stride,
                    const double *cell_rhs, const double *elem, const int64_t *col_ptr,
                    const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
-                   cudaStream_t s);
+                   cudaStream_t s, const float *elem32 = nullptr, int ld32 = 0);
 int geo_stride_for(const Topology &t, const ElementTables &tab);
 
 // Forward / reverse mode of the Lagrange stiffness + mass and the Nedelec

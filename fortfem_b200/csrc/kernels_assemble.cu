@@ -149,7 +149,8 @@ __global__ void triangle_lagrange_geometry_kernel(int n_cells, const int *__rest
 // reversed edges, dense face blocks per face permutation, identity on cells.
 struct NedDims {
   int k, nb, fdc, edge_end, face_end;
-  int kglobal;  // the nb x nb matrix does not fit in shared memory: work in `elem`
+  int kglobal;    // the nb x nb matrix does not fit in shared memory: work in `elem`
+  int load_only;  // element loads only (the matrices come from the tensor-core kernel)
 };
 
 __device__ __forceinline__ void ned_block(const NedDims &D, const int8_t *sg, const uint8_t *fp,
@@ -265,7 +266,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) nedelec_element_kerne
     }
     __syncthreads();
     const size_t nn = (size_t)nb * nb;
-    for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    for (size_t idx = threadIdx.x; !D.load_only && idx < nn; idx += blockDim.x) {
       double s = 0.0;
 #pragma unroll
       for (int g = 0; g < 12; ++g) s += geo[g] * __ldg(ref + (size_t)g * nn + idx);
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) nedelec_element_kerne
     // block per face (T[st+m][st+r] = B[r*fdc+m]), identity on cell moments.
     // Face blocks first: columns (K <- K T), then rows (K <- T^T K), one face
     // at a time through `tmp`; the edge signs are applied on the way out.
-    for (int f = 0; f < 4 && fdc > 0; ++f) {
+    for (int f = 0; f < 4 && fdc > 0 && !D.load_only; ++f) {
       const int st = D.edge_end + f * fdc;
       const double *Bg = face_blocks + (size_t)fp[f] * fdc * fdc;
       for (int q = threadIdx.x; q < fdc * fdc; q += blockDim.x) B[q] = Bg[q];
@@ -322,7 +323,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) nedelec_element_kerne
         K[(st + q % fdc) + (size_t)nb * (q / fdc)] = tmp[q];
       __syncthreads();
     }
-    for (size_t idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    for (size_t idx = threadIdx.x; !D.load_only && idx < nn; idx += blockDim.x) {
       const int i = (int)(idx % nb), j = (int)(idx / nb);
       double v = K[idx];
       if (i < D.edge_end && sg[i / D.k] == -1 && ((i % D.k) % 2) == 0) v = -v;
@@ -360,7 +361,8 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
                               const int *__restrict__ iperm, const int64_t *__restrict__ soff,
                               double *__restrict__ val64, float *__restrict__ val32,
                               double *__restrict__ dinv64, float *__restrict__ dinv32,
-                              double *__restrict__ rhs) {
+                              double *__restrict__ rhs, const float *__restrict__ elem32,
+                              int ld32) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n_free) return;
   const int64_t start = col_ptr[j], end = col_ptr[j + 1];
@@ -407,6 +409,8 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
         for (int s = 0; s < NT; ++s) kil += gco[s] * __ldg(ref + s * nn + off);
       } else if (FAMILY == FFG_TRIANGLE_P1) {
         kil = geo[10 * (size_t)e + i + 3 * l];
+      } else if (elem32) {
+        kil = (double)elem32[(size_t)ld32 * nb * e + i + (size_t)ld32 * l];
       } else {
         kil = elem[nn * e + i + (size_t)nb * l];
       }
@@ -455,7 +459,8 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
                                        const double *__restrict__ elem,
                                        const double *__restrict__ cell_rhs,
                                        const double *__restrict__ g, double *__restrict__ val,
-                                       double *__restrict__ rhs) {
+                                       double *__restrict__ rhs, const float *__restrict__ elem32,
+                                       int ld32) {
   extern __shared__ double col_acc[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
@@ -491,6 +496,8 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
         kil = 0.0;
 #pragma unroll
         for (int t = 0; t < NT; ++t) kil += gco[t] * __ldg(ref + t * nn + off);
+      } else if (elem32) {
+        kil = (double)elem32[(size_t)ld32 * nb * e + i + (size_t)ld32 * l];
       } else {
         kil = elem[nn * e + i + (size_t)nb * l];
       }
@@ -542,8 +549,9 @@ size_t nedelec_smem_bytes(const ElementTables &tab, int fdc, bool kglobal) {
 
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool load_only) {
   NedDims D;
+  D.load_only = load_only ? 1 : 0;
   D.k = t.degree;
   D.nb = t.nb;
   D.fdc = t.degree * (t.degree - 1);
@@ -578,7 +586,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    const AssemblyInputs &in, const double *geo, int stride,
                    const double *cell_rhs, const double *elem, const int64_t *col_ptr,
                    const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
-                   cudaStream_t s) {
+                   cudaStream_t s, const float *elem32, int ld32) {
   const int T = 128;
   const int64_t F = t.n_free();
   if (F == 0) return FFG_OK;
@@ -590,7 +598,8 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
   float *d32 = sell ? sell->dinv32 : nullptr;
 #define FFG_COLUMN_ARGS                                                                        \
   F, col_ptr, row_idx, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd, t.nb, geo, stride, \
-      dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, iperm, soff, v64, v32, d64, d32, rhs
+      dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, iperm, soff, v64, v32, d64, d32, rhs, \
+      elem32, ld32
   // high-order CSC columns: one warp per column (48 KB of columns per block)
   constexpr int kColSmem = 48 * 1024;
   const int col_bytes = t.max_column * (int)sizeof(double);
@@ -606,7 +615,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                                     (size_t)wpb * col_bytes, s>>>(                             \
           F, t.max_column, col_ptr, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd,      \
           t.nb, geo, stride, dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, v64,    \
-          rhs);                                                                                \
+          rhs, elem32, ld32);                                                                  \
     else                                                                                       \
       column_kernel<FAM, false><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);               \
   } while (0)

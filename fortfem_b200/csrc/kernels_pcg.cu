@@ -1350,7 +1350,8 @@ PcgParams make_params(const DeviceSell &A, const double *b, double *x,
   P.tol = opts.tolerance;
   P.delta = opts.inner_tolerance;
   P.guard = opts.breakdown_guard;
-  const double limit = opts.timeout_seconds > 0 ? opts.timeout_seconds : 60.0;
+  // clamped to a million seconds so that the conversion stays in range
+  const double limit = fmin(opts.timeout_seconds > 0 ? opts.timeout_seconds : 60.0, 1.0e6);
   P.limit_ns = (unsigned long long)(limit * 1e9);
   P.cta0 = 0;
   P.ncta = A.grid;

@@ -32,7 +32,7 @@ namespace {
 constexpr int kNoAllocMaxRows = FFG_NOALLOC_MAX_ROWS;  // largest system the array holds
 constexpr int kNoAllocThreads = 1024;   // one CTA solves the whole system
 constexpr int kNoAllocWarps = kNoAllocThreads / 32;
-constexpr int kNoAllocResult = 8;
+constexpr int kNoAllocResult = 8;  // converged, iterations, res, true res, timeout, seconds, bad input
 // layout (doubles): r, z, p, q, D^-1 (kNoAllocMaxRows each), then the result block
 constexpr size_t kNoAllocDoubles = 5 * (size_t)kNoAllocMaxRows + kNoAllocResult;
 
@@ -74,15 +74,36 @@ __device__ void csr_apply(int n, const int64_t *rp, const int *ci, const double 
 // pcg_solve_operator / pcg_iteration_loop (src/solvers/advanced_solvers.f90:831-925)
 // in one CTA; jacobi diagonal as build_sparse_preconditioner (:1139-1154).
 __global__ void __launch_bounds__(kNoAllocThreads, 1)
-    noalloc_pcg_kernel(int n, const int64_t *rp, const int *ci, const double *v, const double *b,
-                       double *x, double *scratch, int jacobi, int relative, double tol,
-                       int max_it, int guard, unsigned long long limit_ns) {
+    noalloc_pcg_kernel(int n, int64_t nnz, const int64_t *rp, const int *ci, const double *v,
+                       const double *b, double *x, double *scratch, int jacobi, int relative,
+                       double tol, int max_it, int guard, unsigned long long limit_ns) {
   __shared__ double red[kNoAllocWarps];
   __shared__ int stop;
   double *r = scratch, *z = r + kNoAllocMaxRows, *p = z + kNoAllocMaxRows;
   double *q = p + kNoAllocMaxRows, *dinv = q + kNoAllocMaxRows;
   double *result = dinv + kNoAllocMaxRows;
   const unsigned long long t0 = now_ns();
+  // The CSR arrays come from the caller: check them before any indexed access
+  // (row_ptr starts at 0, ends at nnz and never decreases; every column index
+  // is a row of the system), so that a malformed matrix is reported, not read
+  // out of bounds.  The column indices are read only once row_ptr has passed.
+  int bad = 0;
+  if (threadIdx.x == 0) bad = (rp[0] != 0 || rp[n] != nnz) ? 1 : 0;
+  for (int i = threadIdx.x; i < n; i += kNoAllocThreads) bad |= rp[i] > rp[i + 1] ? 1 : 0;
+  if (__syncthreads_or(bad) == 0) {
+    for (int64_t k = threadIdx.x; k < nnz; k += kNoAllocThreads)
+      bad |= (ci[k] < 0 || ci[k] >= n) ? 1 : 0;
+    bad = __syncthreads_or(bad);
+  } else {
+    bad = 1;
+  }
+  if (bad) {
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < 6; ++i) result[i] = 0.0;
+      result[6] = 1.0;
+    }
+    return;
+  }
   for (int i = threadIdx.x; i < n; i += kNoAllocThreads) {
     double d = 0.0;
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k)
@@ -153,6 +174,7 @@ __global__ void __launch_bounds__(kNoAllocThreads, 1)
     result[3] = bnorm > 0.0 ? true_res / bnorm : true_res;
     result[4] = timed_out;
     result[5] = 1e-9 * (double)(now_ns() - t0);
+    result[6] = 0.0;
   }
 }
 
@@ -217,22 +239,32 @@ extern "C" void ffg_solve_csr_device_noalloc(int n, int64_t nnz, const int64_t *
     }
     o = *opts;
   }
-  const double limit = o.timeout_seconds > 0 ? o.timeout_seconds : 60.0;
+  // wall limit in ns; clamped to a million seconds so that the conversion
+  // below stays inside the range of unsigned long long
+  const double limit = std::fmin(o.timeout_seconds > 0 ? o.timeout_seconds : 60.0, 1.0e6);
   double *scratch = nullptr;
   int st = noalloc_scratch_address(&scratch);
   if (st) { *status = st; return; }
   cudaStream_t s = (cudaStream_t)stream;
-  noalloc_pcg_kernel<<<1, kNoAllocThreads, 0, s>>>(n, row_ptr, col_ind, values, b, x, scratch,
+  noalloc_pcg_kernel<<<1, kNoAllocThreads, 0, s>>>(n, nnz, row_ptr, col_ind, values, b, x, scratch,
                                                    o.preconditioner != 0, o.tolerance_type == 0,
                                                    o.tolerance, o.max_iterations, o.breakdown_guard,
                                                    (unsigned long long)(limit * 1e9));
   if (cudaGetLastError() != cudaSuccess) { *status = FFG_CUDA_ERROR; return; }
   double res[kNoAllocResult];
   const double *dres = scratch + 5 * (size_t)kNoAllocMaxRows;
-  if (cudaMemcpyAsync(res, dres, sizeof(double) * 6, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+  if (cudaMemcpyAsync(res, dres, sizeof(double) * 7, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess) {
     cudaGetLastError();
     *status = FFG_CUDA_ERROR;
+    return;
+  }
+  if (res[6] != 0.0) {
+    std::fprintf(stderr,
+                 "ffg_solve_csr_device_noalloc: malformed CSR matrix (row_ptr must run from 0 "
+                 "to nnz without decreasing, column indices must lie in [0, n))\n");
+    if (stats) stats->status = FFG_INVALID_INPUT;
+    *status = FFG_INVALID_INPUT;
     return;
   }
   if (stats) {

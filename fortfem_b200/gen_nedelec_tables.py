@@ -17,11 +17,13 @@ The definitions restate the reference:
 * face transform = L C^-1 of the face moment matrices under a vertex
   permutation -- ``src/elements/tetra_face_moment_transforms.f90:296-383``.
 
-Order 6 uses the same monomial construction as orders <= 5.  The reference
-switches to Koornwinder/Dubiner modes of fortnum (not vendored) at order 6, so
-its order-6 basis differs from this one by a change of basis inside each edge,
-face and cell block; only basis-invariant quantities (energies, solutions)
-compare across the two.
+Order 6 keeps the monomial candidate space but, as the reference does from
+order 6, weights the face moments with Dubiner modes and the volume moments
+with Koornwinder modes (``tetra_nedelec_arbitrary_order.f90:642-669``).  Those
+polynomials come from fortnum in the reference (not vendored); here they are
+restated from their standard collapsed-coordinate definitions, so equality
+of the order-6 basis with the reference's depends on fortnum's normalisation
+and is unpinned; basis-invariant quantities (energies, solutions) compare.
 
 Order 1..4 tables are pinned against the reference's generated tables by
 ``tests/golden/nedelec_tables.json`` (see ``tests/golden/make_golden.py``).

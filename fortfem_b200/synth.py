@@ -67,9 +67,11 @@ class ScalarCase:
     meta: dict = field(default_factory=dict)
 
 
-def p2_poisson_case(n: int = 48, delta: float = 0.1, seed: int = 2) -> ScalarCase:
-    """P2 tetrahedral Lagrange Poisson on n^3 x 6 jittered tets, lognormal coefficient."""
-    v, t = box_mesh(n)
+def p2_poisson_case(n: int = 48, delta: float = 0.1, seed: int = 2, mesh=None) -> ScalarCase:
+    """P2 tetrahedral Lagrange Poisson on n^3 x 6 jittered tets, lognormal coefficient.
+    `mesh(n) -> (vertices, cells)` replaces the library's Kuhn box generator
+    (a CPU-only caller passes a restatement of the same generator)."""
+    v, t = (mesh or box_mesh)(n)
     v = jitter_interior(v, 1.0 / n, delta, seed)
     rng = np.random.default_rng(seed + 1000)
     kappa = np.exp(rng.standard_normal(len(t)))
@@ -120,3 +122,37 @@ def grf_source(seed: int, correlation_length: float = 0.1, features: int = 64, d
     def f(points):
         return amp * np.cos(points[..., :dim] @ w.T + b).sum(-1)
     return f
+
+
+@dataclass
+class CurlCase:
+    """A curl mu^-1 curl + kappa I problem with zero tangential trace."""
+    name: str
+    order: int
+    vertices: np.ndarray
+    cells: np.ndarray
+    cell_curl: np.ndarray      # mu^-1 per cell
+    mass: float                # kappa
+    source: object             # f(points (..., 3)) -> (..., 3)
+    meta: dict = field(default_factory=dict)
+
+
+def nedelec_slab_case(order: int, n: int = 24, mesh=None) -> CurlCase:
+    """Three material slabs along z on an n^3 x 6 Kuhn box (no jitter):
+    mu^-1 = 1 / 1000 / 1 by cell centroid, kappa = 1, J = (0, 0, 1) in the
+    central slab."""
+    v, t = (mesh or box_mesh)(n)
+    return CurlCase("nedelec_slabs", order, v, t, slab_reluctivity(v, t), 1.0, slab_current,
+                    dict(n=n))
+
+
+def nedelec_order6_case(n: int = 12, delta: float = 0.05, seed: int = 5, mesh=None,
+                        order: int = 6) -> CurlCase:
+    """Order-6 stress case: n^3 x 6 Kuhn box jittered +-0.05h, mu^-1 ~ U[0.5, 2]
+    per cell, kappa = 10, a smooth random trig vector source."""
+    v, t = (mesh or box_mesh)(n)
+    v = jitter_interior(v, 1.0 / n, delta, seed)
+    rng = np.random.default_rng(seed + 1000)
+    mu = rng.uniform(0.5, 2.0, len(t))
+    return CurlCase("nedelec_order6", order, v, t, mu, 10.0, trig_vector_source(seed),
+                    dict(n=n, delta=delta, seed=seed))

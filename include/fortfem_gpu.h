@@ -61,6 +61,9 @@ extern "C" {
 #define FFG_BOUNDARY_MASK 2 /* caller-supplied uint8 mask over the global DoFs */
 
 /* Solver precision. */
+/* Element contraction of Nedelec problems (ffg_problem_set_assembly_precision) */
+#define FFG_ASSEMBLY_FP64 0   /* FP64 CUDA-core contraction (the 1e-12 parity path) */
+#define FFG_ASSEMBLY_TF32X3 1 /* 3xTF32 tensor-core contraction, FP32 accumulation (orders 3, 4) */
 #define FFG_PRECISION_FP64 0  /* FP64 Jacobi-PCG with the reference's stopping rule */
 #define FFG_PRECISION_MIXED 1 /* FP32 PCG recurrences, FP64 solution and reliable
                                  FP64 residual updates (defect correction) */
@@ -185,6 +188,24 @@ void ffg_assemble_tetra_nedelec_curl_mass_csc_vjp(
     double *vertices_bar, double *curl_coefficient_bar, double *mass_coefficient_bar,
     int *status);
 
+/* assemble_tetra_nedelec_weighted_csc / assemble_arbitrary_order_weighted_csc,
+ * assembly_tetra_nedelec_3d.f90:1870-1931 / :1933-2000 (elements :2406-2514):
+ * curl M curl + mass_coefficient I with a tensor coefficient M.  A GPU
+ * cannot call the reference's Fortran callback (tensor_coefficient_3d,
+ * :56-60), so the caller evaluates it once per cell (at the centroid) and
+ * declares it constant on each cell: cell_tensors holds 9 doubles per
+ * tetrahedron, the column-major 3 x 3 tensor (Fortran value(3,3)).  The
+ * tensors must be symmetric (to 1e-12 of their largest entry) and finite,
+ * else FFG_INVALID_INPUT.  The reference integrates at degree 2k+2 (order 1:
+ * the 4-point rule); the contraction used here is exact for a constant
+ * tensor.  Capacity / query protocol as the other CSC entries. */
+void ffg_assemble_tetra_nedelec_weighted_csc(int n_vertices, const double *vertices,
+                                             int n_tetrahedra, const int *tetrahedra, int order,
+                                             const double *cell_tensors, double mass_coefficient,
+                                             int64_t nnz_capacity, int *n_dofs, int64_t *nnz,
+                                             int64_t *col_ptr, int *row_ind, double *values,
+                                             int *status);
+
 /* assemble_tetra_nedelec_pml_csc, assembly_tetra_nedelec_3d.f90:1613-1685 (element
  * :826-887): the complex curl-curl minus k^2 mass operator with the Cartesian PML
  * tensors of cartesian_curl_curl_pml_coefficients (src/boundary/cartesian_helmholtz_pml.f90:94-108).
@@ -277,10 +298,14 @@ void ffg_csc_matvec(int n, int64_t nnz, const int64_t *col_ptr, const int *row_i
  * CSC arrays serve unchanged.  b and x are device vectors, x holding the
  * initial guess on entry and the solution on exit.  opts as ffg_solve_sparse,
  * except that precision is always FP64.  The work runs on `stream` (a
- * cudaStream_t, 0 = default); the call returns once it has finished.
- * The first call with a device current looks up the array's address on that
- * device, so it should come before any stream capture.  All calls share the
- * array: calls whose work overlaps on one GPU race, so serialise them. */
+ * cudaStream_t, 0 = default); every call synchronises `stream` before it
+ * returns, since it reads its result block back to the host.  The kernel
+ * checks the CSR arrays before any indexed access (row_ptr from 0 to nnz,
+ * never decreasing; column indices in [0, n)) and a malformed matrix returns
+ * FFG_INVALID_INPUT.  The first call with a device current looks up the
+ * array's address on that device, so it should come before any stream
+ * capture.  All calls share the array: calls whose work overlaps on one GPU
+ * race, so serialise them. */
 #define FFG_NOALLOC_MAX_ROWS 65536
 void ffg_solve_csr_device_noalloc(int n, int64_t nnz, const int64_t *row_ptr,
                                   const int *col_ind, const double *values, const double *b,
@@ -327,6 +352,26 @@ void ffg_problem_dof_points(int handle, const double *vertices, double *points, 
 
 /* The constrained mask of the problem (n_dofs bytes, 1 = constrained). */
 void ffg_problem_constrained(int handle, uint8_t *mask, int *status);
+
+/* Nedelec problems of order 3 or 4: how the element matrices are contracted in
+ * every following assembly.  FFG_ASSEMBLY_FP64 (the default) is the FP64
+ * reference-tensor contraction on CUDA cores, equal to the reference's
+ * quadrature loop (assemble_tetra_nedelec_curl_mass_element,
+ * assembly_tetra_nedelec_3d.f90:584-643) to 1e-12.  FFG_ASSEMBLY_TF32X3 runs
+ * the contraction as a GEMM on the tensor cores (tcgen05, TF32 hi/lo operand
+ * split, three products accumulated in FP32) and the orientation transform in
+ * FP32: entries carry about 1e-7 relative error, the geometry stays FP64.
+ * Other orders and families return FFG_INVALID_INPUT. */
+void ffg_problem_set_assembly_precision(int handle, int precision, int *status);
+
+/* Nedelec problems: a symmetric 3 x 3 tensor per cell (9 doubles, column-major,
+ * host array) that replaces the scalar curl coefficient's unit tensor in every
+ * following assembly of this problem (solve, reduced system, batch): the curl
+ * term becomes curl . (curl_coefficient cell_curl[c] M_c) curl, as
+ * solve_tetra_nedelec_weighted_curl_mass (src/solvers/fortfem_tetra_nedelec_solver_3d.f90:41-95)
+ * with a cellwise-constant tensor callback.  NULL clears it.  Non-symmetric or
+ * non-finite tensors return FFG_INVALID_INPUT. */
+void ffg_problem_set_cell_tensor(int handle, const double *cell_tensors, int *status);
 
 /* Assemble the constrained system on the device and solve it:
  *   K(c) x = F(f) on the free DoFs, x = g on the constrained DoFs,

@@ -172,6 +172,12 @@ int or_nedelec_csc(int n_vertices, const double *vertices, int n_tets, const int
                    double curl, double mass, const double *cell_curl, const double *cell_mass,
                    int64_t nnz_capacity, int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_idx,
                    double *values);
+int or_nedelec_weighted_element(const double *v, int order, const double *tensor, double mass,
+                                double *matrix);
+int or_nedelec_weighted_csc(int n_vertices, const double *vertices, int n_tets, const int *tets,
+                            int order, const double *tensors, double mass, int64_t cap,
+                            int *n_dofs, int64_t *nnz, int64_t *col_ptr, int *row_idx,
+                            double *values);
 /* forward (JVP) and reverse (VJP) mode of the element and the CSC assembly */
 int or_nedelec_element_jvp(const double *vertices, int order, int quadrature_degree, double curl,
                            double mass, const double *vertices_dot, double curl_dot,

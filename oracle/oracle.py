@@ -473,6 +473,33 @@ def nedelec_csc(vertices, tets, k, curl=1.0, mass=1.0, cell_curl=None, cell_mass
     return n, cp, ri, v
 
 
+def nedelec_weighted_element(vertices, k, tensor, mass=1.0):
+    """assemble_tetra_nedelec_weighted_element(_order) with a constant 3 x 3 tensor."""
+    n = nedelec_dof_count(k)
+    out = np.zeros(n * n)
+    t = np.asfortranarray(np.asarray(tensor, np.float64).reshape(3, 3)).reshape(-1, order="F")
+    _check(_call("or_nedelec_weighted_element", _arr(vertices, np.float64), k, _arr(t, np.float64),
+                 float(mass), out), "nedelec_weighted_element")
+    return out.reshape(n, n, order="F")
+
+
+def nedelec_weighted_csc(vertices, tets, k, cell_tensors, mass=1.0):
+    """assemble_tetra_nedelec_weighted_csc with one column-major 3 x 3 tensor per cell
+    (cell_tensors of shape (n_cells, 3, 3), entry [c, r, s] = M_c(r, s))."""
+    vertices = _arr(vertices, np.float64); tets = _arr(tets, np.int32)
+    ten = np.ascontiguousarray(np.transpose(np.asarray(cell_tensors, np.float64), (0, 2, 1)))
+    nnz = int(_call("or_nedelec_csc_nnz", k, len(tets), tets, restype=C.c_int64))
+    if nnz < 0:
+        raise OracleError("nedelec_csc_nnz")
+    n = nedelec_dof_map(k, tets)["n_global"]
+    nd = C.c_int(0); nz = C.c_int64(0)
+    cp = np.zeros(n + 1, np.int64); ri = np.zeros(nnz, np.int32); v = np.zeros(nnz)
+    _check(_call("or_nedelec_weighted_csc", len(vertices), vertices, len(tets), tets, k,
+                 ten.reshape(-1), float(mass), C.c_int64(nnz), C.byref(nd), C.byref(nz), cp, ri,
+                 v), "nedelec_weighted_csc")
+    return n, cp, ri, v
+
+
 def nedelec_element_jvp(vertices, k, vertices_dot, curl, mass, curl_dot, mass_dot, q=None):
     if q is None:
         q = 2 * k + 2

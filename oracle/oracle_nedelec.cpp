@@ -506,6 +506,116 @@ int or_nedelec_csc(int nv, const double *verts, int nt, const int *tets, int k, 
                              row_idx, values);
 }
 
+// assemble_tetra_nedelec_weighted_element (order 1, the 4-point rule,
+// assembly_tetra_nedelec_3d.f90:2406-2450) and
+// assemble_tetra_nedelec_weighted_element_order (Duffy rule of degree 2k+2,
+// :2452-2514): K_ij = sum_q det w_q (curl_i . M(x_q) curl_j + m v_i . v_j).
+// The tensor callback is a per-cell constant here (`tensor`, column-major
+// 3 x 3), i.e. a callback that returns the same M at every point of the cell.
+int or_nedelec_weighted_element(const double *v, int k, const double *tensor, double mw,
+                                double *M) {
+  if (k < 1) return 1;
+  double J[9], Ji[9], det;
+  if (!tetra_geometry(v, J, &det)) return 1;
+  inv3(J, det, Ji);
+  std::vector<double> px, py, pz, pw;
+  if (k == 1) {
+    double P[12], W[4];
+    or_tetra_degree_two_rule(P, W);
+    for (int q = 0; q < 4; ++q) {
+      px.push_back(P[3 * q]); py.push_back(P[3 * q + 1]); pz.push_back(P[3 * q + 2]);
+      pw.push_back(W[q]);
+    }
+  } else {
+    RuleN R;
+    make_rule(0, 2 * k + 2, R);
+    px = R.x; py = R.y; pz = R.z; pw = R.w;
+  }
+  const int n = or_nedelec_dof_count(k);
+  std::vector<double> rv(3 * n), rc(3 * n), pv(3 * n), pc(3 * n);
+  std::fill(M, M + (size_t)n * n, 0.0);
+  for (size_t pt = 0; pt < pw.size(); ++pt) {
+    const double P[3] = {px[pt], py[pt], pz[pt]};
+    if (k == 1 ? or_whitney_evaluate(P, rv.data(), rc.data())
+               : or_nedelec_evaluate(k, P, rv.data(), rc.data()))
+      return 1;
+    covariant(J, det, Ji, n, rv.data(), rc.data(), pv.data(), pc.data());
+    const double w = det * pw[pt];
+    for (int col = 0; col < n; ++col) {
+      double mc[3];
+      for (int i = 0; i < 3; ++i)
+        mc[i] = tensor[i] * pc[3 * col] + tensor[i + 3] * pc[3 * col + 1] +
+                tensor[i + 6] * pc[3 * col + 2];
+      for (int row = 0; row < n; ++row) {
+        double dc = 0.0, dv = 0.0;
+        for (int i = 0; i < 3; ++i) dc += pc[3 * row + i] * mc[i];
+        for (int i = 0; i < 3; ++i) dv += pv[3 * row + i] * pv[3 * col + i];
+        M[row + (size_t)n * col] += w * (dc + mw * dv);
+      }
+    }
+  }
+  return 0;
+}
+
+// assemble_tetra_nedelec_weighted_csc / assemble_arbitrary_order_weighted_csc
+// (assembly_tetra_nedelec_3d.f90:1870-1931,1933-2000): order 1 with the edge
+// sign products, order >= 2 with T^T K T; triplets j-outer / i-inner into
+// csc_from_triplet.  `tensors` holds one column-major 3 x 3 tensor per cell.
+int or_nedelec_weighted_csc(int nv, const double *verts, int nt, const int *tets, int k,
+                            const double *tensors, double mw, int64_t cap, int *n_dofs,
+                            int64_t *nnz, int64_t *col_ptr, int *row_idx, double *values) {
+  if (k < 1 || nt < 1 || !tensors) return 1;
+  for (int i = 0; i < 4 * nt; ++i)
+    if (tets[i] < 0 || tets[i] >= nv) return 1;
+  int nb = or_nedelec_dof_count(k), ng = 0;
+  std::vector<int> gd((size_t)nb * nt), eo(6 * (size_t)nt), fp(12 * (size_t)nt);
+  if (or_nedelec_dof_map(k, nt, tets, 0, nullptr, nullptr, nullptr, nullptr, gd.data(), eo.data(),
+                         fp.data(), &ng))
+    return 1;
+  *n_dofs = ng;
+  int64_t ntrip = (int64_t)nt * nb * nb;
+  std::vector<int> rows(ntrip), cols(ntrip);
+  std::vector<double> tv(ntrip), K((size_t)nb * nb), T((size_t)nb * nb), KT((size_t)nb * nb),
+      O((size_t)nb * nb);
+  int64_t e = 0;
+  for (int t = 0; t < nt; ++t) {
+    double v[12];
+    for (int n = 0; n < 4; ++n)
+      for (int d = 0; d < 3; ++d) v[3 * n + d] = verts[3 * tets[4 * t + n] + d];
+    if (or_nedelec_weighted_element(v, k, tensors + 9 * (size_t)t, mw, K.data())) return 1;
+    if (k == 1) {
+      for (int col = 0; col < 6; ++col)
+        for (int row = 0; row < 6; ++row, ++e) {
+          rows[e] = gd[(size_t)nb * t + row];
+          cols[e] = gd[(size_t)nb * t + col];
+          tv[e] = (double)(eo[6 * t + row] * eo[6 * t + col]) * K[row + 6 * col];
+        }
+      continue;
+    }
+    if (or_nedelec_transform(k, eo.data() + 6 * t, fp.data() + 12 * t, T.data())) return 1;
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        double s = 0.0;
+        for (int l = 0; l < nb; ++l) s += K[i + (size_t)nb * l] * T[l + (size_t)nb * j];
+        KT[i + (size_t)nb * j] = s;
+      }
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        double s = 0.0;
+        for (int l = 0; l < nb; ++l) s += T[l + (size_t)nb * i] * KT[l + (size_t)nb * j];
+        O[i + (size_t)nb * j] = s;
+      }
+    for (int col = 0; col < nb; ++col)
+      for (int row = 0; row < nb; ++row, ++e) {
+        rows[e] = gd[(size_t)nb * t + row];
+        cols[e] = gd[(size_t)nb * t + col];
+        tv[e] = O[row + (size_t)nb * col];
+      }
+  }
+  return or_csc_from_triplet(ng, ng, ntrip, rows.data(), cols.data(), tv.data(), cap, nnz, col_ptr,
+                             row_idx, values);
+}
+
 // ------------------------------------------------- forward / reverse mode
 namespace {
 static void mat3_mul(const double *A, const double *B, double *C) {  // column-major C = A B

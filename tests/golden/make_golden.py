@@ -1,9 +1,9 @@
 """Build the golden fixtures under tests/golden/ from the reference checkout.
 
-Run once in a container that has the reference sources (path given by
-``FORTFEM_REFERENCE`` or ``/root/reference``)::
+Run once in a container that has the reference sources, with
+``FORTFEM_REFERENCE`` set to the reference checkout::
 
-    python tests/golden/make_golden.py
+    FORTFEM_REFERENCE=<path to lazy-fortran/fortfem> python tests/golden/make_golden.py
 
 It reads the reference's fortsym-generated Nedelec tables as text and stores
 only canonical digests of their exact rational entries (plus entry counts and a
@@ -22,7 +22,7 @@ import os
 import re
 from fractions import Fraction
 
-REF = os.environ.get("FORTFEM_REFERENCE", "/root/reference")
+REF = os.environ.get("FORTFEM_REFERENCE", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 NUM = r"(-?\d+)\.0_real64(?:\s*/\s*(\d+)\.0_real64)?"
@@ -79,6 +79,9 @@ def parse_face_transforms():
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "src", "generated")):
+        raise SystemExit("set FORTFEM_REFERENCE to a lazy-fortran/fortfem checkout "
+                         "(the directory holding src/generated)")
     coeffs = parse_coefficients()
     faces = parse_face_transforms()
     fixture = {"source": "reference src/generated (fortsym@ca903547), digests only",

@@ -328,3 +328,32 @@ def test_p2_full_size_properties():
         sol, stats = prob.solve(case.vertices, 1.0, 0.0, case.cell_coefficient, None, src)
         assert stats.converged and stats.true_relative_residual <= 1e-10
         assert np.isfinite(sol).all() and sol.max() > 0
+
+
+def test_wall_limit_reports_timeout():
+    """A wall limit far below one solve's time: the persistent PCG kernel
+    checks it every iteration and returns FFG_TIMEOUT (status -7) through
+    solve_sparse and through a problem handle, without waiting on anything."""
+    v, t = jittered_box(8, 0.1, 3)
+    A, st = ff.assemble_tetra_lagrange_stiffness_csc(v, t, 2, 8, 1.0, 0.0)
+    assert st.code == 0
+    b = np.random.default_rng(3).standard_normal(A.nrow)
+    opts = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-14,
+                            max_iterations=100000, precision="fp64", breakdown_guard="spd",
+                            timeout_seconds=1e-9)
+    with pytest.raises(ff.FortfemError) as e:
+        ff.solve_sparse(A, b, np.zeros(A.nrow), opts)
+    assert e.value.code == K.FFG_TIMEOUT
+    with ff.Problem(K.FFG_TETRA_LAGRANGE, 2, t, len(v)) as prob:
+        pts = prob.sample_points(v)
+        src = np.sin(pts[..., 0])
+        for precision in ("fp64", "mixed"):
+            opts.precision = precision
+            with pytest.raises(ff.FortfemError) as e:
+                prob.solve(v, 1.0, 0.0, None, None, src, None, opts)
+            assert e.value.code == K.FFG_TIMEOUT
+        # the next solve on the same handle is unaffected
+        opts.timeout_seconds = 60.0
+        opts.tolerance = 1e-10
+        sol, stats = prob.solve(v, 1.0, 0.0, None, None, src, None, opts)
+        assert stats.converged

@@ -609,3 +609,24 @@ def test_triangle_lagrange_element_properties():
         assert np.abs(k.sum(axis=1)).max() < 1e-11          # constants are in the kernel
         assert abs(m.sum() - area) < 1e-13                   # the mass of 1 is the area
         assert np.abs(k - k.T).max() < 1e-13 and np.linalg.eigvalsh(m).min() > 0
+
+
+# assemble_tetra_nedelec_weighted_element(_order) (assembly_tetra_nedelec_3d.f90:2406-2514):
+# an isotropic tensor c I is the scalar curl coefficient c of the curl-mass
+# element (:584-643, order 1 :2357-2404); any symmetric tensor gives a
+# symmetric matrix, and the tensor enters linearly.
+@pytest.mark.parametrize("k", [1, 2, 3])
+def test_weighted_element_reduces_to_curl_mass(k):
+    rng = np.random.default_rng(k)
+    v = (np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1.0]])
+         + 0.1 * rng.standard_normal((4, 3))).reshape(-1)
+    a = oracle.nedelec_weighted_element(v, k, 1.7 * np.eye(3), 0.9)
+    b = (oracle.whitney_element(v, 1.7, 0.9) if k == 1
+         else oracle.nedelec_element(v, k, 2 * k + 2, 1.7, 0.9))
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    m = rng.standard_normal((3, 3))
+    m = m + m.T
+    w = oracle.nedelec_weighted_element(v, k, m, 0.0)
+    assert np.abs(w - w.T).max() <= 1e-13 * np.abs(w).max()
+    w2 = oracle.nedelec_weighted_element(v, k, 2.0 * m, 0.0)
+    assert np.abs(w2 - 2.0 * w).max() <= 1e-13 * np.abs(w).max()

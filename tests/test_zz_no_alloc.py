@@ -36,12 +36,15 @@ def _systems():
     return [(a3, rng.standard_normal(a3.nrow)), (a2, rng.standard_normal(a2.nrow))]
 
 
-def _noalloc(A, b, opts):
+def _noalloc(A, b, opts, nnz=None, row_idx=None):
     """Solve through the C-ABI with the matrix and vectors in device memory
-    (the CSC arrays of the symmetric matrix read as CSR)."""
+    (the CSC arrays of the symmetric matrix read as CSR).  nnz and row_idx
+    override what is passed, to hand the kernel a malformed matrix whose
+    every array still has its full length."""
     dev = torch.device("cuda:0")
+    ri_host = A.row_idx if row_idx is None else row_idx
     rp = torch.from_numpy(np.ascontiguousarray(A.col_ptr, np.int64)).to(dev)
-    ci = torch.from_numpy(np.ascontiguousarray(A.row_idx, np.int32)).to(dev)
+    ci = torch.from_numpy(np.ascontiguousarray(ri_host, np.int32)).to(dev)
     val = torch.from_numpy(np.ascontiguousarray(A.val, np.float64)).to(dev)
     db = torch.from_numpy(np.ascontiguousarray(b, np.float64)).to(dev)
     dx = torch.zeros(A.nrow, dtype=torch.float64, device=dev)
@@ -51,9 +54,10 @@ def _noalloc(A, b, opts):
     sc = K.SolverStatsC()
     st = C.c_int(99)
     K.load().ffg_solve_csr_device_noalloc(
-        A.nrow, int(A.col_ptr[-1]), C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
-        C.c_void_p(val.data_ptr()), C.c_void_p(db.data_ptr()), C.c_void_p(dx.data_ptr()),
-        C.byref(oc), C.byref(sc), C.c_void_p(stream.cuda_stream), C.byref(st))
+        A.nrow, int(A.col_ptr[-1]) if nnz is None else int(nnz), C.c_void_p(rp.data_ptr()),
+        C.c_void_p(ci.data_ptr()), C.c_void_p(val.data_ptr()), C.c_void_p(db.data_ptr()),
+        C.c_void_p(dx.data_ptr()), C.byref(oc), C.byref(sc), C.c_void_p(stream.cuda_stream),
+        C.byref(st))
     return st.value, sc, dx.cpu().numpy()
 
 
@@ -76,6 +80,66 @@ def test_noalloc_matches_solve_sparse_twice_in_a_row():
     A, b, x = first
     st, sc, x2 = _noalloc(A, b, opts)
     assert st == K.FFG_OK and np.array_equal(x, x2)
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_the_oracle_pcg():
+    """The same two systems against the CPU restatement of the reference's
+    Jacobi-PCG (oracle.pcg_sparse), so that an error shared by both GPU
+    solvers (option handling, the Jacobi diagonal) is caught too."""
+    opts = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
+                            max_iterations=10000, precision="fp64", breakdown_guard="spd")
+    for A, b in _systems():
+        xo, so = oracle.pcg_sparse(A.nrow, A.col_ptr, A.row_idx, A.val, b, tol=1e-10,
+                                   relative=True, max_iterations=10000, jacobi=True, guard=1)
+        st, sc, x = _noalloc(A, b, opts)
+        assert st == K.FFG_OK and so["converged"]
+        assert abs(sc.iterations - so["iterations"]) <= 1
+        assert np.abs(x - xo).max() <= TOL * np.abs(xo).max()
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_timeout_and_non_convergence():
+    A, b = _systems()[0]
+    quick = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
+                             max_iterations=10000, precision="fp64", breakdown_guard="spd",
+                             timeout_seconds=1e-9)
+    st, sc, _ = _noalloc(A, b, quick)
+    assert st == K.FFG_TIMEOUT and sc.status == K.FFG_TIMEOUT and sc.converged == 0
+    assert sc.iterations == 1
+    short = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
+                             max_iterations=1, precision="fp64", breakdown_guard="spd")
+    st, sc, _ = _noalloc(A, b, short)
+    assert st == K.FFG_NOT_CONVERGED and sc.status == K.FFG_NOT_CONVERGED
+    assert sc.converged == 0 and sc.iterations == 1
+    # a huge wall limit is clamped, not wrapped to a tiny one
+    long = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
+                            max_iterations=10000, precision="fp64", breakdown_guard="spd",
+                            timeout_seconds=1e30)
+    st, sc, _ = _noalloc(A, b, long)
+    assert st == K.FFG_OK and sc.converged == 1
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_malformed_csr_before_use():
+    """A row pointer that does not end at nnz, and a column index outside
+    [0, n), are found by the kernel's check before any indexed access."""
+    A, b = _systems()[1]
+    opts = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
+                            max_iterations=100, precision="fp64", breakdown_guard="spd")
+    nnz = int(A.col_ptr[-1])
+    st, sc, _ = _noalloc(A, b, opts, nnz=nnz - 1)
+    assert st == K.FFG_INVALID_INPUT
+    bad = np.array(A.row_idx, np.int32)
+    bad[nnz // 2] = A.nrow
+    st, sc, _ = _noalloc(A, b, opts, row_idx=bad)
+    assert st == K.FFG_INVALID_INPUT
+    bad[nnz // 2] = -1
+    st, sc, _ = _noalloc(A, b, opts, row_idx=bad)
+    assert st == K.FFG_INVALID_INPUT
+    # a well-formed call afterwards still solves
+    st, sc, _ = _noalloc(A, b, opts.__class__(**{**opts.__dict__, "max_iterations": 10000}))
+    assert st == K.FFG_OK
 
 
 @pytest.mark.gpu
