@@ -71,6 +71,13 @@ class SolverStatsC(C.Structure):
                 ("assembly_seconds", C.c_double)]
 
 
+class TuningC(C.Structure):
+    _fields_ = [("element_threads", C.c_int), ("element_ctas_per_sm", C.c_int),
+                ("column_threads", C.c_int), ("tc_ctas_per_sm", C.c_int), ("slice_cost", C.c_int),
+                ("assembly_ms", C.c_double), ("default_assembly_ms", C.c_double),
+                ("solve_ms", C.c_double), ("default_solve_ms", C.c_double)]
+
+
 i32, i64, f64, vp = C.c_int, C.c_int64, C.c_double, C.c_void_p
 pi32, pi64 = C.POINTER(C.c_int), C.POINTER(C.c_int64)
 
@@ -99,6 +106,9 @@ SIGNATURES = {
         None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_problem_set_cell_tensor": (None, [i32, vp, pi32]),
     "ffg_problem_set_assembly_precision": (None, [i32, i32, pi32]),
+    "ffg_problem_autotune": (
+        None, [i32, vp, f64, f64, vp, vp, vp, i32, C.POINTER(TuningC), pi32]),
+    "ffg_problem_set_tuning": (None, [i32, C.POINTER(TuningC), pi32]),
     "ffg_assemble_tetra_nedelec_pml_csc": (
         None, [i32, vp, i32, vp, i32, vp, f64, i64, pi32, pi64, vp, vp, vp, pi32]),
     "ffg_assemble_tetra_nedelec_curvilinear_pml_csc": (
@@ -139,6 +149,7 @@ SIGNATURES = {
     "ffg_problem_sample_points": (None, [i32, vp, vp, pi32]),
     "ffg_problem_dof_points": (None, [i32, vp, vp, pi32]),
     "ffg_problem_constrained": (None, [i32, vp, pi32]),
+    "ffg_problem_topology": (None, [i32, vp, vp, vp, pi32]),
     "ffg_problem_solve": (
         None, [i32, vp, f64, f64, vp, vp, vp, vp, C.POINTER(SolverOptionsC), vp,
                C.POINTER(SolverStatsC), i32, vp, pi32]),

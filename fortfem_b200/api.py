@@ -670,6 +670,31 @@ class Problem:
         K.load().ffg_problem_constrained(self.handle, _ptr(out), C.byref(st))
         return out.astype(bool)
 
+    def topology(self) -> dict:
+        """The problem's DoF map (ffg_problem_topology): global_dofs (n_cells x n_b)
+        and, for Nedelec, edge_sign (n_cells x 6) and face_perm (n_cells x 4)."""
+        gd = np.zeros((self.n_cells, self._nb()), np.int32)
+        es = np.zeros((self.n_cells, 6), np.int8)
+        fp = np.zeros((self.n_cells, 4), np.uint8)
+        st = C.c_int(0)
+        K.load().ffg_problem_topology(self.handle, _ptr(gd), _ptr(es), _ptr(fp), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_topology")
+        out = {"global_dofs": gd}
+        if self.family == K.FFG_TETRA_NEDELEC:
+            out.update(edge_sign=es, face_perm=fp)
+        return out
+
+    def _nb(self) -> int:
+        k = self.degree
+        if self.family == K.FFG_TETRA_NEDELEC:
+            return k * (k + 2) * (k + 3) // 2
+        if self.family == K.FFG_TETRA_LAGRANGE:
+            return (k + 1) * (k + 2) * (k + 3) // 6
+        if self.family == K.FFG_TRIANGLE_LAGRANGE:
+            return (k + 1) * (k + 2) // 2
+        return 3
+
     def _inputs(self, vertices, cell_a, cell_b, samples, g):
         v = _f64(vertices)
         if v.size != self.n_vertices * self.dim:
@@ -763,6 +788,29 @@ class Problem:
         if st.value:
             raise FortfemError(st.value, "ffg_problem_reduced_system")
         return CscMatrix(self.n_free, self.n_free, cp, ri, val), rhs, free
+
+    def autotune(self, vertices, coef_a=1.0, coef_b=0.0, cell_a=None, cell_b=None,
+                 samples=None) -> dict:
+        """Choose this problem's launch shapes by timing candidates on these inputs
+        (ffg_problem_autotune); returns the choice and the measured times."""
+        v, ca, cb, s, _ = self._inputs(vertices, cell_a, cell_b, samples, None)
+        t = K.TuningC()
+        st = C.c_int(0)
+        K.load().ffg_problem_autotune(self.handle, _ptr(v), float(coef_a), float(coef_b),
+                                      _ptr(ca), _ptr(cb), _ptr(s), 0, C.byref(t), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_autotune")
+        return {name: getattr(t, name) for name, _ in K.TuningC._fields_}
+
+    def set_tuning(self, tuning: dict):
+        """Apply launch shapes from an earlier autotune (ffg_problem_set_tuning)."""
+        t = K.TuningC()
+        for name, _ in K.TuningC._fields_:
+            setattr(t, name, tuning.get(name, 0))
+        st = C.c_int(0)
+        K.load().ffg_problem_set_tuning(self.handle, C.byref(t), C.byref(st))
+        if st.value:
+            raise FortfemError(st.value, "ffg_problem_set_tuning")
 
     def set_assembly_precision(self, precision: str):
         """Nedelec orders 3-4: "fp64" (CUDA-core FP64 contraction, the parity

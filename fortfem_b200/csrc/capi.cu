@@ -82,6 +82,7 @@ struct Problem {
   // Nedelec element contraction: FP64 CUDA cores or 3xTF32 tensor cores
   int assembly_precision = FFG_ASSEMBLY_FP64;
   TcPlan tc;
+  LaunchTuning tune;  // launch shapes (autotuned or defaults)
   int *err = nullptr;
   int *err_host = nullptr;   // pinned: degenerate-cell flag of a deferred check
   bool batch_pending = false;  // enqueued by ffg_problem_solve_batch, not yet collected
@@ -154,8 +155,10 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   t.cells.assign(cells, cells + (size_t)t.vpc * n_cells);
   int grid = 0;
   if ((st = pcg_grid_size(&grid))) return st;
-  // Lagrange and P1 topologies are built on the device; Nedelec on the host
-  const bool on_device = family == FFG_TETRA_LAGRANGE || family == FFG_TRIANGLE_P1;
+  // Lagrange, P1 and Nedelec topologies are built on the device; arbitrary-order
+  // triangles on the host
+  const bool on_device =
+      family == FFG_TETRA_LAGRANGE || family == FFG_TRIANGLE_P1 || family == FFG_TETRA_NEDELEC;
   if (on_device) {
     if (!validate_cells(t, msg)) return FFG_INVALID_INPUT;
     if (family == FFG_TRIANGLE_P1 && (t.vpc != 3 || degree != 1)) {
@@ -182,7 +185,6 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
     if ((st = upload(&dt.gd, t.gd))) return st;
     if ((st = upload(&dt.edge_sign, t.edge_sign))) return st;
     if ((st = upload(&dt.face_perm, t.face_perm))) return st;
-    if (!P->tab.face_blocks.empty() && (st = upload(&dt.face_blocks, P->tab.face_blocks))) return st;
     if ((st = upload(&dt.free_index, t.free_index))) return st;
     if ((st = upload(&dt.inc_ptr, t.inc_ptr))) return st;
     if ((st = upload(&dt.inc_cell, t.inc_cell))) return st;
@@ -194,6 +196,7 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
     build_sell(t.col_ptr, t.row_idx, kSellSigma, P->hsell);
     if ((st = upload_sell(P->hsell, grid, P->S))) return st;
   }
+  if (!P->tab.face_blocks.empty() && (st = upload(&dt.face_blocks, P->tab.face_blocks))) return st;
   if (!P->tab.ref.empty() && (st = upload(&dt.ref, P->tab.ref))) return st;
   if (!P->tab.load_basis.empty() && (st = upload(&dt.load_basis, P->tab.load_basis))) return st;
   const int64_t nfree = t.n_free();
@@ -241,6 +244,7 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
   AssemblyInputs in;
   in.coef_a = ca;
   in.coef_b = cb;
+  in.tune = &P.tune;
   const size_t nc = (size_t)t.n_cells;
   const int spc = P.samples_per_cell * (t.family == FFG_TETRA_NEDELEC ? 3 : 1);
   if (!vertices) { msg = "vertices missing"; return FFG_INVALID_INPUT; }
@@ -808,6 +812,186 @@ static bool symmetric_tensors(int64_t n_cells, const double *ten) {
   return true;
 }
 
+// ---------------------------------------------------------------- autotuner
+static void tuning_out(const LaunchTuning &t, ffg_tuning *o) {
+  o->element_threads = t.ned_threads;
+  o->element_ctas_per_sm = t.ned_ctas_per_sm;
+  o->column_threads = t.col_threads;
+  o->tc_ctas_per_sm = t.tc_ctas_per_sm;
+  o->slice_cost = t.slice_cost;
+}
+
+static int valid_tuning(const ffg_tuning &t) {
+  auto in = [](int v, std::initializer_list<int> ok) {
+    if (v == 0) return true;
+    for (int x : ok)
+      if (v == x) return true;
+    return false;
+  };
+  return in(t.element_threads, {128, 256}) && t.element_ctas_per_sm >= 0 &&
+         t.element_ctas_per_sm <= 32 && in(t.column_threads, {32, 64, 128, 256, 512}) &&
+         in(t.tc_ctas_per_sm, {1, 2}) && t.slice_cost >= 0 && t.slice_cost <= (1 << 20);
+}
+
+void ffg_problem_set_tuning(int handle, const ffg_tuning *tuning, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (!tuning || !valid_tuning(*tuning) || P->batch_pending) { *status = FFG_INVALID_INPUT; return; }
+  LaunchTuning t;
+  t.ned_threads = tuning->element_threads;
+  t.ned_ctas_per_sm = tuning->element_ctas_per_sm;
+  t.col_threads = tuning->column_threads;
+  t.tc_ctas_per_sm = tuning->tc_ctas_per_sm;
+  t.slice_cost = tuning->slice_cost;
+  int st = FFG_OK;
+  if (P->topo.n_free() > 0 && t.slice_cost != P->tune.slice_cost)
+    st = sell_repartition(P->S, t.slice_cost ? t.slice_cost : 256);
+  if (!st) P->tune = t;
+  *status = st;
+}
+
+void ffg_problem_autotune(int handle, const double *vertices, double ca, double cb,
+                          const double *cell_a, const double *cell_b, const double *samples,
+                          int memory, ffg_tuning *tuning, int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  if (!vertices || (memory != 0 && memory != 1) || P->batch_pending) {
+    *status = FFG_INVALID_INPUT;
+    return;
+  }
+  const Topology &t = P->topo;
+  const size_t nc = (size_t)t.n_cells;
+  const int spc = P->samples_per_cell * (t.family == FFG_TETRA_NEDELEC ? 3 : 1);
+  // device-resident inputs for every candidate
+  const double *v = vertices, *a = cell_a, *b = cell_b, *smp = samples;
+  if (memory == 0) {
+    auto h2d = [&](double *dst, const double *src, size_t n) -> const double * {
+      if (!src) return nullptr;
+      return cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess
+                 ? dst
+                 : nullptr;
+    };
+    v = h2d(P->in_vertices, vertices, (size_t)t.n_vertices * P->dim);
+    a = h2d(P->in_cell_a, cell_a, nc);
+    b = h2d(P->in_cell_b, cell_b, nc);
+    smp = h2d(P->in_samples, samples, nc * spc);
+    if (!v) { *status = FFG_CUDA_ERROR; return; }
+  }
+  std::string msg;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto time_assembly = [&](const LaunchTuning &cand, double &ms) -> int {
+    P->tune = cand;
+    ms = 1e30;
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaEventRecord(e0, 0);
+      int st = assemble(*P, v, ca, cb, a, b, smp, nullptr, 1, true, 0, msg);
+      cudaEventRecord(e1, 0);
+      if (st) return st;
+      if (cudaEventSynchronize(e1) != cudaSuccess) return FFG_CUDA_ERROR;
+      float f = 0;
+      cudaEventElapsedTime(&f, e0, e1);
+      ms = std::min(ms, (double)f);
+    }
+    return FFG_OK;
+  };
+  ffg_tuning rep;
+  std::memset(&rep, 0, sizeof(rep));
+  LaunchTuning best;  // defaults
+  int st = FFG_OK;
+  double best_ms = 0;
+  if ((st = time_assembly(best, best_ms))) goto done;
+  rep.default_assembly_ms = best_ms;
+  {
+    // element kernel shapes first, then the column gather's block size
+    std::vector<LaunchTuning> cands;
+    if (t.family == FFG_TETRA_NEDELEC && P->assembly_precision == FFG_ASSEMBLY_TF32X3) {
+      for (int c : {1, 2}) {
+        LaunchTuning x = best;
+        x.tc_ctas_per_sm = c;
+        cands.push_back(x);
+      }
+    } else if (t.family == FFG_TETRA_NEDELEC) {
+      for (int th : {128, 256})
+        for (int c : {4, 8, 16}) {
+          LaunchTuning x = best;
+          x.ned_threads = th;
+          x.ned_ctas_per_sm = c;
+          cands.push_back(x);
+        }
+    }
+    for (const auto &x : cands) {
+      double ms = 0;
+      if ((st = time_assembly(x, ms))) goto done;
+      if (ms < best_ms) { best_ms = ms; best = x; }
+    }
+    const LaunchTuning base = best;
+    for (int th : {64, 128, 256}) {
+      LaunchTuning x = base;
+      x.col_threads = th;
+      double ms = 0;
+      if ((st = time_assembly(x, ms))) goto done;
+      if (ms < best_ms) { best_ms = ms; best = x; }
+    }
+  }
+  rep.assembly_ms = best_ms;
+  P->tune = best;
+  // PCG partition: a fixed 60-iteration mixed run on the assembled system
+  if (t.n_free() > 0) {
+    if ((st = assemble(*P, v, ca, cb, a, b, smp, nullptr, 1, true, 0, msg))) goto done;
+    ffg_solver_options o;
+    fill_default(o);
+    o.tolerance = 0.0;
+    o.max_iterations = 60;
+    o.timeout_seconds = 10.0;
+    o.breakdown_guard = 1;
+    auto time_solve = [&](int cost, double &ms) -> int {
+      int s2 = sell_repartition(P->S, cost);
+      if (s2) return s2;
+      ms = 1e30;
+      for (int r = 0; r < 3; ++r) {
+        cudaMemset(P->x, 0, sizeof(double) * (size_t)t.n_free());
+        ffg_solver_stats stt;
+        cudaEventRecord(e0, 0);
+        s2 = pcg_solve(P->S, P->rhs, P->x, o, P->work, &stt, 0, msg);
+        cudaEventRecord(e1, 0);
+        if (s2) return s2;
+        if (cudaEventSynchronize(e1) != cudaSuccess) return FFG_CUDA_ERROR;
+        float f = 0;
+        cudaEventElapsedTime(&f, e0, e1);
+        ms = std::min(ms, (double)f);
+      }
+      return FFG_OK;
+    };
+    double sms_best = 0;
+    if ((st = time_solve(256, sms_best))) goto done;
+    rep.default_solve_ms = sms_best;
+    int best_cost = 256;
+    for (int cost : {16, 64, 128, 512, 1024}) {
+      double ms = 0;
+      if ((st = time_solve(cost, ms))) goto done;
+      if (ms < sms_best) { sms_best = ms; best_cost = cost; }
+    }
+    rep.solve_ms = sms_best;
+    P->tune.slice_cost = best_cost;
+    if ((st = sell_repartition(P->S, best_cost))) goto done;
+  }
+done:
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st) {
+    report(1, msg);
+    P->tune = LaunchTuning();
+    sell_repartition(P->S, 256);
+    *status = st;
+    return;
+  }
+  tuning_out(P->tune, &rep);
+  if (tuning) *tuning = rep;
+  *status = FFG_OK;
+}
+
 void ffg_problem_set_assembly_precision(int handle, int precision, int *status) {
   auto P = find_problem(handle);
   if (!P) { *status = FFG_BAD_HANDLE; return; }
@@ -853,6 +1037,19 @@ void ffg_problem_set_cell_tensor(int handle, const double *tensors, int *status)
                        cudaMemcpyHostToDevice) != cudaSuccess) {
     *status = FFG_CUDA_ERROR;
     return;
+  }
+  *status = FFG_OK;
+}
+
+void ffg_problem_topology(int handle, int *global_dofs, int8_t *edge_sign, uint8_t *face_perm,
+                          int *status) {
+  auto P = find_problem(handle);
+  if (!P) { *status = FFG_BAD_HANDLE; return; }
+  const Topology &t = P->topo;
+  if (global_dofs) std::memcpy(global_dofs, t.gd.data(), sizeof(int) * t.gd.size());
+  if (t.family == FFG_TETRA_NEDELEC) {
+    if (edge_sign) std::memcpy(edge_sign, t.edge_sign.data(), t.edge_sign.size());
+    if (face_perm) std::memcpy(face_perm, t.face_perm.data(), t.face_perm.size());
   }
   *status = FFG_OK;
 }

@@ -150,7 +150,9 @@ int upload_sell(const HostSell &h, int grid, DeviceSell &d);
 // grid + 1 CTA slice boundaries, wslice the slices of every warp (warp by
 // warp, CTA-major) and woff (grid * 32 + 1) where each warp's list starts.
 void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector<int> &cs,
-                    std::vector<int> &wslice, std::vector<int> &woff);
+                    std::vector<int> &wslice, std::vector<int> &woff, int slice_cost = 256);
+// Re-deal an uploaded operator's slices to CTAs and warps with another slice cost.
+int sell_repartition(DeviceSell &d, int slice_cost);
 void free_sell(DeviceSell &d);
 
 struct SolveWork {
@@ -223,6 +225,16 @@ int build_topology_device(Topology &t, int boundary_mode, const uint8_t *mask, i
                           DeviceTopology &dt, int64_t **csc_col_ptr, int **csc_row,
                           DeviceSell &S, std::string &msg);
 
+// Launch shapes chosen by the autotuner (ffg_problem_autotune); zero fields
+// keep the built-in defaults.
+struct LaunchTuning {
+  int ned_threads = 0;      // Nedelec FP64 element kernel: threads per CTA (128 or 256)
+  int ned_ctas_per_sm = 0;  // its grid: CTAs per SM
+  int col_threads = 0;      // column-owner gather: threads per block
+  int tc_ctas_per_sm = 0;   // 3xTF32 tensor-core kernel: CTAs per SM (1 or 2)
+  int slice_cost = 0;       // PCG work partition: cost of a slice beyond its entries
+};
+
 struct AssemblyInputs {
   const double *vertices = nullptr;  // device
   double coef_a = 1.0, coef_b = 0.0;
@@ -236,6 +248,7 @@ struct AssemblyInputs {
   // Nedelec: 12 contraction weights per cell supplied by the caller (device,
   // nullable); replaces the curl / mass weights computed from the geometry
   const double *geo_override = nullptr;
+  const LaunchTuning *tune = nullptr;  // launch shapes (null: defaults)
 };
 
 // Per-cell geometry/coefficient block and element right-hand sides.

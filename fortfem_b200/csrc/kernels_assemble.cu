@@ -559,7 +559,8 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   D.face_end = D.edge_end + 4 * D.fdc;
   D.kglobal = nedelec_smem_bytes(tab, D.fdc, false) > 200 * 1024 ? 1 : 0;
   const size_t smem = nedelec_smem_bytes(tab, D.fdc, D.kglobal != 0);
-  const bool small = D.nb <= 45;  // orders 1-3
+  const LaunchTuning *tu = in.tune;
+  const bool small = (tu && tu->ned_threads) ? tu->ned_threads == 128 : D.nb <= 45;  // orders 1-3
   if (smem > 48 * 1024) {
     const cudaError_t e =
         small ? cudaFuncSetAttribute(nedelec_element_kernel<128>,
@@ -571,7 +572,8 @@ int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopo
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * (small ? 16 : 8));
+  const int per_sm = (tu && tu->ned_ctas_per_sm) ? tu->ned_ctas_per_sm : (small ? 16 : 8);
+  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * per_sm);
 #define FFG_NED_ARGS                                                                           \
   t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,     \
       tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem, \
@@ -587,7 +589,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    const double *cell_rhs, const double *elem, const int64_t *col_ptr,
                    const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
                    cudaStream_t s, const float *elem32, int ld32) {
-  const int T = 128;
+  const int T = (in.tune && in.tune->col_threads) ? in.tune->col_threads : 128;
   const int64_t F = t.n_free();
   if (F == 0) return FFG_OK;
   const int *iperm = sell ? sell->iperm : nullptr;

@@ -1219,8 +1219,8 @@ int upload_sell(const HostSell &h, int grid, DeviceSell &d) {
 // slices are sorted by length inside each sigma window, so every 32nd slice
 // lands on a warp-dependent mix of long and short ones.
 void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector<int> &cs,
-                    std::vector<int> &wslice, std::vector<int> &woff) {
-  constexpr int64_t kSliceCost = 256;
+                    std::vector<int> &wslice, std::vector<int> &woff, int slice_cost) {
+  const int64_t kSliceCost = slice_cost;
   const int64_t ns = n_slices;
   auto cost = [&](int64_t s) { return soff[s + 1] - soff[s] + kSliceCost; };
   std::vector<int64_t> cum((size_t)ns + 1, 0);
@@ -1255,6 +1255,24 @@ void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector
     }
   }
   woff[(size_t)grid * kWarps] = (int)wslice.size();
+}
+
+int sell_repartition(DeviceSell &d, int slice_cost) {
+  if (d.grid <= 0 || !d.soff || !d.cta_slice || !d.woff) return FFG_INVALID_INPUT;
+  std::vector<int64_t> soff((size_t)d.n_slices + 1);
+  if (cudaMemcpy(soff.data(), d.soff, sizeof(int64_t) * soff.size(), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return FFG_CUDA_ERROR;
+  std::vector<int> cs, ws, wo;
+  sell_partition(soff.data(), d.n_slices, d.grid, cs, ws, wo, slice_cost);
+  bool ok = cudaMemcpy(d.cta_slice, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice) ==
+            cudaSuccess;
+  if (!ws.empty())
+    ok = ok && cudaMemcpy(d.wslice, ws.data(), sizeof(int) * ws.size(), cudaMemcpyHostToDevice) ==
+                   cudaSuccess;
+  ok = ok && cudaMemcpy(d.woff, wo.data(), sizeof(int) * wo.size(), cudaMemcpyHostToDevice) ==
+                 cudaSuccess;
+  return ok ? FFG_OK : FFG_CUDA_ERROR;
 }
 
 void free_sell(DeviceSell &d) {

@@ -600,7 +600,8 @@ int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const Assembl
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int groups = (int)((t.n_cells + kTcThreads - 1) / kTcThreads);
-  const int grid = std::min(groups, 2 * sms);
+  const int per_sm = (in.tune && in.tune->tc_ctas_per_sm) ? in.tune->tc_ctas_per_sm : 2;
+  const int grid = std::min(groups, per_sm * sms);
   cudaError_t e;
   if (t.degree == 3) {
     e = cudaFuncSetAttribute(nedelec_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -1,4 +1,4 @@
-// Device build of the Lagrange / P1 problem topology: the same arrays as the
+// Device build of the Lagrange / P1 / Nedelec problem topology: the same arrays as the
 // host build in topology.cpp (first-appearance DoF numbering, Dirichlet set,
 // constrained CSC pattern, incidences, slot maps) and the solver's SELL layout
 // of build_sell, made with sorts and scans instead of hash maps, so that a
@@ -23,7 +23,7 @@ namespace ffg {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kMaxLocalDofs = 35;  // Lagrange degree 4
+constexpr int kMaxLocalDofs = 216;  // Nedelec order 6 (Lagrange degree 4: 35)
 inline unsigned nblk(int64_t n) { return (unsigned)((n + kT - 1) / kT); }
 
 // Device buffer that frees itself.
@@ -171,6 +171,105 @@ __global__ void number_kernel(int64_t n, const int *first, const int *id, int *g
   if (i < n) gd[i] = id[first[i]];
 }
 
+// ------------------------------------------------------- Nedelec numbering
+// Local edges and faces in the reference's order (tetra_edge_dof_map.f90:10-77,
+// tetra_nedelec_global_dof_map.f90:15-105).
+__constant__ int kNedEdges[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+__constant__ int kNedFaces[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+
+// (min, max) vertex key of local edge q = 6 c + le, and its orientation
+// (+1 iff the first local vertex has the smaller global index)
+__global__ void ned_edge_keys_kernel(int n_cells, const int *cells, uint64_t *key, int *pos,
+                                     int8_t *sign) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 6 * (int64_t)n_cells) return;
+  const int c = (int)(q / 6), le = (int)(q % 6);
+  const int a = cells[4 * (int64_t)c + kNedEdges[le][0]];
+  const int b = cells[4 * (int64_t)c + kNedEdges[le][1]];
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  key[q] = ((uint64_t)(uint32_t)lo << 32) | (uint32_t)hi;
+  pos[q] = (int)q;
+  sign[q] = a < b ? 1 : -1;
+}
+
+// sorted-vertex key of local face q = 4 c + lf and the permutation index of
+// its local vertex order (ranks of the local vertices among the sorted ones,
+// numbered 123, 132, 213, 231, 312, 321 -> 0..5)
+__global__ void ned_face_keys_kernel(int n_cells, const int *cells, uint64_t *ka, uint64_t *kb,
+                                     int *pos, uint8_t *perm) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 4 * (int64_t)n_cells) return;
+  const int c = (int)(q / 4), lf = (int)(q % 4);
+  int lv[3], f[3];
+  for (int i = 0; i < 3; ++i) lv[i] = f[i] = cells[4 * (int64_t)c + kNedFaces[lf][i]];
+  for (int i = 1; i < 3; ++i)
+    for (int j = i; j > 0 && f[j - 1] > f[j]; --j) {
+      const int t = f[j]; f[j] = f[j - 1]; f[j - 1] = t;
+    }
+  int r[3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      if (f[j] == lv[i]) r[i] = j + 1;
+  const int code = 100 * r[0] + 10 * r[1] + r[2];
+  perm[q] = code == 123 ? 0 : code == 132 ? 1 : code == 213 ? 2 : code == 231 ? 3 : code == 312 ? 4 : 5;
+  ka[q] = ((uint64_t)(uint32_t)f[0] << 32) | (uint32_t)f[1];
+  kb[q] = (uint64_t)(uint32_t)f[2];
+  pos[q] = (int)q;
+}
+
+// first-appearance ids: id of the run's first position (ids in position order)
+__global__ void run_start1_kernel(int64_t n, const uint64_t *ks, int *st) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) st[i] = (i == 0 || ks[i] != ks[i - 1]) ? (int)i : 0;
+}
+
+__global__ void ned_gd_kernel(int n_cells, int k, int64_t edc, int64_t n_faces,
+                              const int *edge_first, const int *edge_id, const int *face_first,
+                              const int *face_id, int *gd) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_cells) return;
+  const int fdc = k * (k - 1), cdc = k * (k - 1) * (k - 2) / 2;
+  const int nb = 6 * k + 4 * fdc + cdc;
+  int *g = gd + (int64_t)nb * c;
+  for (int e = 0; e < 6; ++e) {
+    const int64_t ed = edge_id[edge_first[6 * (int64_t)c + e]];
+    for (int m = 0; m < k; ++m) g[e * k + m] = (int)(ed * k + m);
+  }
+  for (int lf = 0; lf < 4; ++lf) {
+    const int64_t fa = face_id[face_first[4 * (int64_t)c + lf]];
+    for (int m = 0; m < fdc; ++m) g[6 * k + lf * fdc + m] = (int)(edc + fa * fdc + m);
+  }
+  for (int m = 0; m < cdc; ++m)
+    g[6 * k + 4 * fdc + m] = (int)(edc + n_faces * fdc + (int64_t)c * cdc + m);
+}
+
+// incidence-one faces of a Nedelec mesh (build_zero_tangential_mask,
+// fortfem_tetra_nedelec_solver_3d.f90:416-458): every DoF of the face's three
+// edges and every face DoF
+__global__ void ned_boundary_kernel(int64_t n, const uint64_t *ka, const uint64_t *kb,
+                                    const int *ord, int k, const int *gd, uint8_t *con) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  auto same = [&](int64_t x, int64_t y) {
+    return kb[x] == kb[y] && ka[ord[x]] == ka[ord[y]];
+  };
+  if ((i > 0 && same(i, i - 1)) || (i + 1 < n && same(i, i + 1))) return;
+  const int q = ord[i], c = q / 4, lf = q % 4;
+  const int fdc = k * (k - 1), cdc = k * (k - 1) * (k - 2) / 2;
+  const int nb = 6 * k + 4 * fdc + cdc;
+  const int *g = gd + (int64_t)nb * c;
+  for (int le = 0; le < 6; ++le) {
+    bool oa = false, ob = false;
+    for (int j = 0; j < 3; ++j) {
+      oa = oa || kNedFaces[lf][j] == kNedEdges[le][0];
+      ob = ob || kNedFaces[lf][j] == kNedEdges[le][1];
+    }
+    if (oa && ob)
+      for (int m = 0; m < k; ++m) con[g[le * k + m]] = 1;
+  }
+  for (int m = 0; m < fdc; ++m) con[g[6 * k + lf * fdc + m]] = 1;
+}
+
 // ---------------------------------------------------------- constraints
 __global__ void tet_face_keys_kernel(int n_cells, const int *cells, uint64_t *ka, uint64_t *kb,
                                      int *val) {
@@ -287,7 +386,7 @@ __global__ void pattern_pairs_kernel(int n_cells, int nb, const int *gd, const i
                                      const int *at, uint64_t *key) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_cells) return;
-  int f[kMaxLocalDofs], m = 0;
+  int f[kMaxLocalDofs], m = 0;  // Nedelec order 6: 216 local DoFs
   for (int l = 0; l < nb; ++l) {
     const int x = free_index[gd[(int64_t)nb * c + l]];
     if (x >= 0) f[m++] = x;
@@ -422,11 +521,18 @@ int build_topology_device(Topology &t, int mode, const uint8_t *mask, int grid,
                           DeviceTopology &dt, int64_t **csc_col_ptr, int **csc_row,
                           DeviceSell &S, std::string &msg) {
   const bool p1 = t.family == FFG_TRIANGLE_P1;
-  if (!p1 && t.family != FFG_TETRA_LAGRANGE) { msg = "device topology: family"; return FFG_INVALID_INPUT; }
+  const bool ned = t.family == FFG_TETRA_NEDELEC;
+  if (!p1 && !ned && t.family != FFG_TETRA_LAGRANGE) {
+    msg = "device topology: family";
+    return FFG_INVALID_INPUT;
+  }
   const int nc = t.n_cells;
   std::vector<int> idx;
   if (p1) {
     t.nb = 3;
+  } else if (ned) {
+    if (t.degree < 1 || t.degree > 6) { msg = "Nedelec order must be 1..6"; return FFG_INVALID_INPUT; }
+    t.nb = nedelec_dof_count(t.degree);
   } else {
     if (t.degree < 1 || t.degree > 4) { msg = "Lagrange degree must be 1..4"; return FFG_INVALID_INPUT; }
     std::vector<double> nodes;
@@ -443,10 +549,61 @@ int build_topology_device(Topology &t, int mode, const uint8_t *mask, int grid,
   FFG_TRY(cudaMemcpy(cells.p, t.cells.data(), sizeof(int) * t.cells.size(), cudaMemcpyHostToDevice));
   FFG_ALLOC(gd, (size_t)nl);
   int st;
+  // Nedelec face keys stay for the boundary faces
+  Buf<uint64_t> nfa, nfb_sorted;
+  Buf<int> nford;
+  Buf<int8_t> esign;
+  Buf<uint8_t> fperm;
   // ---- DoF numbering
   if (p1) {
     FFG_TRY(cudaMemcpy(gd.p, cells.p, sizeof(int) * nl, cudaMemcpyDeviceToDevice));
     t.n_dofs = t.n_vertices;
+  } else if (ned) {
+    const int k = t.degree, fdc = k * (k - 1), cdc = k * (k - 1) * (k - 2) / 2;
+    const int64_t nle = 6 * (int64_t)nc, nlf = 4 * (int64_t)nc;
+    // edges by first appearance
+    Buf<uint64_t> ek, eks;
+    Buf<int> epos, eord, est, erun, efirst, eflag, eid;
+    FFG_ALLOC(ek, nle); FFG_ALLOC(eks, nle); FFG_ALLOC(epos, nle); FFG_ALLOC(eord, nle);
+    FFG_ALLOC(esign, nle);
+    ned_edge_keys_kernel<<<nblk(nle), kT>>>(nc, cells.p, ek.p, epos.p, esign.p);
+    if ((st = sort_pairs(tmp, ek.p, eks.p, epos.p, eord.p, (int)nle))) return st;
+    FFG_ALLOC(est, nle); FFG_ALLOC(erun, nle);
+    run_start1_kernel<<<nblk(nle), kT>>>(nle, eks.p, est.p);
+    if ((st = inclusive_max(tmp, est.p, erun.p, (int)nle))) return st;
+    FFG_ALLOC(efirst, nle); FFG_ALLOC(eflag, nle); FFG_ALLOC(eid, nle);
+    first_pos_kernel<<<nblk(nle), kT>>>(nle, eord.p, erun.p, efirst.p);
+    first_flag_kernel<<<nblk(nle), kT>>>(nle, efirst.p, eflag.p);
+    if ((st = exclusive_sum(tmp, eflag.p, eid.p, (int)nle))) return st;
+    int last_e = 0, last_ef = 0;
+    if ((st = read1(eid.p + nle - 1, last_e)) || (st = read1(eflag.p + nle - 1, last_ef))) return st;
+    const int64_t n_edges = (int64_t)last_e + last_ef;
+    // faces by first appearance
+    Buf<uint64_t> fkb, fk1;
+    Buf<int> fpos, fo1, fst, frun, ffirst, fflag2, fid;
+    FFG_ALLOC(nfa, nlf); FFG_ALLOC(fkb, nlf); FFG_ALLOC(fk1, nlf); FFG_ALLOC(nfb_sorted, nlf);
+    FFG_ALLOC(fpos, nlf); FFG_ALLOC(fo1, nlf); FFG_ALLOC(nford, nlf); FFG_ALLOC(fperm, nlf);
+    ned_face_keys_kernel<<<nblk(nlf), kT>>>(nc, cells.p, nfa.p, fkb.p, fpos.p, fperm.p);
+    if ((st = sort_pairs(tmp, nfa.p, fk1.p, fpos.p, fo1.p, (int)nlf))) return st;
+    gather_u64_kernel<<<nblk(nlf), kT>>>(nlf, fkb.p, fo1.p, fk1.p);
+    if ((st = sort_pairs(tmp, fk1.p, nfb_sorted.p, fo1.p, nford.p, (int)nlf))) return st;
+    FFG_ALLOC(fst, nlf); FFG_ALLOC(frun, nlf);
+    run_start_kernel<<<nblk(nlf), kT>>>(nlf, nfa.p, nfb_sorted.p, nford.p, fst.p);
+    if ((st = inclusive_max(tmp, fst.p, frun.p, (int)nlf))) return st;
+    FFG_ALLOC(ffirst, nlf); FFG_ALLOC(fflag2, nlf); FFG_ALLOC(fid, nlf);
+    first_pos_kernel<<<nblk(nlf), kT>>>(nlf, nford.p, frun.p, ffirst.p);
+    first_flag_kernel<<<nblk(nlf), kT>>>(nlf, ffirst.p, fflag2.p);
+    if ((st = exclusive_sum(tmp, fflag2.p, fid.p, (int)nlf))) return st;
+    int last_f = 0, last_ff = 0;
+    if ((st = read1(fid.p + nlf - 1, last_f)) || (st = read1(fflag2.p + nlf - 1, last_ff))) return st;
+    const int64_t n_faces = (int64_t)last_f + last_ff;
+    const int64_t edc = (int64_t)k * n_edges;
+    const int64_t total = edc + n_faces * fdc + (int64_t)nc * cdc;
+    if (total >= (1LL << 31)) { msg = "too many DoFs"; return FFG_INVALID_INPUT; }
+    ned_gd_kernel<<<nblk(nc), kT>>>(nc, k, edc, n_faces, efirst.p, eid.p, ffirst.p, fid.p, gd.p);
+    t.n_edges = (int)n_edges;
+    t.n_faces = (int)n_faces;
+    t.n_dofs = total;
   } else {
     FFG_ALLOC(d_idx, idx.size());
     FFG_TRY(cudaMemcpy(d_idx.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice));
@@ -482,7 +639,10 @@ int build_topology_device(Topology &t, int mode, const uint8_t *mask, int grid,
     FFG_TRY(cudaMemcpy(m.p, mask, (size_t)N, cudaMemcpyHostToDevice));
     mask_kernel<<<nblk(N), kT>>>(N, m.p, con.p);
   } else if (mode == FFG_BOUNDARY_ALL) {
-    if (p1) {
+    if (ned) {
+      ned_boundary_kernel<<<nblk(4 * (int64_t)nc), kT>>>(4 * (int64_t)nc, nfa.p, nfb_sorted.p,
+                                                        nford.p, t.degree, gd.p, con.p);
+    } else if (p1) {
       const int64_t ne = 3 * (int64_t)nc;
       Buf<uint64_t> k, ks;
       Buf<int> v, vs;
@@ -661,6 +821,14 @@ int build_topology_device(Topology &t, int mode, const uint8_t *mask, int grid,
   FFG_TRY(cudaMemcpy(t.col_ptr.data(), col_ptr.p, sizeof(int64_t) * (F + 1), cudaMemcpyDeviceToHost));
   FFG_TRY(cudaMemcpy(t.row_idx.data(), row.p, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
   t.max_column = maxc;
+  if (ned) {
+    t.edge_sign.resize(6 * (size_t)nc);
+    t.face_perm.resize(4 * (size_t)nc);
+    FFG_TRY(cudaMemcpy(t.edge_sign.data(), esign.p, 6 * (size_t)nc, cudaMemcpyDeviceToHost));
+    FFG_TRY(cudaMemcpy(t.face_perm.data(), fperm.p, 4 * (size_t)nc, cudaMemcpyDeviceToHost));
+    dt.edge_sign = esign.release();
+    dt.face_perm = fperm.release();
+  }
   // ---- hand the device arrays over
   dt.cells = cells.release();
   dt.gd = gd.release();

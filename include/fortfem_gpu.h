@@ -350,8 +350,50 @@ void ffg_problem_sample_points(int handle, const double *vertices, double *point
  * P1): 3 * n_dofs doubles.  Callers evaluate boundary_value there. */
 void ffg_problem_dof_points(int handle, const double *vertices, double *points, int *status);
 
+/* The DoF map of the problem, as ffg_build_topology returns it for the host
+ * build: global_dofs (n_cells x n_b, the reference's first-appearance
+ * numbering) and, for Nedelec, edge_sign (6 per cell: +1 when the local edge
+ * runs from the smaller to the larger global vertex, as
+ * build_tetra_edge_dof_map, tetra_edge_dof_map.f90:54-60) and face_perm (4
+ * per cell: index 0..5 of the local face vertices' ranks 123, 132, 213, 231,
+ * 312, 321, the face permutations of build_tetra_nedelec_dof_map,
+ * tetra_nedelec_global_dof_map.f90:68-90).  Null arrays are skipped. */
+void ffg_problem_topology(int handle, int *global_dofs, int8_t *edge_sign, uint8_t *face_perm,
+                          int *status);
+
 /* The constrained mask of the problem (n_dofs bytes, 1 = constrained). */
 void ffg_problem_constrained(int handle, uint8_t *mask, int *status);
+
+/* Launch shapes of a problem's kernels and the times that chose them.  Zero
+ * shape fields mean the built-in default. */
+typedef struct {
+  int element_threads;     /* Nedelec FP64 element kernel: threads per CTA (128 or 256) */
+  int element_ctas_per_sm; /* ... and its grid in CTAs per SM */
+  int column_threads;      /* column-owner gather: threads per block */
+  int tc_ctas_per_sm;      /* 3xTF32 tensor-core kernel: CTAs per SM (1 or 2) */
+  int slice_cost;          /* PCG work partition: cost of a slice beyond its entries */
+  double assembly_ms;         /* best assembly time measured (device-resident inputs) */
+  double default_assembly_ms; /* the built-in defaults, same measurement */
+  double solve_ms;            /* best time of a fixed 60-iteration mixed PCG run */
+  double default_solve_ms;    /* the built-in partition, same run */
+} ffg_tuning;
+
+/* No counterpart in the reference (whose loops have no launch shapes).
+ * Chooses the problem's launch shapes by measurement on its own inputs (as
+ * ffg_problem_solve takes them): the element kernel's CTA size and grid
+ * (Nedelec FP64) or the tensor-core kernel's CTAs per SM (3xTF32), the column
+ * gather's block size, then the PCG work partition's slice cost, each
+ * candidate timed with CUDA events (best of three) and the fastest kept for
+ * every following assembly and solve of the problem.  Results of assembly and
+ * solve do not depend on the shapes except through the CTA partition of the
+ * PCG dot products (reduced in a fixed order for a given partition).  Fills
+ * `tuning` with the choice and the times. */
+void ffg_problem_autotune(int handle, const double *vertices, double coef_a, double coef_b,
+                          const double *cell_a, const double *cell_b, const double *samples,
+                          int memory, ffg_tuning *tuning, int *status);
+/* Apply launch shapes (from an earlier ffg_problem_autotune, possibly of
+ * another process); the time fields are ignored. */
+void ffg_problem_set_tuning(int handle, const ffg_tuning *tuning, int *status);
 
 /* Nedelec problems of order 3 or 4: how the element matrices are contracted in
  * every following assembly.  FFG_ASSEMBLY_FP64 (the default) is the FP64

@@ -83,7 +83,6 @@ def test_tf32x3_constant_field_energy(k):
     tets = np.array([[0, 1, 2, 3], [0, 2, 1, 4]], dtype=np.int32)
     field = np.array([1.0, 2.0, -1.0])
     with ff.Problem(K.FFG_TETRA_NEDELEC, k, tets, len(verts), boundary="none") as prob:
-        pts = prob.dof_points(verts)
         R, _, free = _reduced(prob, verts, None, None, None, "tf32x3")
     # interpolate the constant field: the L2 projection solve is exact for it
     n, cp, ri, val = oracle.nedelec_csc(verts, tets, k, 0.0, 1.0)
@@ -98,7 +97,6 @@ def test_tf32x3_constant_field_energy(k):
     # constant field has no curl and |f|^2 vol = 6 * (2 / 6) = 2
     energy = dofs @ ff.spmv(A, dofs)
     assert abs(energy - 0.7 * 2.0) <= 1e-6 * 1.4
-    del pts
 
 
 def test_tf32x3_selection_rules():

@@ -60,3 +60,67 @@ def test_device_topology_full_size_p2_counts():
         assert prob.n_dofs == 912673 and prob.n_free == 857375 and prob.nnz == 23881263
         A, _, _ = prob.reduced_system(case.vertices, 1.0, 0.0, case.cell_coefficient)
         assert np.array_equal(A.col_ptr, host["col_ptr"]) and np.array_equal(A.row_idx, host["row_idx"])
+
+
+_PERMS = np.array([[1, 2, 3], [1, 3, 2], [2, 1, 3], [2, 3, 1], [3, 1, 2], [3, 2, 1]])
+
+
+def _check_nedelec_maps(prob, k, t):
+    """The device build's DoF map, edge orientations and face permutations
+    against the oracle's restatement of build_tetra_nedelec_dof_map."""
+    topo = prob.topology()
+    ref = oracle.nedelec_dof_map(k, t)
+    assert prob.n_dofs == ref["n_global"]
+    assert np.array_equal(topo["global_dofs"], ref["global_dofs"])
+    assert np.array_equal(topo["edge_sign"].astype(np.int32), ref["edge_orientations"])
+    assert np.array_equal(_PERMS[topo["face_perm"]], ref["face_permutations"])
+
+
+NED_CASES = [(1, "all"), (2, "all"), (2, "none"), (3, "all"), (3, "mask"), (4, "all"), (6, "all")]
+
+
+@pytest.mark.parametrize("k,boundary", NED_CASES)
+def test_device_nedelec_topology_equals_host_build(k, boundary):
+    n = {1: 4, 2: 3, 3: 2, 4: 2, 6: 1}[k]
+    v, t = oracle.box_mesh([n, n + 1, n])
+    bnd = boundary
+    if boundary == "mask":
+        n_dofs = ff.build_topology(K.FFG_TETRA_NEDELEC, k, t, len(v), boundary="none")["n_dofs"]
+        bnd = (np.random.default_rng(k).random(n_dofs) < 0.2).astype(np.uint8)
+    host = ff.build_topology(K.FFG_TETRA_NEDELEC, k, t, len(v), boundary=bnd)
+    with ff.Problem(K.FFG_TETRA_NEDELEC, k, t, len(v), boundary=bnd) as prob:
+        assert prob.n_dofs == host["n_dofs"] and prob.n_free == host["n_free"]
+        assert np.array_equal(prob.constrained(), host["constrained"])
+        assert np.array_equal(prob.topology()["global_dofs"], host["global_dofs"])
+        A, rhs, free = prob.reduced_system(v, 1.0, 0.5)
+        assert np.array_equal(A.col_ptr, host["col_ptr"]) and np.array_equal(A.row_idx, host["row_idx"])
+        assert np.array_equal(free, np.flatnonzero(~host["constrained"]))
+        _check_nedelec_maps(prob, k, t)
+        if boundary == "all":
+            assert np.array_equal(prob.constrained(), oracle.pec_mask(k, t))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_device_nedelec_topology_slab_24cube(k):
+    """The 24^3 x 6 slab mesh: numbering, orientations, permutations and the
+    PEC mask against the oracle entry for entry; the constrained pattern
+    against the host build for orders 1-2 (the host build of orders 3-4 sorts
+    10^8+ couplings on the CPU)."""
+    import time
+    case = synth.nedelec_slab_case(k, mesh=lambda m: oracle.box_mesh([m, m, m]))
+    t0 = time.perf_counter()
+    prob = ff.Problem(K.FFG_TETRA_NEDELEC, k, case.cells, len(case.vertices), boundary="all")
+    setup = time.perf_counter() - t0
+    try:
+        print(f"order {k}: device topology setup {setup:.3f} s, {prob.n_dofs} DoFs, nnz {prob.nnz}")
+        assert prob.n_dofs == {1: 102024, 2: 542736, 3: 1570968, 4: 3435552}[k]
+        _check_nedelec_maps(prob, k, case.cells)
+        assert np.array_equal(prob.constrained(), oracle.pec_mask(k, case.cells))
+        if k <= 2:
+            host = ff.build_topology(K.FFG_TETRA_NEDELEC, k, case.cells, len(case.vertices),
+                                     boundary="all")
+            A, _, _ = prob.reduced_system(case.vertices, 1.0, 1.0, case.cell_curl)
+            assert np.array_equal(A.col_ptr, host["col_ptr"])
+            assert np.array_equal(A.row_idx, host["row_idx"])
+    finally:
+        prob.close()
