@@ -122,6 +122,8 @@ SIGNATURES = {
     "ffg_dist_update": (None, [i64, vp, f64, vp, vp, vp, vp, vp, vp, vp, vp, vp, pi32]),
     "ffg_dist_dot": (None, [i64, vp, vp, vp, vp, vp, vp, pi32]),
     "ffg_dist_direction": (None, [i64, vp, f64, vp, vp, vp, pi32]),
+    "ffg_dist_cgs_dots": (None, [i64, vp, vp, vp, vp, vp, vp, vp, pi32]),
+    "ffg_dist_cgs_update": (None, [i64, vp, f64, f64, vp, vp, vp, vp, vp, vp, vp, vp, pi32]),
     "ffg_dist_gather": (None, [i64, vp, vp, vp, vp, pi32]),
     "ffg_dist_scatter": (None, [i64, vp, vp, vp, vp, pi32]),
     "ffg_problem_evaluate": (

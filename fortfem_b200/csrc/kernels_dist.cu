@@ -118,6 +118,47 @@ __global__ void dot_kernel(int64_t n, const uint8_t *__restrict__ owned,
   if (threadIdx.x == 0) partial[blockIdx.x] = t;
 }
 
+// Single-reduction PCG (Chronopoulos-Gear): partials of (r, z), (w, z) and
+// (r, r) over owned rows, w = A z.
+__global__ void cgs_dots_kernel(int64_t n, const uint8_t *__restrict__ owned,
+                                const double *__restrict__ r, const double *__restrict__ z,
+                                const double *__restrict__ w, double *__restrict__ partial) {
+  __shared__ double red[kDotThreads / 32];
+  double rz = 0.0, wz = 0.0, rr = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (!owned[i]) continue;
+    rz += r[i] * z[i];
+    wz += w[i] * z[i];
+    rr += r[i] * r[i];
+  }
+  const double a = block_sum(rz, red), b = block_sum(wz, red), c = block_sum(rr, red);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = a;
+    partial[kDotBlocks + blockIdx.x] = b;
+    partial[2 * kDotBlocks + blockIdx.x] = c;
+  }
+}
+
+// p = z + beta p, s = w + beta s (s = A p by recurrence), x += alpha p,
+// r -= alpha s, z = D^-1 r on owned rows.
+__global__ void cgs_update_kernel(int64_t n, const uint8_t *__restrict__ owned, double alpha,
+                                  double beta, const double *__restrict__ w,
+                                  const double *__restrict__ dinv, double *__restrict__ p,
+                                  double *__restrict__ s, double *__restrict__ x,
+                                  double *__restrict__ r, double *__restrict__ z) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !owned[i]) return;
+  const double pi = z[i] + beta * p[i];
+  const double si = w[i] + beta * s[i];
+  p[i] = pi;
+  s[i] = si;
+  x[i] += alpha * pi;
+  const double ri = r[i] - alpha * si;
+  r[i] = ri;
+  z[i] = dinv[i] * ri;
+}
+
 // out[k] = sum of the kDotBlocks partials of slot k, in block order.
 __global__ void finish_kernel(int nslot, const double *__restrict__ partial,
                               double *__restrict__ out) {
@@ -196,6 +237,25 @@ void ffg_dist_dot(int64_t n, const uint8_t *owned, const double *a, const double
   if (n < 0 || !work || !dot) { *status = FFG_INVALID_INPUT; return; }
   dot_kernel<<<kDotBlocks, kDotThreads, 0, s>>>(n, owned, a, b, work);
   finish_kernel<<<1, 32, 0, s>>>(1, work, dot);
+  *status = launched();
+}
+
+void ffg_dist_cgs_dots(int64_t n, const uint8_t *owned, const double *r, const double *z,
+                       const double *w, double *work, double *dots, void *stream, int *status) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n < 0 || !work || !dots) { *status = FFG_INVALID_INPUT; return; }
+  cgs_dots_kernel<<<kDotBlocks, kDotThreads, 0, s>>>(n, owned, r, z, w, work);
+  finish_kernel<<<1, 32, 0, s>>>(3, work, dots);
+  *status = launched();
+}
+
+void ffg_dist_cgs_update(int64_t n, const uint8_t *owned, double alpha, double beta,
+                         const double *w, const double *dinv, double *p, double *s, double *x,
+                         double *r, double *z, void *stream, int *status) {
+  if (n < 0) { *status = FFG_INVALID_INPUT; return; }
+  if (n > 0)
+    cgs_update_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        n, owned, alpha, beta, w, dinv, p, s, x, r, z);
   *status = launched();
 }
 

@@ -227,6 +227,20 @@ class DeviceOps:
         self._check(st, "ffg_dist_dot")
         return float(self.dots[0].item())
 
+    def cgs_dots(self, owned, r, z, w):
+        st = C.c_int(0)
+        K.load().ffg_dist_cgs_dots(self.n, _p(owned), _p(r), _p(z), _p(w), _p(self.work),
+                                   _p(self.dots), None, C.byref(st))
+        self._check(st, "ffg_dist_cgs_dots")
+        return self.dots[:3].cpu().numpy().copy()
+
+    def cgs_update(self, owned, alpha, beta, w, p, s, x, r, z):
+        st = C.c_int(0)
+        K.load().ffg_dist_cgs_update(self.n, _p(owned), float(alpha), float(beta), _p(w),
+                                     _p(self.dinv), _p(p), _p(s), _p(x), _p(r), _p(z), None,
+                                     C.byref(st))
+        self._check(st, "ffg_dist_cgs_update")
+
     def direction(self, owned, beta, z, p):
         st = C.c_int(0)
         K.load().ffg_dist_direction(self.n, _p(owned), float(beta), _p(z), _p(p), None,
@@ -259,6 +273,7 @@ class ShardStats:
     final_residual: float = 0.0
     initial_residual: float = 0.0
     exchanged_values: int = 0
+    allreduces: int = 0
 
 
 class ShardedSolver:
@@ -320,9 +335,22 @@ class ShardedSolver:
             moved += idx.numel()
         return moved
 
-    def solve(self, tol=1e-10, max_iterations=100000, relative=True, x0=None) -> ShardStats:
+    def solve(self, tol=1e-10, max_iterations=100000, relative=True, x0=None,
+              variant="reference") -> ShardStats:
         """Solve the assembled system (ops.assemble first).  Returns the stats;
-        the rank's owned solution rows are in self.x (SELL order)."""
+        the rank's owned solution rows are in self.x (SELL order).
+
+        variant "reference": the reference's Jacobi-PCG recurrences
+        (advanced_solvers.f90:880-925), two all-reduces and one halo exchange
+        of p per iteration.  "single_reduction": the Chronopoulos-Gear form of
+        the same method, whose (r, z), (A z, z) and (r, r) travel in ONE
+        all-reduce of three doubles per iteration, with q = A p carried by
+        recurrence and one halo exchange of z; it stops on the same
+        recursive-residual rule, with rounding of a different order."""
+        if variant == "single_reduction":
+            return self._solve_single_reduction(tol, max_iterations, relative, x0)
+        if variant != "reference":
+            raise ValueError(f"unknown variant {variant!r}")
         ops, owned = self.ops, self.owned
         n = ops.n
         x = ops.zeros(n) if x0 is None else x0
@@ -331,6 +359,7 @@ class ShardedSolver:
         self.exchange(x)
         ops.spmv(x, q)
         rr, rz, bb = self._allreduce(ops.start(owned, q, r, z, p))
+        st.allreduces += 1
         st.exchanged_values += self.exchange(p)
         r0 = np.sqrt(rr)
         st.initial_residual = r0
@@ -342,10 +371,12 @@ class ShardedSolver:
         while not st.converged and it < max_iterations:
             ops.spmv(p, q)
             (pq,) = self._allreduce([ops.dot(owned, p, q)])
+            st.allreduces += 1
             if abs(pq) < 1.0e-14:   # the reference's breakdown test
                 break
             alpha = rz / pq
             rr, rz_new = self._allreduce(ops.update(owned, alpha, p, q, x, r, z))
+            st.allreduces += 1
             it += 1
             res = np.sqrt(rr)
             if res <= target:
@@ -357,6 +388,49 @@ class ShardedSolver:
             st.exchanged_values += self.exchange(p)
         st.iterations = it
         st.final_residual = float(res)
+        self.x = x
+        return st
+
+    def _solve_single_reduction(self, tol, max_iterations, relative, x0) -> ShardStats:
+        ops, owned = self.ops, self.owned
+        n = ops.n
+        x = ops.zeros(n) if x0 is None else x0
+        r, z, p, s, w = ops.zeros(n), ops.zeros(n), ops.zeros(n), ops.zeros(n), ops.zeros(n)
+        st = ShardStats()
+        self.exchange(x)
+        ops.spmv(x, w)
+        ops.start(owned, w, r, z, p)          # r = b - A x, z = D^-1 r (its dots are not needed)
+        st.exchanged_values += self.exchange(z)
+        ops.spmv(z, w)
+        gamma_old = alpha_old = 0.0
+        target = None
+        it = 0
+        res = 0.0
+        p.zero_()
+        while True:
+            gamma, delta, rr = self._allreduce(ops.cgs_dots(owned, r, z, w))
+            st.allreduces += 1
+            res = float(np.sqrt(rr))
+            if target is None:
+                st.initial_residual = res
+                target = tol * res if relative else tol
+            if res <= target:
+                st.converged = True
+                break
+            if it >= max_iterations:
+                break
+            beta = gamma / gamma_old if it > 0 else 0.0
+            denom = delta - (beta * gamma / alpha_old if it > 0 else 0.0)   # p^T A p
+            if abs(denom) < 1.0e-14:   # the reference's breakdown test
+                break
+            alpha = gamma / denom
+            ops.cgs_update(owned, alpha, beta, w, p, s, x, r, z)
+            it += 1
+            st.exchanged_values += self.exchange(z)
+            ops.spmv(z, w)
+            gamma_old, alpha_old = gamma, alpha
+        st.iterations = it
+        st.final_residual = res
         self.x = x
         return st
 
@@ -381,7 +455,8 @@ def local_inputs(plan: RankPlan, vertices, cell_a=None, cell_b=None, samples=Non
 def solve_sharded(family: int, degree: int, vertices, cells, coef_a=1.0, coef_b=0.0,
                   cell_a=None, cell_b=None, samples=None, constrained_values=None,
                   boundary="all", rule=K.FFG_RULE_DUFFY, quadrature_degree=0, tol=1e-10,
-                  max_iterations=100000, device=None, group=None, plans=None):
+                  max_iterations=100000, device=None, group=None, plans=None,
+                  variant="reference"):
     """Solve one system over the ranks of the process group (one GPU each):
     returns (full solution on every rank, ShardStats).  samples is the
     cell-major array of source samples at the problem's sample points, as
@@ -400,7 +475,7 @@ def solve_sharded(family: int, degree: int, vertices, cells, coef_a=1.0, coef_b=
                                          constrained_values)
         ops.assemble(v, coef_a, coef_b, ca, cb, smp, g)
         solver = ShardedSolver(plan, ops, group)
-        st = solver.solve(tol=tol, max_iterations=max_iterations)
+        st = solver.solve(tol=tol, max_iterations=max_iterations, variant=variant)
         full = gather_solution(solver, plan.n_dofs, plan.free_dofs, constrained_values)
         return full, st
     finally:

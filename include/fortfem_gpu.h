@@ -570,6 +570,16 @@ void ffg_dist_dot(int64_t n, const uint8_t *owned, const double *a, const double
 void ffg_dist_direction(int64_t n, const uint8_t *owned, double beta, const double *z, double *p,
                         void *stream, int *status);
 
+/* Single-reduction form of the same iteration (Chronopoulos-Gear PCG, one
+ * all-reduce per iteration): dots (device, 3) = (r, z), (w, z), (r, r) over
+ * owned rows with w = A z; then p = z + beta p, s = w + beta s, x += alpha p,
+ * r -= alpha s, z = D^-1 r on owned rows. */
+void ffg_dist_cgs_dots(int64_t n, const uint8_t *owned, const double *r, const double *z,
+                       const double *w, double *work, double *dots, void *stream, int *status);
+void ffg_dist_cgs_update(int64_t n, const uint8_t *owned, double alpha, double beta,
+                         const double *w, const double *dinv, double *p, double *s, double *x,
+                         double *r, double *z, void *stream, int *status);
+
 /* dst[i] = src[idx[i]] (pack a halo) and dst[idx[i]] = src[i] (unpack), i < m. */
 void ffg_dist_gather(int64_t m, const int *idx, const double *src, double *dst, void *stream,
                      int *status);

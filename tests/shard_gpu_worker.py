@@ -2,7 +2,7 @@
 exchange their halos through gloo (host memory), so no kernel waits on
 another rank.  Run by tests/test_gpu_sharding.py.
 
-Usage: python shard_gpu_worker.py <family> <degree> <n> <out.npz>  (RANK,
+Usage: python shard_gpu_worker.py <family> <degree> <n> <out.npz> [variant]  (RANK,
 WORLD_SIZE, MASTER_ADDR, MASTER_PORT in the environment)."""
 import datetime
 import os
@@ -22,6 +22,7 @@ from shard_gpu_case import case  # noqa: E402
 
 def main():
     family, degree, n, out = int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]), sys.argv[4]
+    variant = sys.argv[5] if len(sys.argv) > 5 else "reference"
     rank, world, _ = replicas.env()
     torch.cuda.set_device(0)
     dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
@@ -29,9 +30,9 @@ def main():
     full, st = sharding.solve_sharded(family, degree, c["v"], c["t"], c["coef"][0], c["coef"][1],
                                       samples=c["samples"], constrained_values=c["g"],
                                       quadrature_degree=c["q"], tol=1e-10,
-                                      device=torch.device("cuda", 0))
+                                      device=torch.device("cuda", 0), variant=variant)
     np.savez(out, full=full, iterations=st.iterations, converged=st.converged,
-             exchanged=st.exchanged_values)
+             exchanged=st.exchanged_values, allreduces=st.allreduces)
     dist.barrier()
     dist.destroy_process_group()
 

@@ -79,6 +79,20 @@ class NumpyOps:
         o = owned.numpy()[: self.n].astype(bool)
         return float(a.numpy()[: self.n][o] @ b.numpy()[: self.n][o])
 
+    def cgs_dots(self, owned, r, z, w):
+        o = owned.numpy()[: self.n].astype(bool)
+        R, Z, W = (a.numpy()[: self.n][o] for a in (r, z, w))
+        return np.array([R @ Z, W @ Z, R @ R])
+
+    def cgs_update(self, owned, alpha, beta, w, p, s, x, r, z):
+        o = owned.numpy()[: self.n].astype(bool)
+        W, P, S, X, R, Z = (a.numpy()[: self.n] for a in (w, p, s, x, r, z))
+        P[o] = Z[o] + beta * P[o]
+        S[o] = W[o] + beta * S[o]
+        X[o] += alpha * P[o]
+        R[o] -= alpha * S[o]
+        Z[o] = self.dinv[o] * R[o]
+
     def direction(self, owned, beta, z, p):
         o = owned.numpy()[: self.n].astype(bool)
         P, Z = p.numpy()[: self.n], z.numpy()[: self.n]
@@ -96,6 +110,7 @@ class NumpyOps:
 
 def main():
     family, degree, n, out = int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]), sys.argv[4]
+    variant = sys.argv[5] if len(sys.argv) > 5 else "reference"
     rank, world, _ = replicas.env()
     dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=30))
     v, t = oracle.box_mesh([n, n, n])
@@ -121,10 +136,11 @@ def main():
         g = np.cos(np.arange(nd) * 0.37)
     ops = NumpyOps(plan, family, degree, v, source, g, coef)
     solver = sharding.ShardedSolver(plan, ops)
-    st = solver.solve(tol=1e-10, max_iterations=5000)
+    st = solver.solve(tol=1e-10, max_iterations=5000, variant=variant)
     full = sharding.gather_solution(solver, nd, free, g)
     res = {"rank": rank, "iterations": st.iterations, "converged": bool(st.converged),
-           "owned": int(plan.owned.sum()), "exchanged": int(st.exchanged_values)}
+           "owned": int(plan.owned.sum()), "exchanged": int(st.exchanged_values),
+           "allreduces": int(st.allreduces)}
     if rank == 0:
         # the single-system solve of the same problem by the oracle
         if family == K.FFG_TETRA_LAGRANGE:

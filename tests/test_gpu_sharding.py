@@ -69,10 +69,13 @@ def single_gpu(family, degree, c):
     return sol
 
 
-@pytest.mark.parametrize("family,degree,n,world", [(K.FFG_TETRA_LAGRANGE, 2, 5, 2),
-                                                   (K.FFG_TETRA_LAGRANGE, 1, 6, 3),
-                                                   (K.FFG_TETRA_NEDELEC, 2, 3, 2)])
-def test_ranks_on_one_gpu_equal_the_single_system(family, degree, n, world, tmp_path):
+@pytest.mark.parametrize("family,degree,n,world,variant",
+                         [(K.FFG_TETRA_LAGRANGE, 2, 5, 2, "reference"),
+                          (K.FFG_TETRA_LAGRANGE, 1, 6, 3, "reference"),
+                          (K.FFG_TETRA_NEDELEC, 2, 3, 2, "reference"),
+                          (K.FFG_TETRA_LAGRANGE, 2, 5, 2, "single_reduction"),
+                          (K.FFG_TETRA_NEDELEC, 2, 3, 3, "single_reduction")])
+def test_ranks_on_one_gpu_equal_the_single_system(family, degree, n, world, variant, tmp_path):
     port = _free_port()
     procs, outs = [], []
     for rank in range(world):
@@ -80,7 +83,8 @@ def test_ranks_on_one_gpu_equal_the_single_system(family, degree, n, world, tmp_
         env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
                    MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
         procs.append(subprocess.Popen([sys.executable, os.path.join(HERE, "shard_gpu_worker.py"),
-                                       str(family), str(degree), str(n), str(out)], env=env))
+                                       str(family), str(degree), str(n), str(out), variant],
+                                      env=env))
         outs.append(out)
     codes = []
     for p in procs:
@@ -96,7 +100,9 @@ def test_ranks_on_one_gpu_equal_the_single_system(family, degree, n, world, tmp_
     one = single_gpu(family, degree, c)
     for r in res:
         assert bool(r["converged"]) == rst["converged"]
-        assert abs(int(r["iterations"]) - rst["iterations"]) <= 1
+        assert abs(int(r["iterations"]) - rst["iterations"]) <= (1 if variant == "reference" else 2)
+        if variant == "single_reduction":
+            assert int(r["allreduces"]) == int(r["iterations"]) + 1
         assert np.abs(r["full"] - ref).max() <= _rtol(family) * np.abs(ref).max()
         assert np.abs(r["full"] - one).max() <= _rtol(family) * np.abs(one).max()
         assert int(r["exchanged"]) > 0

@@ -25,7 +25,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _run(args, world, tmp_path, timeout=120):
+def _run(args, world, tmp_path, timeout=120, extra=()):
     port = _free_port()
     procs, outs = [], []
     for rank in range(world):
@@ -33,7 +33,7 @@ def _run(args, world, tmp_path, timeout=120):
         env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
                    MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
         procs.append(subprocess.Popen([sys.executable, os.path.join(HERE, "shard_worker.py"),
-                                       *map(str, args), str(out)], env=env))
+                                       *map(str, args), str(out), *extra], env=env))
         outs.append(out)
     codes = []
     for p in procs:
@@ -102,3 +102,20 @@ def test_sharded_pcg_matches_the_single_system(family, degree, n, world, tmp_pat
     assert abs(res[0]["iterations"] - res[0]["serial_iterations"]) <= 1
     assert res[0]["error"] < 1e-9
     assert all(r["exchanged"] > 0 for r in res)
+
+
+@pytest.mark.parametrize("family,degree,n", [(K.FFG_TETRA_LAGRANGE, 2, 4),
+                                             (K.FFG_TETRA_NEDELEC, 1, 3)])
+@pytest.mark.parametrize("world", [2, 3])
+def test_single_reduction_pcg_one_allreduce_per_iteration(family, degree, n, world, tmp_path):
+    """The Chronopoulos-Gear form: one all-reduce per iteration (plus the final
+    convergence check), the same stopping rule, the single-system solution."""
+    codes, res = _run([family, degree, n], world, tmp_path, extra=("single_reduction",))
+    assert codes == [0] * world
+    its = {r["iterations"] for r in res}
+    assert len(its) == 1
+    it = res[0]["iterations"]
+    assert all(r["allreduces"] == it + 1 for r in res)
+    assert {r["converged"] for r in res} == {res[0]["serial_converged"]}
+    assert abs(it - res[0]["serial_iterations"]) <= 2
+    assert res[0]["error"] < 1e-8
