@@ -1240,18 +1240,80 @@ void ffg_problem_solve_batch(int count, const int *handles, const double *const 
   cudaStream_t s = (cudaStream_t)stream;
   std::string msg;
   int st = FFG_OK;
+  // Lagrange-tetrahedron and P1 systems with scalar coefficients (the serving
+  // families) are assembled together, one launch per phase and family; the
+  // rest one system at a time
+  std::vector<AsmSys> lag, p1;
+  std::vector<AsmSys> all((size_t)count);
+  std::vector<char> batched((size_t)count, 0);
+  for (int i = 0; i < count; ++i) {
+    Problem &P = *probs[i];
+    const Topology &t = P.topo;
+    if ((t.family != FFG_TETRA_LAGRANGE && t.family != FFG_TRIANGLE_P1) || P.cell_tensor)
+      continue;
+    AsmSys a;
+    a.n_cells = t.n_cells;
+    a.nq = P.tab.nq_load;
+    a.stride = P.geo_stride;
+    a.nb = t.nb;
+    a.n_free = t.n_free();
+    a.n_dofs = t.n_dofs;
+    a.cells = P.dt.cells;
+    a.verts = vertices[i];
+    a.ca = coef_a[i];
+    a.cb = coef_b[i];
+    a.cell_a = cell_a ? cell_a[i] : nullptr;
+    a.cell_b = cell_b ? cell_b[i] : nullptr;
+    a.samples = samples ? samples[i] : nullptr;
+    a.geo = P.geo;
+    a.err = P.err;
+    a.col_ptr = P.csc_col_ptr;
+    a.row_idx = P.csc_row;
+    a.inc_ptr = P.dt.inc_ptr;
+    a.inc_cell = P.dt.inc_cell;
+    a.inc_local = P.dt.inc_local;
+    a.slot = P.dt.slot;
+    a.gd = P.dt.gd;
+    a.ref = P.dt.ref;
+    a.load_basis = P.dt.load_basis;
+    a.g = g ? g[i] : nullptr;
+    a.iperm = P.S.iperm;
+    a.free_index = P.dt.free_index;
+    a.soff = P.S.soff;
+    a.val64 = P.S.val64;
+    a.val32 = P.S.val32;
+    a.dinv64 = P.S.dinv64;
+    a.dinv32 = P.S.dinv32;
+    a.rhs = P.rhs;
+    a.x = P.x;
+    a.solution = solutions[i];
+    all[i] = a;
+    batched[i] = 1;
+    (t.family == FFG_TETRA_LAGRANGE ? lag : p1).push_back(a);
+  }
+  for (int i = 0; i < count; ++i)
+    if (batched[i]) cudaEventRecord(probs[i]->ev[0], s);
+  if (!lag.empty()) st = launch_batch_assembly(FFG_TETRA_LAGRANGE, (int)lag.size(), lag.data(), s);
+  if (!st && !p1.empty()) st = launch_batch_assembly(FFG_TRIANGLE_P1, (int)p1.size(), p1.data(), s);
   for (int i = 0; i < count && !st; ++i) {
     Problem &P = *probs[i];
-    cudaEventRecord(P.ev[0], s);
-    st = assemble(P, vertices[i], coef_a[i], coef_b[i], cell_a ? cell_a[i] : nullptr,
-                  cell_b ? cell_b[i] : nullptr, samples ? samples[i] : nullptr,
-                  g ? g[i] : nullptr, 1, true, s, msg, true);
-    if (st) break;
     const Topology &t = P.topo;
+    if (batched[i]) {
+      // the degenerate-cell flag is read with the statistics
+      if (cudaMemcpyAsync(P.err_host, P.err, sizeof(int), cudaMemcpyDeviceToHost, s) !=
+          cudaSuccess)
+        st = FFG_CUDA_ERROR;
+    } else {
+      cudaEventRecord(P.ev[0], s);
+      st = assemble(P, vertices[i], coef_a[i], coef_b[i], cell_a ? cell_a[i] : nullptr,
+                    cell_b ? cell_b[i] : nullptr, samples ? samples[i] : nullptr,
+                    g ? g[i] : nullptr, 1, true, s, msg, true);
+      if (st) break;
+      cudaMemsetAsync(P.x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
+    }
     if (!o.preconditioner)
       set_ones_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(t.n_free(), P.S.dinv64,
                                                                           P.S.dinv32);
-    cudaMemsetAsync(P.x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
     cudaEventRecord(P.ev[1], s);
   }
   if (!st) {
@@ -1274,19 +1336,28 @@ void ffg_problem_solve_batch(int count, const int *handles, const double *const 
         st = pcg_launch(*A[i], b[i], x[i], o, *w[i], s, msg);
     }
   }
+  for (int i = 0; i < count && !st; ++i) cudaEventRecord(probs[i]->ev[2], s);
+  {
+    std::vector<AsmSys> sols;
+    for (int i = 0; i < count; ++i)
+      if (batched[i]) sols.push_back(all[i]);
+    if (!st && !sols.empty()) st = launch_batch_solutions((int)sols.size(), sols.data(), s);
+  }
   for (int i = 0; i < count && !st; ++i) {
     Problem &P = *probs[i];
     const Topology &t = P.topo;
-    cudaEventRecord(P.ev[2], s);
-    if (g && g[i])
-      cudaMemcpyAsync(P.full, g[i], sizeof(double) * (size_t)t.n_dofs, cudaMemcpyDeviceToDevice, s);
-    else
-      cudaMemsetAsync(P.full, 0, sizeof(double) * (size_t)t.n_dofs, s);
-    if (t.n_free() > 0)
-      scatter_solution_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(
-          t.n_free(), P.S.perm, P.free_dofs, P.x, P.full);
-    cudaMemcpyAsync(solutions[i], P.full, sizeof(double) * (size_t)t.n_dofs,
-                    cudaMemcpyDeviceToDevice, s);
+    if (!batched[i]) {
+      if (g && g[i])
+        cudaMemcpyAsync(P.full, g[i], sizeof(double) * (size_t)t.n_dofs, cudaMemcpyDeviceToDevice,
+                        s);
+      else
+        cudaMemsetAsync(P.full, 0, sizeof(double) * (size_t)t.n_dofs, s);
+      if (t.n_free() > 0)
+        scatter_solution_kernel<<<(unsigned)((t.n_free() + 255) / 256), 256, 0, s>>>(
+            t.n_free(), P.S.perm, P.free_dofs, P.x, P.full);
+      cudaMemcpyAsync(solutions[i], P.full, sizeof(double) * (size_t)t.n_dofs,
+                      cudaMemcpyDeviceToDevice, s);
+    }
     if (cudaEventRecord(P.ev[3], s) != cudaSuccess) st = FFG_CUDA_ERROR;
   }
   if (st) {

@@ -292,6 +292,44 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
                    cudaStream_t s, const float *elem32 = nullptr, int ld32 = 0);
 int geo_stride_for(const Topology &t, const ElementTables &tab);
+// Batched assembly of independent Lagrange-tetrahedron or P1 systems (the
+// serving families) into their SELL operators, one launch per phase.
+constexpr int kMaxAsmBatch = 48;
+struct AsmSys {
+  int n_cells = 0, nq = 0, stride = 0, nb = 0;
+  int64_t n_free = 0, n_dofs = 0;
+  const int *cells = nullptr;
+  const double *verts = nullptr;
+  double ca = 1.0, cb = 0.0;
+  const double *cell_a = nullptr, *cell_b = nullptr, *samples = nullptr;
+  double *geo = nullptr;
+  int *err = nullptr;
+  const int64_t *col_ptr = nullptr;
+  const int *row_idx = nullptr;
+  const int64_t *inc_ptr = nullptr;
+  const int *inc_cell = nullptr;
+  const uint8_t *inc_local = nullptr;
+  const uint16_t *slot = nullptr;
+  const int *gd = nullptr;
+  const double *ref = nullptr, *load_basis = nullptr, *g = nullptr;
+  const int *iperm = nullptr, *free_index = nullptr;
+  const int64_t *soff = nullptr;
+  double *val64 = nullptr, *dinv64 = nullptr, *rhs = nullptr, *x = nullptr, *solution = nullptr;
+  float *val32 = nullptr, *dinv32 = nullptr;
+};
+struct AsmBatch {
+  int count;
+  int64_t cell_begin[kMaxAsmBatch + 1];
+  int64_t col_begin[kMaxAsmBatch + 1];
+  int64_t dof_begin[kMaxAsmBatch + 1];
+  AsmSys sys[kMaxAsmBatch];
+};
+static_assert(sizeof(AsmBatch) <= 32000, "kernel parameter block too large");
+// err = 0, geometry, SELL scatter with x = 0, for `count` systems of `family`
+int launch_batch_assembly(int family, int count, const AsmSys *sys, cudaStream_t s);
+// full solutions (constrained values from g or 0, free values from x)
+int launch_batch_solutions(int count, const AsmSys *sys, cudaStream_t s);
+
 
 // Forward / reverse mode of the Lagrange stiffness + mass and the Nedelec
 // curl + mass assembly (kernels_ad.cu; the Nedelec forward mode runs through

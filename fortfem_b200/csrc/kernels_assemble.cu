@@ -30,14 +30,13 @@ __constant__ int kPb[6] = {0, 1, 2, 1, 2, 2};
 
 // ------------------------------------------------------------ K1 geometry
 // Lagrange: geo = [k det G_ab (6), m det, det f_q (n_q)], G = J^-1 J^-T.
-__global__ void lagrange_geometry_kernel(int n_cells, const int *__restrict__ cells,
-                                         const double *__restrict__ verts, double ca, double cb,
-                                         const double *__restrict__ cell_a,
-                                         const double *__restrict__ cell_b,
-                                         const double *__restrict__ samples, int nq,
-                                         double *__restrict__ geo, int stride, int *err) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n_cells) return;
+__device__ __forceinline__ void lagrange_geometry_cell(int c, const int *__restrict__ cells,
+                                                      const double *__restrict__ verts, double ca,
+                                                      double cb, const double *__restrict__ cell_a,
+                                                      const double *__restrict__ cell_b,
+                                                      const double *__restrict__ samples, int nq,
+                                                      double *__restrict__ geo, int stride,
+                                                      int *err) {
   double J[9], Ji[9], v0[3];
   tet_jacobian(cells, verts, c, J, v0);
   const double det = det3(J);
@@ -61,17 +60,26 @@ __global__ void lagrange_geometry_kernel(int n_cells, const int *__restrict__ ce
   for (int q = 0; q < nq; ++q) g[7 + q] = samples ? det * samples[(size_t)nq * c + q] : 0.0;
 }
 
+__global__ void lagrange_geometry_kernel(int n_cells, const int *__restrict__ cells,
+                                         const double *__restrict__ verts, double ca, double cb,
+                                         const double *__restrict__ cell_a,
+                                         const double *__restrict__ cell_b,
+                                         const double *__restrict__ samples, int nq,
+                                         double *__restrict__ geo, int stride, int *err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n_cells)
+    lagrange_geometry_cell(c, cells, verts, ca, cb, cell_a, cell_b, samples, nq, geo, stride, err);
+}
+
 // P1 triangles: closed-form local matrix of assemble_scalar_p1_matrix
 // (src/fortfem_forms_simple.f90:1702-1717) and the load area/3 of
 // assemble_scalar_p1_load (:1749-1758) with a per-cell source value.
-__global__ void p1_geometry_kernel(int n_cells, const int *__restrict__ tris,
-                                   const double *__restrict__ verts, double stiff, double mass,
-                                   const double *__restrict__ cell_a,
-                                   const double *__restrict__ cell_b,
-                                   const double *__restrict__ samples, double *__restrict__ geo,
-                                   int *err) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n_cells) return;
+__device__ __forceinline__ void p1_geometry_cell(int c, const int *__restrict__ tris,
+                                                 const double *__restrict__ verts, double stiff,
+                                                 double mass, const double *__restrict__ cell_a,
+                                                 const double *__restrict__ cell_b,
+                                                 const double *__restrict__ samples,
+                                                 double *__restrict__ geo, int *err) {
   double x[3], y[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -98,6 +106,16 @@ __global__ void p1_geometry_kernel(int n_cells, const int *__restrict__ tris,
       g[a + 3 * b] = ks * area * (gx[a] * gx[b] + gy[a] * gy[b]) +
                      km * area * (a == b ? 2.0 : 1.0) / 12.0;
   g[9] = samples ? samples[c] * area / 3.0 : 0.0;
+}
+
+__global__ void p1_geometry_kernel(int n_cells, const int *__restrict__ tris,
+                                   const double *__restrict__ verts, double stiff, double mass,
+                                   const double *__restrict__ cell_a,
+                                   const double *__restrict__ cell_b,
+                                   const double *__restrict__ samples, double *__restrict__ geo,
+                                   int *err) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < n_cells) p1_geometry_cell(c, tris, verts, stiff, mass, cell_a, cell_b, samples, geo, err);
 }
 
 // Arbitrary-order triangles: geo = [k |det| G_00, k |det| G_11, k |det| G_01,
@@ -349,7 +367,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) nedelec_element_kerne
 // operator, which by symmetry is column j), with the FP32 copy, the Jacobi
 // diagonal and the rhs in the SELL numbering.
 template <int FAMILY, bool SELL>
-__global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_ptr,
+__device__ __forceinline__ void column_body(int64_t j, const int64_t *__restrict__ col_ptr,
                               const int *__restrict__ row_idx, const int64_t *__restrict__ inc_ptr,
                               const int *__restrict__ inc_cell,
                               const uint8_t *__restrict__ inc_local,
@@ -363,8 +381,6 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
                               double *__restrict__ dinv64, float *__restrict__ dinv32,
                               double *__restrict__ rhs, const float *__restrict__ elem32,
                               int ld32) {
-  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_free) return;
   const int64_t start = col_ptr[j], end = col_ptr[j + 1];
   int64_t base, stride_out, out_row;
   if (SELL) {
@@ -435,6 +451,28 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
     dinv64[out_row] = di;
     dinv32[out_row] = (float)di;
   }
+}
+
+template <int FAMILY, bool SELL>
+__global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_ptr,
+                              const int *__restrict__ row_idx, const int64_t *__restrict__ inc_ptr,
+                              const int *__restrict__ inc_cell,
+                              const uint8_t *__restrict__ inc_local,
+                              const uint16_t *__restrict__ slot, const int *__restrict__ gd,
+                              int nb, const double *__restrict__ geo, int stride,
+                              const double *__restrict__ ref, const double *__restrict__ load_basis,
+                              int nq, const double *__restrict__ elem,
+                              const double *__restrict__ cell_rhs, const double *__restrict__ g,
+                              const int *__restrict__ iperm, const int64_t *__restrict__ soff,
+                              double *__restrict__ val64, float *__restrict__ val32,
+                              double *__restrict__ dinv64, float *__restrict__ dinv32,
+                              double *__restrict__ rhs, const float *__restrict__ elem32,
+                              int ld32) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n_free)
+    column_body<FAMILY, SELL>(j, col_ptr, row_idx, inc_ptr, inc_cell, inc_local, slot, gd, nb, geo,
+                              stride, ref, load_basis, nq, elem, cell_rhs, g, iperm, soff, val64,
+                              val32, dinv64, dinv32, rhs, elem32, ld32);
 }
 
 // CSC columns of high-order elements (n_b >= 16), one warp per free column:
@@ -519,7 +557,111 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
 
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
+// ------------------------------------------- batched assembly (serving)
+// Independent systems of one family assembled by one launch per phase: a
+// thread finds its system by binary search over the prefix sums of cells
+// (geometry) or free columns (scatter) and runs the same per-cell / per-column
+// body as the single-system kernels, so every system's values are the bits
+// it gets alone.
+__device__ __forceinline__ int batch_find(const int64_t *begin, int count, int64_t g) {
+  int lo = 0, hi = count;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (begin[mid] <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void batch_prep_kernel(const __grid_constant__ AsmBatch B) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < B.count) *B.sys[s].err = 0;
+}
+
+template <int FAMILY>
+__global__ void batch_geometry_kernel(const __grid_constant__ AsmBatch B) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= B.cell_begin[B.count]) return;
+  const int s = batch_find(B.cell_begin, B.count, g);
+  const AsmSys &S = B.sys[s];
+  const int c = (int)(g - B.cell_begin[s]);
+  if (FAMILY == FFG_TETRA_LAGRANGE)
+    lagrange_geometry_cell(c, S.cells, S.verts, S.ca, S.cb, S.cell_a, S.cell_b, S.samples, S.nq,
+                           S.geo, S.stride, S.err);
+  else
+    p1_geometry_cell(c, S.cells, S.verts, S.ca, S.cb, S.cell_a, S.cell_b, S.samples, S.geo, S.err);
+}
+
+// the SELL-layout scatter of every system, and x = 0 for its solve
+template <int FAMILY>
+__global__ void batch_column_kernel(const __grid_constant__ AsmBatch B) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= B.col_begin[B.count]) return;
+  const int s = batch_find(B.col_begin, B.count, g);
+  const AsmSys &S = B.sys[s];
+  const int64_t j = g - B.col_begin[s];
+  S.x[j] = 0.0;
+  column_body<FAMILY, true>(j, S.col_ptr, S.row_idx, S.inc_ptr, S.inc_cell, S.inc_local, S.slot,
+                            S.gd, S.nb, S.geo, S.stride, S.ref, S.load_basis, S.nq, nullptr,
+                            nullptr, S.g, S.iperm, S.soff, S.val64, S.val32, S.dinv64, S.dinv32,
+                            S.rhs, nullptr, 0);
+}
+
+// every system's full solution: constrained DoFs from g (or 0), free DoFs
+// from the solver's x (SELL order)
+__global__ void batch_solution_kernel(const __grid_constant__ AsmBatch B) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= B.dof_begin[B.count]) return;
+  const int s = batch_find(B.dof_begin, B.count, g);
+  const AsmSys &S = B.sys[s];
+  const int64_t d = g - B.dof_begin[s];
+  const int f = S.free_index[d];
+  S.solution[d] = f >= 0 ? S.x[S.iperm[f]] : (S.g ? S.g[d] : 0.0);
+}
+
 }  // namespace
+
+int launch_batch_assembly(int family, int count, const AsmSys *sys, cudaStream_t s) {
+  if (family != FFG_TETRA_LAGRANGE && family != FFG_TRIANGLE_P1) return FFG_INVALID_INPUT;
+  for (int c0 = 0; c0 < count; c0 += kMaxAsmBatch) {
+    AsmBatch B;
+    B.count = std::min(kMaxAsmBatch, count - c0);
+    B.cell_begin[0] = B.col_begin[0] = B.dof_begin[0] = 0;
+    for (int i = 0; i < B.count; ++i) {
+      B.sys[i] = sys[c0 + i];
+      B.cell_begin[i + 1] = B.cell_begin[i] + B.sys[i].n_cells;
+      B.col_begin[i + 1] = B.col_begin[i] + B.sys[i].n_free;
+      B.dof_begin[i + 1] = B.dof_begin[i] + B.sys[i].n_dofs;
+    }
+    batch_prep_kernel<<<1, kMaxAsmBatch, 0, s>>>(B);
+    const int64_t nc = B.cell_begin[B.count], nf = B.col_begin[B.count];
+    if (family == FFG_TETRA_LAGRANGE) {
+      if (nc) batch_geometry_kernel<FFG_TETRA_LAGRANGE><<<blocks_for(nc, 128), 128, 0, s>>>(B);
+      if (nf) batch_column_kernel<FFG_TETRA_LAGRANGE><<<blocks_for(nf, 128), 128, 0, s>>>(B);
+    } else {
+      if (nc) batch_geometry_kernel<FFG_TRIANGLE_P1><<<blocks_for(nc, 128), 128, 0, s>>>(B);
+      if (nf) batch_column_kernel<FFG_TRIANGLE_P1><<<blocks_for(nf, 128), 128, 0, s>>>(B);
+    }
+    if (cudaGetLastError() != cudaSuccess) return FFG_CUDA_ERROR;
+  }
+  return FFG_OK;
+}
+
+int launch_batch_solutions(int count, const AsmSys *sys, cudaStream_t s) {
+  for (int c0 = 0; c0 < count; c0 += kMaxAsmBatch) {
+    AsmBatch B;
+    B.count = std::min(kMaxAsmBatch, count - c0);
+    B.dof_begin[0] = 0;
+    for (int i = 0; i < B.count; ++i) {
+      B.sys[i] = sys[c0 + i];
+      B.dof_begin[i + 1] = B.dof_begin[i] + B.sys[i].n_dofs;
+    }
+    const int64_t nd = B.dof_begin[B.count];
+    if (nd) batch_solution_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(B);
+    if (cudaGetLastError() != cudaSuccess) return FFG_CUDA_ERROR;
+  }
+  return FFG_OK;
+}
 
 int launch_cell_geometry(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                          const AssemblyInputs &in, double *geo, int stride, double *cell_rhs,

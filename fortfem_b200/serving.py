@@ -9,16 +9,20 @@ released least-recently-used when it does not, and keeps launching work while
 earlier work is still on the GPU:
 
 * small systems (at most ``small_rows`` free DoFs) are packed into batches that
-  solve one system per thread block in a single launch
-  (``ffg_problem_solve_batch`` with ``FFG_BATCH_CTA_PER_SYSTEM``); up to
-  ``streams`` such batches are in flight at once and overlap on the device;
+  are assembled together (one launch per phase) and solved one system per
+  thread block in a single launch (``ffg_problem_solve_batch`` with
+  ``FFG_BATCH_CTA_PER_SYSTEM``); up to ``streams`` such batches are in flight
+  at once and overlap on the device;
 * a large system runs on the whole GPU (``FFG_BATCH_WHOLE_DEVICE``), alone:
   its cooperative launch needs every SM, so it waits until the small batches
   in flight have drained, and no new batch starts until it is done.
 
-Requests are served first-come first-served: a small batch takes the small
-requests queued before the first waiting large one.  A request whose mesh size
-is already in flight waits for the next batch.
+Requests of one mesh size can share a batch and run in overlapping batches:
+the engine keeps a pool of problems per size (each with its own workspace)
+and grows it while memory allows.  Requests are served first come, first
+served, except that small requests may run ahead of a waiting large one for
+at most ``bypass_window`` seconds after the large one arrived; after that the
+large request stops admission until the device has drained and it has run.
 
 Each request carries only its seeds; its inputs (jittered vertices, lognormal
 cell coefficients, a Gaussian-random-field source) are synthesized on the
@@ -33,7 +37,7 @@ from __future__ import annotations
 
 import math
 import time
-from collections import deque
+from collections import Counter, deque
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
 
@@ -113,41 +117,51 @@ class Scheduler:
     small_rows: int = 32768
     max_batch: int = 48
     streams: int = 2
+    bypass_window: float = 0.05
     queue: deque = field(default_factory=deque)
     inflight: List[Batch] = field(default_factory=list)
 
     def is_small(self, r: Request) -> bool:
         return free_dofs(r.key) <= self.small_rows
 
-    def busy_keys(self):
-        return {r.key for b in self.inflight for r in b.requests}
+    def busy_counts(self) -> Counter:
+        return Counter(r.key for b in self.inflight for r in b.requests)
 
-    def next_batch(self, can_host) -> Optional[Batch]:
-        """The batch to launch now, or None.  `can_host(key)` says whether the
-        engine can provide a problem for that mesh size now."""
+    def _starved(self, r: Request, now) -> bool:
+        return now is None or now - r.arrival >= self.bypass_window
+
+    def next_batch(self, can_host, now: Optional[float] = None) -> Optional[Batch]:
+        """The batch to launch now, or None.  `can_host(key, count)` says
+        whether the engine can provide `count` problems of that mesh size at
+        once; `now` (seconds, the arrivals' clock) lets small requests pass a
+        large one that has waited less than bypass_window (without it the
+        queue is strictly first come, first served)."""
         if not self.queue:
             return None
         if any(b.mode == "whole_device" for b in self.inflight):
             return None
         head = self.queue[0]
-        busy = self.busy_keys()
         if not self.is_small(head):
-            if self.inflight or not can_host(head.key):
+            if not self.inflight and can_host(head.key, 1):
+                self.queue.popleft()
+                return Batch("whole_device", [head], 0)
+            if self._starved(head, now):
                 return None
-            self.queue.popleft()
-            return Batch("whole_device", [head], 0)
         used = {b.slot for b in self.inflight}
         free_slots = [s for s in range(self.streams) if s not in used]
         if not free_slots:
             return None
-        picked, keys = [], set()
+        busy = self.busy_counts()
+        picked, counts = [], Counter()
         for r in self.queue:
             if not self.is_small(r):
-                break
-            if r.key in busy or r.key in keys or not can_host(r.key):
+                if self._starved(r, now):
+                    break
+                continue
+            if not can_host(r.key, busy[r.key] + counts[r.key] + 1):
                 continue
             picked.append(r)
-            keys.add(r.key)
+            counts[r.key] += 1
             if len(picked) == self.max_batch:
                 break
         if not picked:
@@ -185,7 +199,7 @@ def serve(requests: List[Request], engine, scheduler: Optional[Scheduler] = None
                 sch.inflight.remove(b)
         launched = False
         while True:
-            b = sch.next_batch(engine.can_host)
+            b = sch.next_batch(engine.can_host, clock() - t0)
             if b is None:
                 break
             b.token = engine.launch(b)
@@ -241,7 +255,7 @@ class DeviceEngine:
 
     def __init__(self, device: int = 0, memory_fraction: float = 0.8, options=None,
                  keep_solutions: bool = False, features: int = 64, corr_length: float = 0.1,
-                 streams: int = 2):
+                 streams: int = 2, max_instances: int = 8):
         import torch
         from .api import SolverOptions
         self.torch = torch
@@ -249,10 +263,12 @@ class DeviceEngine:
         free, _ = torch.cuda.mem_get_info(self.device)
         self.budget = int(free * memory_fraction)
         self.used = 0
-        self.meshes: Dict[Tuple[str, int], _Mesh] = {}
+        # a pool of problems per mesh size; `idle` holds the ones not in flight
+        self.meshes: Dict[Tuple[str, int], List[_Mesh]] = {}
+        self.idle: Dict[Tuple[str, int], List[_Mesh]] = {}
         self.bytes: Dict[Tuple[str, int], int] = {}
         self.last_use: Dict[Tuple[str, int], float] = {}
-        self.inflight_keys: set = set()
+        self.max_instances = max_instances
         self.options = options or SolverOptions(method="pcg", preconditioner="jacobi",
                                                 tolerance=1e-10, precision="mixed",
                                                 max_iterations=1000000, timeout_seconds=10)
@@ -271,36 +287,45 @@ class DeviceEngine:
         m = _Mesh(key, self.device)
         torch.cuda.synchronize(self.device)
         after, _ = torch.cuda.mem_get_info(self.device)
-        self.meshes[key] = m
-        self.bytes[key] = max(before - after, 0)
-        self.used += self.bytes[key]
+        self.meshes.setdefault(key, []).append(m)
+        self.idle.setdefault(key, []).append(m)
+        b = max(before - after, 0)
+        self.bytes[key] = self.bytes.get(key, 0) + b
+        self.used += b
         self.setup_seconds += time.perf_counter() - t0
         return m
 
     def _estimate(self, key) -> int:
         # bytes per free DoF seen so far for this family (P2 about 2.5 KB, P1 about 0.4 KB)
-        same = [(k, b) for k, b in self.bytes.items() if k[0] == key[0] and b > 0]
+        same = [(k, b / len(self.meshes[k])) for k, b in self.bytes.items()
+                if k[0] == key[0] and b > 0 and self.meshes.get(k)]
         per = (sum(b for _, b in same) / sum(free_dofs(k) for k, _ in same)) if same else \
             (2500.0 if key[0] == "p2" else 400.0)
         return int(per * free_dofs(key)) + (64 << 20)
 
     def _evict_for(self, need: int) -> bool:
-        idle = sorted((k for k in self.meshes if k not in self.inflight_keys),
+        # whole pools of sizes with nothing in flight, least recently used first
+        idle = sorted((k for k, ms in self.meshes.items() if len(self.idle.get(k, [])) == len(ms)),
                       key=lambda k: self.last_use.get(k, 0.0))
         for k in idle:
             if self.used + need <= self.budget:
                 break
-            self.meshes.pop(k).problem.close()
+            for m in self.meshes.pop(k):
+                m.problem.close()
+            self.idle.pop(k, None)
             self.used -= self.bytes.pop(k)
         return self.used + need <= self.budget
 
-    def can_host(self, key) -> bool:
-        if key in self.meshes:
-            return True
-        need = self._estimate(key)
-        if self.used + need > self.budget and not self._evict_for(need):
+    def can_host(self, key, count: int = 1) -> bool:
+        """Whether `count` problems of this mesh size can be in flight at
+        once, creating pool members while memory allows."""
+        if count > self.max_instances:
             return False
-        self._create(key)
+        while len(self.meshes.get(key, [])) < count:
+            need = self._estimate(key)
+            if self.used + need > self.budget and not self._evict_for(need):
+                return False
+            self._create(key)
         return True
 
     def prepare(self, requests: List[Request]) -> float:
@@ -342,9 +367,8 @@ class DeviceEngine:
         torch = self.torch
         from .api import solve_batch
         s = self.streams[b.slot]
-        meshes = [self.meshes[r.key] for r in b.requests]
+        meshes = [self.idle[r.key].pop() for r in b.requests]
         for r in b.requests:
-            self.inflight_keys.add(r.key)
             self.last_use[r.key] = time.perf_counter()
         with torch.cuda.stream(s):
             ins = [self._inputs(m, r) for m, r in zip(meshes, b.requests)]
@@ -368,16 +392,18 @@ class DeviceEngine:
         out = []
         for m, h, r in zip(meshes, host, reqs):
             st = m.problem.batch_stats()
-            self.inflight_keys.discard(r.key)
+            self.idle[r.key].append(m)
             out.append(Result(r.rid, 0.0, bool(st.converged), st.iterations,
                               st.true_relative_residual, "", 0, h.numpy() if self.keep else None,
                               st.assembly_time + st.solve_time))
         return out
 
     def close(self):
-        for m in self.meshes.values():
-            m.problem.close()
+        for ms in self.meshes.values():
+            for m in ms:
+                m.problem.close()
         self.meshes.clear()
+        self.idle.clear()
 
 
 def run_requests(reqs: List[Request], small_rows: int = 32768, max_batch: int = 48,

@@ -36,23 +36,34 @@ def test_scheduler_batches_small_requests_fifo():
     sch = S.Scheduler(small_rows=1000, max_batch=3, streams=2)
     reqs = [S.Request(i, "p1", 10 + i, i) for i in range(5)]
     sch.queue.extend(reqs)
-    b = sch.next_batch(lambda k: True)
+    b = sch.next_batch(lambda k, n: True)
     assert b.mode == "cta_per_system" and [r.rid for r in b.requests] == [0, 1, 2]
     sch.inflight.append(b)
-    b2 = sch.next_batch(lambda k: True)
+    b2 = sch.next_batch(lambda k, n: True)
     assert [r.rid for r in b2.requests] == [3, 4] and b2.slot != b.slot
     sch.inflight.append(b2)
-    assert sch.next_batch(lambda k: True) is None        # both stream slots busy
+    assert sch.next_batch(lambda k, n: True) is None        # both stream slots busy
 
 
-def test_scheduler_same_mesh_size_never_shares_a_batch_or_overlaps():
+def test_scheduler_same_mesh_size_shares_batches_up_to_the_pool():
+    reqs = [S.Request(0, "p1", 10, 1), S.Request(1, "p1", 10, 2), S.Request(2, "p1", 11, 3),
+            S.Request(3, "p1", 10, 4)]
+    # a pool of one problem per size: one request of a size at a time
     sch = S.Scheduler(small_rows=1000, max_batch=8, streams=2)
-    sch.queue.extend([S.Request(0, "p1", 10, 1), S.Request(1, "p1", 10, 2),
-                      S.Request(2, "p1", 11, 3)])
-    b = sch.next_batch(lambda k: True)
+    sch.queue.extend(reqs)
+    b = sch.next_batch(lambda k, n: n <= 1)
     assert [r.rid for r in b.requests] == [0, 2]
     sch.inflight.append(b)
-    assert sch.next_batch(lambda k: True) is None        # size 10 still in flight
+    assert sch.next_batch(lambda k, n: n <= 1) is None   # size 10 still in flight
+    # a pool of two: two of size 10 in the first batch, the third in the next
+    sch = S.Scheduler(small_rows=1000, max_batch=8, streams=2)
+    sch.queue.extend(reqs)
+    b = sch.next_batch(lambda k, n: n <= 2)
+    assert [r.rid for r in b.requests] == [0, 1, 2]
+    sch.inflight.append(b)
+    assert sch.next_batch(lambda k, n: n <= 2) is None
+    sch.inflight.clear()
+    assert [r.rid for r in sch.next_batch(lambda k, n: n <= 2).requests] == [3]
 
 
 def test_scheduler_large_request_waits_for_drain_and_runs_alone():
@@ -61,21 +72,37 @@ def test_scheduler_large_request_waits_for_drain_and_runs_alone():
     large = S.Request(1, "p2", 20, 2)
     later = S.Request(2, "p1", 6, 3)
     sch.queue.extend([small, large, later])
-    b = sch.next_batch(lambda k: True)
+    b = sch.next_batch(lambda k, n: True)
     assert [r.rid for r in b.requests] == [0]            # stops at the first large request
     sch.inflight.append(b)
-    assert sch.next_batch(lambda k: True) is None        # the large one waits for the drain
+    assert sch.next_batch(lambda k, n: True) is None        # the large one waits for the drain
     sch.inflight.clear()
-    b = sch.next_batch(lambda k: True)
+    b = sch.next_batch(lambda k, n: True)
     assert b.mode == "whole_device" and [r.rid for r in b.requests] == [1]
     sch.inflight.append(b)
-    assert sch.next_batch(lambda k: True) is None        # nothing runs beside it
+    assert sch.next_batch(lambda k, n: True) is None        # nothing runs beside it
+
+
+def test_small_requests_pass_a_large_one_only_within_the_window():
+    sch = S.Scheduler(small_rows=100, max_batch=8, streams=2, bypass_window=0.05)
+    busy = S.Request(9, "p1", 4, 9, arrival=0.0)
+    large = S.Request(1, "p2", 20, 2, arrival=1.00)
+    small = S.Request(2, "p1", 6, 3, arrival=1.01)
+    sch.inflight.append(S.Batch("cta_per_system", [busy], 0))
+    sch.queue.extend([large, small])
+    b = sch.next_batch(lambda k, n: True, now=1.02)      # the large one waited 20 ms
+    assert b.mode == "cta_per_system" and [r.rid for r in b.requests] == [2]
+    sch.queue.append(S.Request(3, "p1", 7, 4, arrival=1.07))
+    assert sch.next_batch(lambda k, n: True, now=1.08) is None   # waited 80 ms: no more passing
+    sch.inflight.clear()
+    b = sch.next_batch(lambda k, n: True, now=1.09)
+    assert b.mode == "whole_device" and [r.rid for r in b.requests] == [1]
 
 
 def test_scheduler_skips_sizes_the_engine_cannot_host():
     sch = S.Scheduler(small_rows=1000, max_batch=8, streams=1)
     sch.queue.extend([S.Request(0, "p1", 10, 1), S.Request(1, "p1", 12, 2)])
-    b = sch.next_batch(lambda k: k[1] != 10)
+    b = sch.next_batch(lambda k, n: k[1] != 10)
     assert [r.rid for r in b.requests] == [1]
     assert [r.rid for r in sch.queue] == [0]
 
@@ -87,7 +114,7 @@ class FakeEngine:
         self.clock = clock
         self.launched = []
 
-    def can_host(self, key):
+    def can_host(self, key, count=1):
         return True
 
     def launch(self, b):
@@ -117,10 +144,8 @@ def test_serve_replays_every_request_once_with_latencies():
     assert all(r.latency > 0 for r in res)
     modes = {r.mode for r in res}
     assert modes <= {"cta_per_system", "whole_device"}
-    # whole-device batches hold one request; no batch repeats a mesh size
+    # whole-device batches hold one request and run with nothing beside them
     for b in eng.launched:
-        keys = [r.key for r in b.requests]
-        assert len(keys) == len(set(keys))
         if b.mode == "whole_device":
             assert len(b.requests) == 1
     stats = S.percentiles([r.latency for r in res])

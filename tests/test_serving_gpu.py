@@ -36,7 +36,7 @@ def test_batch_matches_alone_and_the_cooperative_path():
         assert np.array_equal(alone.solution, m.solution)
         whole = _run(eng, "whole_device", [r])[0]
         assert whole.converged and whole.true_relative_residual <= 1e-10
-        mesh = eng.meshes[r.key]
+        mesh = eng.meshes[r.key][0]
         v, kappa, src = eng._inputs(mesh, r)
         ref = torch.empty(mesh.problem.n_dofs, dtype=torch.float64, device=eng.device)
         st = mesh.problem.solve_device(v, ref, 1.0, 0.0, kappa, None, src, None, eng.options)
@@ -55,7 +55,7 @@ def test_one_block_system_with_more_than_32_slices_per_warp():
     eng = S.DeviceEngine(keep_solutions=True)
     r = S.Request(0, "p2", 18, 211)
     assert eng.can_host(r.key)
-    mesh = eng.meshes[r.key]
+    mesh = eng.meshes[r.key][0]
     assert mesh.problem.n_free > 32 * 32 * 32
     one = _run(eng, "cta_per_system", [r])[0]
     assert one.converged and one.true_relative_residual <= 1e-10
@@ -84,4 +84,25 @@ def test_serving_stream_results_same_alone_and_in_the_mix():
         mode = "cta_per_system" if sch.is_small(r) else "whole_device"
         alone = _run(eng, mode, [r])[0]
         assert np.array_equal(alone.solution, got.solution)
+    eng.close()
+
+
+def test_same_size_requests_share_a_batch_and_overlap():
+    """Three requests of one mesh size in one batch (three pool members), and
+    a fourth in a batch on the other stream while the first is in flight:
+    every result is the bits it gets alone."""
+    eng = S.DeviceEngine(keep_solutions=True)
+    reqs = [S.Request(i, "p2", 6, 300 + i) for i in range(3)] + [S.Request(3, "p1", 30, 400)]
+    assert eng.can_host(("p2", 6), 4) and eng.can_host(("p1", 30), 1)
+    assert len(eng.meshes[("p2", 6)]) == 4
+    t1 = eng.launch(S.Batch("cta_per_system", reqs[:3], 0))
+    t2 = eng.launch(S.Batch("cta_per_system", [reqs[3], S.Request(4, "p2", 6, 500)], 1))
+    torch.cuda.synchronize()
+    got = eng.collect(t1) + eng.collect(t2)
+    assert all(g.converged and g.true_relative_residual <= 1e-10 for g in got)
+    for r, g in zip(reqs + [S.Request(4, "p2", 6, 500)], got):
+        alone = _run(eng, "cta_per_system", [r])[0]
+        assert np.array_equal(alone.solution, g.solution)
+    # different seeds on one mesh size give different systems
+    assert not np.array_equal(got[0].solution, got[1].solution)
     eng.close()
