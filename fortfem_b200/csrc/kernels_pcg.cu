@@ -31,10 +31,10 @@
 // ends when ||b - A x||_2 <= tol*||b||_2.  A replacement is also forced when
 // the FP32 residual grows tenfold past the last true residual (the search
 // direction then restarts) or plateaus for four times the previous
-// replacement interval.  If replacements stop reducing the true residual, or
-// the FP32 p^T A p is not positive (condition number beyond FP32 reach, as
-// for curl-curl operators with a small mass term), the solve continues in the
-// FP64 loop from the current x.
+// replacement interval.  If replacements stop reducing the true residual the
+// solve continues in the FP64 loop from the current x; if the FP32 p^T A p is
+// not positive (condition number beyond FP32 reach, as for curl-curl
+// operators with a small mass term) the FP64 loop starts again from x = 0.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -548,6 +548,7 @@ __device__ __forceinline__ bool is_finite_d(double x) { return isfinite(x); }
 
 struct Outcome {
   int iterations = 0, updates = 0, converged = 0, status = FFG_OK, stagnated = 0, aborted = 0;
+  int restart = 0;  // the FP32 phase broke down: the FP64 loop starts again from x = 0
   double true_res = 0.0, final_res = 0.0, bnorm = 0.0;
 };
 
@@ -892,9 +893,12 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     const double pAp = red[0];
     if (!(pAp > 0.0 && is_finite_d(pAp))) {
       // an FP32 p^T A p that is not positive (cancellation on a near-null
-      // direction of the operator) ends the FP32 phase before x is touched;
-      // the FP64 loop continues from the current x
+      // direction of the operator) ends the FP32 phase: the operator is
+      // beyond FP32's reach, so the FP64 loop starts again from x = 0 (an x
+      // built by FP32 steps on such an operator carries near-null error
+      // components that FP64 CG reduces far more slowly than from zero)
       o.stagnated = 1;
+      o.restart = 1;
       break;
     }
     const double alpha = rz / pAp;
@@ -1055,7 +1059,11 @@ __device__ __forceinline__ void pcg_body(const PcgParams &P) {
   } else {
     cg_mixed(P, phase, t_start, o, tm);
     if (!o.aborted && o.stagnated && !o.converged && o.status == FFG_OK) {
-      continued = 1;
+      continued = o.restart ? 2 : 1;
+      if (o.restart) {
+        for_rows_even(P, [&](int row) { P.x[row] = 0.0; });
+        if (!grid_barrier(P, phase)) return;
+      }
       cg64(P, phase, t_start, true, o, tm);
     }
   }

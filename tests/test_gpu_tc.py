@@ -76,13 +76,17 @@ def test_tf32x3_many_cell_groups_match_fp64_path(k):
 
 
 # test/test_tetra_nedelec_sparse_assembly_slow.f90:31-85: the constant field
-# (1, 2, -1) has energy 3 on the two-cell mesh at every order (mass 1, curl 0)
+# (1, 2, -1) has energy 3 on the two-cell mesh at every order (mass 1, curl 0).
+# The energy is what is left of |x|^T |A| |x| (3.0e4 at order 3, 1.2e6 at
+# order 4) after cancellation, so the 3xTF32 matrix (about 2^-22 relative per
+# entry) reproduces it to 2^-22 |x|^T |A| |x|, checked here with twice that.
 @pytest.mark.parametrize("k", [3, 4])
 def test_tf32x3_constant_field_energy(k):
     verts = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [0, 0, -1.0]])
     tets = np.array([[0, 1, 2, 3], [0, 2, 1, 4]], dtype=np.int32)
     field = np.array([1.0, 2.0, -1.0])
     with ff.Problem(K.FFG_TETRA_NEDELEC, k, tets, len(verts), boundary="none") as prob:
+        R64, _, _ = _reduced(prob, verts, None, None, None, "fp64")
         R, _, free = _reduced(prob, verts, None, None, None, "tf32x3")
     # interpolate the constant field: the L2 projection solve is exact for it
     n, cp, ri, val = oracle.nedelec_csc(verts, tets, k, 0.0, 1.0)
@@ -96,7 +100,12 @@ def test_tf32x3_constant_field_energy(k):
     # R is the full system here (no constraint), curl 1.3 and mass 0.7: the
     # constant field has no curl and |f|^2 vol = 6 * (2 / 6) = 2
     energy = dofs @ ff.spmv(A, dofs)
-    assert abs(energy - 0.7 * 2.0) <= 1e-6 * 1.4
+    A64 = sp.csc_matrix((np.abs(R64.val), R64.row_idx, R64.col_ptr), shape=(R.nrow, R.nrow))
+    bound = 2.0 * 2.0 ** -22 * (np.abs(dofs) @ (A64 @ np.abs(dofs)))
+    print(f"order {k}: energy error {abs(energy - 1.4):.2e}, bound {bound:.2e}")
+    assert abs(energy - 0.7 * 2.0) <= bound
+    energy64 = dofs @ ff.spmv(ff.CscMatrix(R.nrow, R.nrow, R64.col_ptr, R64.row_idx, R64.val), dofs)
+    assert abs(energy64 - 1.4) <= 1e-8 * 1.4
 
 
 def test_tf32x3_selection_rules():
