@@ -66,6 +66,8 @@ def parse(argv=None):
     ap.add_argument("--order", type=int, default=1, help="Nedelec order of the c3 workload")
     ap.add_argument("--size", type=int, default=0, help="mesh size (0: the workload's own)")
     ap.add_argument("--assembly", default="fp64", choices=["fp64", "tf32x3"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed16"],
+                    help="inner SpMV operator of the mixed solve: FP32 or row-scaled FP16")
     ap.add_argument("--autotune", action="store_true", help="autotune launch shapes in setup")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
@@ -341,13 +343,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def pcg_bytes(stats, nnz, nf, fp64_continuation):
+def pcg_bytes(stats, nnz, nf, fp64_continuation, half=False):
     """Algorithmic bytes of one pcg_kernel launch: per FP32 inner iteration the
     FP32 SpMV with a 4-byte index plus eight FP32 vector streams (8 nnz + 44 n
-    + 4), per FP64 iteration or residual replacement the FP64 SpMV plus FP64
-    vectors (12 nnz + 4 (n + 1) + 32 n).  A solve that continued in FP64 is
-    counted at the FP64 rate for all its iterations (an upper bound)."""
-    inner = 8 * nnz + 44 * nf + 4
+    + 4; with the FP16 operator 6 nnz + 48 n + 4, the row scales included),
+    per FP64 iteration or residual replacement the FP64 SpMV plus FP64 vectors
+    (12 nnz + 4 (n + 1) + 32 n).  A solve that continued in FP64 is counted at
+    the FP64 rate for all its iterations (an upper bound)."""
+    inner = (6 * nnz + 48 * nf + 4) if half else (8 * nnz + 44 * nf + 4)
     outer = 12 * nnz + 4 * (nf + 1) + 32 * nf
     it = float(np.mean([s.iterations for s in stats]))
     ref = float(np.mean([s.refinements for s in stats]))
@@ -391,7 +394,7 @@ def run_ours(args):
     out_d = torch.zeros(prob.n_dofs, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
     mixed = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=TOL,
-                             precision="mixed", max_iterations=args.max_iterations,
+                             precision=args.precision, max_iterations=args.max_iterations,
                              timeout_seconds=args.timeout)
 
     def step(opts=mixed):
@@ -437,12 +440,12 @@ def run_ours(args):
 
     # roofline of the persistent PCG kernel (algorithmic bytes / kernel time)
     nnz, nf = prob.nnz, prob.n_free
-    alg = pcg_bytes(stats, nnz, nf, phases["fp64_continuation"])
+    alg = pcg_bytes(stats, nnz, nf, phases["fp64_continuation"], args.precision == "mixed16")
     kt = float(np.mean([s.solve_time for s in stats]))
     peak, peak_kind = measured_peaks()
     achieved = alg / kt / 1e9
     traffic = None
-    if work.kind == "c2" and (args.size or 48) == 48:
+    if work.kind == "c2" and (args.size or 48) == 48 and args.precision == "mixed":
         traffic = PCG_TRAFFIC_BYTES * alg / PCG_TRAFFIC_ALG_BYTES
     roofline = {"kernel": "pcg_kernel (persistent mixed Jacobi-PCG)", "bound": "hbm",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -459,7 +462,9 @@ def run_ours(args):
             "config": {"workload": work.name, "cells": prob.n_cells, "n_dofs": prob.n_dofs,
                        "n_free": nf, "nnz_constrained": nnz, **work.desc,
                        "assembly": args.assembly,
-                       "solver": "mixed: FP32 Jacobi-PCG inner, FP64 iterative refinement",
+                       "solver": ("mixed: FP32 Jacobi-PCG inner" +
+                                  (" on a row-scaled FP16 operator" if args.precision == "mixed16"
+                                   else "") + ", FP64 iterative refinement"),
                        "tolerance": TOL, "parallelism": f"replicas x{world}",
                        "l2": ("inputs larger than L2" if nnz * 12 > 126e6 else
                               "operator smaller than L2 (resident between steps)")},

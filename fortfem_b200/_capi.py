@@ -38,6 +38,7 @@ FFG_ASSEMBLY_FP64 = 0
 FFG_ASSEMBLY_TF32X3 = 1
 FFG_PRECISION_FP64 = 0
 FFG_PRECISION_MIXED = 1
+FFG_PRECISION_MIXED16 = 2
 FFG_OPTIONS_VERSION = 1
 FFG_NOALLOC_MAX_ROWS = 65536
 FFG_BATCH_CTA_PER_SYSTEM = 0

@@ -63,7 +63,7 @@ class SolverOptions:
     preconditioner: str = "none"
     tolerance_type: str = "relative"
     verbosity: int = 0
-    precision: str = "fp64"          # "fp64" (reference semantics) or "mixed"
+    precision: str = "fp64"          # "fp64" (reference semantics), "mixed" or "mixed16"
     inner_tolerance: float = 0.1      # mixed: reliable-update threshold
     max_refinements: int = 1000       # mixed: cap on reliable updates
     timeout_seconds: float = 60.0
@@ -75,7 +75,11 @@ class SolverOptions:
         o = K.SolverOptionsC()
         o.version = K.FFG_OPTIONS_VERSION
         o.preconditioner = 1 if (self.preconditioner == "jacobi" and self.method != "cg") else 0
-        o.precision = K.FFG_PRECISION_MIXED if self.precision == "mixed" else K.FFG_PRECISION_FP64
+        modes = {"fp64": K.FFG_PRECISION_FP64, "mixed": K.FFG_PRECISION_MIXED,
+                 "mixed16": K.FFG_PRECISION_MIXED16}
+        if self.precision not in modes:
+            raise FortfemError(K.FFG_INVALID_INPUT, f"precision {self.precision!r}")
+        o.precision = modes[self.precision]
         o.tolerance_type = 1 if self.tolerance_type == "absolute" else 0
         o.tolerance = float(self.tolerance)
         o.max_iterations = int(self.max_iterations)

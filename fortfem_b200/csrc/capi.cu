@@ -338,7 +338,8 @@ int check_options(const ffg_solver_options *o, ffg_solver_options &out) {
   if (!o) return FFG_OK;
   if (o->version != FFG_OPTIONS_VERSION) return FFG_INVALID_INPUT;
   out = *o;
-  if (out.precision != FFG_PRECISION_FP64 && out.precision != FFG_PRECISION_MIXED)
+  if (out.precision != FFG_PRECISION_FP64 && out.precision != FFG_PRECISION_MIXED &&
+      out.precision != FFG_PRECISION_MIXED16)
     return FFG_INVALID_INPUT;
   if (out.tolerance < 0 || out.max_iterations < 0) return FFG_INVALID_INPUT;
   if (out.inner_tolerance <= 0 || out.inner_tolerance >= 1) out.inner_tolerance = 0.1;
@@ -1178,7 +1179,8 @@ void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
   }
   cudaMemsetAsync(P->x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
   if (t.n_free() > 0) {
-    st = pcg_solve(P->S, P->rhs, P->x, o, P->work, &local, s, msg);
+    if (o.precision == FFG_PRECISION_MIXED16) st = sell_half(P->S, s);
+    if (!st) st = pcg_solve(P->S, P->rhs, P->x, o, P->work, &local, s, msg);
     if (st) { report(o.verbosity, msg); *status = st; if (stats) { local.status = st; *stats = local; } return; }
   } else {
     local.converged = 1;
@@ -1328,7 +1330,11 @@ void ffg_problem_solve_batch(int count, const int *handles, const double *const 
         x.push_back(P->x);
         w.push_back(&P->work);
       }
-    if (mode == FFG_BATCH_CTA_PER_SYSTEM) {
+    if (o.precision == FFG_PRECISION_MIXED16)
+      for (auto &P : probs)
+        if (!st && P->topo.n_free() > 0) st = sell_half(P->S, s);
+    if (st) {
+    } else if (mode == FFG_BATCH_CTA_PER_SYSTEM) {
       if (!A.empty())
         st = pcg_launch_batch((int)A.size(), A.data(), b.data(), x.data(), o, w.data(), s, msg);
     } else {
@@ -1857,7 +1863,8 @@ void ffg_solve_sparse(int n, int64_t nnz, const int64_t *col_ptr, const int *row
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, 0);
-    st = pcg_solve(S, db, dx, o, w, &local, 0, msg);
+    if (o.precision == FFG_PRECISION_MIXED16) st = sell_half(S, 0);
+    if (!st) st = pcg_solve(S, db, dx, o, w, &local, 0, msg);
     cudaEventRecord(e1, 0);
     cudaEventSynchronize(e1);
     float ms = 0;

@@ -135,6 +135,8 @@ struct DeviceSell {
   int *col = nullptr;
   double *val64 = nullptr;  // padded entries, zero in the padding
   float *val32 = nullptr;
+  uint16_t *val16 = nullptr;  // FP16 bits of val32 / rscale (FFG_PRECISION_MIXED16, on demand)
+  float *rscale = nullptr;    // per-row scale of val16: the row's largest |entry|
   double *dinv64 = nullptr;  // Jacobi inverse diagonal, new numbering
   float *dinv32 = nullptr;
   int *perm = nullptr, *iperm = nullptr;
@@ -154,6 +156,8 @@ void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector
 // Re-deal an uploaded operator's slices to CTAs and warps with another slice cost.
 int sell_repartition(DeviceSell &d, int slice_cost);
 void free_sell(DeviceSell &d);
+// The FP16 copy of an operator's FP32 values, row-scaled (allocated on first use).
+int sell_half(DeviceSell &d, cudaStream_t s);
 
 struct SolveWork {
   double *r64 = nullptr, *partial = nullptr;

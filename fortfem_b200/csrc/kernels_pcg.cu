@@ -35,6 +35,7 @@
 // solve continues in the FP64 loop from the current x; if the FP32 p^T A p is
 // not positive (condition number beyond FP32 reach, as for curl-curl
 // operators with a small mass term) the FP64 loop starts again from x = 0.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -71,6 +72,8 @@ struct PcgParams {
   const int16_t *dcol;
   const int *col;
   const float *v32;
+  const __half *v16;  // FFG_PRECISION_MIXED16: FP16 operator, row r scaled by rs[r]
+  const float *rs;
   const double *v64;
   const float *d32;
   const double *d64;
@@ -610,6 +613,32 @@ struct ZGather {
   }
 };
 
+// The same two gathers on the FP16 operator: entries are FP16 bits of
+// a_ij / s_i, so the row's sum is scaled by s_i before it is used.
+struct ZGatherH {
+  ZGather g;
+  const float *__restrict__ rs;
+  using Acc = float;
+  __device__ __forceinline__ void accumulate(Acc &acc, __half v, int c) const {
+    acc += __half2float(v) * g.z[c];
+  }
+  __device__ __forceinline__ double finish(int row, float acc) const {
+    return g.finish(row, acc * rs[row]);
+  }
+};
+
+struct PairGatherH {
+  PairGather<float, float2> g;
+  const float *__restrict__ rs;
+  using Acc = float;
+  __device__ __forceinline__ void accumulate(Acc &acc, __half v, int c) const {
+    acc += __half2float(v) * g.column(c);
+  }
+  __device__ __forceinline__ double finish(int row, float acc) const {
+    return g.finish(row, acc * rs[row]);
+  }
+};
+
 // r64 = b - A x with the FP64 operator, returning the row's term of (r64, r64);
 // with p given, also q = A p (FP64 products, stored in FP32) in the same pass.
 struct ResidualGather {
@@ -881,8 +910,12 @@ __device__ __noinline__ void cg_mixed(const PcgParams &P, unsigned int &phase,
     part[0] = 0.0;
     const float bt = (float)beta;
     float2 *zn = zp[cur ^ 1];
-    part[0] = direct ? spmv(P, P.v32, PairGather<float, float2>{zp[cur], zn, q, bt})
-                     : spmv(P, P.v32, ZGather{z, p, q, bt});
+    if (P.v16)
+      part[0] = direct ? spmv(P, P.v16, PairGatherH{{zp[cur], zn, q, bt}, P.rs})
+                       : spmv(P, P.v16, ZGatherH{{z, p, q, bt}, P.rs});
+    else
+      part[0] = direct ? spmv(P, P.v32, PairGather<float, float2>{zp[cur], zn, q, bt})
+                       : spmv(P, P.v32, ZGather{z, p, q, bt});
     write_partials(P, phase, part, 1);
     t1 = stamp(P);
     if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -1265,6 +1298,59 @@ void sell_partition(const int64_t *soff, int64_t n_slices, int grid, std::vector
   woff[(size_t)grid * kWarps] = (int)wslice.size();
 }
 
+namespace {
+// val16 = FP16(val32 / s_r) with s_r the row's largest |val32| (1 for an
+// empty row); one thread per row walks the row's entries in its slice.
+__global__ void sell_half_kernel(int64_t n, const int64_t *__restrict__ soff,
+                                 const float *__restrict__ v32, __half *__restrict__ v16,
+                                 float *__restrict__ rs) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t s = r / kSliceRows, e0 = soff[s] + r % kSliceRows;
+  const int width = (int)((soff[s + 1] - soff[s]) / kSliceRows);
+  float m = 0.f;
+  for (int k = 0; k < width; ++k) m = fmaxf(m, fabsf(v32[e0 + (int64_t)k * kSliceRows]));
+  const float sc = m > 0.f ? m : 1.f;
+  const float inv = 1.f / sc;
+  for (int k = 0; k < width; ++k) {
+    const int64_t e = e0 + (int64_t)k * kSliceRows;
+    v16[e] = __float2half_rn(v32[e] * inv);
+  }
+  rs[r] = sc;
+}
+
+// padding rows of the last slice: zero values, unit scale
+__global__ void sell_half_pad_kernel(int64_t n, int64_t n_slices, const int64_t *__restrict__ soff,
+                                     __half *__restrict__ v16) {
+  const int64_t r = n + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_slices * kSliceRows) return;
+  const int64_t s = r / kSliceRows, e0 = soff[s] + r % kSliceRows;
+  const int width = (int)((soff[s + 1] - soff[s]) / kSliceRows);
+  for (int k = 0; k < width; ++k) v16[e0 + (int64_t)k * kSliceRows] = __float2half_rn(0.f);
+}
+}  // namespace
+
+int sell_half(DeviceSell &d, cudaStream_t s) {
+  if (d.n <= 0) return FFG_OK;
+  const size_t P = (size_t)std::max<int64_t>(d.padded, 1);
+  if (!d.val16 && cudaMalloc((void **)&d.val16, sizeof(uint16_t) * P) != cudaSuccess) {
+    cudaGetLastError();
+    return FFG_OUT_OF_MEMORY;
+  }
+  if (!d.rscale && cudaMalloc((void **)&d.rscale, sizeof(float) * (size_t)d.n) != cudaSuccess) {
+    cudaGetLastError();
+    return FFG_OUT_OF_MEMORY;
+  }
+  __half *v16 = reinterpret_cast<__half *>(d.val16);
+  sell_half_kernel<<<(unsigned)((d.n + 255) / 256), 256, 0, s>>>(d.n, d.soff, d.val32, v16,
+                                                                  d.rscale);
+  const int64_t pad = d.n_slices * kSliceRows - d.n;
+  if (pad > 0)
+    sell_half_pad_kernel<<<(unsigned)((pad + 255) / 256), 256, 0, s>>>(d.n, d.n_slices, d.soff,
+                                                                      v16);
+  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+}
+
 int sell_repartition(DeviceSell &d, int slice_cost) {
   if (d.grid <= 0 || !d.soff || !d.cta_slice || !d.woff) return FFG_INVALID_INPUT;
   std::vector<int64_t> soff((size_t)d.n_slices + 1);
@@ -1284,7 +1370,8 @@ int sell_repartition(DeviceSell &d, int slice_cost) {
 }
 
 void free_sell(DeviceSell &d) {
-  void *ptrs[] = {d.soff, d.dcol, d.col, d.val64, d.val32, d.dinv64, d.dinv32, d.perm, d.iperm,
+  void *ptrs[] = {d.soff, d.dcol, d.col, d.val64, d.val32, d.val16, d.rscale, d.dinv64, d.dinv32,
+                  d.perm, d.iperm,
                   d.cta_slice, d.wslice, d.woff};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1353,6 +1440,9 @@ PcgParams make_params(const DeviceSell &A, const double *b, double *x,
   P.dcol = A.dcol;
   P.col = A.col;
   P.v32 = A.val32;
+  P.v16 = opts.precision == FFG_PRECISION_MIXED16 ? reinterpret_cast<const __half *>(A.val16)
+                                                  : nullptr;
+  P.rs = A.rscale;
   P.v64 = A.val64;
   P.d32 = A.dinv32;
   P.d64 = A.dinv64;

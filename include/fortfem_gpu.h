@@ -67,6 +67,11 @@ extern "C" {
 #define FFG_PRECISION_FP64 0  /* FP64 Jacobi-PCG with the reference's stopping rule */
 #define FFG_PRECISION_MIXED 1 /* FP32 PCG recurrences, FP64 solution and reliable
                                  FP64 residual updates (defect correction) */
+#define FFG_PRECISION_MIXED16 2 /* as FFG_PRECISION_MIXED with the inner SpMV's operator
+                                 * stored in FP16, each row scaled by its largest entry
+                                 * (4 bytes an entry with the 16-bit column offset
+                                 * instead of 6); the residual replacements still use
+                                 * the FP64 operator, so the stopping rule is unchanged */
 
 #define FFG_OPTIONS_VERSION 1
 
@@ -74,7 +79,7 @@ extern "C" {
 typedef struct {
   int version;           /* FFG_OPTIONS_VERSION */
   int preconditioner;    /* 0 = "none", 1 = "jacobi" */
-  int precision;         /* FFG_PRECISION_FP64 or FFG_PRECISION_MIXED */
+  int precision;         /* FFG_PRECISION_FP64, _MIXED or _MIXED16 */
   int tolerance_type;    /* 0 = "relative", 1 = "absolute" */
   double tolerance;      /* FP64 mode: on the recursive residual as the reference;
                             mixed mode: on the true FP64 residual ||b-Ax|| (relative to ||b||) */

@@ -357,3 +357,36 @@ def test_wall_limit_reports_timeout():
         opts.tolerance = 1e-10
         sol, stats = prob.solve(v, 1.0, 0.0, None, None, src, None, opts)
         assert stats.converged
+
+
+@pytest.mark.parametrize("family,degree", [(K.FFG_TETRA_LAGRANGE, 2), (K.FFG_TRIANGLE_P1, 1),
+                                           (K.FFG_TETRA_NEDELEC, 2)])
+def test_mixed16_operator_reaches_the_same_true_residual(family, degree):
+    """The inner SpMV on the row-scaled FP16 operator: the reliable updates
+    use the FP64 operator, so the solve still stops at a true relative
+    residual of 1e-10 and agrees with the FP32-operator solve to the
+    residual-derived bound."""
+    if family == K.FFG_TRIANGLE_P1:
+        v, t = oracle.unit_square_mesh(49)
+        v = synth.jitter_interior_2d(v, 1 / 48, 0.1, 2)
+    else:
+        v, t = jittered_box(6 if family == K.FFG_TETRA_LAGRANGE else 4, 0.1, 2)
+    kappa = np.exp(np.random.default_rng(2).standard_normal(len(t)))
+    with ff.Problem(family, degree, t, len(v)) as prob:
+        pts = prob.sample_points(v)
+        if family == K.FFG_TETRA_NEDELEC:
+            src = synth.trig_vector_source(3)(pts)
+            cb = 20.0
+        else:
+            src = np.sin(np.pi * pts[..., 0]) + pts[..., 1]
+            cb = 0.0
+        sols = {}
+        for prec in ("mixed", "mixed16"):
+            opts = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
+                                    precision=prec, max_iterations=100000)
+            sols[prec] = prob.solve(v, 1.0, cb, kappa, None, src, None, opts)
+    for prec, (x, st) in sols.items():
+        assert st.converged and st.true_relative_residual <= 1e-10, (prec, st)
+    x32, x16 = sols["mixed"][0], sols["mixed16"][0]
+    assert np.abs(x16 - x32).max() <= 1e-6 * np.abs(x32).max()
+    print(f"mixed {sols['mixed'][1].iterations} it, mixed16 {sols['mixed16'][1].iterations} it")
