@@ -714,6 +714,9 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
   const double target = P.relative ? P.tol * (continuation ? bnorm : rnorm) : P.tol;
   double true_res = rnorm, last_true = rnorm;
   int stall = 0;
+  // continuation: restarted cycles; a cycle ends when the recursive residual
+  // reaches the target or after twice the first cycle's iterations
+  int cycle_its = 0, first_cycle = 0;
   int converged = (rnorm <= target) ? 1 : 0;
   double rz = 0.0;
   if (!converged) {
@@ -791,10 +794,18 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
     true_res = est;
     if (red[2] != 0.0) { o.status = FFG_TIMEOUT; break; }
     if (est <= target && !continuation) { converged = 1; break; }
-    if (est <= target) {
+    ++cycle_its;
+    bool restart = false;
+    if (continuation &&
+        (est <= target || (first_cycle > 0 && cycle_its >= 2 * first_cycle))) {
       // the continuation's target is the true residual: check b - A x and,
-      // while it still falls, replace the recursive residual with it
+      // while it still falls, start a new CG cycle from it (the recursive
+      // residual of a long FP64 run drifts from the true one, and a cycle
+      // whose recursive residual cannot reach the target is cut off)
       t0 = stamp(P);
+      if (first_cycle == 0) first_cycle = cycle_its;
+      cycle_its = 0;
+      restart = true;
       part[0] = residual(P);
       write_partials(P, phase, part, 1);
       if (!grid_barrier(P, phase)) { o.aborted = 1; return; }
@@ -821,7 +832,7 @@ __device__ __noinline__ void cg64(const PcgParams &P, unsigned int &phase,
       tm.u += stamp(P) - t0;
       rz_new = red[0];
     }
-    beta = rz != 0.0 ? rz_new / rz : 0.0;
+    beta = (rz != 0.0 && !restart) ? rz_new / rz : 0.0;
     rz = rz_new;
     cur ^= 1;
   }

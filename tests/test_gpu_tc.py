@@ -118,6 +118,11 @@ def test_tf32x3_selection_rules():
             prob.set_assembly_precision("fp64")
 
 
+# The solution of a 3xTF32-assembled system differs from the FP64-assembled
+# one by up to cond(A) times the matrix perturbation (about 1e-7): on a
+# mass-dominated system (mass 50) that is below 1e-5; on the curl-dominated
+# unit-mass systems it grows with their condition number (6e-3 measured on
+# 4^3 x 6 at order 3 with mass 1).
 @pytest.mark.parametrize("k", [3, 4])
 def test_tf32x3_solve_matches_fp64_assembled_solve(k):
     v, t = oracle.box_mesh([4, 4, 4])
@@ -129,10 +134,10 @@ def test_tf32x3_solve_matches_fp64_assembled_solve(k):
         opts = ff.SolverOptions(method="pcg", preconditioner="jacobi", tolerance=1e-10,
                                 precision="mixed", max_iterations=200000)
         prob.set_assembly_precision("tf32x3")
-        x3, s3 = prob.solve(v, 1.0, 1.0, mu, None, src, None, opts)
+        x3, s3 = prob.solve(v, 1.0, 50.0, mu, None, src, None, opts)
         prob.set_assembly_precision("fp64")
-        x64, s64 = prob.solve(v, 1.0, 1.0, mu, None, src, None, opts)
+        x64, s64 = prob.solve(v, 1.0, 50.0, mu, None, src, None, opts)
     assert s3.converged and s64.converged
     err = np.linalg.norm(x3 - x64) / np.linalg.norm(x64)
     print(f"order {k}: 3xTF32-assembled solution vs FP64-assembled {err:.2e}")
-    assert err <= 1e-4
+    assert err <= 1e-5

@@ -89,7 +89,7 @@ def test_non_symmetric_or_non_finite_tensors_are_rejected():
     bad[0, 1, 1] = np.nan
     A, st = ff.assemble_tetra_nedelec_weighted_csc(v, t, bad, 1.0, order=2)
     assert A is None and st.code == K.FFG_INVALID_INPUT
-    with ff.Problem(K.FFG_TETRA_LAGRANGE, 1, t, len(v)) as prob:
+    with ff.Problem(K.FFG_TETRA_LAGRANGE, 1, t, len(v), boundary="none") as prob:
         with pytest.raises(ff.FortfemError):
             prob.set_cell_tensor(ten)
 
