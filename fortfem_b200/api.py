@@ -817,7 +817,7 @@ class Problem:
             raise FortfemError(st.value, "ffg_problem_set_tuning")
 
     def set_assembly_precision(self, precision: str):
-        """Nedelec orders 3-4: "fp64" (CUDA-core FP64 contraction, the parity
+        """Nedelec orders 3-6: "fp64" (CUDA-core FP64 contraction, the parity
         path) or "tf32x3" (tensor-core 3xTF32 contraction, FP32 accumulation)
         for every following assembly (ffg_problem_set_assembly_precision)."""
         modes = {"fp64": K.FFG_ASSEMBLY_FP64, "tf32x3": K.FFG_ASSEMBLY_TF32X3}

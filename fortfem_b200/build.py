@@ -26,7 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3",
 SOURCES = ["topology.cpp", "basis.cpp", "kernels_assemble.cu", "kernels_pcg.cu", "capi.cu",
            "noalloc.cu", "topology_gpu.cu", "kernels_ad.cu",
            "kernels_probe.cu", "kernels_pml.cu",
-           "kernels_dist.cu", "kernels_weighted.cu", "kernels_tc.cu"]
+           "kernels_dist.cu", "kernels_weighted.cu", "kernels_tc.cu", "kernels_oriented.cu"]
 
 
 def _headers():

@@ -82,6 +82,7 @@ struct Problem {
   // Nedelec element contraction: FP64 CUDA cores or 3xTF32 tensor cores
   int assembly_precision = FFG_ASSEMBLY_FP64;
   TcPlan tc;
+  OrientedTables ort;  // Nedelec: oriented tensors by vertex-order class (dt.ort)
   LaunchTuning tune;  // launch shapes (autotuned or defaults)
   int *err = nullptr;
   int *err_host = nullptr;   // pinned: degenerate-cell flag of a deferred check
@@ -100,6 +101,7 @@ struct Problem {
       if (p) cudaFree(p);
     free_sell(S);
     tc_free_plan(tc);
+    ort_free(ort);
     solve_work_free(work);
     if (err_host) cudaFreeHost(err_host);
     for (auto &e : ev)
@@ -206,6 +208,10 @@ int create_problem(int family, int degree, int n_vertices, int n_cells, const in
   if (!P->tab.face_blocks.empty() && (st = upload(&dt.face_blocks, P->tab.face_blocks))) return st;
   if (!P->tab.ref.empty() && (st = upload(&dt.ref, P->tab.ref))) return st;
   if (!P->tab.load_basis.empty() && (st = upload(&dt.load_basis, P->tab.load_basis))) return st;
+  if (family == FFG_TETRA_NEDELEC) {
+    if ((st = ort_build(t, P->tab, P->ort))) return st;
+    dt.ort = &P->ort;
+  }
   const int64_t nfree = t.n_free();
   // per-step buffers
   const size_t nc = (size_t)n_cells;
@@ -287,7 +293,7 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
     }
     if (P.assembly_precision == FFG_ASSEMBLY_TF32X3) {
       // matrices on the tensor cores (FP32, leading dimension tc.ld), loads in FP64
-      if (!P.tc.tile_n && (st = tc_build_plan(t.degree, P.tab, P.tc))) return st;
+      if (!P.tc.bimage && (st = tc_build_plan(t, P.ort, P.tc, s))) return st;
       if (in.samples) {
         st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s, true);
       } else {
@@ -300,7 +306,7 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
       float *e32 = reinterpret_cast<float *>(P.elem);
       st = launch_nedelec_tc(t, P.dt, in, P.tc, e32, P.err, s);
       elem32 = e32;
-      ld32 = P.tc.ld;
+      ld32 = t.nb;
     } else {
       st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s);
     }
@@ -836,7 +842,7 @@ static int valid_tuning(const ffg_tuning &t) {
       if (v == x) return true;
     return false;
   };
-  return in(t.element_threads, {128, 256}) && t.element_ctas_per_sm >= 0 &&
+  return in(t.element_threads, {256}) && t.element_ctas_per_sm >= 0 &&
          t.element_ctas_per_sm <= 32 && in(t.column_threads, {32, 64, 128, 256, 512}) &&
          in(t.tc_ctas_per_sm, {1, 2}) && t.slice_cost >= 0 && t.slice_cost <= (1 << 20);
 }
@@ -921,13 +927,12 @@ void ffg_problem_autotune(int handle, const double *vertices, double ca, double 
         cands.push_back(x);
       }
     } else if (t.family == FFG_TETRA_NEDELEC) {
-      for (int th : {128, 256})
-        for (int c : {4, 8, 16}) {
-          LaunchTuning x = best;
-          x.ned_threads = th;
-          x.ned_ctas_per_sm = c;
-          cands.push_back(x);
-        }
+      for (int c : {2, 4, 16}) {
+        LaunchTuning x = best;
+        x.ned_threads = 256;
+        x.ned_ctas_per_sm = c;
+        cands.push_back(x);
+      }
     }
     for (const auto &x : cands) {
       double ms = 0;

@@ -53,6 +53,9 @@ struct Topology {
   int64_t nnz() const { return (int64_t)row_idx.size(); }
 };
 
+// Edge signs (6) and face permutation indices (4) of a Nedelec cell from its
+// four global vertex indices.
+void nedelec_orientation(const int *v, int8_t *sign, uint8_t *perm);
 // Build the DoF numbering of a family (first-appearance order of the
 // reference).  Returns FFG_OK or FFG_INVALID_INPUT.
 int build_dofs(Topology &t, std::string &msg);
@@ -219,7 +222,37 @@ struct DeviceTopology {
   double *ref = nullptr;         // reference tensors
   double *load_basis = nullptr;
   double *face_blocks = nullptr;
+  const struct OrientedTables *ort = nullptr;  // Nedelec: oriented tensors and cell classes
 };
+
+// Oriented Nedelec tensors (kernels_oriented.cu).  A cell's orientation
+// transform T depends only on the order of its four global vertex indices,
+// so cells fall in 24 classes (the Lehmer code of that order) and
+// T^T R_s T and T^T (w_q v(q)) are tabulated per class; cells are listed
+// class by class in tiles of at most 64.
+constexpr int kOrtClasses = 24;
+constexpr int kOrtTileCells = 64;
+struct OrientedTables {
+  int order = 0, nb = 0, nql = 0, n_tiles = 0, n_chunks = 0;
+  // kOrtClasses x n_chunks x 12 x 128: per class, per 128-entry chunk of the
+  // column-major nb x nb matrices, the twelve terms' entries (zero past nb^2)
+  double *ref = nullptr;
+  double *load = nullptr;  // kOrtClasses x 3 nql x nb: row 3q + a is T^T (w_q v_a(q))
+  int *order_cells = nullptr;  // cells in class order (ascending within a class)
+  int4 *tiles = nullptr;       // {class, first position in order_cells, count, 0}
+  int class_count[kOrtClasses] = {};
+};
+// Classes of the cells (host connectivity) and the tables of the classes present.
+int ort_build(const Topology &t, const ElementTables &tab, OrientedTables &o);
+struct AssemblyInputs;
+// Oriented element matrices (n_cells * nb * nb, unless load_only) and element
+// loads (n_cells * nb; zero without samples) by the class tables.
+int launch_nedelec_oriented(const Topology &t, const OrientedTables &o, const DeviceTopology &dt,
+                            const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
+                            cudaStream_t s, bool load_only);
+void ort_free(OrientedTables &o);
+// Class of a cell with distinct vertex indices v[0..3].
+int ort_class(const int *v);
 
 // Lagrange / P1 topology built on the device (topology_gpu.cu): the arrays of
 // build_dofs + build_constraints + build_pattern + build_sell, equal entry for
@@ -232,8 +265,8 @@ int build_topology_device(Topology &t, int boundary_mode, const uint8_t *mask, i
 // Launch shapes chosen by the autotuner (ffg_problem_autotune); zero fields
 // keep the built-in defaults.
 struct LaunchTuning {
-  int ned_threads = 0;      // Nedelec FP64 element kernel: threads per CTA (128 or 256)
-  int ned_ctas_per_sm = 0;  // its grid: CTAs per SM
+  int ned_threads = 0;      // Nedelec FP64 element kernels: threads per CTA (256)
+  int ned_ctas_per_sm = 0;  // grid target of the matrix kernel in CTAs per SM (default 8)
   int col_threads = 0;      // column-owner gather: threads per block
   int tc_ctas_per_sm = 0;   // 3xTF32 tensor-core kernel: CTAs per SM (1 or 2)
   int slice_cost = 0;       // PCG work partition: cost of a slice beyond its entries
@@ -259,18 +292,20 @@ struct AssemblyInputs {
 int launch_cell_geometry(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                          const AssemblyInputs &in, double *geo, int geo_stride, double *cell_rhs,
                          int *err, cudaStream_t s);
-// 3xTF32 tensor-core contraction of Nedelec element matrices (orders 3, 4):
-// tile plan and B operand images of one order, in device memory.
+// 3xTF32 tensor-core contraction of Nedelec element matrices (orders 3 to 6):
+// the cells in 128-cell groups of one orientation class and the B operand
+// images (TF32 hi / lo) of every (class, 128-entry chunk) of the oriented table.
 struct TcPlan {
-  int order = 0, n_tiles = 0, ld = 0;  // ld: leading dimension of the FP32 element matrices
-  int *tile_n = nullptr, *tile_pair0 = nullptr, *pair_code = nullptr, *boff = nullptr;
-  float *bimage = nullptr, *face_t = nullptr;
+  int order = 0, n_chunks = 0, n_groups = 0;
+  float *bimage = nullptr;  // kOrtClasses x n_chunks x (hi, lo) images, 16 KB each
+  int4 *groups = nullptr;   // {class, first position in order_cells, count <= 128, 0}
   size_t image_bytes = 0;
 };
 bool tc_supported_order(int k);
-int tc_build_plan(int k, const ElementTables &tab, TcPlan &plan);
+int tc_build_plan(const Topology &t, const OrientedTables &o, TcPlan &plan, cudaStream_t s);
 void tc_free_plan(TcPlan &plan);
-// Oriented element matrices T^T K T in FP32 (n_cells x nb x plan.ld, column-major).
+// Oriented element matrices in FP32 (n_cells x nb x nb, column-major, leading
+// dimension nb), the weights from the geometry or in.geo_override.
 int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const AssemblyInputs &in,
                       const TcPlan &plan, float *elem, int *err, cudaStream_t s);
 
@@ -280,9 +315,9 @@ int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const Assembl
 // caller-weight mode.
 int launch_weighted_weights(const Topology &t, const DeviceTopology &dt, const AssemblyInputs &in,
                             const double *tensor, double *geo, int *err, cudaStream_t s);
-// Nedelec: oriented element matrices (n_cells * nb * nb) and oriented element loads.
-// load_only: the element loads alone (the matrices come from the tensor-core
-// kernel).
+// Nedelec: oriented element matrices (n_cells * nb * nb) and oriented element
+// loads by the class tables of dt.ort.  load_only: the element loads alone
+// (the matrices come from the tensor-core kernel).
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
                    cudaStream_t s, bool load_only = false);

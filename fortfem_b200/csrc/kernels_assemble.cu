@@ -158,209 +158,6 @@ __global__ void triangle_lagrange_geometry_kernel(int n_cells, const int *__rest
   for (int q = 0; q < nq; ++q) g[4 + q] = samples ? area * samples[(size_t)nq * c + q] : 0.0;
 }
 
-// ------------------------------------------------- K2 Nedelec element matrices
-// One CTA per cell: K = (c/det) sum C^ab (J^T J)_ab + m det sum V^ab (J^-1 J^-T)_ab,
-// then the oriented matrix T^T K T of assemble_arbitrary_order_curl_mass_csc
-// (:2340-2342; order 1: s_i s_j, :2097-2107) and the oriented load T^T F.
-// Transform structure (build_tetra_nedelec_basis_transform,
-// tetra_nedelec_global_dof_map.f90:107-155): -1 on even (0-based) moments of
-// reversed edges, dense face blocks per face permutation, identity on cells.
-struct NedDims {
-  int k, nb, fdc, edge_end, face_end;
-  int kglobal;    // the nb x nb matrix does not fit in shared memory: work in `elem`
-  int load_only;  // element loads only (the matrices come from the tensor-core kernel)
-};
-
-__device__ __forceinline__ void ned_block(const NedDims &D, const int8_t *sg, const uint8_t *fp,
-                                          const double *face_blocks, int d, int &start, int &size,
-                                          const double *&col, double &diag) {
-  // For local DoF d, the non-zeros of column d of T: T[start + r][d] = col[r]
-  // (face block), or the single diagonal entry `diag` (edges, cells).
-  if (d < D.edge_end) {
-    const int e = d / D.k, m = d % D.k;
-    start = d;
-    size = 1;
-    col = nullptr;
-    diag = (sg[e] == -1 && (m % 2) == 0) ? -1.0 : 1.0;
-  } else if (d < D.face_end) {
-    const int f = (d - D.edge_end) / D.fdc, r = (d - D.edge_end) % D.fdc;
-    start = D.edge_end + f * D.fdc;
-    size = D.fdc;
-    col = face_blocks + (size_t)fp[f] * D.fdc * D.fdc + (size_t)D.fdc * r;
-    diag = 0.0;
-  } else {
-    start = d;
-    size = 1;
-    col = nullptr;
-    diag = 1.0;
-  }
-}
-
-// At most 64 registers, so that 1024 threads of CTAs share an SM and overlap
-// one another's per-cell barriers (the thread-0 geometry spills a little).
-// THREADS = 128 for orders <= 3 (eight cells in flight per SM), 256 above,
-// where shared memory limits the resident CTAs; measured on the 24^3 x 6
-// slab system (one 256-thread CTA per 96 registers before): order 2 3.8 ->
-// 1.9 ms, order 3 10.9 -> 6.3 ms, order 4 26.2 -> 24.0 ms.
-template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS) nedelec_element_kernel(int n_cells, const int *__restrict__ cells,
-                                       const double *__restrict__ verts, double ca, double cb,
-                                       const double *__restrict__ cell_a,
-                                       const double *__restrict__ cell_b,
-                                       const double *__restrict__ samples, int nql, NedDims D,
-                                       const double *__restrict__ ref,
-                                       const double *__restrict__ load_basis,
-                                       const int8_t *__restrict__ edge_sign,
-                                       const uint8_t *__restrict__ face_perm,
-                                       const double *__restrict__ face_blocks,
-                                       double *__restrict__ elem, double *__restrict__ cell_rhs,
-                                       int *err, const double *__restrict__ verts_dot,
-                                       double ca_dot, double cb_dot,
-                                       const double *__restrict__ geo_in) {
-  extern __shared__ double sm[];
-  const int nb = D.nb, fdc = D.fdc;
-  // K (nb x nb, column-major) lives in shared memory, or (order 6: 373 KB) in
-  // the cell's slice of `elem`, where the finished matrix is written anyway
-  double *K = D.kglobal ? nullptr : sm;
-  double *F = D.kglobal ? sm : sm + (size_t)nb * nb;  // nb
-  double *lf = F + nb;                 // 3 * nql: det J^-1 f_q
-  double *tmp = lf + 3 * nql;          // nb * fdc: one face block of K T or T^T K
-  double *B = tmp + (size_t)nb * fdc;  // fdc * fdc: the face block of T in use
-  __shared__ double geo[12];
-  __shared__ double Ji_s[9];
-  __shared__ double det_s;
-  __shared__ int ok_s;
-  for (int c = blockIdx.x; c < n_cells; c += gridDim.x) {
-    if (D.kglobal) K = elem + (size_t)nb * nb * c;
-    if (threadIdx.x == 0) {
-      double J[9], Ji[9], v0[3];
-      tet_jacobian(cells, verts, c, J, v0);
-      const double det = det3(J);
-      ok_s = valid_jacobian(J, det) ? 1 : 0;
-      if (!ok_s) atomicCAS(err, 0, FFG_INVALID_INPUT);
-      inv3(J, ok_s ? det : 1.0, Ji);
-      const double cw = ca * (cell_a ? cell_a[c] : 1.0);
-      const double mw = cb * (cell_b ? cell_b[c] : 1.0);
-      if (geo_in) {
-        // caller-computed weights (the complex PML tensors, one part at a time)
-        for (int s = 0; s < 12; ++s) geo[s] = ok_s ? geo_in[12 * (size_t)c + s] : 0.0;
-      } else if (!verts_dot) {
-        for (int s = 0; s < 6; ++s) {
-          const int a = kPa[s], b = kPb[s];
-          const double JtJ = J[3 * a] * J[3 * b] + J[3 * a + 1] * J[3 * b + 1] + J[3 * a + 2] * J[3 * b + 2];
-          const double G = Ji[a] * Ji[b] + Ji[a + 3] * Ji[b + 3] + Ji[a + 6] * Ji[b + 6];
-          geo[s] = ok_s ? cw / det * JtJ : 0.0;
-          geo[6 + s] = ok_s ? mw * det * G : 0.0;
-        }
-      } else {
-        // tangent weights: d(c/det J^T J) and d(m det J^-1 J^-T), with
-        // d det = det tr(J^-1 dJ) and d J^-1 = -J^-1 dJ J^-1
-        double Jd[9], T[9], Jid[9], w0[3];
-        tet_jacobian(cells, verts_dot, c, Jd, w0);
-        for (int col = 0; col < 3; ++col)
-          for (int r = 0; r < 3; ++r)
-            T[r + 3 * col] = Ji[r] * Jd[3 * col] + Ji[r + 3] * Jd[3 * col + 1] + Ji[r + 6] * Jd[3 * col + 2];
-        for (int col = 0; col < 3; ++col)
-          for (int r = 0; r < 3; ++r)
-            Jid[r + 3 * col] = -(T[r] * Ji[3 * col] + T[r + 3] * Ji[3 * col + 1] + T[r + 6] * Ji[3 * col + 2]);
-        const double dd = det * (T[0] + T[4] + T[8]);
-        const double cwd = ca_dot * (cell_a ? cell_a[c] : 1.0);
-        const double mwd = cb_dot * (cell_b ? cell_b[c] : 1.0);
-        for (int s = 0; s < 6; ++s) {
-          const int a = kPa[s], b = kPb[s];
-          double JtJ = 0.0, dJtJ = 0.0, G = 0.0, dG = 0.0;
-          for (int r = 0; r < 3; ++r) {
-            JtJ += J[3 * a + r] * J[3 * b + r];
-            dJtJ += Jd[3 * a + r] * J[3 * b + r] + J[3 * a + r] * Jd[3 * b + r];
-            G += Ji[a + 3 * r] * Ji[b + 3 * r];
-            dG += Jid[a + 3 * r] * Ji[b + 3 * r] + Ji[a + 3 * r] * Jid[b + 3 * r];
-          }
-          geo[s] = ok_s ? cwd / det * JtJ - cw * dd / (det * det) * JtJ + cw / det * dJtJ : 0.0;
-          geo[6 + s] = ok_s ? mwd * det * G + mw * dd * G + mw * det * dG : 0.0;
-        }
-      }
-      for (int i = 0; i < 9; ++i) Ji_s[i] = Ji[i];
-      det_s = ok_s ? det : 0.0;
-    }
-    __syncthreads();
-    const size_t nn = (size_t)nb * nb;
-    for (size_t idx = threadIdx.x; !D.load_only && idx < nn; idx += blockDim.x) {
-      double s = 0.0;
-#pragma unroll
-      for (int g = 0; g < 12; ++g) s += geo[g] * __ldg(ref + (size_t)g * nn + idx);
-      K[idx] = s;
-    }
-    for (int q = threadIdx.x; samples && q < nql; q += blockDim.x) {
-      const double *sp = samples + 3 * ((size_t)nql * c + q);
-      const double f[3] = {sp[0], sp[1], sp[2]};
-      // (J^-1 f)_a = sum_k Ji(a,k) f_k ; physical value = J^-T v, so f.v = (J^-1 f).v
-      for (int a = 0; a < 3; ++a)
-        lf[3 * q + a] = det_s * (Ji_s[a] * f[0] + Ji_s[a + 3] * f[1] + Ji_s[a + 6] * f[2]);
-    }
-    __syncthreads();
-    // without source samples (the matrix-only entry points) the load is zero
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-      double s = 0.0;
-      for (int q = 0; samples && q < nql; ++q) {
-        const double *lb = load_basis + ((size_t)q * nb + i) * 3;
-        s += lf[3 * q] * lb[0] + lf[3 * q + 1] * lb[1] + lf[3 * q + 2] * lb[2];
-      }
-      F[i] = s;
-    }
-    __syncthreads();
-    const int8_t *sg = edge_sign + 6 * (size_t)c;
-    const uint8_t *fp = face_perm + 4 * (size_t)c;
-    double *O = elem + nn * c;
-    // T^T K T with T block diagonal: +-1 on edge moments, a dense fdc x fdc
-    // block per face (T[st+m][st+r] = B[r*fdc+m]), identity on cell moments.
-    // Face blocks first: columns (K <- K T), then rows (K <- T^T K), one face
-    // at a time through `tmp`; the edge signs are applied on the way out.
-    for (int f = 0; f < 4 && fdc > 0 && !D.load_only; ++f) {
-      const int st = D.edge_end + f * fdc;
-      const double *Bg = face_blocks + (size_t)fp[f] * fdc * fdc;
-      for (int q = threadIdx.x; q < fdc * fdc; q += blockDim.x) B[q] = Bg[q];
-      __syncthreads();
-      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x) {
-        const int i = q % nb, r = q / nb;
-        double acc = 0.0;
-        for (int m = 0; m < fdc; ++m) acc += K[i + (size_t)nb * (st + m)] * B[r * fdc + m];
-        tmp[q] = acc;
-      }
-      __syncthreads();
-      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x)
-        K[(q % nb) + (size_t)nb * (st + q / nb)] = tmp[q];
-      __syncthreads();
-      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x) {
-        const int r = q % fdc, j = q / fdc;
-        double acc = 0.0;
-        for (int m = 0; m < fdc; ++m) acc += B[r * fdc + m] * K[(st + m) + (size_t)nb * j];
-        tmp[q] = acc;
-      }
-      __syncthreads();
-      for (int q = threadIdx.x; q < nb * fdc; q += blockDim.x)
-        K[(st + q % fdc) + (size_t)nb * (q / fdc)] = tmp[q];
-      __syncthreads();
-    }
-    for (size_t idx = threadIdx.x; !D.load_only && idx < nn; idx += blockDim.x) {
-      const int i = (int)(idx % nb), j = (int)(idx / nb);
-      double v = K[idx];
-      if (i < D.edge_end && sg[i / D.k] == -1 && ((i % D.k) % 2) == 0) v = -v;
-      if (j < D.edge_end && sg[j / D.k] == -1 && ((j % D.k) % 2) == 0) v = -v;
-      O[idx] = v;
-    }
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-      int si, ni;
-      const double *ci;
-      double di;
-      ned_block(D, sg, fp, face_blocks, i, si, ni, ci, di);
-      double s = 0.0;
-      for (int m = 0; m < ni; ++m) s += (ci ? ci[m] : di) * F[si + m];
-      cell_rhs[(size_t)nb * c + i] = s;
-    }
-    __syncthreads();
-  }
-}
-
 // ----------------------------------------------------- K3 column-owner scatter
 // SELL = false: values into the CSC value array (rhs in free-DoF order).
 // SELL = true: values into the solver's slices (row iperm[j] of the SELL
@@ -555,6 +352,155 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
   if (lane == 0) rhs[j] = b - lift;
 }
 
+// SELL rows of Nedelec elements (16 <= n_b <= 128), one 256-thread CTA per
+// half slice (16 rows, so that four CTAs share an SM and one's write-out
+// overlaps the others' gathers): warp w gathers rows w and w + 8 of the half
+// (free column j = perm[row]) with its lanes over the element's local rows
+// i, as csc_column_warp_kernel does for a CSC column, into the half's image
+// in shared memory (slot s of row r at s * 17 + r), every entry receiving
+// its terms in ascending incidence order as in column_kernel; then the CTA
+// writes the half's FP64 and FP32 values (128 contiguous bytes of FP64 per
+// slot step) and each row's Jacobi diagonal and right-hand side.  Both rows'
+// columns, incidence ranges and first 32 incidences are loaded before either
+// is gathered; U incidences' element columns and slot rows (NI values per
+// lane each) are loaded before any of them is added.
+struct SliceArgs {
+  int nb, ld32;
+  int64_t n;  // rows (free DoFs)
+  const int *perm;
+  const int64_t *soff, *col_ptr, *inc_ptr;
+  const int *row_idx, *inc_cell, *gd;
+  const uint8_t *inc_local;
+  const uint16_t *slot;
+  const double *elem, *cell_rhs, *g;
+  const float *elem32;
+  double *val64, *dinv64, *rhs;
+  float *val32, *dinv32;
+};
+constexpr int kSliceHalf = kSliceRows / 2;      // rows of a CTA
+constexpr int kSliceStride = kSliceHalf + 1;    // shared-memory row pitch of a half-slice image
+constexpr int kSliceThreads = 256;
+constexpr int kSliceRowsPerWarp = kSliceHalf / (kSliceThreads / 32);
+static_assert(kSliceRowsPerWarp == 2, "two rows per warp");
+
+// The incidences of one row: its column j, range [p0, p1) and the first 32
+// incidences' cells, local indices and element loads, one per lane.
+struct SliceRowHead {
+  int j;
+  int64_t p0, p1;
+  int e, l;
+  double f;
+};
+
+__device__ __forceinline__ void slice_head(const SliceArgs &A, int64_t row, int lane,
+                                           SliceRowHead &h) {
+  h.j = row < A.n ? A.perm[row] : -1;
+  h.p0 = h.j >= 0 ? A.inc_ptr[h.j] : 0;
+  h.p1 = h.j >= 0 ? A.inc_ptr[h.j + 1] : 0;
+  h.e = 0;
+  h.l = 0;
+  h.f = 0.0;
+  if (h.p0 + lane < h.p1) {
+    h.e = A.inc_cell[h.p0 + lane];
+    h.l = A.inc_local[h.p0 + lane];
+  }
+}
+
+template <int NI, int U>
+__device__ __forceinline__ void slice_row(const SliceArgs &A, double *img, int r, int64_t row,
+                                          int lane, SliceRowHead h) {
+  const int j = h.j;
+  const int nb = A.nb;
+  double b = 0.0, lift = 0.0;
+  const int64_t p0 = h.p0, p1 = h.p1;
+  for (int64_t pb = p0; pb < p1; pb += 32) {
+    const int cnt = (int)min((int64_t)32, p1 - pb);
+    int my_e = h.e, my_l = h.l;
+    if (pb != p0) {
+      my_e = lane < cnt ? A.inc_cell[pb + lane] : 0;
+      my_l = lane < cnt ? A.inc_local[pb + lane] : 0;
+    }
+    const double my_f = lane < cnt ? A.cell_rhs[(size_t)nb * my_e + my_l] : 0.0;
+    for (int u0 = 0; u0 < cnt; u0 += U) {
+      double kil[U][NI];
+      uint16_t sl[U][NI];
+      int ev[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int uu = min(u0 + u, cnt - 1);
+        const int e = __shfl_sync(0xffffffffu, my_e, uu);
+        const int l = __shfl_sync(0xffffffffu, my_l, uu);
+        ev[u] = e;
+        const uint16_t *slp = A.slot + (size_t)(pb + uu) * nb;
+#pragma unroll
+        for (int c = 0; c < NI; ++c) {
+          const int i = lane + 32 * c;
+          const bool in = i < nb && u0 + u < cnt;
+          kil[u][c] = !in ? 0.0
+                      : A.elem32 ? (double)A.elem32[(size_t)A.ld32 * nb * e + i + (size_t)A.ld32 * l]
+                                 : A.elem[(size_t)nb * nb * e + i + (size_t)nb * l];
+          sl[u][c] = in ? slp[i] : kConstrainedSlot;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (u0 + u >= cnt) break;
+#pragma unroll
+        for (int c = 0; c < NI; ++c) {
+          const int i = lane + 32 * c;
+          if (i >= nb) continue;
+          if (sl[u][c] == kConstrainedSlot) {
+            if (A.g) lift += kil[u][c] * A.g[A.gd[(size_t)nb * ev[u] + i]];
+          } else {
+            img[sl[u][c] * kSliceStride + r] += kil[u][c];
+          }
+        }
+        __syncwarp();
+      }
+    }
+    for (int u = 0; u < cnt; ++u) b += __shfl_sync(0xffffffffu, my_f, u);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lift += __shfl_xor_sync(0xffffffffu, lift, o);
+  if (lane == 0) {
+    // the diagonal's slot: local row l of any incidence (e, l) of column j
+    // has global DoF j, so its slot entry is the diagonal
+    const int dslot = p1 > p0 ? A.slot[(size_t)p0 * nb + h.l] : kConstrainedSlot;
+    const double d = dslot != kConstrainedSlot ? img[dslot * kSliceStride + r] : 0.0;
+    const double di = (fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
+    A.dinv64[row] = di;
+    A.dinv32[row] = (float)di;
+    A.rhs[row] = b - lift;
+  }
+}
+
+template <int NI, int U>
+__global__ void __launch_bounds__(kSliceThreads, 4) sell_slice_kernel(const __grid_constant__ SliceArgs A) {
+  extern __shared__ double img[];
+  const int64_t k = blockIdx.x >> 1;
+  const int half = blockIdx.x & 1;
+  const int64_t s0 = A.soff[k];
+  const int width = (int)((A.soff[k + 1] - s0) / kSliceRows);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row0 = k * kSliceRows + half * kSliceHalf;
+  // both rows' heads before the image is cleared, so their loads overlap it
+  SliceRowHead h0, h1;
+  slice_head(A, row0 + w, lane, h0);
+  slice_head(A, row0 + w + kSliceThreads / 32, lane, h1);
+  for (int q = threadIdx.x; q < width * kSliceStride; q += blockDim.x) img[q] = 0.0;
+  __syncthreads();
+  if (h0.j >= 0) slice_row<NI, U>(A, img, w, row0 + w, lane, h0);
+  if (h1.j >= 0) slice_row<NI, U>(A, img, w + kSliceThreads / 32, row0 + w + kSliceThreads / 32, lane, h1);
+  __syncthreads();
+  for (int q = threadIdx.x; q < width * kSliceHalf; q += blockDim.x) {
+    const int sl = q / kSliceHalf, r = q % kSliceHalf;
+    const double v = img[sl * kSliceStride + r];
+    const int64_t at = s0 + (int64_t)sl * kSliceRows + half * kSliceHalf + r;
+    A.val64[at] = v;
+    A.val32[at] = (float)v;
+  }
+}
+
 inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 // ------------------------------------------- batched assembly (serving)
@@ -684,46 +630,12 @@ int launch_cell_geometry(const Topology &t, const ElementTables &tab, const Devi
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 
-size_t nedelec_smem_bytes(const ElementTables &tab, int fdc, bool kglobal) {
-  return sizeof(double) * ((kglobal ? 0 : (size_t)tab.nb * tab.nb) + tab.nb +
-                           3 * (size_t)tab.nq_load + (size_t)tab.nb * fdc + (size_t)fdc * fdc);
-}
-
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
                    cudaStream_t s, bool load_only) {
-  NedDims D;
-  D.load_only = load_only ? 1 : 0;
-  D.k = t.degree;
-  D.nb = t.nb;
-  D.fdc = t.degree * (t.degree - 1);
-  D.edge_end = 6 * t.degree;
-  D.face_end = D.edge_end + 4 * D.fdc;
-  D.kglobal = nedelec_smem_bytes(tab, D.fdc, false) > 200 * 1024 ? 1 : 0;
-  const size_t smem = nedelec_smem_bytes(tab, D.fdc, D.kglobal != 0);
-  const LaunchTuning *tu = in.tune;
-  const bool small = (tu && tu->ned_threads) ? tu->ned_threads == 128 : D.nb <= 45;  // orders 1-3
-  if (smem > 48 * 1024) {
-    const cudaError_t e =
-        small ? cudaFuncSetAttribute(nedelec_element_kernel<128>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-              : cudaFuncSetAttribute(nedelec_element_kernel<256>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return FFG_CUDA_ERROR;
-  }
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int per_sm = (tu && tu->ned_ctas_per_sm) ? tu->ned_ctas_per_sm : (small ? 16 : 8);
-  const int grid = (int)std::min<int64_t>(t.n_cells, (int64_t)sms * per_sm);
-#define FFG_NED_ARGS                                                                           \
-  t.n_cells, dt.cells, in.vertices, in.coef_a, in.coef_b, in.cell_a, in.cell_b, in.samples,     \
-      tab.nq_load, D, dt.ref, dt.load_basis, dt.edge_sign, dt.face_perm, dt.face_blocks, elem, \
-      cell_rhs, err, in.vertices_dot, in.coef_a_dot, in.coef_b_dot, in.geo_override
-  if (small) nedelec_element_kernel<128><<<grid, 128, smem, s>>>(FFG_NED_ARGS);
-  else nedelec_element_kernel<256><<<grid, 256, smem, s>>>(FFG_NED_ARGS);
-#undef FFG_NED_ARGS
-  return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+  (void)tab;
+  if (!dt.ort) return FFG_INVALID_INPUT;
+  return launch_nedelec_oriented(t, *dt.ort, dt, in, elem, cell_rhs, err, s, load_only);
 }
 
 int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
@@ -750,6 +662,47 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
   const bool by_warp = !sell && t.nb >= 16 && t.family != FFG_TRIANGLE_P1 && t.max_column > 0 &&
                        col_bytes <= kColSmem;
   const int wpb = by_warp ? std::max(1, std::min(8, kColSmem / col_bytes)) : 0;
+  // Nedelec SELL rows: one CTA per slice while the slice image fits
+  const size_t slice_smem = (size_t)t.max_column * kSliceStride * sizeof(double);
+  if (sell && t.family == FFG_TETRA_NEDELEC && t.nb >= 16 && t.nb <= 128 && t.max_column > 0 &&
+      slice_smem <= 200 * 1024 && sell->perm) {
+    SliceArgs A;
+    A.nb = t.nb;
+    A.ld32 = ld32;
+    A.n = F;
+    A.perm = sell->perm;
+    A.soff = sell->soff;
+    A.col_ptr = col_ptr;
+    A.inc_ptr = dt.inc_ptr;
+    A.row_idx = row_idx;
+    A.inc_cell = dt.inc_cell;
+    A.gd = dt.gd;
+    A.inc_local = dt.inc_local;
+    A.slot = dt.slot;
+    A.elem = elem;
+    A.cell_rhs = cell_rhs;
+    A.g = in.g;
+    A.elem32 = elem32;
+    A.val64 = sell->val64;
+    A.dinv64 = sell->dinv64;
+    A.rhs = rhs;
+    A.val32 = sell->val32;
+    A.dinv32 = sell->dinv32;
+    const int ni = (t.nb + 31) / 32;
+    auto go = [&](auto kern) -> int {
+      if (slice_smem > 48 * 1024 &&
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)slice_smem) != cudaSuccess)
+        return FFG_CUDA_ERROR;
+      kern<<<(unsigned)(2 * sell->n_slices), kSliceThreads, slice_smem, s>>>(A);
+      return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
+    };
+    // about eight loads of each kind in flight per lane
+    if (ni == 1) return go(sell_slice_kernel<1, 6>);
+    if (ni == 2) return go(sell_slice_kernel<2, 3>);
+    if (ni == 3) return go(sell_slice_kernel<3, 2>);
+    return go(sell_slice_kernel<4, 1>);
+  }
 #define FFG_LAUNCH(FAM)                                                                        \
   do {                                                                                         \
     if (sell)                                                                                  \

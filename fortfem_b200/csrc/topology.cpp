@@ -173,12 +173,12 @@ int build_nedelec(Topology &t, std::string &msg) {
   int ne = 0;
   for (int c = 0; c < t.n_cells; ++c) {
     const int *v = t.cells.data() + 4 * (size_t)c;
+    nedelec_orientation(v, &t.edge_sign[6 * (size_t)c], &t.face_perm[4 * (size_t)c]);
     for (int le = 0; le < 6; ++le) {
       int a = v[kLocalEdges[le][0]], b = v[kLocalEdges[le][1]];
       auto it = emap.emplace(edge_key(a, b), ne);
       if (it.second) ++ne;
       cell_edge[6 * (size_t)c + le] = it.first->second;
-      t.edge_sign[6 * (size_t)c + le] = (a < b) ? 1 : -1;
     }
   }
   std::unordered_map<Key128, int, Key128Hash> fmap;
@@ -188,17 +188,10 @@ int build_nedelec(Topology &t, std::string &msg) {
     for (int c = 0; c < t.n_cells; ++c) {
       const int *v = t.cells.data() + 4 * (size_t)c;
       for (int lf = 0; lf < 4; ++lf) {
-        int lv[3] = {v[kLocalFaces[lf][0]], v[kLocalFaces[lf][1]], v[kLocalFaces[lf][2]]};
-        int cv[3] = {lv[0], lv[1], lv[2]};
-        std::sort(cv, cv + 3);
-        auto it = fmap.emplace(face_key(lv[0], lv[1], lv[2]), nf);
+        auto it = fmap.emplace(
+            face_key(v[kLocalFaces[lf][0]], v[kLocalFaces[lf][1]], v[kLocalFaces[lf][2]]), nf);
         if (it.second) ++nf;
         cell_face[4 * (size_t)c + lf] = it.first->second;
-        int perm[3];
-        for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j)
-            if (cv[j] == lv[i]) perm[i] = j + 1;
-        t.face_perm[4 * (size_t)c + lf] = (uint8_t)perm_index(perm);
       }
     }
   }
@@ -222,6 +215,27 @@ int build_nedelec(Topology &t, std::string &msg) {
 }
 
 }  // namespace
+
+// Orientation of a Nedelec cell from its global vertex indices (the
+// reference's convention, tetra_edge_dof_map.f90:54-60 and
+// tetra_nedelec_global_dof_map.f90:68-74): edge le is reversed (-1) when its
+// first local vertex has the larger index; face lf gets the index 0..5 of the
+// permutation taking its local vertex order to ascending index order (ranks
+// 123, 132, 213, 231, 312, 321).
+void nedelec_orientation(const int *v, int8_t *sign, uint8_t *perm) {
+  for (int le = 0; le < 6; ++le)
+    sign[le] = v[kLocalEdges[le][0]] < v[kLocalEdges[le][1]] ? 1 : -1;
+  for (int lf = 0; lf < 4; ++lf) {
+    const int lv[3] = {v[kLocalFaces[lf][0]], v[kLocalFaces[lf][1]], v[kLocalFaces[lf][2]]};
+    int cv[3] = {lv[0], lv[1], lv[2]};
+    std::sort(cv, cv + 3);
+    int p[3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        if (cv[j] == lv[i]) p[i] = j + 1;
+    perm[lf] = (uint8_t)perm_index(p);
+  }
+}
 
 bool validate_cells(const Topology &t, std::string &msg) { return check_cells(t, msg); }
 

@@ -63,7 +63,7 @@ extern "C" {
 /* Solver precision. */
 /* Element contraction of Nedelec problems (ffg_problem_set_assembly_precision) */
 #define FFG_ASSEMBLY_FP64 0   /* FP64 CUDA-core contraction (the 1e-12 parity path) */
-#define FFG_ASSEMBLY_TF32X3 1 /* 3xTF32 tensor-core contraction, FP32 accumulation (orders 3, 4) */
+#define FFG_ASSEMBLY_TF32X3 1 /* 3xTF32 tensor-core contraction, FP32 accumulation (orders 3-6) */
 #define FFG_PRECISION_FP64 0  /* FP64 Jacobi-PCG with the reference's stopping rule */
 #define FFG_PRECISION_MIXED 1 /* FP32 PCG recurrences, FP64 solution and reliable
                                  FP64 residual updates (defect correction) */
@@ -372,8 +372,9 @@ void ffg_problem_constrained(int handle, uint8_t *mask, int *status);
 /* Launch shapes of a problem's kernels and the times that chose them.  Zero
  * shape fields mean the built-in default. */
 typedef struct {
-  int element_threads;     /* Nedelec FP64 element kernel: threads per CTA (128 or 256) */
-  int element_ctas_per_sm; /* ... and its grid in CTAs per SM */
+  int element_threads;     /* Nedelec FP64 element kernels: threads per CTA (256) */
+  int element_ctas_per_sm; /* the matrix kernel's grid target in CTAs per SM (the
+                              entry range of a cell tile is split to reach it) */
   int column_threads;      /* column-owner gather: threads per block */
   int tc_ctas_per_sm;      /* 3xTF32 tensor-core kernel: CTAs per SM (1 or 2) */
   int slice_cost;          /* PCG work partition: cost of a slice beyond its entries */
@@ -385,8 +386,8 @@ typedef struct {
 
 /* No counterpart in the reference (whose loops have no launch shapes).
  * Chooses the problem's launch shapes by measurement on its own inputs (as
- * ffg_problem_solve takes them): the element kernel's CTA size and grid
- * (Nedelec FP64) or the tensor-core kernel's CTAs per SM (3xTF32), the column
+ * ffg_problem_solve takes them): the element matrix kernel's grid (Nedelec
+ * FP64) or the tensor-core kernel's CTAs per SM (3xTF32), the column
  * gather's block size, then the PCG work partition's slice cost, each
  * candidate timed with CUDA events (best of three) and the fastest kept for
  * every following assembly and solve of the problem.  Results of assembly and
@@ -400,14 +401,15 @@ void ffg_problem_autotune(int handle, const double *vertices, double coef_a, dou
  * another process); the time fields are ignored. */
 void ffg_problem_set_tuning(int handle, const ffg_tuning *tuning, int *status);
 
-/* Nedelec problems of order 3 or 4: how the element matrices are contracted in
- * every following assembly.  FFG_ASSEMBLY_FP64 (the default) is the FP64
- * reference-tensor contraction on CUDA cores, equal to the reference's
- * quadrature loop (assemble_tetra_nedelec_curl_mass_element,
+/* Nedelec problems of orders 3 to 6: how the element matrices are contracted
+ * in every following assembly.  FFG_ASSEMBLY_FP64 (the default) is the FP64
+ * oriented reference-tensor contraction on CUDA cores, equal to the
+ * reference's quadrature loop (assemble_tetra_nedelec_curl_mass_element,
  * assembly_tetra_nedelec_3d.f90:584-643) to 1e-12.  FFG_ASSEMBLY_TF32X3 runs
  * the contraction as a GEMM on the tensor cores (tcgen05, TF32 hi/lo operand
- * split, three products accumulated in FP32) and the orientation transform in
- * FP32: entries carry about 1e-7 relative error, the geometry stays FP64.
+ * split, three products accumulated in FP32) against the same oriented
+ * tensors: entries carry about 1e-7 relative error, the geometry and the
+ * loads stay FP64.
  * Other orders and families return FFG_INVALID_INPUT. */
 void ffg_problem_set_assembly_precision(int handle, int precision, int *status);
 

@@ -101,6 +101,51 @@ def test_nedelec_load_matches_oracle(k):
     assert rel_frob(rhs, ref) <= FROB
 
 
+def relabelled_box(n, seed):
+    """A jittered box mesh with its vertices renumbered at random: every
+    cell's orientation (edge signs, face permutations) follows the order of
+    its global vertex indices, so all 24 orders appear."""
+    v, t = jittered_box(n, 0.1, seed)
+    perm = np.random.default_rng(seed).permutation(len(v))
+    v2 = np.empty_like(v)
+    v2[perm] = v
+    return v2, perm[t].astype(np.int32)
+
+
+def vertex_order_classes(t):
+    return {tuple(np.argsort(np.argsort(c))) for c in t}
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_nedelec_all_vertex_orders_match_oracle(k):
+    v, t = relabelled_box(4, 100 + k)
+    assert len(vertex_order_classes(t)) == 24
+    rng = np.random.default_rng(k)
+    cc = rng.uniform(0.5, 2.0, len(t))
+    cm = rng.uniform(0.5, 2.0, len(t))
+    A, st = ff.assemble_tetra_nedelec_curl_mass_csc(v, t, 1.7, 0.9, order=k, cell_curl=cc,
+                                                    cell_mass=cm)
+    assert st.code == 0
+    n, cp, ri, val = oracle.nedelec_csc(v, t, k, 1.7, 0.9, cc, cm)
+    assert A.nrow == n and np.array_equal(A.col_ptr, cp) and np.array_equal(A.row_idx, ri)
+    assert rel_frob(A.val, val) <= FROB
+    pts = oracle.nedelec_load_points(v, t, k)
+    src = np.stack([np.sin(pts[..., 1]), pts[..., 0] * pts[..., 2], np.cos(pts[..., 0])], -1)
+    rhs, st = ff.assemble_tetra_nedelec_vector_load_samples(v, t, k, src)
+    assert st.code == 0
+    assert rel_frob(rhs, oracle.nedelec_load_samples(v, t, k, src)) <= FROB
+
+
+def test_nedelec_order6_all_vertex_orders_match_oracle():
+    v, t = relabelled_box(2, 136)  # 48 cells in 23 of the 24 orders
+    assert len(vertex_order_classes(t)) == 23
+    A, st = ff.assemble_tetra_nedelec_curl_mass_csc(v, t, 1.7, 0.9, order=6)
+    assert st.code == 0
+    n, cp, ri, val = oracle.nedelec_csc(v, t, 6, 1.7, 0.9)
+    assert np.array_equal(A.col_ptr, cp) and np.array_equal(A.row_idx, ri)
+    assert rel_frob(A.val, val) <= 1e-10
+
+
 def test_p1_csc_matches_oracle():
     v, t = oracle.unit_square_mesh(17)
     v = synth.jitter_interior_2d(v, 1 / 16, 0.1, 4)
