@@ -234,10 +234,11 @@ constexpr int kOrtClasses = 24;
 constexpr int kOrtTileCells = 64;
 struct OrientedTables {
   int order = 0, nb = 0, nql = 0, n_tiles = 0, n_chunks = 0;
+  int64_t load_stride = 0;  // doubles per class in `load` (3 nql nb rounded up to even)
   // kOrtClasses x n_chunks x 12 x 128: per class, per 128-entry chunk of the
   // column-major nb x nb matrices, the twelve terms' entries (zero past nb^2)
   double *ref = nullptr;
-  double *load = nullptr;  // kOrtClasses x 3 nql x nb: row 3q + a is T^T (w_q v_a(q))
+  double *load = nullptr;  // kOrtClasses x load_stride: row 3q + a (nb values) is T^T (w_q v_a(q))
   int *order_cells = nullptr;  // cells in class order (ascending within a class)
   int4 *tiles = nullptr;       // {class, first position in order_cells, count, 0}
   int class_count[kOrtClasses] = {};

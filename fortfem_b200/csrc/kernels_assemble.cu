@@ -406,13 +406,19 @@ __device__ __forceinline__ void slice_head(const SliceArgs &A, int64_t row, int 
   }
 }
 
-template <int NI, int U>
+template <int NI, int U, bool F32>
 __device__ __forceinline__ void slice_row(const SliceArgs &A, double *img, int r, int64_t row,
                                           int lane, SliceRowHead h) {
-  const int j = h.j;
   const int nb = A.nb;
   double b = 0.0, lift = 0.0;
   const int64_t p0 = h.p0, p1 = h.p1;
+  // local rows of this lane and whether they exist (nb <= 32 NI)
+  bool has[NI];
+#pragma unroll
+  for (int c = 0; c < NI; ++c) has[c] = lane + 32 * c < nb;
+  // element columns: FP64 nb x nb or FP32 with leading dimension ld32, per cell
+  const int ld = F32 ? A.ld32 : nb;
+  const size_t cell_stride = (size_t)ld * nb;
   for (int64_t pb = p0; pb < p1; pb += 32) {
     const int cnt = (int)min((int64_t)32, p1 - pb);
     int my_e = h.e, my_l = h.l;
@@ -421,38 +427,35 @@ __device__ __forceinline__ void slice_row(const SliceArgs &A, double *img, int r
       my_l = lane < cnt ? A.inc_local[pb + lane] : 0;
     }
     const double my_f = lane < cnt ? A.cell_rhs[(size_t)nb * my_e + my_l] : 0.0;
+    // per lane: the offset of its incidence's element column
+    const size_t my_col = (size_t)my_e * cell_stride + (size_t)ld * my_l;
     for (int u0 = 0; u0 < cnt; u0 += U) {
       double kil[U][NI];
       uint16_t sl[U][NI];
       int ev[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int uu = min(u0 + u, cnt - 1);
-        const int e = __shfl_sync(0xffffffffu, my_e, uu);
-        const int l = __shfl_sync(0xffffffffu, my_l, uu);
-        ev[u] = e;
-        const uint16_t *slp = A.slot + (size_t)(pb + uu) * nb;
+        const bool live = u0 + u < cnt;
+        const int uu = live ? u0 + u : u0;
+        const size_t col = __shfl_sync(0xffffffffu, my_col, uu) + lane;
+        ev[u] = __shfl_sync(0xffffffffu, my_e, uu);
+        const uint16_t *slp = A.slot + (size_t)(pb + uu) * nb + lane;
 #pragma unroll
         for (int c = 0; c < NI; ++c) {
-          const int i = lane + 32 * c;
-          const bool in = i < nb && u0 + u < cnt;
-          kil[u][c] = !in ? 0.0
-                      : A.elem32 ? (double)A.elem32[(size_t)A.ld32 * nb * e + i + (size_t)A.ld32 * l]
-                                 : A.elem[(size_t)nb * nb * e + i + (size_t)nb * l];
-          sl[u][c] = in ? slp[i] : kConstrainedSlot;
+          const bool in = has[c] && live;
+          if (F32) kil[u][c] = in ? (double)A.elem32[col + 32 * c] : 0.0;
+          else kil[u][c] = in ? A.elem[col + 32 * c] : 0.0;
+          sl[u][c] = in ? slp[32 * c] : kConstrainedSlot;
         }
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        if (u0 + u >= cnt) break;
 #pragma unroll
         for (int c = 0; c < NI; ++c) {
-          const int i = lane + 32 * c;
-          if (i >= nb) continue;
-          if (sl[u][c] == kConstrainedSlot) {
-            if (A.g) lift += kil[u][c] * A.g[A.gd[(size_t)nb * ev[u] + i]];
-          } else {
+          if (sl[u][c] != kConstrainedSlot) {
             img[sl[u][c] * kSliceStride + r] += kil[u][c];
+          } else if (A.g && has[c] && u0 + u < cnt) {
+            lift += kil[u][c] * A.g[A.gd[(size_t)nb * ev[u] + lane + 32 * c]];
           }
         }
         __syncwarp();
@@ -474,23 +477,25 @@ __device__ __forceinline__ void slice_row(const SliceArgs &A, double *img, int r
   }
 }
 
-template <int NI, int U>
+template <int NI, int U, bool F32>
 __global__ void __launch_bounds__(kSliceThreads, 4) sell_slice_kernel(const __grid_constant__ SliceArgs A) {
   extern __shared__ double img[];
-  const int64_t k = blockIdx.x >> 1;
-  const int half = blockIdx.x & 1;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kW = kSliceThreads / 32;
+  const int64_t hs = blockIdx.x;
+  const int64_t k = hs >> 1;
+  const int half = (int)(hs & 1);
   const int64_t s0 = A.soff[k];
   const int width = (int)((A.soff[k + 1] - s0) / kSliceRows);
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row0 = k * kSliceRows + half * kSliceHalf;
+  const int64_t row0 = hs * kSliceHalf;
   // both rows' heads before the image is cleared, so their loads overlap it
   SliceRowHead h0, h1;
   slice_head(A, row0 + w, lane, h0);
-  slice_head(A, row0 + w + kSliceThreads / 32, lane, h1);
+  slice_head(A, row0 + w + kW, lane, h1);
   for (int q = threadIdx.x; q < width * kSliceStride; q += blockDim.x) img[q] = 0.0;
   __syncthreads();
-  if (h0.j >= 0) slice_row<NI, U>(A, img, w, row0 + w, lane, h0);
-  if (h1.j >= 0) slice_row<NI, U>(A, img, w + kSliceThreads / 32, row0 + w + kSliceThreads / 32, lane, h1);
+  if (h0.j >= 0) slice_row<NI, U, F32>(A, img, w, row0 + w, lane, h0);
+  if (h1.j >= 0) slice_row<NI, U, F32>(A, img, w + kW, row0 + w + kW, lane, h1);
   __syncthreads();
   for (int q = threadIdx.x; q < width * kSliceHalf; q += blockDim.x) {
     const int sl = q / kSliceHalf, r = q % kSliceHalf;
@@ -698,10 +703,16 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
       return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
     };
     // about eight loads of each kind in flight per lane
-    if (ni == 1) return go(sell_slice_kernel<1, 6>);
-    if (ni == 2) return go(sell_slice_kernel<2, 3>);
-    if (ni == 3) return go(sell_slice_kernel<3, 2>);
-    return go(sell_slice_kernel<4, 1>);
+    if (elem32) {
+      if (ni == 1) return go(sell_slice_kernel<1, 4, true>);
+      if (ni == 2) return go(sell_slice_kernel<2, 2, true>);
+      if (ni == 3) return go(sell_slice_kernel<3, 2, true>);
+      return go(sell_slice_kernel<4, 1, true>);
+    }
+    if (ni == 1) return go(sell_slice_kernel<1, 4, false>);
+    if (ni == 2) return go(sell_slice_kernel<2, 2, false>);
+    if (ni == 3) return go(sell_slice_kernel<3, 2, false>);
+    return go(sell_slice_kernel<4, 1, false>);
   }
 #define FFG_LAUNCH(FAM)                                                                        \
   do {                                                                                         \

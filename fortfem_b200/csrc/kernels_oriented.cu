@@ -32,7 +32,6 @@ namespace {
 
 constexpr int kOrtThreads = 256;   // eight warps, eight cells each
 constexpr int kOrtChunk = 128;     // output entries per pass: four per lane
-constexpr int kOrtQ = 16;          // load points staged per pass
 
 
 struct OrtArgs {
@@ -48,7 +47,8 @@ struct OrtArgs {
   const int *order;         // cells in class order
   const int4 *tiles;
   const double *ref;        // kOrtClasses x n_chunks x 12 x kOrtChunk (entries chunk-major)
-  const double *load;       // kOrtClasses x 3 nql x nb
+  const double *load;       // kOrtClasses x load_stride: 3 nql x nb per class
+  int64_t load_stride;      // 3 nql nb rounded up to an even count (16-byte aligned classes)
   int n_chunks;             // ceil(nb^2 / kOrtChunk)
   int parts, chunks_per_part;  // entry chunks of a tile split over `parts` CTAs
   double *elem, *cell_rhs;
@@ -130,8 +130,8 @@ __device__ __forceinline__ void ort_geometry(const OrtArgs &A, int c, bool weigh
 constexpr int kOrtStage = 12 * kOrtChunk / kOrtThreads;  // table values per thread and chunk
 
 __global__ void __launch_bounds__(kOrtThreads, 2) ort_matrix_kernel(const __grid_constant__ OrtArgs A) {
-  __shared__ double W[12][kOrtTileCells];
-  __shared__ double Rs[2][12 * kOrtChunk];
+  __shared__ __align__(16) double W[12][kOrtTileCells];
+  __shared__ __align__(16) double Rs[2][12 * kOrtChunk];
   __shared__ int cell_s[kOrtTileCells];
   const int4 tile = A.tiles[blockIdx.x / A.parts];
   const int part = blockIdx.x % A.parts;
@@ -179,11 +179,15 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_matrix_kernel(const __grid
       double r[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) r[j] = buf[s * kOrtChunk + lane + 32 * j];
+      const double2 *w2p = reinterpret_cast<const double2 *>(&W[s][8 * warp]);
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const double wc = W[s][8 * warp + c];
+      for (int c2 = 0; c2 < 4; ++c2) {
+        const double2 w2 = w2p[c2];  // the weights of two cells in one broadcast load
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[c][j] = fma(wc, r[j], acc[c][j]);
+        for (int j = 0; j < 4; ++j) {
+          acc[2 * c2][j] = fma(w2.x, r[j], acc[2 * c2][j]);
+          acc[2 * c2 + 1][j] = fma(w2.y, r[j], acc[2 * c2 + 1][j]);
+        }
       }
     }
     const int64_t base = (int64_t)ch * kOrtChunk;
@@ -203,17 +207,46 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_matrix_kernel(const __grid
 
 // Element loads of one tile: F[cell][i] = sum_{q,a} (det J^-1 f_q)_a L'_{class}[3q + a][i],
 // with lanes over 32 J entries per pass (J chosen so the passes waste the
-// fewest lanes for n_b) and the sample factors of kOrtQ points at a time
-// staged in shared memory; each thread fetches its samples of the next
-// points into registers while the current ones are consumed.
-constexpr int kOrtPairs = kOrtTileCells * kOrtQ / kOrtThreads;  // (cell, point) pairs per thread
+// fewest lanes for n_b) and Q points at a time: their 3 Q table rows (one
+// contiguous block) come into shared memory by cp.async, double-buffered,
+// and their sample factors det J^-1 f_q of the 64 cells are staged beside
+// them; each thread fetches its samples of the next points into registers
+// while the current ones are consumed.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait1() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
 
-template <int J>
+constexpr int kOrtLfPitch = kOrtTileCells + 2;  // even: 16-byte aligned rows of LF
+
+template <int Q>
+struct OrtLoadSmem {
+  double Ji[9][kOrtTileCells];
+  double det[kOrtTileCells];
+  alignas(16) double LF[3 * Q][kOrtLfPitch];
+  int cell[kOrtTileCells];
+};
+
+template <int J, int Q>
 __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_constant__ OrtArgs A) {
-  __shared__ double Ji_s[9][kOrtTileCells];
-  __shared__ double det_s[kOrtTileCells];
-  __shared__ double LF[3 * kOrtQ][kOrtTileCells + 1];
-  __shared__ int cell_s[kOrtTileCells];
+  extern __shared__ __align__(16) unsigned char ort_raw[];
+  OrtLoadSmem<Q> &S = *reinterpret_cast<OrtLoadSmem<Q> *>(ort_raw);
+  const int nb = A.nb, nql = A.nql;
+  // two buffers of 3 Q table rows (an even count of doubles each)
+  const int rows_cap = (3 * Q * nb + 1) & ~1;
+  double *Lb = reinterpret_cast<double *>(ort_raw + sizeof(OrtLoadSmem<Q>));
+  constexpr int kPairs = kOrtTileCells * Q / kOrtThreads;  // (cell, point) pairs per thread
   const int4 tile = A.tiles[blockIdx.x];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid < kOrtTileCells) {
@@ -227,21 +260,33 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_c
       for (int i = 0; i < 9; ++i) Ji[i] = 0.0;
     }
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Ji_s[i][tid] = Ji[i];
-    det_s[tid] = det;
-    cell_s[tid] = c;
+    for (int i = 0; i < 9; ++i) S.Ji[i][tid] = Ji[i];
+    S.det[tid] = det;
+    S.cell[tid] = c;
   }
   __syncthreads();
-  const int nb = A.nb, nql = A.nql;
-  const double *L = A.load + (size_t)tile.x * 3 * nql * nb;
-  double f[kOrtPairs][3];
-  // pair u of this thread: cell (tid + 256 u) / kOrtQ, point (tid + 256 u) % kOrtQ
+  const double *L = A.load + (size_t)tile.x * A.load_stride;
+  const int n_chunks = (nql + Q - 1) / Q;
+  // the table rows of point chunk ci into buffer ci & 1 (16-byte pieces; the
+  // table is padded so that a trailing odd double may be read)
+  auto stage = [&](int ci) {
+    if (ci < n_chunks) {
+      const int q0 = ci * Q, nq = min(Q, nql - q0);
+      const int pieces = (3 * nq * nb + 1) / 2;
+      const double *src = L + (size_t)3 * q0 * nb;
+      double *dst = Lb + (size_t)(ci & 1) * rows_cap;
+      for (int i = tid; i < pieces; i += kOrtThreads) cp_async16(dst + 2 * i, src + 2 * i);
+    }
+    cp_async_commit();
+  };
+  double f[kPairs][3];
+  // pair u of this thread: cell (tid + 256 u) / Q, point (tid + 256 u) % Q
   auto fetch = [&](int q0) {
 #pragma unroll
-    for (int u = 0; u < kOrtPairs; ++u) {
-      const int p = tid + kOrtThreads * u, c = p / kOrtQ, q = q0 + p % kOrtQ;
+    for (int u = 0; u < kPairs; ++u) {
+      const int p = tid + kOrtThreads * u, c = p / Q, q = q0 + p % Q;
       const bool live = c < tile.z && q < nql;
-      const double *sp = A.samples + 3 * ((size_t)nql * (live ? cell_s[c] : 0) + (live ? q : 0));
+      const double *sp = A.samples + 3 * ((size_t)nql * (live ? S.cell[c] : 0) + (live ? q : 0));
 #pragma unroll
       for (int a = 0; a < 3; ++a) f[u][a] = live ? sp[a] : 0.0;
     }
@@ -252,48 +297,48 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_c
     for (int c = 0; c < 8; ++c)
 #pragma unroll
       for (int j = 0; j < J; ++j) acc[c][j] = 0.0;
+    __syncthreads();  // the previous pass has consumed both buffers
+    stage(0);
     fetch(0);
-    for (int q0 = 0; q0 < nql; q0 += kOrtQ) {
-      const int nq = min(kOrtQ, nql - q0);
-      __syncthreads();  // the previous points consumed
+    for (int ci = 0; ci < n_chunks; ++ci) {
+      const int q0 = ci * Q, nq = min(Q, nql - q0);
+      __syncthreads();  // chunk ci - 1 consumed: its buffer and LF may be rewritten
+      stage(ci + 1);
 #pragma unroll
-      for (int u = 0; u < kOrtPairs; ++u) {
-        const int p = tid + kOrtThreads * u, c = p / kOrtQ, q = p % kOrtQ;
-        const double d = det_s[c];
+      for (int u = 0; u < kPairs; ++u) {
+        const int p = tid + kOrtThreads * u, c = p / Q, q = p % Q;
+        const double d = S.det[c];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
-          LF[3 * q + a][c] =
-              d * (Ji_s[a][c] * f[u][0] + Ji_s[a + 3][c] * f[u][1] + Ji_s[a + 6][c] * f[u][2]);
+          S.LF[3 * q + a][c] =
+              d * (S.Ji[a][c] * f[u][0] + S.Ji[a + 3][c] * f[u][1] + S.Ji[a + 6][c] * f[u][2]);
       }
-      __syncthreads();
-      if (q0 + kOrtQ < nql) fetch(q0 + kOrtQ);
-      // a point (three rows) per step, two points unrolled up to J = 2: about
-      // six table loads per lane in flight
-#pragma unroll(J <= 2 ? 2 : 1)
-      for (int q = 0; q < nq; ++q) {
-        double r[3][J];
+      cp_async_wait1();  // this thread's pieces of chunk ci have landed
+      __syncthreads();   // everyone's pieces and factors are visible
+      if (ci + 1 < n_chunks) fetch(q0 + Q);
+      const double *rows = Lb + (size_t)(ci & 1) * rows_cap;
+      for (int qa = 0; qa < 3 * nq; ++qa) {
+        double r[J];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const double *row = L + (size_t)(3 * (q0 + q) + a) * nb;
+        for (int j = 0; j < J; ++j) {
+          const int i = base + lane + 32 * j;
+          r[j] = i < nb ? rows[(size_t)qa * nb + i] : 0.0;
+        }
+        const double2 *lf = reinterpret_cast<const double2 *>(&S.LF[qa][8 * warp]);
+#pragma unroll
+        for (int c2 = 0; c2 < 4; ++c2) {
+          const double2 w2 = lf[c2];
 #pragma unroll
           for (int j = 0; j < J; ++j) {
-            const int i = base + lane + 32 * j;
-            r[a][j] = i < nb ? __ldg(row + i) : 0.0;
+            acc[2 * c2][j] = fma(w2.x, r[j], acc[2 * c2][j]);
+            acc[2 * c2 + 1][j] = fma(w2.y, r[j], acc[2 * c2 + 1][j]);
           }
         }
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int c = 0; c < 8; ++c) {
-            const double wc = LF[3 * q + a][8 * warp + c];
-#pragma unroll
-            for (int j = 0; j < J; ++j) acc[c][j] = fma(wc, r[a][j], acc[c][j]);
-          }
       }
     }
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      const int cell = cell_s[8 * warp + c];
+      const int cell = S.cell[8 * warp + c];
       if (cell < 0) continue;
 #pragma unroll
       for (int j = 0; j < J; ++j) {
@@ -302,6 +347,7 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_c
       }
     }
   }
+  cp_async_wait_all();
 }
 
 // Entries per lane of the load kernel for n_b: the fewest padded lanes over
@@ -397,7 +443,8 @@ int ort_build(const Topology &t, const ElementTables &tab, OrientedTables &o) {
   const size_t class_stride = (size_t)n_chunks * 12 * kOrtChunk;
   std::vector<double> ref((size_t)kOrtClasses * class_stride, 0.0);
   std::vector<double> Out(nn);
-  std::vector<double> load((size_t)kOrtClasses * 3 * nql * nb, 0.0);
+  const size_t load_stride = ((size_t)3 * nql * nb + 1) & ~(size_t)1;
+  std::vector<double> load((size_t)kOrtClasses * load_stride, 0.0);
   std::vector<double> X(nn);
   std::vector<TCol> T(nb);
   for (int q = 0; q < kOrtClasses; ++q) {
@@ -431,7 +478,7 @@ int ort_build(const Topology &t, const ElementTables &tab, OrientedTables &o) {
             Out[idx];
     }
     // L'[3p + a][i] = sum_m T[m][i] (w_p v_a(p))_m, load_basis ((p nb + m) 3 + a)
-    double *Lq = &load[(size_t)q * 3 * nql * nb];
+    double *Lq = &load[(size_t)q * load_stride];
     for (int p = 0; p < nql; ++p)
       for (int a = 0; a < 3; ++a)
         for (int i = 0; i < nb; ++i) {
@@ -462,6 +509,7 @@ int ort_build(const Topology &t, const ElementTables &tab, OrientedTables &o) {
   o.nb = nb;
   o.nql = nql;
   o.n_chunks = n_chunks;
+  o.load_stride = (int64_t)load_stride;
   o.n_tiles = (int)tiles.size();
   std::memcpy(o.class_count, count, sizeof(count));
   return FFG_OK;
@@ -491,6 +539,7 @@ int launch_nedelec_oriented(const Topology &t, const OrientedTables &o, const De
   A.tiles = o.tiles;
   A.ref = o.ref;
   A.load = o.load;
+  A.load_stride = o.load_stride;
   A.elem = elem;
   A.cell_rhs = cell_rhs;
   A.err = err;
@@ -506,12 +555,25 @@ int launch_nedelec_oriented(const Topology &t, const OrientedTables &o, const De
   if (!load_only)
     ort_matrix_kernel<<<(unsigned)((int64_t)o.n_tiles * A.parts), kOrtThreads, 0, s>>>(A);
   if (in.samples) {
+    // Q = 16 points per stage up to order 4, 8 above (shared memory)
+    auto go = [&](auto kern, int Q, size_t fixed) -> int {
+      const size_t smem = fixed + 2 * sizeof(double) * (((size_t)3 * Q * o.nb + 1) & ~(size_t)1);
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+        return FFG_CUDA_ERROR;
+      kern<<<o.n_tiles, kOrtThreads, smem, s>>>(A);
+      return FFG_OK;
+    };
+    const bool wide = o.nb > 70;
+    const size_t f16 = sizeof(OrtLoadSmem<16>), f8 = sizeof(OrtLoadSmem<8>);
+    int st;
     switch (load_lanes(o.nb)) {
-      case 1: ort_load_kernel<1><<<o.n_tiles, kOrtThreads, 0, s>>>(A); break;
-      case 2: ort_load_kernel<2><<<o.n_tiles, kOrtThreads, 0, s>>>(A); break;
-      case 3: ort_load_kernel<3><<<o.n_tiles, kOrtThreads, 0, s>>>(A); break;
-      default: ort_load_kernel<4><<<o.n_tiles, kOrtThreads, 0, s>>>(A); break;
+      case 1: st = go(ort_load_kernel<1, 16>, 16, f16); break;
+      case 2: st = go(ort_load_kernel<2, 16>, 16, f16); break;
+      case 3: st = wide ? go(ort_load_kernel<3, 8>, 8, f8) : go(ort_load_kernel<3, 16>, 16, f16); break;
+      default: st = go(ort_load_kernel<4, 8>, 8, f8); break;
     }
+    if (st) return st;
   } else if (cudaMemsetAsync(cell_rhs, 0, sizeof(double) * t.nb * (size_t)t.n_cells, s) !=
              cudaSuccess) {
     return FFG_CUDA_ERROR;
