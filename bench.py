@@ -564,7 +564,7 @@ def run_ours(args):
         line["serving"] = {k: sv[k] for k in (
             "requests", "rate_per_s", "wall_s", "setup_s", "latency_ms", "latency_ms_by_mode",
             "converged", "not_converged", "max_true_relative_residual", "free_dofs_per_s",
-            "whole_device", "mean_batch")}
+            "whole_device", "cta_groups", "mean_batch")}
         line["serving"]["workload"] = ("70% P1 unit square n ~ logU[32,1024] squares/side, "
                                        "30% P2 Kuhn box n ~ logU[8,40]; lognormal cell "
                                        "coefficient, GRF source (RFF, corr. length 0.1), "

@@ -43,6 +43,7 @@ FFG_OPTIONS_VERSION = 1
 FFG_NOALLOC_MAX_ROWS = 65536
 FFG_BATCH_CTA_PER_SYSTEM = 0
 FFG_BATCH_WHOLE_DEVICE = 1
+FFG_BATCH_CTA_GROUPS = 2
 FFG_POINT_REFERENCE = 0
 FFG_POINT_PHYSICAL = 1
 FFG_PROBE_AVERAGE = 0

@@ -1004,7 +1004,8 @@ def solve_tetra_nedelec_weighted_curl_mass(vertices, tetrahedra, order, curl_coe
 
 
 _BATCH_MODES = {"cta_per_system": K.FFG_BATCH_CTA_PER_SYSTEM,
-                "whole_device": K.FFG_BATCH_WHOLE_DEVICE}
+                "whole_device": K.FFG_BATCH_WHOLE_DEVICE,
+                "cta_groups": K.FFG_BATCH_CTA_GROUPS}
 
 
 def solve_batch(problems, vertices, solutions, coef_a, coef_b, cell_a=None, cell_b=None,

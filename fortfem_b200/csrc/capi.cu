@@ -1246,7 +1246,8 @@ void ffg_problem_solve_batch(int count, const int *handles, const double *const 
                              const ffg_solver_options *opts, double *const *solutions, int mode,
                              void *stream, int *status) {
   if (count < 1 || !handles || !vertices || !coef_a || !coef_b || !solutions ||
-      (mode != FFG_BATCH_CTA_PER_SYSTEM && mode != FFG_BATCH_WHOLE_DEVICE)) {
+      (mode != FFG_BATCH_CTA_PER_SYSTEM && mode != FFG_BATCH_WHOLE_DEVICE &&
+       mode != FFG_BATCH_CTA_GROUPS)) {
     *status = FFG_INVALID_INPUT;
     return;
   }
@@ -1361,6 +1362,9 @@ void ffg_problem_solve_batch(int count, const int *handles, const double *const 
     } else if (mode == FFG_BATCH_CTA_PER_SYSTEM) {
       if (!A.empty())
         st = pcg_launch_batch((int)A.size(), A.data(), b.data(), x.data(), o, w.data(), s, msg);
+    } else if (mode == FFG_BATCH_CTA_GROUPS) {
+      if (!A.empty())
+        st = pcg_launch_groups((int)A.size(), A.data(), b.data(), x.data(), o, w.data(), s, msg);
     } else {
       for (size_t i = 0; i < A.size() && !st; ++i)
         st = pcg_launch(*A[i], b[i], x[i], o, *w[i], s, msg);

@@ -198,6 +198,13 @@ int pcg_launch(const DeviceSell &A, const double *b, double *x, const ffg_solver
 int pcg_launch_batch(int count, const DeviceSell *const *A, const double *const *b,
                      double *const *x, const ffg_solver_options &opts, SolveWork *const *w,
                      cudaStream_t stream, std::string &msg);
+// Independent systems in shared cooperative launches, each on a group of
+// pcg_group_ctas(n) CTAs (16384 rows per CTA, at least 2, at most the grid);
+// consecutive systems share a launch while their groups fit the grid.
+int pcg_group_ctas(int64_t n, int grid);
+int pcg_launch_groups(int count, const DeviceSell *const *A, const double *const *b,
+                      double *const *x, const ffg_solver_options &opts, SolveWork *const *w,
+                      cudaStream_t stream, std::string &msg);
 int pcg_collect(SolveWork &w, ffg_solver_stats *stats, std::string &msg);
 int pcg_grid_size(int *grid);
 

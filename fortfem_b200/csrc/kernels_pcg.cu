@@ -212,6 +212,10 @@ __device__ __forceinline__ void slice_range(const PcgParams &P, int &s0, int &s1
   if (P.ncta == 1) {
     s0 = 0;
     s1 = P.n_slices;
+  } else if (!P.cta_slice) {
+    // a CTA group of a batch: equal slice counts
+    s0 = (int)((int64_t)cta_of(P) * P.n_slices / P.ncta);
+    s1 = (int)((int64_t)(cta_of(P) + 1) * P.n_slices / P.ncta);
   } else {
     s0 = P.cta_slice[cta_of(P)];
     s1 = P.cta_slice[cta_of(P) + 1];
@@ -1150,6 +1154,36 @@ __global__ void __launch_bounds__(kThreads, 1) pcg_batch_kernel(const __grid_con
   pcg_body(Ps);
 }
 
+// Up to kMaxGroups independent systems in one cooperative launch, system i
+// on CTAs [first[i], first[i + 1]) with its own barrier counter, partial
+// sums and control word.  The launch makes every CTA resident together, so
+// a group's barrier waits only on CTAs that are running; the group size
+// depends on the system alone (pcg_group_ctas), so its result does not
+// depend on the other systems of the launch.
+constexpr int kMaxGroups = 16;
+constexpr int64_t kGroupRows = 16384;  // rows per CTA of a group
+struct PcgGroups {
+  PcgParams sys[kMaxGroups];
+  int first[kMaxGroups + 1];
+  int count;
+};
+__global__ void __launch_bounds__(kThreads, 1) pcg_group_kernel(const __grid_constant__ PcgGroups B) {
+  __shared__ PcgParams Ps;
+  if (threadIdx.x == 0) {
+    int i = 0;
+    while (i + 1 < B.count && B.first[i + 1] <= (int)blockIdx.x) ++i;
+    Ps = B.sys[i];
+    Ps.cta0 = B.first[i];
+    Ps.ncta = B.first[i + 1] - B.first[i];
+    // the operator's partition is for the whole grid: groups split evenly
+    Ps.cta_slice = nullptr;
+    Ps.wslice = nullptr;
+    Ps.woff = nullptr;
+  }
+  __syncthreads();
+  pcg_body(Ps);
+}
+
 // Drop-in FP64 CSR SpMV, one thread per row (spmv / csc_matvec semantics).
 __global__ void csr_spmv64_kernel(int64_t n, const int64_t *rp, const int *ci, const double *v,
                                   const double *x, double *y) {
@@ -1198,6 +1232,8 @@ bool staged_smem_ready() {
         cudaFuncSetAttribute((const void *)pcg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kStageSmem) == cudaSuccess &&
         cudaFuncSetAttribute((const void *)pcg_batch_kernel,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem) == cudaSuccess &&
+        cudaFuncSetAttribute((const void *)pcg_group_kernel,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmem) == cudaSuccess;
     if (!ok) cudaGetLastError();
     state[dev] = ok ? 1 : -1;
@@ -1546,6 +1582,65 @@ int pcg_launch_batch(int count, const DeviceSell *const *A, const double *const 
                           kResultDoubles * sizeof(double), cudaMemcpyDeviceToHost,
                           stream) != cudaSuccess)
         return FFG_CUDA_ERROR;
+  }
+  return FFG_OK;
+}
+
+int pcg_group_ctas(int64_t n, int grid) {
+  const int64_t g = (n + kGroupRows - 1) / kGroupRows;
+  return (int)std::max<int64_t>(2, std::min<int64_t>(g, grid));
+}
+
+int pcg_launch_groups(int count, const DeviceSell *const *A, const double *const *b,
+                      double *const *x, const ffg_solver_options &opts, SolveWork *const *w,
+                      cudaStream_t stream, std::string &msg) {
+  static_assert(sizeof(PcgGroups) <= 32000, "kernel parameter block too large");
+  int grid = 0;
+  int st = pcg_grid_size(&grid);
+  if (st) return st;
+  for (int i = 0; i < count; ++i)
+    if (w[i]->n != A[i]->n || A[i]->n < 1 || w[i]->grid < pcg_group_ctas(A[i]->n, grid)) {
+      msg = "solver workspace mismatch";
+      return FFG_INVALID_INPUT;
+    }
+  const int staged = staged_smem_ready() ? 1 : 0;
+  // consecutive systems fill a launch while their groups fit the grid
+  for (int i0 = 0; i0 < count;) {
+    PcgGroups B;
+    B.count = 0;
+    B.first[0] = 0;
+    int i = i0;
+    while (i < count && B.count < kMaxGroups) {
+      const int g = pcg_group_ctas(A[i]->n, grid);
+      if (B.count > 0 && B.first[B.count] + g > grid) break;
+      B.sys[B.count] = make_params(*A[i], b[i], x[i], opts, *w[i]);
+      B.sys[B.count].staged = staged;
+      B.first[B.count + 1] = B.first[B.count] + g;
+      ++B.count;
+      w[i]->control_host[0] = 0;
+      if (cudaMemsetAsync(w[i]->barrier, 0, 64, stream) != cudaSuccess ||
+          cudaMemsetAsync(w[i]->control, 0, 64, stream) != cudaSuccess ||
+          cudaMemsetAsync(w[i]->result, 0, kResultDoubles * sizeof(double), stream) !=
+              cudaSuccess)
+        return FFG_CUDA_ERROR;
+      ++i;
+    }
+    void *args[] = {&B};
+    const cudaError_t e = cudaLaunchCooperativeKernel(
+        (const void *)pcg_group_kernel, dim3(B.first[B.count]), dim3(kThreads), args,
+        staged ? kStageSmem : 0, stream);
+    if (e != cudaSuccess) {
+      msg = std::string("cooperative group launch failed: ") + cudaGetErrorString(e);
+      cudaGetLastError();
+      return FFG_CUDA_ERROR;
+    }
+    for (int k = i0; k < i; ++k)
+      if (cudaMemcpyAsync(w[k]->result_host, w[k]->result, kResultDoubles * sizeof(double),
+                          cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+          cudaMemcpyAsync(w[k]->control_host, w[k]->control, 2 * sizeof(int),
+                          cudaMemcpyDeviceToHost, stream) != cudaSuccess)
+        return FFG_CUDA_ERROR;
+    i0 = i;
   }
   return FFG_OK;
 }

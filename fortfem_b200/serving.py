@@ -118,11 +118,42 @@ class Scheduler:
     max_batch: int = 48
     streams: int = 2
     bypass_window: float = 0.05
+    # large requests side by side in one cooperative launch ("cta_groups"),
+    # each on group_ctas(key) of `grid` thread blocks, instead of one after
+    # another on the whole device
+    groups: bool = False
+    grid: int = 148
+    group_rows: int = 16384
+    max_groups: int = 16
     queue: deque = field(default_factory=deque)
     inflight: List[Batch] = field(default_factory=list)
 
     def is_small(self, r: Request) -> bool:
         return free_dofs(r.key) <= self.small_rows
+
+    def group_ctas(self, key) -> int:
+        """Thread blocks of a system in a group launch (ffg_problem_solve_batch's
+        FFG_BATCH_CTA_GROUPS rule: group_rows rows per block, 2 to grid)."""
+        return max(2, min(-(-free_dofs(key) // self.group_rows), self.grid))
+
+    def _large_batch(self, head: Request, can_host) -> Batch:
+        picked, counts = [head], Counter({head.key: 1})
+        used = self.group_ctas(head.key)
+        if self.groups:
+            for r in list(self.queue)[1:]:
+                if len(picked) == self.max_groups:
+                    break
+                if self.is_small(r):
+                    continue
+                g = self.group_ctas(r.key)
+                if used + g > self.grid or not can_host(r.key, counts[r.key] + 1):
+                    continue
+                picked.append(r)
+                counts[r.key] += 1
+                used += g
+        for r in picked:
+            self.queue.remove(r)
+        return Batch("cta_groups" if self.groups else "whole_device", picked, 0)
 
     def busy_counts(self) -> Counter:
         return Counter(r.key for b in self.inflight for r in b.requests)
@@ -138,13 +169,12 @@ class Scheduler:
         queue is strictly first come, first served)."""
         if not self.queue:
             return None
-        if any(b.mode == "whole_device" for b in self.inflight):
+        if any(b.mode != "cta_per_system" for b in self.inflight):
             return None
         head = self.queue[0]
         if not self.is_small(head):
             if not self.inflight and can_host(head.key, 1):
-                self.queue.popleft()
-                return Batch("whole_device", [head], 0)
+                return self._large_batch(head, can_host)
             if self._starved(head, now):
                 return None
         used = {b.slot for b in self.inflight}
@@ -303,9 +333,11 @@ class DeviceEngine:
             (2500.0 if key[0] == "p2" else 400.0)
         return int(per * free_dofs(key)) + (64 << 20)
 
-    def _evict_for(self, need: int) -> bool:
-        # whole pools of sizes with nothing in flight, least recently used first
-        idle = sorted((k for k, ms in self.meshes.items() if len(self.idle.get(k, [])) == len(ms)),
+    def _evict_for(self, need: int, keep=frozenset()) -> bool:
+        # whole pools of sizes with nothing in flight, least recently used
+        # first, sparing the sizes in `keep`
+        idle = sorted((k for k, ms in self.meshes.items()
+                       if k not in keep and len(self.idle.get(k, [])) == len(ms)),
                       key=lambda k: self.last_use.get(k, 0.0))
         for k in idle:
             if self.used + need <= self.budget:
@@ -316,14 +348,15 @@ class DeviceEngine:
             self.used -= self.bytes.pop(k)
         return self.used + need <= self.budget
 
-    def can_host(self, key, count: int = 1) -> bool:
+    def can_host(self, key, count: int = 1, keep=frozenset()) -> bool:
         """Whether `count` problems of this mesh size can be in flight at
-        once, creating pool members while memory allows."""
+        once, creating pool members while memory allows (evicting idle pools
+        of other sizes than `key` and those in `keep`)."""
         if count > self.max_instances:
             return False
         while len(self.meshes.get(key, [])) < count:
             need = self._estimate(key)
-            if self.used + need > self.budget and not self._evict_for(need):
+            if self.used + need > self.budget and not self._evict_for(need, keep | {key}):
                 return False
             self._create(key)
         return True
@@ -367,6 +400,13 @@ class DeviceEngine:
         torch = self.torch
         from .api import solve_batch
         s = self.streams[b.slot]
+        # a size admitted while the batch was formed may have been evicted
+        # for a later one: host every size of the batch, sparing the others
+        keep = frozenset(r.key for r in b.requests)
+        for k, c in Counter(r.key for r in b.requests).items():
+            busy = len(self.meshes.get(k, [])) - len(self.idle.get(k, []))
+            if not self.can_host(k, busy + c, keep):
+                raise RuntimeError(f"no device memory for {c} problems of size {k}")
         meshes = [self.idle[r.key].pop() for r in b.requests]
         for r in b.requests:
             self.last_use[r.key] = time.perf_counter()
@@ -407,12 +447,17 @@ class DeviceEngine:
 
 
 def run_requests(reqs: List[Request], small_rows: int = 32768, max_batch: int = 48,
-                 streams: int = 2, keep_solutions: bool = False, device: int = 0):
+                 streams: int = 2, keep_solutions: bool = False, device: int = 0,
+                 groups: bool = True):
     """Serve `reqs` (arrival times relative to now) on one GPU; returns
-    (results, wall seconds, setup seconds)."""
+    (results, wall seconds, setup seconds).  Large requests run side by side
+    in CTA groups (`groups`) or one after another on the whole device."""
+    import torch
     eng = DeviceEngine(device, keep_solutions=keep_solutions, streams=streams)
     setup = eng.prepare(reqs)
-    sch = Scheduler(small_rows=small_rows, max_batch=max_batch, streams=streams)
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    sch = Scheduler(small_rows=small_rows, max_batch=max_batch, streams=streams, groups=groups,
+                    grid=sms)
     t0 = time.perf_counter()
     res = serve(reqs, eng, sch) if reqs else []
     wall = time.perf_counter() - t0
@@ -426,7 +471,7 @@ def summarize(reqs: List[Request], res: List[Result], wall: float, setup: float,
     dofs = sum(free_dofs(r.key) for r in reqs)
     by_id = {r.rid: r for r in reqs}
     by_mode = {}
-    for mode in ("cta_per_system", "whole_device"):
+    for mode in ("cta_per_system", "whole_device", "cta_groups"):
         lat = [r.latency for r in res if r.mode == mode]
         if lat:
             by_mode[mode] = {"requests": len(lat), **percentiles(lat),
@@ -440,15 +485,17 @@ def summarize(reqs: List[Request], res: List[Result], wall: float, setup: float,
                               for r in res if not r.converged],
             "free_dofs_per_s": dofs / wall,
             "whole_device": sum(r.mode == "whole_device" for r in res),
+            "cta_groups": sum(r.mode == "cta_groups" for r in res),
             "mean_batch": float(np.mean([r.batch_size for r in res])), "results": res}
 
 
 def run_stream(count: int = 512, rate: float = 20.0, seed: int = 4, small_rows: int = 32768,
                max_batch: int = 48, streams: int = 2, keep_solutions: bool = False,
-               device: int = 0) -> dict:
+               device: int = 0, groups: bool = True) -> dict:
     """Serve a Poisson stream end to end on one GPU; returns latency statistics."""
     reqs = poisson_stream(count, rate, seed)
-    res, wall, setup = run_requests(reqs, small_rows, max_batch, streams, keep_solutions, device)
+    res, wall, setup = run_requests(reqs, small_rows, max_batch, streams, keep_solutions, device,
+                                    groups)
     return summarize(reqs, res, wall, setup, rate)
 
 
@@ -461,7 +508,10 @@ if __name__ == "__main__":
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--small-rows", type=int, default=32768)
     ap.add_argument("--streams", type=int, default=2)
+    ap.add_argument("--no-groups", action="store_true",
+                    help="large requests one after another on the whole device")
     a = ap.parse_args()
-    out = run_stream(a.requests, a.rate, a.seed, a.small_rows, streams=a.streams)
+    out = run_stream(a.requests, a.rate, a.seed, a.small_rows, streams=a.streams,
+                     groups=not a.no_groups)
     out.pop("results")
     print(json.dumps(out))

@@ -468,9 +468,16 @@ void ffg_problem_phase_times(int handle, double *seconds, int *status);
  * one thread block of its own in a single launch (for many small systems;
  * a system's result does not depend on the rest of the batch);
  * FFG_BATCH_WHOLE_DEVICE solves them one after another on the whole GPU (for
- * large systems).  A problem may belong to one unfinished batch at a time. */
+ * large systems); FFG_BATCH_CTA_GROUPS solves them side by side in shared
+ * cooperative launches, each system on a group of thread blocks sized by its
+ * row count alone (16384 rows per block, at least 2, at most one per SM), so
+ * that mid-size systems, whose iterations are bound by the grid barrier
+ * rather than by bandwidth, share the GPU while a system's result still does
+ * not depend on the rest of the batch.  A problem may belong to one
+ * unfinished batch at a time. */
 #define FFG_BATCH_CTA_PER_SYSTEM 0
 #define FFG_BATCH_WHOLE_DEVICE 1
+#define FFG_BATCH_CTA_GROUPS 2
 void ffg_problem_solve_batch(int count, const int *handles, const double *const *vertices,
                              const double *coef_a, const double *coef_b,
                              const double *const *cell_a, const double *const *cell_b,

@@ -99,6 +99,27 @@ def test_small_requests_pass_a_large_one_only_within_the_window():
     assert b.mode == "whole_device" and [r.rid for r in b.requests] == [1]
 
 
+def test_scheduler_groups_large_requests_that_fit_the_grid():
+    # free DoFs: p1 n -> (n-1)^2; group_rows 100 -> blocks ceil(free / 100), 2 .. grid
+    sch = S.Scheduler(small_rows=100, max_batch=8, streams=2, groups=True, grid=10,
+                      group_rows=100, max_groups=3)
+    assert sch.group_ctas(("p1", 12)) == 2            # 121 free DoFs
+    assert sch.group_ctas(("p1", 31)) == 9            # 900
+    assert sch.group_ctas(("p1", 60)) == 10           # capped at the grid
+    reqs = [S.Request(0, "p1", 12, 1), S.Request(1, "p1", 5, 2), S.Request(2, "p1", 31, 3),
+            S.Request(3, "p1", 16, 4), S.Request(4, "p1", 13, 5), S.Request(5, "p1", 14, 6)]
+    sch.queue.extend(reqs)
+    b = sch.next_batch(lambda k, n: True)
+    # head (2 blocks) + 16 (3 blocks) + 13 (2 blocks): 31 (9) does not fit, the small one waits,
+    # and max_groups stops the scan
+    assert b.mode == "cta_groups" and [r.rid for r in b.requests] == [0, 3, 4]
+    sch.inflight.append(b)
+    assert sch.next_batch(lambda k, n: True) is None        # nothing runs beside a group launch
+    sch.inflight.clear()
+    b = sch.next_batch(lambda k, n: True)
+    assert b.mode == "cta_per_system" and [r.rid for r in b.requests] == [1]
+
+
 def test_scheduler_skips_sizes_the_engine_cannot_host():
     sch = S.Scheduler(small_rows=1000, max_batch=8, streams=1)
     sch.queue.extend([S.Request(0, "p1", 10, 1), S.Request(1, "p1", 12, 2)])

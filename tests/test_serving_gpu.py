@@ -49,6 +49,27 @@ def test_batch_matches_alone_and_the_cooperative_path():
     eng.close()
 
 
+def test_group_batch_matches_alone_and_the_whole_device():
+    """Large systems side by side in one cooperative launch (FFG_BATCH_CTA_GROUPS),
+    each on its own group of 2 to 22 thread blocks: the same bits as the system
+    alone in a group launch, and within 1e-6 of the whole-device solve."""
+    eng = S.DeviceEngine(keep_solutions=True)
+    reqs = [S.Request(0, "p1", 200, 201), S.Request(1, "p2", 12, 202),
+            S.Request(2, "p1", 600, 203), S.Request(3, "p1", 120, 204)]
+    for r in reqs:
+        assert eng.can_host(r.key)
+    mixed = _run(eng, "cta_groups", reqs)
+    for r, m in zip(reqs, mixed):
+        assert m.converged and m.true_relative_residual <= 1e-10
+        alone = _run(eng, "cta_groups", [r])[0]
+        assert np.array_equal(alone.solution, m.solution)
+        whole = _run(eng, "whole_device", [r])[0]
+        assert whole.converged
+        scale = np.abs(whole.solution).max()
+        assert scale > 0 and np.abs(m.solution - whole.solution).max() <= 1e-6 * scale
+    eng.close()
+
+
 def test_one_block_system_with_more_than_32_slices_per_warp():
     # 18^3 x 6 P2: 42,875 free rows, 1,340 slices, so each of the block's 32
     # warps walks about 42 slices (past the 32 a warp keeps in registers)
