@@ -285,6 +285,7 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
   int st;
   const float *elem32 = nullptr;
   int ld32 = 0;
+  int64_t cs32 = 0;
   if (t.family == FFG_TETRA_NEDELEC) {
     if (P.cell_tensor) {
       st = launch_weighted_weights(t, P.dt, in, P.cell_tensor, P.geo_w, P.err, s);
@@ -307,6 +308,7 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
       st = launch_nedelec_tc(t, P.dt, in, P.tc, e32, P.err, s);
       elem32 = e32;
       ld32 = t.nb;
+      cs32 = tc_cell_stride(t.nb);
     } else {
       st = launch_nedelec(t, P.tab, P.dt, in, P.elem, P.cell_rhs, P.err, s);
     }
@@ -315,7 +317,7 @@ int assemble(Problem &P, const double *vertices, double ca, double cb, const dou
   }
   if (st) return st;
   st = launch_columns(t, P.tab, P.dt, in, P.geo, P.geo_stride, P.cell_rhs, P.elem, P.csc_col_ptr,
-                      P.csc_row, sell ? &P.S : nullptr, P.csc_val, P.rhs, s, elem32, ld32);
+                      P.csc_row, sell ? &P.S : nullptr, P.csc_val, P.rhs, s, elem32, ld32, cs32);
   if (st) return st;
   if (defer_check) {
     // the flag is read with the statistics, after the stream has passed

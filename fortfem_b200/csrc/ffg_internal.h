@@ -310,10 +310,13 @@ struct TcPlan {
   size_t image_bytes = 0;
 };
 bool tc_supported_order(int k);
+// floats per cell of the tensor-core element matrices: nb^2 rounded up to 32
+int64_t tc_cell_stride(int nb);
 int tc_build_plan(const Topology &t, const OrientedTables &o, TcPlan &plan, cudaStream_t s);
 void tc_free_plan(TcPlan &plan);
-// Oriented element matrices in FP32 (n_cells x nb x nb, column-major, leading
-// dimension nb), the weights from the geometry or in.geo_override.
+// Oriented element matrices in FP32 (column-major nb x nb, leading dimension
+// nb, tc_cell_stride(nb) floats per cell), the weights from the geometry or
+// in.geo_override.
 int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const AssemblyInputs &in,
                       const TcPlan &plan, float *elem, int *err, cudaStream_t s);
 
@@ -329,7 +332,9 @@ int launch_weighted_weights(const Topology &t, const DeviceTopology &dt, const A
 int launch_nedelec(const Topology &t, const ElementTables &tab, const DeviceTopology &dt,
                    const AssemblyInputs &in, double *elem, double *cell_rhs, int *err,
                    cudaStream_t s, bool load_only = false);
-// Column-owner gather into the constrained operator.  With `sell` set the
+// Column-owner gather into the constrained operator (element matrices from
+// `elem`, FP64 nb x nb per cell, or `elem32`, FP32 column-major with leading
+// dimension ld32 and cs32 floats per cell).  With `sell` set the
 // values go to the slices (FP64 + FP32 copy, Jacobi diagonal, rhs in the
 // SELL numbering); otherwise to the CSC value array `csc_val` with the rhs in
 // free-DoF order.  row_idx is the CSC row index array (device).
@@ -337,7 +342,8 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    const AssemblyInputs &in, const double *geo, int geo_stride,
                    const double *cell_rhs, const double *elem, const int64_t *col_ptr,
                    const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
-                   cudaStream_t s, const float *elem32 = nullptr, int ld32 = 0);
+                   cudaStream_t s, const float *elem32 = nullptr, int ld32 = 0,
+                   int64_t cs32 = 0);
 int geo_stride_for(const Topology &t, const ElementTables &tab);
 // Batched assembly of independent Lagrange-tetrahedron or P1 systems (the
 // serving families) into their SELL operators, one launch per phase.

@@ -177,7 +177,7 @@ __device__ __forceinline__ void column_body(int64_t j, const int64_t *__restrict
                               double *__restrict__ val64, float *__restrict__ val32,
                               double *__restrict__ dinv64, float *__restrict__ dinv32,
                               double *__restrict__ rhs, const float *__restrict__ elem32,
-                              int ld32) {
+                              int ld32, int64_t cs32) {
   const int64_t start = col_ptr[j], end = col_ptr[j + 1];
   int64_t base, stride_out, out_row;
   if (SELL) {
@@ -223,7 +223,7 @@ __device__ __forceinline__ void column_body(int64_t j, const int64_t *__restrict
       } else if (FAMILY == FFG_TRIANGLE_P1) {
         kil = geo[10 * (size_t)e + i + 3 * l];
       } else if (elem32) {
-        kil = (double)elem32[(size_t)ld32 * nb * e + i + (size_t)ld32 * l];
+        kil = (double)elem32[(size_t)cs32 * e + i + (size_t)ld32 * l];
       } else {
         kil = elem[nn * e + i + (size_t)nb * l];
       }
@@ -264,12 +264,12 @@ __global__ void column_kernel(int64_t n_free, const int64_t *__restrict__ col_pt
                               double *__restrict__ val64, float *__restrict__ val32,
                               double *__restrict__ dinv64, float *__restrict__ dinv32,
                               double *__restrict__ rhs, const float *__restrict__ elem32,
-                              int ld32) {
+                              int ld32, int64_t cs32) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j < n_free)
     column_body<FAMILY, SELL>(j, col_ptr, row_idx, inc_ptr, inc_cell, inc_local, slot, gd, nb, geo,
                               stride, ref, load_basis, nq, elem, cell_rhs, g, iperm, soff, val64,
-                              val32, dinv64, dinv32, rhs, elem32, ld32);
+                              val32, dinv64, dinv32, rhs, elem32, ld32, cs32);
 }
 
 // CSC columns of high-order elements (n_b >= 16), one warp per free column:
@@ -295,7 +295,7 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
                                        const double *__restrict__ cell_rhs,
                                        const double *__restrict__ g, double *__restrict__ val,
                                        double *__restrict__ rhs, const float *__restrict__ elem32,
-                                       int ld32) {
+                                       int ld32, int64_t cs32) {
   extern __shared__ double col_acc[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp;
@@ -332,7 +332,7 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
 #pragma unroll
         for (int t = 0; t < NT; ++t) kil += gco[t] * __ldg(ref + t * nn + off);
       } else if (elem32) {
-        kil = (double)elem32[(size_t)ld32 * nb * e + i + (size_t)ld32 * l];
+        kil = (double)elem32[(size_t)cs32 * e + i + (size_t)ld32 * l];
       } else {
         kil = elem[nn * e + i + (size_t)nb * l];
       }
@@ -366,6 +366,7 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
 // lane each) are loaded before any of them is added.
 struct SliceArgs {
   int nb, ld32;
+  int64_t cs32;  // FP32 element matrices: elements per cell
   int64_t n;  // rows (free DoFs)
   const int *perm;
   const int64_t *soff, *col_ptr, *inc_ptr;
@@ -418,7 +419,7 @@ __device__ __forceinline__ void slice_row(const SliceArgs &A, double *img, int r
   for (int c = 0; c < NI; ++c) has[c] = lane + 32 * c < nb;
   // element columns: FP64 nb x nb or FP32 with leading dimension ld32, per cell
   const int ld = F32 ? A.ld32 : nb;
-  const size_t cell_stride = (size_t)ld * nb;
+  const size_t cell_stride = F32 ? (size_t)A.cs32 : (size_t)nb * nb;
   for (int64_t pb = p0; pb < p1; pb += 32) {
     const int cnt = (int)min((int64_t)32, p1 - pb);
     int my_e = h.e, my_l = h.l;
@@ -555,7 +556,7 @@ __global__ void batch_column_kernel(const __grid_constant__ AsmBatch B) {
   column_body<FAMILY, true>(j, S.col_ptr, S.row_idx, S.inc_ptr, S.inc_cell, S.inc_local, S.slot,
                             S.gd, S.nb, S.geo, S.stride, S.ref, S.load_basis, S.nq, nullptr,
                             nullptr, S.g, S.iperm, S.soff, S.val64, S.val32, S.dinv64, S.dinv32,
-                            S.rhs, nullptr, 0);
+                            S.rhs, nullptr, 0, 0);
 }
 
 // every system's full solution: constrained DoFs from g (or 0), free DoFs
@@ -647,7 +648,8 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                    const AssemblyInputs &in, const double *geo, int stride,
                    const double *cell_rhs, const double *elem, const int64_t *col_ptr,
                    const int *row_idx, DeviceSell *sell, double *csc_val, double *rhs,
-                   cudaStream_t s, const float *elem32, int ld32) {
+                   cudaStream_t s, const float *elem32, int ld32, int64_t cs32) {
+  if (elem32 && cs32 <= 0) cs32 = (int64_t)ld32 * t.nb;
   const int T = (in.tune && in.tune->col_threads) ? in.tune->col_threads : 128;
   const int64_t F = t.n_free();
   if (F == 0) return FFG_OK;
@@ -660,7 +662,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
 #define FFG_COLUMN_ARGS                                                                        \
   F, col_ptr, row_idx, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd, t.nb, geo, stride, \
       dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, iperm, soff, v64, v32, d64, d32, rhs, \
-      elem32, ld32
+      elem32, ld32, cs32
   // high-order CSC columns: one warp per column (48 KB of columns per block)
   constexpr int kColSmem = 48 * 1024;
   const int col_bytes = t.max_column * (int)sizeof(double);
@@ -674,6 +676,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
     SliceArgs A;
     A.nb = t.nb;
     A.ld32 = ld32;
+    A.cs32 = cs32;
     A.n = F;
     A.perm = sell->perm;
     A.soff = sell->soff;
@@ -723,7 +726,7 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
                                     (size_t)wpb * col_bytes, s>>>(                             \
           F, t.max_column, col_ptr, dt.inc_ptr, dt.inc_cell, dt.inc_local, dt.slot, dt.gd,      \
           t.nb, geo, stride, dt.ref, dt.load_basis, tab.nq_load, elem, cell_rhs, in.g, v64,    \
-          rhs, elem32, ld32);                                                                  \
+          rhs, elem32, ld32, cs32);                                                                  \
     else                                                                                       \
       column_kernel<FAM, false><<<blocks_for(F, T), T, 0, s>>>(FFG_COLUMN_ARGS);               \
   } while (0)

@@ -46,7 +46,8 @@ namespace ffg {
 
 namespace {
 
-constexpr int kTcThreads = 128;  // one warpgroup: one thread (TMEM lane) per cell
+constexpr int kTcThreads = 128;  // cells per CTA: one TMEM lane each (M)
+constexpr int kTcBlock = 256;    // two warpgroups: both drain the accumulators
 constexpr int kTcN = 128;        // element entries per tile (N), one FP64 table chunk
 constexpr int kTcCols = 2 * kTcN;  // tensor-memory columns of a CTA: two accumulators
 constexpr unsigned long long kTcWaitNs = 2000000000ull;  // 2 s per wait
@@ -165,7 +166,8 @@ __device__ __forceinline__ float tf32_round(float x) {
 
 struct TcArgs {
   int nb, n_chunks;
-  int64_t nn;  // entries of an element matrix (nb^2)
+  int64_t nn;       // entries of an element matrix (nb^2)
+  int64_t cstride;  // floats per cell in `elem` (nn rounded up to 32: 128-byte rows)
   const int *cells;
   const double *verts;
   double ca, cb;
@@ -187,7 +189,8 @@ constexpr int kBFloats = kBImage / 4;
 struct TcSmem {
   alignas(1024) unsigned char a[2 * kAHalf];   // A hi, A lo
   alignas(1024) unsigned char b[2][kBImage];   // two B buffers
-  float stage[4][32][33];                      // epilogue transpose, one per warp
+  float stage[kTcBlock / 32][32][33];          // epilogue transpose, one per warp
+  int cell[kTcThreads];                        // cell of each TMEM lane (-1: none)
   uint64_t bbar[2];                            // B copy of a buffer complete
   uint64_t mbar[2];                            // MMAs into an accumulator complete
   uint32_t tmem;
@@ -196,7 +199,7 @@ struct TcSmem {
 
 // Work unit u of a CTA: its group gi = u / n_chunks (global group
 // blockIdx.x + gi * gridDim.x) and tile t = u % n_chunks.
-__global__ void __launch_bounds__(kTcThreads, 2) nedelec_tc_kernel(const __grid_constant__ TcArgs A) {
+__global__ void __launch_bounds__(kTcBlock, 2) nedelec_tc_kernel(const __grid_constant__ TcArgs A) {
   extern __shared__ unsigned char tc_raw[];
   TcSmem &S = *reinterpret_cast<TcSmem *>(
       (unsigned char *)(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023));
@@ -220,7 +223,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) nedelec_tc_kernel(const __grid_
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = S.tmem;
-  const uint32_t tlane = tmem + ((uint32_t)(32 * warp) << 16);
+  // warp w drains TMEM lanes 32 (w % 4) .. +31 (its lane quarter), columns
+  // 64 (w / 4) .. +63 of each accumulator
+  const int quarter = warp & 3, half = warp >> 2;
+  const uint32_t tlane = tmem + ((uint32_t)(32 * quarter) << 16);
   const int nch = A.n_chunks;
   const int my_groups =
       (int)blockIdx.x < A.n_groups ? (A.n_groups - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
@@ -273,7 +279,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) nedelec_tc_kernel(const __grid_
     double w[12];
 #pragma unroll
     for (int s = 0; s < 12; ++s) w[s] = 0.0;
-    if (tid < grp.z) {
+    if (tid < kTcThreads && tid < grp.z) {
       cell = A.order[grp.y + tid];
       double J[9], Ji[9], v0[3];
       tet_jacobian(A.cells, A.verts, cell, J, v0);
@@ -301,16 +307,19 @@ __global__ void __launch_bounds__(kTcThreads, 2) nedelec_tc_kernel(const __grid_
         }
       }
     }
-    float *ahi = reinterpret_cast<float *>(S.a);
-    float *alo = reinterpret_cast<float *>(S.a + kAHalf);
+    if (tid < kTcThreads) {
+      float *ahi = reinterpret_cast<float *>(S.a);
+      float *alo = reinterpret_cast<float *>(S.a + kAHalf);
 #pragma unroll
-    for (int s = 0; s < 16; ++s) {
-      const double x = s < 12 ? w[s] : 0.0;
-      const float hi = tf32_round((float)x);
-      const float lo = tf32_round((float)(x - (double)hi));
-      // chunk s/4, row tid, element s%4
-      ahi[(s >> 2) * (kTcThreads * 4) + tid * 4 + (s & 3)] = hi;
-      alo[(s >> 2) * (kTcThreads * 4) + tid * 4 + (s & 3)] = lo;
+      for (int s = 0; s < 16; ++s) {
+        const double x = s < 12 ? w[s] : 0.0;
+        const float hi = tf32_round((float)x);
+        const float lo = tf32_round((float)(x - (double)hi));
+        // chunk s/4, row tid, element s%4
+        ahi[(s >> 2) * (kTcThreads * 4) + tid * 4 + (s & 3)] = hi;
+        alo[(s >> 2) * (kTcThreads * 4) + tid * 4 + (s & 3)] = lo;
+      }
+      S.cell[tid] = cell;
     }
     fence_proxy_async();
     __syncthreads();
@@ -340,8 +349,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) nedelec_tc_kernel(const __grid_
       // the MMAs of unit u have read B buffer `buf`: refill it with unit u + 2
       if (tid == 0 && u + 2 < total) issue_copy(u + 2);
       const int64_t e0 = (int64_t)t * kTcN;
+      const int my_cell = S.cell[32 * quarter + lane];
 #pragma unroll 1
-      for (int ch = 0; ch < kTcN / 32; ++ch) {
+      for (int ch = 2 * half; ch < 2 * half + 2; ++ch) {
         float v[32];
         tmem_ld32(tlane + (uint32_t)(buf * kTcN + 32 * ch), v);
         tmem_wait_ld();
@@ -349,10 +359,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) nedelec_tc_kernel(const __grid_
         for (int k = 0; k < 32; ++k) S.stage[warp][lane][k] = v[k];
         __syncwarp();
         const int64_t e = e0 + 32 * ch + lane;
+        // one 128-byte, line-aligned row of a cell per store instruction
 #pragma unroll 4
         for (int c = 0; c < 32; ++c) {
-          const int cc = __shfl_sync(0xffffffffu, cell, c);
-          if (cc >= 0 && e < A.nn) A.elem[(size_t)cc * A.nn + e] = S.stage[warp][c][lane];
+          const int cc = __shfl_sync(0xffffffffu, my_cell, c);
+          if (cc >= 0 && e < A.nn) A.elem[(size_t)cc * A.cstride + e] = S.stage[warp][c][lane];
         }
         __syncwarp();
       }
@@ -415,6 +426,8 @@ size_t tc_smem_bytes() {
 
 bool tc_supported_order(int k) { return k >= 3 && k <= 6; }
 
+int64_t tc_cell_stride(int nb) { return ((int64_t)nb * nb + 31) / 32 * 32; }
+
 int tc_build_plan(const Topology &t, const OrientedTables &o, TcPlan &plan, cudaStream_t s) {
   if (!tc_supported_order(t.degree) || o.order != t.degree || !o.ref) return FFG_INVALID_INPUT;
   tc_free_plan(plan);
@@ -465,6 +478,7 @@ int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const Assembl
   A.nb = t.nb;
   A.n_chunks = plan.n_chunks;
   A.nn = (int64_t)t.nb * t.nb;
+  A.cstride = tc_cell_stride(t.nb);
   A.cells = dt.cells;
   A.verts = in.vertices;
   A.ca = in.coef_a;
@@ -487,7 +501,7 @@ int launch_nedelec_tc(const Topology &t, const DeviceTopology &dt, const Assembl
   if (cudaFuncSetAttribute(nedelec_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem) != cudaSuccess)
     return FFG_CUDA_ERROR;
-  nedelec_tc_kernel<<<grid, kTcThreads, smem, s>>>(A);
+  nedelec_tc_kernel<<<grid, kTcBlock, smem, s>>>(A);
   return cudaGetLastError() == cudaSuccess ? FFG_OK : FFG_CUDA_ERROR;
 }
 
