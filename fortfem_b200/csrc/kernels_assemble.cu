@@ -478,6 +478,85 @@ __device__ __forceinline__ void slice_row(const SliceArgs &A, double *img, int r
   }
 }
 
+// Two rows of a warp gathered in lockstep (both with at most 32 incidences):
+// batch u0 loads U incidences of each row before either is added, so both
+// rows' element columns are in flight together; each row still receives its
+// terms in ascending incidence order, into its own column of the image.
+template <int NI, int U, bool F32>
+__device__ __forceinline__ void slice_pair(const SliceArgs &A, double *img, const int (&r)[2],
+                                           const int64_t (&row)[2], int lane,
+                                           const SliceRowHead (&h)[2]) {
+  const int nb = A.nb;
+  const int ld = F32 ? A.ld32 : nb;
+  const size_t cell_stride = F32 ? (size_t)A.cs32 : (size_t)nb * nb;
+  bool has[NI];
+#pragma unroll
+  for (int c = 0; c < NI; ++c) has[c] = lane + 32 * c < nb;
+  int cnt[2];
+  size_t my_col[2];
+  double my_f[2], b[2] = {0.0, 0.0}, lift[2] = {0.0, 0.0};
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    cnt[q] = h[q].j >= 0 ? (int)(h[q].p1 - h[q].p0) : 0;
+    my_col[q] = (size_t)h[q].e * cell_stride + (size_t)ld * h[q].l;
+    my_f[q] = lane < cnt[q] ? A.cell_rhs[(size_t)nb * h[q].e + h[q].l] : 0.0;
+  }
+  const int n_max = max(cnt[0], cnt[1]);
+  for (int u0 = 0; u0 < n_max; u0 += U) {
+    double kil[2][U][NI];
+    uint16_t sl[2][U][NI];
+    int ev[2][U];
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const bool live = u0 + u < cnt[q];
+        const int uu = live ? u0 + u : 0;
+        const size_t col = __shfl_sync(0xffffffffu, my_col[q], uu) + lane;
+        ev[q][u] = __shfl_sync(0xffffffffu, h[q].e, uu);
+        const uint16_t *slp = A.slot + (size_t)(h[q].p0 + uu) * nb + lane;
+#pragma unroll
+        for (int c = 0; c < NI; ++c) {
+          const bool in = has[c] && live;
+          if (F32) kil[q][u][c] = in ? (double)A.elem32[col + 32 * c] : 0.0;
+          else kil[q][u][c] = in ? A.elem[col + 32 * c] : 0.0;
+          sl[q][u][c] = in ? slp[32 * c] : kConstrainedSlot;
+        }
+      }
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+#pragma unroll
+        for (int c = 0; c < NI; ++c) {
+          if (sl[q][u][c] != kConstrainedSlot) {
+            img[sl[q][u][c] * kSliceStride + r[q]] += kil[q][u][c];
+          } else if (A.g && has[c] && u0 + u < cnt[q]) {
+            lift[q] += kil[q][u][c] * A.g[A.gd[(size_t)nb * ev[q][u] + lane + 32 * c]];
+          }
+        }
+      }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    if (h[q].j < 0) continue;
+    for (int u = 0; u < cnt[q]; ++u) b[q] += __shfl_sync(0xffffffffu, my_f[q], u);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lift[q] += __shfl_xor_sync(0xffffffffu, lift[q], o);
+    if (lane == 0) {
+      // the diagonal's slot: local row l of any incidence (e, l) of column j
+      // has global DoF j, so its slot entry is the diagonal
+      const int dslot = cnt[q] > 0 ? A.slot[(size_t)h[q].p0 * nb + h[q].l] : kConstrainedSlot;
+      const double d = dslot != kConstrainedSlot ? img[dslot * kSliceStride + r[q]] : 0.0;
+      const double di = (fabs(d) > 1.0e-14) ? 1.0 / d : 1.0;
+      A.dinv64[row[q]] = di;
+      A.dinv32[row[q]] = (float)di;
+      A.rhs[row[q]] = b[q] - lift[q];
+    }
+  }
+}
+
 template <int NI, int U, bool F32>
 __global__ void __launch_bounds__(kSliceThreads, 4) sell_slice_kernel(const __grid_constant__ SliceArgs A) {
   extern __shared__ double img[];
@@ -495,8 +574,15 @@ __global__ void __launch_bounds__(kSliceThreads, 4) sell_slice_kernel(const __gr
   slice_head(A, row0 + w + kW, lane, h1);
   for (int q = threadIdx.x; q < width * kSliceStride; q += blockDim.x) img[q] = 0.0;
   __syncthreads();
-  if (h0.j >= 0) slice_row<NI, U, F32>(A, img, w, row0 + w, lane, h0);
-  if (h1.j >= 0) slice_row<NI, U, F32>(A, img, w + kW, row0 + w + kW, lane, h1);
+  if (h0.p1 - h0.p0 <= 32 && h1.p1 - h1.p0 <= 32) {
+    const SliceRowHead hh[2] = {h0, h1};
+    const int rr[2] = {w, w + kW};
+    const int64_t rows[2] = {row0 + w, row0 + w + kW};
+    slice_pair<NI, U, F32>(A, img, rr, rows, lane, hh);
+  } else {
+    if (h0.j >= 0) slice_row<NI, U, F32>(A, img, w, row0 + w, lane, h0);
+    if (h1.j >= 0) slice_row<NI, U, F32>(A, img, w + kW, row0 + w + kW, lane, h1);
+  }
   __syncthreads();
   for (int q = threadIdx.x; q < width * kSliceHalf; q += blockDim.x) {
     const int sl = q / kSliceHalf, r = q % kSliceHalf;
@@ -707,14 +793,14 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
     };
     // about eight loads of each kind in flight per lane
     if (elem32) {
-      if (ni == 1) return go(sell_slice_kernel<1, 4, true>);
-      if (ni == 2) return go(sell_slice_kernel<2, 2, true>);
-      if (ni == 3) return go(sell_slice_kernel<3, 2, true>);
+      if (ni == 1) return go(sell_slice_kernel<1, 2, true>);
+      if (ni == 2) return go(sell_slice_kernel<2, 1, true>);
+      if (ni == 3) return go(sell_slice_kernel<3, 1, true>);
       return go(sell_slice_kernel<4, 1, true>);
     }
-    if (ni == 1) return go(sell_slice_kernel<1, 4, false>);
-    if (ni == 2) return go(sell_slice_kernel<2, 2, false>);
-    if (ni == 3) return go(sell_slice_kernel<3, 2, false>);
+    if (ni == 1) return go(sell_slice_kernel<1, 2, false>);
+    if (ni == 2) return go(sell_slice_kernel<2, 1, false>);
+    if (ni == 3) return go(sell_slice_kernel<3, 1, false>);
     return go(sell_slice_kernel<4, 1, false>);
   }
 #define FFG_LAUNCH(FAM)                                                                        \
