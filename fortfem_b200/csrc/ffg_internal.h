@@ -146,6 +146,8 @@ struct DeviceSell {
   int *cta_slice = nullptr;  // grid + 1 slice boundaries of the CTAs
   int *wslice = nullptr;     // the slices of each warp of the grid, warp by warp
   int *woff = nullptr;       // grid * 32 + 1 starts of the warps' lists in wslice
+  int2 *inc_range = nullptr; // per SELL row: its column's incidence range (the
+                             // slice gather's, built on its first use)
   int grid = 0;
 };
 

@@ -365,6 +365,7 @@ __global__ void csc_column_warp_kernel(int64_t n_free, int max_len,
 // is gathered; U incidences' element columns and slot rows (NI values per
 // lane each) are loaded before any of them is added.
 struct SliceArgs {
+  const int2 *range;  // per SELL row: [p0, p1) of its column's incidences
   int nb, ld32;
   int64_t cs32;  // FP32 element matrices: elements per cell
   int64_t n;  // rows (free DoFs)
@@ -384,27 +385,36 @@ constexpr int kSliceThreads = 256;
 constexpr int kSliceRowsPerWarp = kSliceHalf / (kSliceThreads / 32);
 static_assert(kSliceRowsPerWarp == 2, "two rows per warp");
 
-// The incidences of one row: its column j, range [p0, p1) and the first 32
-// incidences' cells, local indices and element loads, one per lane.
+// The incidences of one row: whether the row exists (j = 0, or -1 past the
+// last row), its incidence range [p0, p1) and the first 32 incidences' cells
+// and local indices, one per lane.
 struct SliceRowHead {
   int j;
   int64_t p0, p1;
   int e, l;
-  double f;
 };
 
 __device__ __forceinline__ void slice_head(const SliceArgs &A, int64_t row, int lane,
                                            SliceRowHead &h) {
-  h.j = row < A.n ? A.perm[row] : -1;
-  h.p0 = h.j >= 0 ? A.inc_ptr[h.j] : 0;
-  h.p1 = h.j >= 0 ? A.inc_ptr[h.j + 1] : 0;
+  h.j = row < A.n ? 0 : -1;
+  const int2 rg = h.j >= 0 ? A.range[row] : make_int2(0, 0);
+  h.p0 = rg.x;
+  h.p1 = rg.y;
   h.e = 0;
   h.l = 0;
-  h.f = 0.0;
   if (h.p0 + lane < h.p1) {
     h.e = A.inc_cell[h.p0 + lane];
     h.l = A.inc_local[h.p0 + lane];
   }
+}
+
+// Incidence range of every SELL row's column (the slice gather's heads).
+__global__ void inc_range_kernel(int64_t n, const int *perm, const int64_t *inc_ptr,
+                                 int2 *range) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int j = perm[r];
+  range[r] = make_int2((int)inc_ptr[j], (int)inc_ptr[j + 1]);
 }
 
 template <int NI, int U, bool F32>
@@ -757,9 +767,18 @@ int launch_columns(const Topology &t, const ElementTables &tab, const DeviceTopo
   const int wpb = by_warp ? std::max(1, std::min(8, kColSmem / col_bytes)) : 0;
   // Nedelec SELL rows: one CTA per slice while the slice image fits
   const size_t slice_smem = (size_t)t.max_column * kSliceStride * sizeof(double);
+  // incidence ranges stored as int32 (every incidence index below 2^31)
+  const int64_t n_inc = t.n_free() > 0 ? (int64_t)t.nb * t.n_cells : 0;
   if (sell && t.family == FFG_TETRA_NEDELEC && t.nb >= 16 && t.nb <= 128 && t.max_column > 0 &&
-      slice_smem <= 200 * 1024 && sell->perm) {
+      slice_smem <= 200 * 1024 && sell->perm && n_inc < (int64_t)INT32_MAX) {
+    if (!sell->inc_range) {
+      if (cudaMalloc((void **)&sell->inc_range, sizeof(int2) * (size_t)F) != cudaSuccess)
+        return FFG_OUT_OF_MEMORY;
+      inc_range_kernel<<<blocks_for(F, 256), 256, 0, s>>>(F, sell->perm, dt.inc_ptr,
+                                                         sell->inc_range);
+    }
     SliceArgs A;
+    A.range = sell->inc_range;
     A.nb = t.nb;
     A.ld32 = ld32;
     A.cs32 = cs32;

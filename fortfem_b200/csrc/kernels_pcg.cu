@@ -1419,7 +1419,7 @@ int sell_repartition(DeviceSell &d, int slice_cost) {
 void free_sell(DeviceSell &d) {
   void *ptrs[] = {d.soff, d.dcol, d.col, d.val64, d.val32, d.val16, d.rscale, d.dinv64, d.dinv32,
                   d.perm, d.iperm,
-                  d.cta_slice, d.wslice, d.woff};
+                  d.cta_slice, d.wslice, d.woff, d.inc_range};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d = DeviceSell();
