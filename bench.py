@@ -73,8 +73,9 @@ def parse(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=-1,
-                    help="requests of the serving leg (0 skips it; default 128 for c2)")
-    ap.add_argument("--serving-rate", type=float, default=20.0)
+                    help="requests of the serving leg (0 skips it; default 1024 for c2; the "
+                         "full C4 stream is 4096)")
+    ap.add_argument("--serving-rate", type=float, default=15.0)
     ap.add_argument("--max-iterations", type=int, default=1000000)
     ap.add_argument("--timeout", type=float, default=60.0, help="device time limit of one solve")
     ap.add_argument("--ref-iterations", type=int, default=0,
@@ -82,7 +83,7 @@ def parse(argv=None):
                          "count to scale the sampled iterations to (a full CPU solve takes hours)")
     a = ap.parse_args(argv)
     if a.serving_requests < 0:
-        a.serving_requests = 128 if a.workload == "c2" else 0
+        a.serving_requests = 1024 if a.workload == "c2" else 0
     return a
 
 
