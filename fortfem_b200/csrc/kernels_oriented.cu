@@ -206,12 +206,13 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_matrix_kernel(const __grid
 }
 
 // Element loads of one tile: F[cell][i] = sum_{q,a} (det J^-1 f_q)_a L'_{class}[3q + a][i],
-// with lanes over 32 J entries per pass (J chosen so the passes waste the
-// fewest lanes for n_b) and Q points at a time: their 3 Q table rows (one
-// contiguous block) come into shared memory by cp.async, double-buffered,
-// and their sample factors det J^-1 f_q of the 64 cells are staged beside
-// them; each thread fetches its samples of the next points into registers
-// while the current ones are consumed.
+// a (64 cells) x (3 n_q) by (3 n_q) x (n_b) product per tile on the FP64
+// tensor cores (mma.sync m8n8k4: warp w takes cells 8w .. 8w+7, NT tiles of 8
+// entries per pass, 4 table rows per step), with Q points at a time: their
+// 3 Q table rows (one contiguous block) come into shared memory by cp.async,
+// double-buffered, and their sample factors det J^-1 f_q of the 64 cells are
+// staged beside them; each thread fetches its samples of the next points
+// into registers while the current ones are consumed.
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
                    (uint32_t)__cvta_generic_to_shared(smem)),
@@ -238,7 +239,15 @@ struct OrtLoadSmem {
   int cell[kOrtTileCells];
 };
 
-template <int J, int Q>
+// D (8 x 8) += A (8 x 4) B (4 x 8) in FP64 on the tensor cores: lane L holds
+// A[L / 4][L % 4], B[L % 4][L / 4] and D[L / 4][2 (L % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int NT, int Q>
 __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_constant__ OrtArgs A) {
   extern __shared__ __align__(16) unsigned char ort_raw[];
   OrtLoadSmem<Q> &S = *reinterpret_cast<OrtLoadSmem<Q> *>(ort_raw);
@@ -291,12 +300,13 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_c
       for (int a = 0; a < 3; ++a) f[u][a] = live ? sp[a] : 0.0;
     }
   };
-  for (int base = 0; base < nb; base += 32 * J) {
-    double acc[8][J];
+  // warp w: cells 8w .. 8w+7 (M), NT tiles of 8 entries (N) per pass, 4 table
+  // rows (K) per step
+  const int kr = lane & 3, cc = lane >> 2;
+  for (int base = 0; base < nb; base += 8 * NT) {
+    double acc[NT][2];
 #pragma unroll
-    for (int c = 0; c < 8; ++c)
-#pragma unroll
-      for (int j = 0; j < J; ++j) acc[c][j] = 0.0;
+    for (int t = 0; t < NT; ++t) acc[t][0] = acc[t][1] = 0.0;
     __syncthreads();  // the previous pass has consumed both buffers
     stage(0);
     fetch(0);
@@ -317,52 +327,38 @@ __global__ void __launch_bounds__(kOrtThreads, 2) ort_load_kernel(const __grid_c
       __syncthreads();   // everyone's pieces and factors are visible
       if (ci + 1 < n_chunks) fetch(q0 + Q);
       const double *rows = Lb + (size_t)(ci & 1) * rows_cap;
-      for (int qa = 0; qa < 3 * nq; ++qa) {
-        double r[J];
+      const int nk = 3 * nq;
+      for (int k0 = 0; k0 < nk; k0 += 4) {
+        const int qa = k0 + kr;
+        const bool kin = qa < nk;
+        const double av = kin ? S.LF[qa][8 * warp + cc] : 0.0;
+        const double *row = rows + (size_t)(kin ? qa : 0) * nb;
 #pragma unroll
-        for (int j = 0; j < J; ++j) {
-          const int i = base + lane + 32 * j;
-          r[j] = i < nb ? rows[(size_t)qa * nb + i] : 0.0;
-        }
-        const double2 *lf = reinterpret_cast<const double2 *>(&S.LF[qa][8 * warp]);
-#pragma unroll
-        for (int c2 = 0; c2 < 4; ++c2) {
-          const double2 w2 = lf[c2];
-#pragma unroll
-          for (int j = 0; j < J; ++j) {
-            acc[2 * c2][j] = fma(w2.x, r[j], acc[2 * c2][j]);
-            acc[2 * c2 + 1][j] = fma(w2.y, r[j], acc[2 * c2 + 1][j]);
-          }
+        for (int t = 0; t < NT; ++t) {
+          const int i = base + 8 * t + cc;
+          const double bv = (kin && i < nb) ? row[i] : 0.0;
+          dmma_8x8x4(acc[t][0], acc[t][1], av, bv);
         }
       }
     }
+    const int cell = S.cell[8 * warp + cc];
+    if (cell >= 0) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const int cell = S.cell[8 * warp + c];
-      if (cell < 0) continue;
-#pragma unroll
-      for (int j = 0; j < J; ++j) {
-        const int i = base + lane + 32 * j;
-        if (i < nb) A.cell_rhs[(size_t)nb * cell + i] = acc[c][j];
+      for (int t = 0; t < NT; ++t) {
+        const int i = base + 8 * t + 2 * kr;
+        if (i < nb) A.cell_rhs[(size_t)nb * cell + i] = acc[t][0];
+        if (i + 1 < nb) A.cell_rhs[(size_t)nb * cell + i + 1] = acc[t][1];
       }
     }
   }
   cp_async_wait_all();
 }
 
-// Entries per lane of the load kernel for n_b: the fewest padded lanes over
-// the passes, the larger J on a tie.
-int load_lanes(int nb) {
-  int best = 1;
-  long best_pad = -1;
-  for (int j = 1; j <= 4; ++j) {
-    const long pad = (long)((nb + 32 * j - 1) / (32 * j)) * 32 * j;
-    if (best_pad < 0 || pad <= best_pad) {
-      best = j;
-      best_pad = pad;
-    }
-  }
-  return best;
+// Entry tiles of 8 per pass of the load kernel: the fewest passes of at
+// most 12 tiles, tiles spread evenly over them.
+int load_tiles(int nb) {
+  const int tiles = (nb + 7) / 8, passes = (tiles + 11) / 12;
+  return (tiles + passes - 1) / passes;
 }
 
 // Ranks of the four vertices of class `cls` (inverse of class_of).
@@ -555,7 +551,6 @@ int launch_nedelec_oriented(const Topology &t, const OrientedTables &o, const De
   if (!load_only)
     ort_matrix_kernel<<<(unsigned)((int64_t)o.n_tiles * A.parts), kOrtThreads, 0, s>>>(A);
   if (in.samples) {
-    // Q = 16 points per stage up to order 4, 8 above (shared memory)
     auto go = [&](auto kern, int Q, size_t fixed) -> int {
       const size_t smem = fixed + 2 * sizeof(double) * (((size_t)3 * Q * o.nb + 1) & ~(size_t)1);
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -564,14 +559,17 @@ int launch_nedelec_oriented(const Topology &t, const OrientedTables &o, const De
       kern<<<o.n_tiles, kOrtThreads, smem, s>>>(A);
       return FFG_OK;
     };
-    const bool wide = o.nb > 70;
+    // Q = 16 points per stage up to order 4, 8 above (shared memory)
+    const bool wide = o.nb > 84;
     const size_t f16 = sizeof(OrtLoadSmem<16>), f8 = sizeof(OrtLoadSmem<8>);
     int st;
-    switch (load_lanes(o.nb)) {
+    switch (load_tiles(o.nb)) {
       case 1: st = go(ort_load_kernel<1, 16>, 16, f16); break;
-      case 2: st = go(ort_load_kernel<2, 16>, 16, f16); break;
-      case 3: st = wide ? go(ort_load_kernel<3, 8>, 8, f8) : go(ort_load_kernel<3, 16>, 16, f16); break;
-      default: st = go(ort_load_kernel<4, 8>, 8, f8); break;
+      case 3: st = go(ort_load_kernel<3, 16>, 16, f16); break;
+      case 6: st = go(ort_load_kernel<6, 16>, 16, f16); break;
+      case 7: st = wide ? go(ort_load_kernel<7, 8>, 8, f8) : go(ort_load_kernel<7, 16>, 16, f16); break;
+      case 11: st = wide ? go(ort_load_kernel<11, 8>, 8, f8) : go(ort_load_kernel<11, 16>, 16, f16); break;
+      default: st = wide ? go(ort_load_kernel<12, 8>, 8, f8) : go(ort_load_kernel<12, 16>, 16, f16); break;
     }
     if (st) return st;
   } else if (cudaMemsetAsync(cell_rhs, 0, sizeof(double) * t.nb * (size_t)t.n_cells, s) !=
