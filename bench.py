@@ -9,7 +9,7 @@ Workloads (--workload; all inputs seeded and synthetic):
 * c3 --order k: first-kind Nedelec curl mu^-1 curl + I on the 24^3 x 6 Kuhn
   box, mu^-1 = 1 / 1000 / 1 in three slabs along z, J = (0, 0, 1) in the
   central slab, zero tangential trace; --assembly tf32x3 contracts the
-  element matrices of orders 3-4 on the tensor cores.
+  element matrices of orders 3-6 on the tensor cores (c5 too).
 * c5: Nedelec order 6 on the 12^3 x 6 box jittered +-0.05h, mu^-1 ~ U[0.5, 2],
   kappa = 10, smooth random trig source.
 
