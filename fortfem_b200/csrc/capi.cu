@@ -128,13 +128,6 @@ int device_ready() {
   return FFG_OK;
 }
 
-// Systems solved by one CTA instead of the cooperative grid: at most 1 MB of
-// SELL operator (values, 16-bit offsets) and FP32 vectors per iteration, which
-// one SM streams in microseconds, so grid barriers would dominate.
-bool small_system(const DeviceSell &S) {
-  return S.dcol && (int64_t)S.padded * 6 + S.n * 48 <= (int64_t)1 << 20;
-}
-
 // Status of a finished solve: a launch or copy error first, then converged,
 // then the wall limit (FFG_TIMEOUT) apart from plain non-convergence.
 int solve_status(int st, const ffg_solver_stats &s) {
@@ -1194,19 +1187,7 @@ void ffg_problem_solve(int handle, const double *vertices, double ca, double cb,
   cudaMemsetAsync(P->x, 0, sizeof(double) * (size_t)std::max<int64_t>(t.n_free(), 1), s);
   if (t.n_free() > 0) {
     if (o.precision == FFG_PRECISION_MIXED16) st = sell_half(P->S, s);
-    if (!st && small_system(P->S)) {
-      // a system whose operator and vectors stream in a few microseconds per
-      // iteration: one CTA solves it (CTA barriers instead of grid barriers)
-      const DeviceSell *A1 = &P->S;
-      const double *b1 = P->rhs;
-      double *x1 = P->x;
-      SolveWork *w1 = &P->work;
-      st = pcg_launch_batch(1, &A1, &b1, &x1, o, &w1, s, msg);
-      if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = FFG_CUDA_ERROR;
-      if (!st) st = pcg_collect(P->work, &local, msg);
-    } else if (!st) {
-      st = pcg_solve(P->S, P->rhs, P->x, o, P->work, &local, s, msg);
-    }
+    if (!st) st = pcg_solve(P->S, P->rhs, P->x, o, P->work, &local, s, msg);
     if (st) { report(o.verbosity, msg); *status = st; if (stats) { local.status = st; *stats = local; } return; }
   } else {
     local.converged = 1;
