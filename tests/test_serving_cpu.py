@@ -171,3 +171,50 @@ def test_serve_replays_every_request_once_with_latencies():
             assert len(b.requests) == 1
     stats = S.percentiles([r.latency for r in res])
     assert stats["p50"] <= stats["p99"] <= stats["p99.9"]
+
+
+class _Pool:
+    """Stand-in for a device problem of one mesh size (memory only)."""
+
+    class problem:
+        @staticmethod
+        def close():
+            pass
+
+
+def _engine_with_budget(budget, per_pool):
+    # the engine's pool logic without a device: creation books `per_pool` bytes
+    eng = object.__new__(S.DeviceEngine)
+    eng.budget, eng.used = budget, 0
+    eng.meshes, eng.idle, eng.bytes, eng.last_use = {}, {}, {}, {}
+    eng.max_instances = 8
+    eng.setup_seconds = 0.0
+
+    def create(key):
+        m = _Pool()
+        eng.meshes.setdefault(key, []).append(m)
+        eng.idle.setdefault(key, []).append(m)
+        eng.bytes[key] = eng.bytes.get(key, 0) + per_pool
+        eng.used += per_pool
+        return m
+
+    eng._create = create
+    eng._estimate = lambda key: per_pool
+    return eng
+
+
+def test_evictions_spare_the_sizes_of_the_batch_being_formed():
+    a, b, c = ("p1", 100), ("p1", 200), ("p1", 300)
+    eng = _engine_with_budget(budget=2, per_pool=1)
+    assert eng.can_host(a) and eng.can_host(b)
+    eng.last_use = {a: 0.0, b: 1.0}           # a is the least recently used
+    # hosting c for a batch that already holds a must evict b, not a
+    assert eng.can_host(c, 1, keep=frozenset({a}))
+    assert set(eng.meshes) == {a, c}
+    # with both other sizes kept there is nothing to evict
+    assert not eng.can_host(b, 1, keep=frozenset({a, c}))
+    # growing a pool never evicts that pool itself
+    eng2 = _engine_with_budget(budget=1, per_pool=1)
+    assert eng2.can_host(a)
+    assert not eng2.can_host(a, 2)
+    assert len(eng2.meshes[a]) == 1
